@@ -1,0 +1,217 @@
+/*
+ * swb200.h -- C ABI of the B200 time-integration library (libswb200.so).
+ *
+ * The library replaces the body of ShallowWaters.jl's time loop,
+ *   time_integration(Prog, Diag, S) -> PrognosticVars      (src/time_integration.jl:2-250)
+ * called from run_model(T, P)                              (src/run_model.jl:25-39).
+ * Everything inside that function -- rhs!, continuity!, the RK/SSPRK stage
+ * combination, ghost_points!, bottom drag, biharmonic diffusion, the
+ * semi-Lagrangian tracer and the NaN check -- runs as CUDA kernels for sm_100a.
+ * The host keeps Parameter, Grid, Constants, Forcing and the initial
+ * conditions and hands their (already rounded) values to this library.
+ *
+ * Array convention (all entry points): a 2-D field of size (m, n) in the
+ * reference's notation is a contiguous host buffer with x fastest, element
+ * (i, j) (1-based, as in Julia) at offset (i-1) + (j-1)*m.  That is Julia's
+ * column-major Array{T,2}, i.e. C's row-major a[j][i].  The element type of
+ * prognostic fields (u, v, eta, sst) is the config's Tprog, the element type
+ * of the static fields (f_q, f_u, f_v, Fx, Fy, H, eta_ref, Feta) is its T.
+ *
+ * Shapes, with N = nx, M = ny, nux = N (periodic) or N-1 (nonperiodic)
+ * (src/grid.jl:26-31, src/initial_conditions.jl:6-21, src/forcing.jl:11-53):
+ *   u    (nux+4) x (M+4)      v    (N+4) x (M+3)
+ *   eta  (N+2)   x (M+2)      sst  (N+2) x M          -- with halo
+ *   f_q  (N+1)   x (M+1)      f_u  nux x M      f_v  N x (M-1)
+ *   Fx   nux     x M          Fy   N x (M-1)
+ *   H    (N+2)   x (M+2)      eta_ref  N x M    Feta  N x M
+ *
+ * Errors: every entry point returns an sw_error code; the library never
+ * aborts or exits.  sw_last_error(ctx) gives a message for the last failure.
+ * A context owns one CUDA stream and is not thread-safe; distinct contexts may
+ * be used from distinct threads.  Host pointers are never retained after a
+ * call returns.
+ */
+#ifndef SWB200_H
+#define SWB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SWB200_ABI_VERSION 1
+
+/* Number formats of Parameter.T / Tprog / Tcomm (src/default_parameters.jl:3-6). */
+enum sw_number_format {
+    SW_FLOAT16 = 1,
+    SW_FLOAT32 = 2,
+    SW_FLOAT64 = 3
+};
+
+/* Parameter.time_scheme (src/default_parameters.jl:50). */
+enum sw_time_scheme { SW_RK = 0, SW_SSPRK2 = 1, SW_SSPRK3 = 2, SW_4SSPRK3 = 3 };
+/* Parameter.dynamics (src/default_parameters.jl:68). */
+enum sw_dynamics { SW_NONLINEAR = 0, SW_LINEAR = 1 };
+/* Parameter.adv_scheme (src/default_parameters.jl:67). */
+enum sw_adv_scheme { SW_ARAKAWA_HSU = 0, SW_SADOURNY = 1 };
+/* Parameter.bottom_drag (src/default_parameters.jl:71). */
+enum sw_bottom_drag { SW_DRAG_QUADRATIC = 0, SW_DRAG_LINEAR = 1, SW_DRAG_NONE = 2 };
+/* Parameter.diffusion (src/default_parameters.jl:76). */
+enum sw_diffusion { SW_DIFF_CONSTANT = 0, SW_DIFF_SMAGORINSKY = 1 };
+/* Device storage of the prognostic fields.  NATIVE keeps Tprog.  BF16/F16
+ * store u, v, eta and sst in 16 bits (u, v scaled by storage_scale_uv) with
+ * FP32 tendencies and FP32-compensated (Kahan) accumulation; Tprog must be
+ * Float32.  This form has no counterpart in the reference. */
+enum sw_storage { SW_STORE_NATIVE = 0, SW_STORE_BF16 = 1, SW_STORE_F16 = 2 };
+
+enum sw_error {
+    SW_OK = 0,
+    SW_ERR_ARG = 1,          /* bad shape, option or pointer                     */
+    SW_ERR_CUDA = 2,         /* a CUDA call failed                               */
+    SW_NAN_DETECTED = 3,     /* feedback.nans_detected (src/feedback.jl:61-72)   */
+    SW_ERR_TIMEOUT = 4,      /* a bounded device wait ran out                    */
+    SW_ERR_UNSUPPORTED = 5,  /* option combination not built                     */
+    SW_ERR_NOMEM = 6,        /* device allocation failed                         */
+    SW_ERR_DEPARTURE = 7,    /* tracer departure point left the wrapped domain   */
+    SW_ERR_NODEVICE = 8      /* no CUDA device                                   */
+};
+
+/* Everything time_integration reads from S.parameters, S.grid and
+ * S.constants.  Scalar constants are the reference's values AFTER rounding to
+ * T or Tprog (src/constants.jl:58-115, src/grid.jl:68-83), carried in double
+ * (exact for Float16/Float32 values). */
+typedef struct sw_config {
+    int32_t abi_version;         /* = SWB200_ABI_VERSION                        */
+
+    /* Grid sizes (src/grid.jl:21-56). */
+    int32_t nx, ny;
+    int32_t periodic;            /* 1: bc == "periodic" (ep = 1), 0: nonperiodic */
+    int32_t halo, haloeta;       /* must be 2 and 1 (src/grid.jl:50-51)          */
+    int32_t halosstx, halossty;  /* must be 1 and 0 (src/grid.jl:52-53)          */
+
+    /* Number formats (src/default_parameters.jl:3-6). */
+    int32_t T, Tprog, Tcomm;     /* enum sw_number_format                        */
+
+    /* Time stepping (src/default_parameters.jl:50-58, src/grid.jl:68-87). */
+    int32_t time_scheme;         /* enum sw_time_scheme                          */
+    int32_t RKo, RKs, RKn;
+    int32_t nstep_diff, nstep_advcor;
+    int32_t nadvstep, nadvstep_half;
+    int32_t nout;
+    int32_t dtint;
+    int64_t nt;                  /* steps run by sw_time_integration             */
+
+    /* Physics options. */
+    int32_t dynamics, adv_scheme, bottom_drag, diffusion;
+    int32_t tracer_advection, tracer_consumption;
+    int32_t surface_relax, surface_forcing;
+    int32_t seasonal_wind_x, seasonal_wind_y;
+
+    /* Constants in Tprog (src/constants.jl:58-72, 93; src/grid.jl:74). */
+    double RKaDt[4], RKbDt[3];
+    double Dt_Ds, Dt_D, Dt_D_half;
+    double one_minus_alpha;
+    double Dt_diff;
+    /* SSPRK3 coefficients (src/constants.jl:4-27). */
+    int32_t ssp_n, ssp_s, ssp_kn, ssp_mn;
+    double ssp_Dt_Dn, ssp_kna, ssp_knb, ssp_Dt_Dnc;
+
+    /* Constants in T (src/constants.jl:94-108, src/grid.jl:80-83). */
+    double g, cD, rD, gamma, cSmag, nuB, rSST, jSST, SSTmin;
+    double dtadvu, dtadvv, half_dtadvu, half_dtadvv;
+    /* Float64 frequencies (src/constants.jl:110-113). */
+    double omegaFeta, omegaFx, omegaFy;
+
+    /* Device storage form (no reference counterpart). */
+    int32_t storage;             /* enum sw_storage                              */
+    double storage_scale_uv;     /* power of two, e.g. 1024                      */
+    int32_t reserved[8];
+} sw_config;
+
+/* S.grid's Coriolis fields and S.forcing (src/grid.jl:93-95,
+ * src/forcing.jl:1-53).  Element type T.  f_u/f_v are only read for linear
+ * dynamics, eta_ref only with surface_relax, Feta only with surface_forcing;
+ * the others must be given. */
+typedef struct sw_static {
+    const void* f_q;
+    const void* f_u;
+    const void* f_v;
+    const void* Fx;
+    const void* Fy;
+    const void* H;
+    const void* eta_ref;
+    const void* Feta;
+} sw_static;
+
+/* Outcome of a run. */
+typedef struct sw_status {
+    int64_t steps_done;   /* time steps completed by this call                  */
+    int64_t step;         /* model step counter after the call (i of the loop)  */
+    int64_t nan_step;     /* step at which NaNs were found, or -1               */
+    int32_t code;         /* enum sw_error of the run                           */
+    int32_t reserved;
+} sw_status;
+
+/* Global diagnostics of the current state, reduced on the device in FP64. */
+typedef struct sw_diag {
+    double mass;          /* sum of eta over the interior                       */
+    double energy;        /* 1/2 sum h*(Ix(u^2)+Iy(v^2)) + 1/2 g sum eta^2      */
+    double max_speed;     /* max |u|, |v| over the interior (for a CFL check)   */
+    int64_t nan_count;    /* NaNs in u, v, eta, sst                             */
+} sw_diag;
+
+/* Per-kernel device times of a profiled run (CUDA events on the context's
+ * stream).  Kinds: 0 rk stage, 1 tail (drag+diffusion), 2 tracer,
+ * 3 advection/Coriolis refresh, 4 NaN check, 5 other. */
+#define SW_PROFILE_KINDS 6
+typedef struct sw_profile {
+    double step_ms_total;              /* sum of per-step device times          */
+    double kernel_ms[SW_PROFILE_KINDS];
+    int64_t launches[SW_PROFILE_KINDS];
+    int64_t steps;
+} sw_profile;
+
+typedef struct sw_ctx sw_ctx;
+
+/* Drop-in for time_integration (src/time_integration.jl:2-250): uploads the
+ * state (with halo, as built by initial_conditions/add_halo,
+ * src/initial_conditions.jl:26-164, src/ghost_points.jl:2-27), runs cfg->nt
+ * steps and writes the final state back into the same buffers.  On NaN
+ * detection it stops like the reference (src/time_integration.jl:235-237):
+ * u, v, eta are those before the failing step, sst after it, and the return
+ * value is SW_NAN_DETECTED. */
+int sw_time_integration(const sw_config* cfg, const sw_static* st,
+                        void* u, void* v, void* eta, void* sst,
+                        sw_status* status);
+
+/* Context API (the same loop, split so state can stay on the device).
+ * sw_create mirrors preallocate + the constant uploads of run_model
+ * (src/run_model.jl:29-36, src/preallocate.jl:454-471). */
+int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out);
+/* Upload a state with halo (Tprog, shapes above).  Resets the step counter. */
+int sw_set_state(sw_ctx* ctx, const void* u, const void* v,
+                 const void* eta, const void* sst);
+/* Advance nsteps time steps (the loop body src/time_integration.jl:45-243),
+ * continuing the step counter.  Blocks until done. */
+int sw_run(sw_ctx* ctx, int64_t nsteps, sw_status* status);
+/* Download the current state with halo (Tprog). */
+int sw_get_state(sw_ctx* ctx, void* u, void* v, void* eta, void* sst);
+/* FP64 reductions over the current state. */
+int sw_diagnostics(sw_ctx* ctx, sw_diag* out);
+/* sw_run with per-kernel CUDA-event timing; when l2_flush_bytes > 0 a buffer
+ * of that size is written between steps (outside the timed intervals). */
+int sw_run_profiled(sw_ctx* ctx, int64_t nsteps, int64_t l2_flush_bytes,
+                    sw_profile* prof, sw_status* status);
+/* Number of CUDA kernel launches the library has issued on this context. */
+int64_t sw_kernel_launches(const sw_ctx* ctx);
+void sw_destroy(sw_ctx* ctx);
+
+const char* sw_strerror(int code);
+const char* sw_last_error(const sw_ctx* ctx);
+int sw_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SWB200_H */
