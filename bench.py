@@ -1,0 +1,329 @@
+#!/usr/bin/env python
+"""Benchmark: RK4 cell-updates/s of the shallow-water time loop on B200.
+
+Workload: the periodic wind-driven channel at 2048 x 1024 cells (Δ = 976.6 m,
+dtint = 13 s): flat 500 m depth, channel wind with Fx0 drawn U(0.08, 0.16) Pa
+from the seed, RK4 at CFL 1, Arakawa-Hsu advection, Smagorinsky biharmonic
+diffusion, quadratic drag, semi-Lagrangian tracer every step (Uadv = 1000),
+seeded η noise σ = 0.01 m and a ±1 tracer checkerboard.  Plain Float32.
+
+One "step" is one model time step (4 RK stages + tail + tracer).  ``value`` is
+device time (CUDA events on the library's stream) with the state resident in
+HBM and a 256 MiB L2 flush between steps (outside the timed intervals);
+``e2e`` times the drop-in ``sw_time_integration`` call with pinned host
+buffers, uploads and downloads included.  With N GPUs (torchrun) every rank
+runs an independent replica (the single domain is not decomposed) and values
+are aggregates over ranks with the time taken as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "shallowwaters.jl_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "RK4 cell-updates/s on 1 B200, plain FP32 vs chosen form at stated η error"
+UNIT = "cell-updates/s"
+L2_FLUSH = 256 << 20
+# algorithmic bytes per cell of one RK stage launch, Float32, averaged over the
+# 4 stages: stage 1 reads X, H, Fx and writes X1, X0 (44 B); stages 2-3 read
+# X1, X, X0, H, Fx and write X1, X0 (68 B); stage 4 reads X1, X0, H, Fx and
+# writes X0 (44 B)
+STAGE_BYTES_PER_CELL = (44 + 68 + 68 + 44) / 4
+STEP_BYTES_PER_CELL = 264
+
+
+def workload_params(nx=2048, seed=1234):
+    rng = np.random.default_rng(seed)
+    Fx0 = float(rng.uniform(0.08, 0.16))
+    kw = dict(nx=nx, L_ratio=2, bc="periodic", wind_forcing_x="channel", Fx0=Fx0, topography="flat", H=500,
+              g=10, cfl=1, time_scheme="RK", RKo=4, adv_scheme="ArakawaHsu", diffusion="Smagorinsky",
+              bottom_drag="quadratic", tracer_advection=True, Uadv=1000, Ndays=100)
+    return kw, rng
+
+
+def make_state(S, rng):
+    from swb200 import initial_conditions
+    G = S.grid
+    eta = rng.normal(0.0, 0.01, (G.ny, G.nx))
+    i = np.arange(G.nx)[None, :]
+    j = np.arange(G.ny)[:, None]
+    sst = np.where(((i // 10) + (j // 10)) % 2 == 0, 1.0, -1.0)
+    return initial_conditions(S.parameters.Tprog, S, η0=eta, sst0=sst)
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+
+    Q = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid=None):
+        self.uuid = uuid
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                         text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.th = threading.Thread(target=self._read, daemon=True)
+        self.th.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9 and (self.uuid is None or f[0] == self.uuid):
+                self.rows.append(f)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.th.join(timeout=2)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in self.rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(cells):
+    """DRAM bytes per stage launch from the committed ncu summary, scaled to cells."""
+    p = os.path.join(REPO, "profiles", "rk_stage_traffic.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return d["dram_bytes_per_launch"] * cells / d["cells"]
+    except Exception:
+        return None
+
+
+def host_info():
+    model = "unknown"
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True).stdout
+        for line in out.splitlines():
+            if line.startswith("Model name"):
+                model = line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return {"nproc": os.cpu_count(), "model": model}
+
+
+# -------------------------------------------------------------- CPU legs
+def cpu_run(S, Prog, threads, target_s, max_steps):
+    """Times the oracle on the workload: returns (cell-updates/s, steps, seconds, threads)."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle as O
+    used = O.set_threads(threads)
+    o = O.Oracle(S)
+    o.set_state(Prog)
+    t0 = time.perf_counter()
+    o.run(1)
+    t1 = time.perf_counter() - t0
+    n = int(max(2, min(max_steps, math.ceil(target_s / max(t1, 1e-3)))))
+    o.set_state(Prog)
+    t0 = time.perf_counter()
+    o.run(n)
+    dt = time.perf_counter() - t0
+    cells = S.grid.nx * S.grid.ny
+    return cells * n / dt, n, dt, used
+
+
+# --------------------------------------------------------------- main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--nx", type=int, default=2048)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    from swb200 import Model, abi, model_setup, Parameter
+
+    kw, rng = workload_params(args.nx)
+    P = Parameter(**kw)
+    S = model_setup(P)
+    G = S.grid
+    cells = G.nx * G.ny
+    config = {"workload": f"periodic wind-driven channel {G.nx}x{G.ny}, RK4, Arakawa-Hsu, Smagorinsky, "
+                          f"quadratic drag, tracer every step",
+              "nx": G.nx, "ny": G.ny, "dtint_s": G.dtint, "form": "fp32",
+              "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{args.gpus}"}
+    base = {"metric": METRIC, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded η noise, tracer checkerboard, seeded wind amplitude)", "config": config}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        Prog = make_state(S, rng)
+        threads = os.cpu_count() or 1
+        target = 20.0 * (args.steps + args.warmup) / max(args.steps + args.warmup, 1)
+        v, n, dt, used = cpu_run(S, Prog, threads, min(60.0, target), args.steps)
+        hi = host_info()
+        line = dict(base)
+        line.update({"impl": "reference", "value": v, "ms_per_step": 1e3 * dt / n,
+                     "cpu_baseline": {"value": v, "unit": UNIT, "cores": used, "kind": "port",
+                                      "sample": f"{n} steps of the {G.nx}x{G.ny} workload from the same state "
+                                                f"({dt:.1f} s), OpenMP over {used} threads of {hi['model']}"},
+                     "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+        print(json.dumps(line))
+        return 0
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev_uuid = None
+    try:
+        dev_uuid = "GPU-" + str(torch.cuda.get_device_properties(torch.cuda.current_device()).uuid)
+    except Exception:
+        pass
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def allmax(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    Prog = make_state(S, rng)
+    m = Model(S)
+    m.set_state(Prog)
+    m.run(args.warmup)
+
+    clk = ClockSampler(dev_uuid)
+    barrier()
+    clk.start()
+    n0 = m.kernel_launches
+    prof, st = m.run_profiled(args.steps, L2_FLUSH)
+    launches = m.kernel_launches - n0
+    barrier()
+    clk.stop()
+    if st.code != 0:
+        raise SystemExit(f"run failed with code {st.code}")
+    t_dev = allmax(prof.step_ms_total) / 1e3
+    value = args.gpus * cells * args.steps / t_dev
+    stage_ms = prof.kernel_ms[0] / max(prof.launches[0], 1)
+    stage_ms = allmax(stage_ms)
+    achieved = STAGE_BYTES_PER_CELL * cells / (stage_ms / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    kernels = {abi.PROFILE_NAMES[k]: {"launches": int(prof.launches[k]),
+                                      "avg_us": 1e3 * prof.kernel_ms[k] / prof.launches[k],
+                                      "share": prof.kernel_ms[k] / max(sum(prof.kernel_ms), 1e-12)}
+               for k in range(abi.PROFILE_KINDS) if prof.launches[k]}
+    m.close()
+
+    # e2e: drop-in call with pinned host buffers (create, upload, run, download)
+    from swb200 import time_integration  # noqa: F401
+    from swb200.run_model import time_integration as ti
+    pinned = [torch.empty(a.shape, dtype=torch.float32, pin_memory=True).numpy() for a in Prog]
+    for dst, src in zip(pinned, Prog):
+        dst[...] = src
+    import ctypes as C
+    lib = abi.load_library()
+    cfg = abi.make_config(S, nt=args.steps)
+    static = abi.StaticFields(S)
+    status = abi.SwStatus()
+    barrier()
+    t0 = time.perf_counter()
+    rc = lib.sw_time_integration(C.byref(cfg), static.ptr(), *abi.state_ptrs(*pinned), C.byref(status))
+    t_e2e = time.perf_counter() - t0
+    barrier()
+    if rc != 0:
+        raise SystemExit(f"sw_time_integration failed: {rc}")
+    t_e2e = allmax(t_e2e)
+    state_bytes = sum(a.nbytes for a in pinned)
+    static_bytes = sum(a.nbytes for a in static.arrays.values())
+    e2e = {"value": args.gpus * cells * args.steps / t_e2e, "unit": UNIT,
+           "h2d_bytes_per_step": (state_bytes + static_bytes) / args.steps,
+           "d2h_bytes_per_step": state_bytes / args.steps,
+           "call": "sw_time_integration (create + upload + run + download + destroy)"}
+
+    cpu = None
+    if rank == 0 and args.gpus == 1 and not args.no_cpu:
+        v, n, dt, used = cpu_run(S, Prog, 1, args.cpu_seconds, 200)
+        hi = host_info()
+        cpu = {"value": v, "unit": UNIT, "cores": used, "kind": "port",
+               "sample": f"{n} steps of the {G.nx}x{G.ny} workload, single thread, {dt:.1f} s, on {hi['model']} "
+                         f"({hi['nproc']} logical CPUs)"}
+
+    if rank == 0:
+        line = dict(base)
+        line.update({
+            "value": value, "ms_per_step": 1e3 * t_dev / args.steps,
+            "e2e": e2e,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": ncu_traffic(cells),
+                         "kernel": "rk_stage_kernel", "bytes_per_cell": STAGE_BYTES_PER_CELL,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                         else "fallback 6.65 TB/s"},
+            "step_roofline": {"bytes_per_cell_step": STEP_BYTES_PER_CELL,
+                              "achieved_gbs": STEP_BYTES_PER_CELL * cells * args.steps / t_dev / 1e9 / args.gpus},
+            "kernels": kernels,
+            "cpu_baseline": cpu,
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+        })
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -45,8 +45,15 @@ def lib():
         L.oracle_last_error.argtypes = [C.c_void_p]
         L.oracle_last_error.restype = C.c_char_p
         L.oracle_destroy.argtypes = [C.c_void_p]
+        L.oracle_set_threads.argtypes = [C.c_int]
+        L.oracle_set_threads.restype = C.c_int
         _lib = L
     return _lib
+
+
+def set_threads(n: int) -> int:
+    """OpenMP threads for the oracle's loops; returns the count in effect."""
+    return int(lib().oracle_set_threads(int(n)))
 
 
 class Oracle:

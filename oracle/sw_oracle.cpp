@@ -11,6 +11,9 @@
 #include <string>
 
 #include "sw_oracle.hpp"
+#if defined(_OPENMP)
+#include <omp.h>
+#endif
 
 using namespace swo;
 
@@ -145,6 +148,17 @@ const char* oracle_last_error(void* h) {
 }
 
 void oracle_destroy(void* h) { delete static_cast<Base*>(h); }
+
+// Threads used by the OpenMP loops (the reference itself is single-threaded).
+int oracle_set_threads(int n) {
+#if defined(_OPENMP)
+    if (n > 0) omp_set_num_threads(n);
+    return omp_get_max_threads();
+#else
+    (void)n;
+    return 1;
+#endif
+}
 
 int oracle_time_integration(const sw_config* cfg, const sw_static* st, void* u, void* v, void* eta,
                             void* sst, sw_status* status) {

@@ -1,0 +1,659 @@
+// sw_runtime.cu -- libswb200: contexts, device buffers, the time loop and the
+// C ABI of include/swb200.h.
+//
+// Per time step (src/time_integration.jl:45-243) the RK scheme issues
+//   RKo x rk_stage_kernel   (rhs! + continuity! + caxb!/axb! + ghost points)
+//   tail_kernel             (every nstep_diff steps: drag + diffusion + add)
+//   [copy_convert_kernel]   (mid-point velocity copy, nadvstep > 1)
+//   tracer_kernel           (every nadvstep steps)
+//   nan_check_kernel        (every nout steps)
+// on one stream.  Buffers: two state sets S[0], S[1] (u, v, eta), two stage
+// sets A, B, the accumulator Acc (u0, v0, eta0), two tracer buffers.  With
+// state parity p, step i reads S[p] and leaves the new state in S[1-p]; S[p]
+// survives the step, which gives the reference's NaN semantics (return the
+// state from before the failing step).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "swb200.h"
+#include "sw_common.cuh"
+#include "sw_ghost.cuh"
+#include "sw_stage.cuh"
+#include "sw_tail.cuh"
+#include "sw_tracer.cuh"
+
+using namespace swb;
+
+namespace {
+
+constexpr int STAGE_TX = 64, STAGE_TY = 8, STAGE_NT = 256;
+constexpr int TAIL_TX = 32, TAIL_TY = 8, TAIL_NT = 256;
+constexpr int PADX = 72, PADY = 44;     // >= max tile width + 8, tile height + 12
+constexpr int RING_BLOCKS_MAX = 32;
+
+const char* err_name(int c) {
+    switch (c) {
+        case SW_OK: return "ok";
+        case SW_ERR_ARG: return "invalid argument";
+        case SW_ERR_CUDA: return "CUDA error";
+        case SW_NAN_DETECTED: return "NaNs detected";
+        case SW_ERR_TIMEOUT: return "device wait timed out";
+        case SW_ERR_UNSUPPORTED: return "option combination not supported";
+        case SW_ERR_NOMEM: return "device allocation failed";
+        case SW_ERR_DEPARTURE: return "tracer departure point outside the domain";
+        case SW_ERR_NODEVICE: return "no CUDA device";
+    }
+    return "unknown error";
+}
+
+size_t fmt_size(int f) { return f == SW_FLOAT16 ? 2 : f == SW_FLOAT32 ? 4 : f == SW_FLOAT64 ? 8 : 0; }
+
+struct Fields3 { void* u = nullptr; void* v = nullptr; void* e = nullptr; };
+
+}  // namespace
+
+struct sw_ctx;
+struct EngineBase {
+    virtual ~EngineBase() = default;
+    virtual int step(sw_ctx* ctx, long long i) = 0;
+    virtual int ghost_state(sw_ctx* ctx) = 0;
+};
+
+struct sw_ctx {
+    sw_config cfg;
+    Geom g;
+    size_t nelem = 0;          // elements per field buffer (P*R)
+    size_t tsz = 0, tpsz = 0;  // sizeof(T), sizeof(Tprog)
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    std::vector<void*> allocs;
+    Fields3 S[2], A, B, Acc;
+    void* sst[2] = {nullptr, nullptr};
+    void* um = nullptr; void* vm = nullptr;
+    void* flush = nullptr; size_t flush_bytes = 0;
+    // static fields (type T) and their strides
+    struct SF { void* p = nullptr; long sx = 0, sy = 0; } H, fq, Fx, Fy, fu, fv, eref, Feta;
+    DevStatus* dst = nullptr;     // device status
+    DevStatus* hst = nullptr;     // pinned host mirror
+    int p = 0;                    // state parity
+    int sp = 0;                   // tracer parity
+    long long step = 0;           // completed steps
+    long long t = 0;              // model time [s]
+    long long launches = 0;
+    std::string err;
+    std::unique_ptr<EngineBase> eng;
+    // profiling
+    bool prof = false;
+    std::vector<cudaEvent_t> evpool;
+    size_t evnext = 0;
+    struct Mark { int kind; cudaEvent_t a, b; };
+    std::vector<Mark> marks;
+    cudaEvent_t evget();
+};
+
+cudaEvent_t sw_ctx::evget() {
+    if (evnext == evpool.size()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        evpool.push_back(e);
+    }
+    return evpool[evnext++];
+}
+
+namespace {
+
+int fail(sw_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+#define CK(call)                                                                             \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            return fail(ctx, e_ == cudaErrorMemoryAllocation ? SW_ERR_NOMEM : SW_ERR_CUDA,   \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                 \
+    } while (0)
+
+template <class T>
+SField<T> sf(const sw_ctx::SF& s) { return SField<T>{static_cast<const T*>(s.p), s.sx, s.sy}; }
+
+// kernel launch bracketed by profiling events when enabled
+template <class F>
+int launch(sw_ctx* ctx, int kind, F&& f) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (ctx->prof) {
+        a = ctx->evget();
+        b = ctx->evget();
+        cudaEventRecord(a, ctx->stream);
+    }
+    f();
+    ctx->launches++;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(ctx, SW_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+    if (ctx->prof) {
+        cudaEventRecord(b, ctx->stream);
+        ctx->marks.push_back({kind, a, b});
+    }
+    return SW_OK;
+}
+
+// ghost points on every source cell of u, v, eta (used once on an uploaded state)
+template <class Tp>
+__global__ void ghost_state_kernel(Geom g, Tp* u, Tp* v, Tp* e, GhostRule<Tp> gr) {
+    const int N = g.N, M = g.M, ep = g.ep;
+    long long nu_in = (long long)(ep ? N : N - 1) * M, nv_in = (long long)N * (M - 1), ne = (long long)N * M;
+    long long nur = Ring::u_count(ep, N, M), nvr = Ring::v_count(N);
+    long long tot = nu_in + nv_in + ne + nur + nvr;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < tot; k += (long long)gridDim.x * blockDim.x) {
+        long long r = k;
+        if (r < nu_in) {
+            int w = ep ? N : N - 1;
+            int F = (int)(r % w) + (1 - ep), b = (int)(r / w);
+            gr.u(u, g, F, b, u[g.idx(F, b)]);
+            continue;
+        }
+        r -= nu_in;
+        if (r < nv_in) {
+            int a = (int)(r % N), G = (int)(r / N) + 1;
+            gr.v(v, g, a, G, v[g.idx(a, G)]);
+            continue;
+        }
+        r -= nv_in;
+        if (r < ne) {
+            int a = (int)(r % N), b = (int)(r / N);
+            gr.eta(e, g, a, b, e[g.idx(a, b)]);
+            continue;
+        }
+        r -= ne;
+        if (r < nur) {
+            int F, b;
+            Ring::u_at((int)r, ep, N, M, F, b);
+            gr.u(u, g, F, b, u[g.idx(F, b)]);
+            continue;
+        }
+        r -= nur;
+        int a, G;
+        Ring::v_at((int)r, N, M, a, G);
+        gr.v(v, g, a, G, v[g.idx(a, G)]);
+    }
+}
+
+template <class T, class Tp>
+struct Engine : EngineBase {
+    int stage_smem = 0, tail_smem = 0;
+
+    int init(sw_ctx* ctx) {
+        stage_smem = 8 * (STAGE_TX + 8) * (STAGE_TY + 3) * (int)sizeof(T);
+        tail_smem = 12 * (TAIL_TX + 8) * (TAIL_TY + 4) * (int)sizeof(T);
+        CK(cudaFuncSetAttribute(rk_stage_kernel<T, Tp, STAGE_TX, STAGE_TY, STAGE_NT>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, stage_smem));
+        CK(cudaFuncSetAttribute(tail_kernel<T, Tp, TAIL_TX, TAIL_TY, TAIL_NT>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, tail_smem));
+        return SW_OK;
+    }
+
+    GhostRule<Tp> rule(sw_ctx* ctx) const {
+        GhostRule<Tp> r;
+        r.ep = ctx->g.ep; r.N = ctx->g.N; r.M = ctx->g.M; r.Tcomm = ctx->cfg.Tcomm;
+        r.oma = (Tp)ctx->cfg.one_minus_alpha;
+        return r;
+    }
+
+    static int ring_blocks(const Geom& g, int nt) {
+        int n = Ring::u_count(g.ep, g.N, g.M) + Ring::v_count(g.N);
+        return std::min(RING_BLOCKS_MAX, (n + nt - 1) / nt);
+    }
+
+    int ghost_state(sw_ctx* ctx) override {
+        const Geom& g = ctx->g;
+        Fields3& X = ctx->S[ctx->p];
+        return launch(ctx, 5, [&] {
+            ghost_state_kernel<Tp><<<148, 256, 0, ctx->stream>>>(g, (Tp*)X.u, (Tp*)X.v, (Tp*)X.e, rule(ctx));
+        });
+    }
+
+    int step(sw_ctx* ctx, long long i) override {
+        const sw_config& c = ctx->cfg;
+        const Geom& g = ctx->g;
+        Fields3& X = ctx->S[ctx->p];
+        Fields3& Y = ctx->S[1 - ctx->p];
+        const bool tail_now = (i % c.nstep_diff) == 0;
+        const T one = T(1);
+        T Fxt = c.seasonal_wind_x ? (T)std::sin(c.omegaFx * (double)ctx->t) : one;
+        T Fyt = c.seasonal_wind_y ? (T)std::sin(c.omegaFy * (double)ctx->t) : one;
+
+        // ------------------------------------------------ RK stages (:55-78)
+        const int ntx = (g.N + STAGE_TX - 1) / STAGE_TX, nty = (g.M + STAGE_TY - 1) / STAGE_TY;
+        const int nblk = ntx * nty + ring_blocks(g, STAGE_NT);
+        for (int k = 1; k <= c.RKo; k++) {
+            StageArgs<T, Tp> a;
+            a.g = g; a.ntx = ntx; a.nty = nty;
+            const Fields3& in = (k == 1) ? X : ((k % 2 == 0) ? ctx->A : ctx->B);
+            Fields3& out1 = (k % 2 == 1) ? ctx->A : ctx->B;
+            a.u1 = (const Tp*)in.u; a.v1 = (const Tp*)in.v; a.e1 = (const Tp*)in.e;
+            a.uX = (const Tp*)X.u; a.vX = (const Tp*)X.v; a.eX = (const Tp*)X.e;
+            a.u0i = (const Tp*)ctx->Acc.u; a.v0i = (const Tp*)ctx->Acc.v; a.e0i = (const Tp*)ctx->Acc.e;
+            a.first = (k == 1); a.last = (k == c.RKo);
+            if (!a.last) { a.u1o = (Tp*)out1.u; a.v1o = (Tp*)out1.v; a.e1o = (Tp*)out1.e; }
+            else { a.u1o = a.v1o = a.e1o = nullptr; }
+            if (a.last) {
+                // the final X0: u, v to Acc when the tail follows, else straight into
+                // the new state; eta always into the new state (the tail keeps eta)
+                a.u0o = (Tp*)(tail_now ? ctx->Acc.u : Y.u);
+                a.v0o = (Tp*)(tail_now ? ctx->Acc.v : Y.v);
+                a.e0o = (Tp*)Y.e;
+            } else {
+                a.u0o = (Tp*)ctx->Acc.u; a.v0o = (Tp*)ctx->Acc.v; a.e0o = (Tp*)ctx->Acc.e;
+            }
+            a.H = sf<T>(ctx->H); a.fq = sf<T>(ctx->fq); a.Fx = sf<T>(ctx->Fx); a.Fy = sf<T>(ctx->Fy);
+            a.a = (Tp)c.RKaDt[k - 1];
+            a.b = (k < c.RKo) ? (Tp)c.RKbDt[k - 1] : Tp(0);
+            a.g_ = (T)c.g;
+            a.Fxt = Fxt; a.Fyt = Fyt;
+            a.gr = rule(ctx);
+            a.st = ctx->dst;
+            int rc = launch(ctx, 0, [&] {
+                rk_stage_kernel<T, Tp, STAGE_TX, STAGE_TY, STAGE_NT>
+                    <<<nblk, STAGE_NT, stage_smem, ctx->stream>>>(a);
+            });
+            if (rc) return rc;
+        }
+
+        // -------------------------------------- drag + diffusion (:216-221)
+        if (tail_now) {
+            TailArgs<T, Tp> a;
+            const int tx = (g.N + TAIL_TX - 1) / TAIL_TX, ty = (g.M + TAIL_TY - 1) / TAIL_TY;
+            a.g = g; a.ntx = tx; a.nty = ty;
+            a.u0 = (const Tp*)ctx->Acc.u; a.v0 = (const Tp*)ctx->Acc.v; a.e0 = (const Tp*)Y.e;
+            a.uo = (Tp*)Y.u; a.vo = (Tp*)Y.v;
+            a.H = sf<T>(ctx->H);
+            a.drag = c.bottom_drag;
+            a.smag = (c.diffusion == SW_DIFF_SMAGORINSKY);
+            a.cD = (T)c.cD; a.rD = (T)c.rD; a.cSmag = (T)c.cSmag; a.nuB = (T)c.nuB;
+            a.Dt_diff = (Tp)c.Dt_diff;
+            a.gr = rule(ctx);
+            a.st = ctx->dst;
+            int nb = tx * ty + ring_blocks(g, TAIL_NT);
+            int rc = launch(ctx, 1, [&] {
+                tail_kernel<T, Tp, TAIL_TX, TAIL_TY, TAIL_NT><<<nb, TAIL_NT, tail_smem, ctx->stream>>>(a);
+            });
+            if (rc) return rc;
+        }
+        ctx->t += c.dtint;
+
+        // ------------------------------------------------ tracer (:226-228)
+        if (c.tracer_advection) {
+            if (c.nadvstep > 1 && ((i + c.nadvstep_half) % c.nadvstep) == 0) {
+                int rc = launch(ctx, 5, [&] {
+                    copy_convert_kernel<T, Tp><<<296, 256, 0, ctx->stream>>>(
+                        (const Tp*)Y.u, (const Tp*)Y.v, (T*)ctx->um, (T*)ctx->vm, (long long)ctx->nelem, ctx->dst);
+                });
+                if (rc) return rc;
+            }
+            if ((i % c.nadvstep) == 0) {
+                TracerArgs<T, Tp> a;
+                a.g = g;
+                a.u = (const Tp*)Y.u; a.v = (const Tp*)Y.v;
+                a.um = (const T*)ctx->um; a.vm = (const T*)ctx->vm;
+                a.um_is_u = (c.nadvstep == 1);
+                a.sst = (const Tp*)ctx->sst[ctx->sp];
+                a.sst_o = (Tp*)ctx->sst[1 - ctx->sp];
+                a.dtadvu = (T)c.dtadvu; a.dtadvv = (T)c.dtadvv;
+                a.half_dtadvu = (T)c.half_dtadvu; a.half_dtadvv = (T)c.half_dtadvv;
+                a.consumption = c.tracer_consumption;
+                a.jSST = (T)c.jSST; a.SSTmin = (T)c.SSTmin;
+                a.gr = rule(ctx);
+                a.st = ctx->dst;
+                long long n = (long long)g.N * g.M;
+                int nb = (int)std::min<long long>((n + 255) / 256, 148 * 16);
+                int rc = launch(ctx, 2, [&] { tracer_kernel<T, Tp><<<nb, 256, 0, ctx->stream>>>(a); });
+                if (rc) return rc;
+                ctx->sp = 1 - ctx->sp;
+            }
+        }
+
+        // ------------------------------------------- NaN check (:232-237)
+        if ((i % c.nout) == 0) {
+            int rc = launch(ctx, 4, [&] {
+                nan_check_kernel<Tp><<<148, 256, 0, ctx->stream>>>(g, (const Tp*)X.u, (const Tp*)X.v, (const Tp*)X.e,
+                                                                  (const Tp*)ctx->sst[ctx->sp], i, ctx->dst);
+            });
+            if (rc) return rc;
+        }
+        return SW_OK;
+    }
+};
+
+// ------------------------------------------------------------------ helpers
+
+int check_config(const sw_config* c, std::string& why) {
+    if (c->abi_version != SWB200_ABI_VERSION) { why = "abi_version mismatch"; return SW_ERR_ARG; }
+    if (c->nx < 4 || c->ny < 4) { why = "nx and ny must be >= 4"; return SW_ERR_ARG; }
+    if (c->halo != 2 || c->haloeta != 1 || c->halosstx != 1 || c->halossty != 0) {
+        why = "halo sizes must be (2,1,1,0) as in src/grid.jl:50-53";
+        return SW_ERR_ARG;
+    }
+    if (!fmt_size(c->T) || !fmt_size(c->Tprog) || !fmt_size(c->Tcomm)) { why = "unknown number format"; return SW_ERR_ARG; }
+    if (c->nstep_diff < 1 || c->nadvstep < 1 || c->nout < 1 || c->dtint < 1) { why = "step counts must be >= 1"; return SW_ERR_ARG; }
+    if (c->time_scheme != SW_RK) { why = "time_scheme other than RK not built yet"; return SW_ERR_UNSUPPORTED; }
+    if (c->RKo < 2 || c->RKo > 4) { why = "RKo must be 2, 3 or 4"; return SW_ERR_ARG; }
+    if (c->dynamics != SW_NONLINEAR) { why = "linear dynamics not built yet"; return SW_ERR_UNSUPPORTED; }
+    if (c->adv_scheme != SW_ARAKAWA_HSU) { why = "Sadourny advection not built yet"; return SW_ERR_UNSUPPORTED; }
+    if (c->nstep_advcor != 0) { why = "nstep_advcor > 0 not built yet"; return SW_ERR_UNSUPPORTED; }
+    if (c->surface_relax || c->surface_forcing) { why = "surface relaxation/forcing not built yet"; return SW_ERR_UNSUPPORTED; }
+    if (c->storage != SW_STORE_NATIVE) { why = "16-bit storage not built yet"; return SW_ERR_UNSUPPORTED; }
+    bool ok = (c->T == SW_FLOAT32 && c->Tprog == SW_FLOAT32) || (c->T == SW_FLOAT64 && c->Tprog == SW_FLOAT64) ||
+              (c->T == SW_FLOAT32 && c->Tprog == SW_FLOAT64);
+    if (!ok) { why = "(T, Tprog) pair not built"; return SW_ERR_UNSUPPORTED; }
+    return SW_OK;
+}
+
+// Upload a host field (T, x fastest, host column 0 at physical x = hx0, row 0 at
+// y = hy0, size w x h) as a strided SField: constant fields and fields that vary
+// along one axis only are stored as broadcast vectors.
+int upload_static(sw_ctx* ctx, sw_ctx::SF& out, const void* host, int w, int h, int hx0, int hy0) {
+    const size_t ts = ctx->tsz;
+    const unsigned char* src = static_cast<const unsigned char*>(host);
+    auto el = [&](int i, int j) { return src + ((size_t)j * w + i) * ts; };
+    bool const_x = true, const_y = true;
+    for (int j = 0; j < h && const_x; j++)
+        for (int i = 1; i < w; i++)
+            if (std::memcmp(el(i, j), el(0, j), ts)) { const_x = false; break; }
+    for (int j = 1; j < h && const_y; j++)
+        if (std::memcmp(el(0, j), el(0, 0), ts * (size_t)w)) const_y = false;
+    const Geom& g = ctx->g;
+    std::vector<unsigned char> buf;
+    if (const_x && const_y) {
+        buf.assign(ts, 0);
+        std::memcpy(buf.data(), el(0, 0), ts);
+        out.sx = 0; out.sy = 0;
+    } else if (const_x) {                      // varies with y only: indexed by row
+        buf.assign((size_t)g.R * ts, 0);
+        for (int j = 0; j < h; j++) std::memcpy(&buf[(size_t)(hy0 + j + ROW0) * ts], el(0, j), ts);
+        out.sx = 0; out.sy = 1;
+    } else if (const_y) {                      // varies with x only: indexed by column
+        buf.assign((size_t)g.P * ts, 0);
+        for (int i = 0; i < w; i++) std::memcpy(&buf[(size_t)(hx0 + i + COL0) * ts], el(i, 0), ts);
+        out.sx = 1; out.sy = 0;
+    } else {
+        buf.assign((size_t)g.P * g.R * ts, 0);
+        for (int j = 0; j < h; j++)
+            std::memcpy(&buf[((size_t)(hy0 + j + ROW0) * g.P + (hx0 + COL0)) * ts], el(0, j), ts * (size_t)w);
+        out.sx = 1; out.sy = g.P;
+    }
+    CK(cudaMalloc(&out.p, buf.size()));
+    ctx->allocs.push_back(out.p);
+    CK(cudaMemcpy(out.p, buf.data(), buf.size(), cudaMemcpyHostToDevice));
+    return SW_OK;
+}
+
+// state transfers: host arrays with halo <-> device layout
+struct HostShape { int w, h, x0, y0; };
+HostShape shape_u(const Geom& g) { return {(g.ep ? g.N : g.N - 1) + 4, g.M + 4, g.ep ? -2 : -1, -2}; }
+HostShape shape_v(const Geom& g) { return {g.N + 4, g.M + 3, -2, -1}; }
+HostShape shape_e(const Geom& g) { return {g.N + 2, g.M + 2, -1, -1}; }
+HostShape shape_s(const Geom& g) { return {g.N + 2, g.M, -1, 0}; }
+
+int copy_in(sw_ctx* ctx, void* dev, const void* host, HostShape s) {
+    const size_t es = ctx->tpsz;
+    char* d = static_cast<char*>(dev) + ((size_t)(s.y0 + ROW0) * ctx->g.P + (s.x0 + COL0)) * es;
+    CK(cudaMemcpy2DAsync(d, ctx->g.P * es, host, s.w * es, s.w * es, s.h, cudaMemcpyHostToDevice, ctx->stream));
+    return SW_OK;
+}
+int copy_out(sw_ctx* ctx, void* host, const void* dev, HostShape s) {
+    const size_t es = ctx->tpsz;
+    const char* d = static_cast<const char*>(dev) + ((size_t)(s.y0 + ROW0) * ctx->g.P + (s.x0 + COL0)) * es;
+    CK(cudaMemcpy2DAsync(host, s.w * es, d, ctx->g.P * es, s.w * es, s.h, cudaMemcpyDeviceToHost, ctx->stream));
+    return SW_OK;
+}
+
+int run_steps(sw_ctx* ctx, long long nsteps, sw_status* status) {
+    const sw_config& c = ctx->cfg;
+    long long done = 0;
+    int code = SW_OK;
+    for (long long s = 0; s < nsteps; s++) {
+        long long i = ctx->step + 1;
+        int rc = ctx->eng->step(ctx, i);
+        if (rc) return rc;
+        done++;
+        bool check = (i % c.nout) == 0;
+        if (check) {
+            CK(cudaMemcpyAsync(ctx->hst, ctx->dst, sizeof(DevStatus), cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            if (ctx->hst->error) {
+                code = ctx->hst->error;
+                ctx->step = i;
+                break;
+            }
+            if (ctx->hst->stop) {
+                // state stays S[p] (before this step); the tracer already moved sst
+                ctx->step = i;
+                code = SW_NAN_DETECTED;
+                break;
+            }
+        }
+        ctx->p = 1 - ctx->p;
+        ctx->step = i;
+    }
+    if (code == SW_OK) {
+        CK(cudaMemcpyAsync(ctx->hst, ctx->dst, sizeof(DevStatus), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (ctx->hst->error) code = ctx->hst->error;
+    }
+    if (status) {
+        status->steps_done = done;
+        status->step = ctx->step;
+        status->nan_step = (code == SW_NAN_DETECTED) ? ctx->step : -1;
+        status->code = code;
+    }
+    if (code == SW_ERR_DEPARTURE) ctx->err = "tracer departure point outside the domain";
+    if (code == SW_NAN_DETECTED) ctx->err = "NaNs detected at time step " + std::to_string(ctx->step);
+    return code;
+}
+
+}  // namespace
+
+// ======================================================================= C ABI
+extern "C" {
+
+int sw_abi_version(void) { return SWB200_ABI_VERSION; }
+
+const char* sw_strerror(int code) { return err_name(code); }
+
+const char* sw_last_error(const sw_ctx* ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+int64_t sw_kernel_launches(const sw_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+void sw_destroy(sw_ctx* ctx) {
+    if (!ctx) return;
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (void* p : ctx->allocs) cudaFree(p);
+    if (ctx->hst) cudaFreeHost(ctx->hst);
+    for (auto e : ctx->evpool) cudaEventDestroy(e);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
+    if (!cfg || !st || !out) return SW_ERR_ARG;
+    *out = nullptr;
+    std::string why;
+    int rc = check_config(cfg, why);
+    if (rc) {
+        fprintf(stderr, "swb200: %s\n", why.c_str());
+        return rc;
+    }
+    if (!st->f_q || !st->Fx || !st->Fy || !st->H) return SW_ERR_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return SW_ERR_NODEVICE;
+
+    std::unique_ptr<sw_ctx> holder(new sw_ctx());
+    sw_ctx* ctx = holder.get();
+    ctx->cfg = *cfg;
+    CK(cudaGetDevice(&ctx->device));
+    Geom& g = ctx->g;
+    g.N = cfg->nx; g.M = cfg->ny; g.ep = cfg->periodic ? 1 : 0;
+    g.P = ((g.N + 8 + PADX) + 31) / 32 * 32;
+    g.R = g.M + 4 + PADY;
+    ctx->nelem = (size_t)g.P * g.R;
+    ctx->tsz = fmt_size(cfg->T);
+    ctx->tpsz = fmt_size(cfg->Tprog);
+    CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+
+    auto alloc = [&](void** p, size_t bytes) -> int {
+        CK(cudaMalloc(p, bytes));
+        ctx->allocs.push_back(*p);
+        CK(cudaMemsetAsync(*p, 0, bytes, ctx->stream));
+        return SW_OK;
+    };
+    const size_t fb = ctx->nelem * ctx->tpsz;
+    for (Fields3* f : {&ctx->S[0], &ctx->S[1], &ctx->A, &ctx->B, &ctx->Acc})
+        for (void** p : {&f->u, &f->v, &f->e})
+            if ((rc = alloc(p, fb))) return rc;
+    if ((rc = alloc(&ctx->sst[0], fb))) return rc;
+    if ((rc = alloc(&ctx->sst[1], fb))) return rc;
+    if (cfg->tracer_advection && cfg->nadvstep > 1) {
+        if ((rc = alloc(&ctx->um, ctx->nelem * ctx->tsz))) return rc;
+        if ((rc = alloc(&ctx->vm, ctx->nelem * ctx->tsz))) return rc;
+    }
+    {
+        void* p = nullptr;
+        if ((rc = alloc(&p, sizeof(DevStatus)))) return rc;
+        ctx->dst = static_cast<DevStatus*>(p);
+    }
+    CK(cudaMallocHost(&ctx->hst, sizeof(DevStatus)));
+    std::memset(ctx->hst, 0, sizeof(DevStatus));
+
+    const int N = g.N, M = g.M, nux = g.ep ? N : N - 1;
+    if ((rc = upload_static(ctx, ctx->fq, st->f_q, N + 1, M + 1, 0, 0))) return rc;
+    if ((rc = upload_static(ctx, ctx->Fx, st->Fx, nux, M, 1 - g.ep, 0))) return rc;
+    if ((rc = upload_static(ctx, ctx->Fy, st->Fy, N, M - 1, 0, 1))) return rc;
+    if ((rc = upload_static(ctx, ctx->H, st->H, N + 2, M + 2, -1, -1))) return rc;
+
+    if (cfg->T == SW_FLOAT32 && cfg->Tprog == SW_FLOAT32) {
+        auto* e = new Engine<float, float>(); ctx->eng.reset(e); if ((rc = e->init(ctx))) return rc;
+    } else if (cfg->T == SW_FLOAT64 && cfg->Tprog == SW_FLOAT64) {
+        auto* e = new Engine<double, double>(); ctx->eng.reset(e); if ((rc = e->init(ctx))) return rc;
+    } else {
+        auto* e = new Engine<float, double>(); ctx->eng.reset(e); if ((rc = e->init(ctx))) return rc;
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    *out = holder.release();
+    return SW_OK;
+}
+
+int sw_set_state(sw_ctx* ctx, const void* u, const void* v, const void* eta, const void* sst) {
+    if (!ctx || !u || !v || !eta || !sst) return SW_ERR_ARG;
+    ctx->p = 0; ctx->sp = 0; ctx->step = 0; ctx->t = 0;
+    int rc;
+    if ((rc = copy_in(ctx, ctx->S[0].u, u, shape_u(ctx->g)))) return rc;
+    if ((rc = copy_in(ctx, ctx->S[0].v, v, shape_v(ctx->g)))) return rc;
+    if ((rc = copy_in(ctx, ctx->S[0].e, eta, shape_e(ctx->g)))) return rc;
+    if ((rc = copy_in(ctx, ctx->sst[0], sst, shape_s(ctx->g)))) return rc;
+    CK(cudaMemsetAsync(ctx->dst, 0, sizeof(DevStatus), ctx->stream));
+    // ghost_points!(u,v,eta) opens every step (src/time_integration.jl:48); it is
+    // idempotent after the first, so it is applied once here
+    if ((rc = ctx->eng->ghost_state(ctx))) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SW_OK;
+}
+
+int sw_get_state(sw_ctx* ctx, void* u, void* v, void* eta, void* sst) {
+    if (!ctx || !u || !v || !eta || !sst) return SW_ERR_ARG;
+    const Fields3& X = ctx->S[ctx->p];
+    int rc;
+    if ((rc = copy_out(ctx, u, X.u, shape_u(ctx->g)))) return rc;
+    if ((rc = copy_out(ctx, v, X.v, shape_v(ctx->g)))) return rc;
+    if ((rc = copy_out(ctx, eta, X.e, shape_e(ctx->g)))) return rc;
+    if ((rc = copy_out(ctx, sst, ctx->sst[ctx->sp], shape_s(ctx->g)))) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SW_OK;
+}
+
+int sw_run(sw_ctx* ctx, int64_t nsteps, sw_status* status) {
+    if (!ctx || nsteps < 0) return SW_ERR_ARG;
+    return run_steps(ctx, nsteps, status);
+}
+
+int sw_run_profiled(sw_ctx* ctx, int64_t nsteps, int64_t l2_flush_bytes, sw_profile* prof, sw_status* status) {
+    if (!ctx || !prof || nsteps < 0) return SW_ERR_ARG;
+    std::memset(prof, 0, sizeof(*prof));
+    if (l2_flush_bytes > 0 && (size_t)l2_flush_bytes > ctx->flush_bytes) {
+        if (ctx->flush) cudaFree(ctx->flush);
+        CK(cudaMalloc(&ctx->flush, (size_t)l2_flush_bytes));
+        ctx->flush_bytes = (size_t)l2_flush_bytes;
+    }
+    ctx->prof = true;
+    ctx->marks.clear();
+    ctx->evnext = 0;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> steps;
+    int code = SW_OK;
+    long long done = 0;
+    for (long long s = 0; s < nsteps; s++) {
+        if (l2_flush_bytes > 0) CK(cudaMemsetAsync(ctx->flush, (int)(s & 0xff), (size_t)l2_flush_bytes, ctx->stream));
+        cudaEvent_t a = ctx->evget(), b = ctx->evget();
+        CK(cudaEventRecord(a, ctx->stream));
+        sw_status st1;
+        code = run_steps(ctx, 1, &st1);
+        CK(cudaEventRecord(b, ctx->stream));
+        steps.push_back({a, b});
+        done += st1.steps_done;
+        if (code) break;
+    }
+    ctx->prof = false;
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (auto& pr : steps) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, pr.first, pr.second);
+        prof->step_ms_total += ms;
+    }
+    for (auto& m : ctx->marks) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, m.a, m.b);
+        prof->kernel_ms[m.kind] += ms;
+        prof->launches[m.kind]++;
+    }
+    prof->steps = done;
+    if (status) {
+        status->steps_done = done;
+        status->step = ctx->step;
+        status->code = code;
+        status->nan_step = code == SW_NAN_DETECTED ? ctx->step : -1;
+    }
+    return code;
+}
+
+int sw_diagnostics(sw_ctx* ctx, sw_diag* out) {
+    if (!ctx || !out) return SW_ERR_ARG;
+    return fail(ctx, SW_ERR_UNSUPPORTED, "sw_diagnostics not built yet");
+}
+
+int sw_time_integration(const sw_config* cfg, const sw_static* st, void* u, void* v, void* eta, void* sst,
+                        sw_status* status) {
+    sw_ctx* ctx = nullptr;
+    int rc = sw_create(cfg, st, &ctx);
+    if (rc) return rc;
+    rc = sw_set_state(ctx, u, v, eta, sst);
+    if (!rc) {
+        int rr = sw_run(ctx, cfg->nt, status);
+        if (rr == SW_OK || rr == SW_NAN_DETECTED) {
+            int rg = sw_get_state(ctx, u, v, eta, sst);
+            rc = rg ? rg : rr;
+        } else {
+            rc = rr;
+        }
+    }
+    if (rc && rc != SW_NAN_DETECTED) fprintf(stderr, "swb200: %s\n", ctx->err.c_str());
+    sw_destroy(ctx);
+    return rc;
+}
+
+}  // extern "C"

@@ -10,9 +10,10 @@ from .model_setup import Grid, Constants, Forcing, ModelSetup, model_setup
 from .initial_conditions import (PrognosticVars, initial_conditions, add_halo, remove_halo,
                                  ghost_points, ghost_points_sst)
 from .run_model import run_model, time_integration, NaNsDetected
+from .model import Model
 from . import abi
 
 __all__ = ["Parameter", "Grid", "Constants", "Forcing", "ModelSetup", "model_setup",
            "PrognosticVars", "initial_conditions", "add_halo", "remove_halo",
            "ghost_points", "ghost_points_sst", "run_model", "time_integration",
-           "NaNsDetected", "abi"]
+           "NaNsDetected", "Model", "abi"]

@@ -1,0 +1,146 @@
+"""GPU parity: the CUDA time loop against the CPU oracle, through the C ABI.
+
+Both receive the same config, static fields and seeded state; the library is
+built without FMA contraction, so the comparison is bit for bit on the full
+arrays with halo (u, v, η, sst) after every checked step count.  Sizes are
+small and odd where possible so partial tiles and all boundary code paths run.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import assert_bitwise, seeded_inputs
+from swb200 import Model, Parameter, initial_conditions, model_setup, run_model
+
+pytestmark = pytest.mark.gpu
+
+
+def both(kw, nsteps, seed=1, checkpoints=None):
+    P = Parameter(**kw)
+    S = model_setup(P)
+    Prog = initial_conditions(P.Tprog, S, **seeded_inputs(S, seed))
+    o = O.Oracle(S)
+    o.set_state(Prog)
+    m = Model(S)
+    m.set_state(Prog)
+    done = 0
+    for n in (checkpoints or [nsteps]):
+        so = o.run(n - done)
+        sg = m.run(n - done)
+        done = n
+        assert so.code == sg.code, (so.code, sg.code)
+        a, b = o.get_state(), m.get_state()
+        for x, y, name in zip(a, b, ("u", "v", "η", "sst")):
+            assert_bitwise(y, x, f"{name} after {n} steps")
+    return S, m
+
+
+BASE = dict(nx=40, Ndays=0.5, Uadv=1000)
+
+CASES = {
+    "periodic_const": dict(),
+    "periodic_smag": dict(diffusion="Smagorinsky"),
+    "nonperiodic": dict(bc="nonperiodic"),
+    "nonperiodic_freeslip_seamount_gyre": dict(bc="nonperiodic", α=0, topography="seamount",
+                                               wind_forcing_x="double_gyre"),
+    "periodic_seamount_smag": dict(topography="seamount", diffusion="Smagorinsky"),
+    "periodic_ridges_linear_drag": dict(topography="ridges", bottom_drag="linear"),
+    "partial_slip_no_drag": dict(bc="nonperiodic", α=0.5, bottom_drag="none"),
+    "rk3": dict(RKo=3, cfl=0.6),
+    "rk2": dict(RKo=2, cfl=0.3),
+    "seasonal_wind": dict(seasonal_wind_x=True, seasonal_wind_y=True, wind_forcing_y="channel", Fy0=0.05),
+    "fy_channel_nonperiodic": dict(bc="nonperiodic", wind_forcing_y="channel", Fy0=0.05),
+    "tracer_consumption": dict(tracer_consumption=True),
+    "tracer_every_30": dict(Uadv=2.0, Ndays=1),
+    "tracer_default_uadv": dict(Uadv=0.25, nx=24, Ndays=2),
+    "nstep_diff_3": dict(nstep_diff=3),
+    "tcomm_float16": dict(Tcomm=np.float16),
+    "float64": dict(T=np.float64),
+    "float64_nonperiodic_smag": dict(T=np.float64, bc="nonperiodic", diffusion="Smagorinsky"),
+    "mixed_f32_f64": dict(T=np.float32, Tprog=np.float64),
+    "odd_37": dict(nx=37),
+    "odd_37_nonperiodic": dict(nx=37, bc="nonperiodic", diffusion="Smagorinsky"),
+    "wide_130": dict(nx=130, L_ratio=4, Ndays=0.2),
+    "square_64_nonperiodic": dict(nx=64, L_ratio=1, bc="nonperiodic", Ndays=0.2),
+}
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_bitwise_parity(name):
+    kw = dict(BASE)
+    kw.update(CASES[name])
+    both(kw, 0, checkpoints=[1, 2, 7, 20])
+
+
+def test_reference_config_c1_one_day():
+    """configs[0]'s physics (periodic channel, Smagorinsky, quadratic drag,
+    tracer every step) at 100x50 for one day: identical to the oracle."""
+    kw = dict(nx=100, L_ratio=2, bc="periodic", wind_forcing_x="channel", Fx0=0.12, topography="flat",
+              H=500, g=10, cfl=1, adv_scheme="ArakawaHsu", diffusion="Smagorinsky",
+              bottom_drag="quadratic", tracer_advection=True, Uadv=1000, Ndays=1)
+    both(kw, 0, checkpoints=[1, 50, 307])
+
+
+def test_no_forcing_known_answer():                       # test/runtests.jl:4-9
+    prog = run_model(Ndays=1, Fx0=0)
+    assert np.all(prog.u == 0) and np.all(prog.v == 0) and np.all(prog.η == 0)
+
+
+@pytest.mark.parametrize("kw", [dict(bc="periodic"), dict(bc="nonperiodic"), dict(α=0)])
+def test_boundary_conditions(kw):                         # test/runtests.jl:11-20
+    prog = run_model(Ndays=1, **kw)
+    assert np.all(np.abs(prog.η) < 10)
+
+
+def test_mixed_precision_f32_f64():                       # test/runtests.jl:33-35
+    prog = run_model(np.float32, Tprog=np.float64, Ndays=1)
+    assert prog.u.dtype == np.float64
+    assert np.all(np.abs(prog.η) < 10) and np.all(prog.u != 0)
+
+
+def test_rk3():                                           # test/runtests.jl:42-46
+    prog = run_model(time_scheme="RK", RKo=3, cfl=0.6, nstep_advcor=0)
+    assert np.all(np.abs(prog.η) < 10) and np.all(prog.u != 0)
+
+
+def test_nan_detection_matches_reference():
+    """NaNs in the state stop the run at the first multiple of nout, returning
+    u, v, η from before that step (src/time_integration.jl:235-237)."""
+    P = Parameter(nx=20, Ndays=2, Uadv=1000, tracer_advection=False)
+    S = model_setup(P)
+    Prog = initial_conditions(P.Tprog, S)
+    Prog.u[5, 7] = np.nan
+    o = O.Oracle(S)
+    o.set_state(Prog)
+    so = o.run(S.grid.nt)
+    m = Model(S)
+    m.set_state(Prog)
+    sg = m.run(S.grid.nt)
+    assert sg.code == so.code == 3
+    assert sg.nan_step == so.nan_step == S.grid.nout
+    for x, y, name in zip(o.get_state(), m.get_state(), ("u", "v", "η", "sst")):
+        assert_bitwise(y, x, name)
+
+
+def test_time_integration_drop_in_equals_stepping():
+    """sw_time_integration (host buffers in/out) equals the context API."""
+    from swb200 import time_integration
+    P = Parameter(nx=40, Ndays=0.3, Uadv=1000, diffusion="Smagorinsky")
+    S = model_setup(P)
+    Prog = initial_conditions(P.Tprog, S, **seeded_inputs(S, 3))
+    out, st = time_integration(Prog, S)
+    assert st.code == 0 and st.steps_done == S.grid.nt
+    ref, sto = O.run_model(P=P, **seeded_inputs(S, 3))
+    for x, y, name in zip(ref, out, ("u", "v", "η", "sst")):
+        assert_bitwise(y, x, name)
+
+
+def test_kernel_launch_count():
+    P = Parameter(nx=40, Ndays=0.3, Uadv=1000)
+    S = model_setup(P)
+    m = Model(S)
+    m.set_state(initial_conditions(P.Tprog, S))
+    n0 = m.kernel_launches
+    m.run(10)
+    # 4 stages + tail + tracer per step, plus NaN checks every nout steps
+    assert m.kernel_launches - n0 >= 60
