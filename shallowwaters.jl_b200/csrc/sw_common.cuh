@@ -21,6 +21,14 @@
 
 #include "swb200.h"
 
+// unroll factor of the row-streaming loops
+#ifndef SWB_UNROLL
+#define SWB_UNROLL 2
+#endif
+#define SWB_PRAGMA(x) _Pragma(#x)
+#define SWB_UNROLL_PRAGMA(n) SWB_PRAGMA(unroll n)
+#define SWB_ROW_UNROLL SWB_UNROLL_PRAGMA(SWB_UNROLL)
+
 namespace swb {
 
 constexpr int COL0 = 4;
@@ -31,8 +39,8 @@ struct Geom {
     int ep;        // 1 periodic, 0 nonperiodic
     int P;         // pitch (elements)
     int R;         // rows
-    __host__ __device__ inline long idx(int x, int y) const {
-        return (long)(y + ROW0) * P + (x + COL0);
+    __host__ __device__ inline int idx(int x, int y) const {
+        return (y + ROW0) * P + (x + COL0);
     }
     // interior ranges (inclusive lower, exclusive upper)
     __host__ __device__ inline int u_x0() const { return 1 - ep; }
@@ -46,8 +54,8 @@ struct Geom {
 template <class T>
 struct SField {
     const T* p;
-    long sx, sy;   // element strides along x and y
-    __device__ inline T at(int x, int y) const { return p[(long)(y + ROW0) * sy + (long)(x + COL0) * sx]; }
+    int sx, sy;    // element strides along x and y
+    __device__ __forceinline__ T at(int x, int y) const { return p[(y + ROW0) * sy + (x + COL0) * sx]; }
 };
 
 // number conversion (Julia's T(x))

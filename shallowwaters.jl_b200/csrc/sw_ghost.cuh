@@ -16,13 +16,23 @@ struct GhostRule {
     int ep, N, M, Tcomm;
     Tp oma;   // one_minus_α (src/constants.jl:86)
 
+    __device__ __forceinline__ Tp comm(Tp val) const {
+        return (Tcomm == SW_FLOAT16 || (Tcomm == SW_FLOAT32 && sizeof(Tp) == 8)) ? via_comm(Tcomm, val) : val;
+    }
+    // Is (x, y) a source of a ghost copy?  Cheap tests for the hot loops.
+    __device__ __forceinline__ bool u_src(int F, int b) const {
+        return ep ? (F <= 1 || F >= N - 2) : (b <= 1 || b >= M - 2);
+    }
+    __device__ __forceinline__ bool v_src(int a) const { return a <= 1 || a >= N - 2; }
+    __device__ __forceinline__ bool eta_src(int a, int b) const { return a == 0 || a == N - 1 || b == 0 || b == M - 1; }
+
     // u at (F, b) was set to val: write the halo cells copied from it.
     // periodic  u[1]=u[end-3], u[2]=u[end-2], u[end-1]=u[3], u[end]=u[4]  (:64-69)
     // nonperiodic u[:,1]=(1-α)u[:,4], u[:,2]=(1-α)u[:,3], u[:,end-1]=(1-α)u[:,end-2],
     //             u[:,end]=(1-α)u[:,end-3]                                 (:51-56)
     __device__ inline void u(Tp* __restrict__ dst, const Geom& g, int F, int b, Tp val) const {
         if (ep) {
-            Tp c = via_comm(Tcomm, val);
+            Tp c = comm(val);
             if (F == 0 || F == 1) dst[g.idx(F + N, b)] = c;
             if (F == N - 2 || F == N - 1) dst[g.idx(F - N, b)] = c;
         } else {
@@ -36,7 +46,7 @@ struct GhostRule {
     // v at (a, G): periodic x copies (:93-98); nonperiodic (1-α) mirror in x (:80-85)
     __device__ inline void v(Tp* __restrict__ dst, const Geom& g, int a, int G, Tp val) const {
         if (ep) {
-            Tp c = via_comm(Tcomm, val);
+            Tp c = comm(val);
             if (a == 0 || a == 1) dst[g.idx(a + N, G)] = c;
             if (a == N - 2 || a == N - 1) dst[g.idx(a - N, G)] = c;
         } else {
@@ -51,7 +61,7 @@ struct GhostRule {
     // take the column-copied value (src/ghost_points.jl:102-133)
     __device__ inline void eta(Tp* __restrict__ dst, const Geom& g, int a, int b, Tp val) const {
         int xs[2], nx = 0;
-        Tp cx = ep ? via_comm(Tcomm, val) : val;
+        Tp cx = ep ? comm(val) : val;
         if (ep) {
             if (a == N - 1) xs[nx++] = -1;
             if (a == 0) xs[nx++] = N;
@@ -73,7 +83,7 @@ struct GhostRule {
     // sst at (a, b): periodic / zero-gradient copies in x (src/ghost_points.jl:136-179)
     __device__ inline void sst(Tp* __restrict__ dst, const Geom& g, int a, int b, Tp val) const {
         if (ep) {
-            Tp c = via_comm(Tcomm, val);
+            Tp c = comm(val);
             if (a == N - 1) dst[g.idx(-1, b)] = c;
             if (a == 0) dst[g.idx(N, b)] = c;
         } else {

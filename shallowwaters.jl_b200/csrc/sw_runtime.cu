@@ -12,11 +12,15 @@
 // state parity p, step i reads S[p] and leaves the new state in S[1-p]; S[p]
 // survives the step, which gives the reference's NaN semantics (return the
 // state from before the failing step).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -26,6 +30,7 @@
 #include "sw_common.cuh"
 #include "sw_ghost.cuh"
 #include "sw_stage.cuh"
+#include "sw_stage2.cuh"
 #include "sw_tail.cuh"
 #include "sw_tracer.cuh"
 
@@ -33,9 +38,15 @@ using namespace swb;
 
 namespace {
 
-constexpr int STAGE_TX = 64, STAGE_TY = 8, STAGE_NT = 256;
-constexpr int TAIL_TX = 32, TAIL_TY = 8, TAIL_NT = 256;
-constexpr int PADX = 72, PADY = 44;     // >= max tile width + 8, tile height + 12
+#ifndef SWB_STAGE_TY
+#define SWB_STAGE_TY 32
+#endif
+#ifndef SWB_TAIL_TY
+#define SWB_TAIL_TY 16
+#endif
+constexpr int STAGE_TY = SWB_STAGE_TY;  // rows per warp strip of the stage kernel
+constexpr int TAIL_TY = SWB_TAIL_TY;    // rows per warp strip of the tail kernel
+constexpr int PADX = 72, PADY = 44;     // column/row padding: strips read up to TY+3 rows and 30 columns past the edge
 constexpr int RING_BLOCKS_MAX = 32;
 
 const char* err_name(int c) {
@@ -79,7 +90,14 @@ struct sw_ctx {
     void* um = nullptr; void* vm = nullptr;
     void* flush = nullptr; size_t flush_bytes = 0;
     // static fields (type T) and their strides
-    struct SF { void* p = nullptr; long sx = 0, sy = 0; } H, fq, Fx, Fy, fu, fv, eref, Feta;
+    struct SF { void* p = nullptr; int sx = 0, sy = 0; } H, fq, Fx, Fy, fu, fv, eref, Feta;
+    // TMA descriptors per state buffer: input box (BOXW_IN x K) and point-wise box (BOXW_X x K)
+    struct Maps { CUtensorMap in, x, in2, x2; };
+    TileSched* sched = nullptr;   // device tile counter of the TMA stage kernel
+    std::map<const void*, Maps> tmaps;
+    bool use_tma = false;
+    bool packed = false;          // FP32x2 stage kernel for Float32 (opt-in: SWB200_PACKED=1)
+    int nsm = 148;
     DevStatus* dst = nullptr;     // device status
     DevStatus* hst = nullptr;     // pinned host mirror
     int p = 0;                    // state parity
@@ -121,6 +139,58 @@ int fail(sw_ctx* c, int code, const std::string& msg) {
             return fail(ctx, e_ == cudaErrorMemoryAllocation ? SW_ERR_NOMEM : SW_ERR_CUDA,   \
                         std::string(#call) + ": " + cudaGetErrorString(e_));                 \
     } while (0)
+
+#ifndef SWB_TMA_TY
+#define SWB_TMA_TY 8
+#endif
+#ifndef SWB_TMA_K
+#define SWB_TMA_K 4
+#endif
+#ifndef SWB_TMA_S
+#define SWB_TMA_S 2
+#endif
+constexpr int STAGE_TMA_TY = SWB_TMA_TY, STAGE_TMA_K = SWB_TMA_K, STAGE_TMA_S = SWB_TMA_S;
+#ifndef SWB_S2_TY
+#define SWB_S2_TY 16
+#endif
+#ifndef SWB_S2_K
+#define SWB_S2_K 4
+#endif
+#ifndef SWB_S2_S
+#define SWB_S2_S 2
+#endif
+constexpr int STAGE2_TY = SWB_S2_TY, STAGE2_K = SWB_S2_K, STAGE2_S = SWB_S2_S;
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// 2-D map over a P x R field buffer; boxes of boxw x boxh elements, zero fill
+// outside the buffer
+bool make_map(CUtensorMap* m, void* base, size_t elsize, int P, int R, int boxw, int boxh) {
+    auto fn = encode_fn();
+    if (!fn) return false;
+    CUtensorMapDataType dt = elsize == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                           : elsize == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+    cuuint64_t dims[2] = {(cuuint64_t)P, (cuuint64_t)R};
+    cuuint64_t strides[1] = {(cuuint64_t)P * elsize};
+    cuuint32_t box[2] = {(cuuint32_t)boxw, (cuuint32_t)boxh};
+    cuuint32_t es[2] = {1, 1};
+    CUresult r = fn(m, dt, 2, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
 
 template <class T>
 SField<T> sf(const sw_ctx::SF& s) { return SField<T>{static_cast<const T*>(s.p), s.sx, s.sy}; }
@@ -188,17 +258,7 @@ __global__ void ghost_state_kernel(Geom g, Tp* u, Tp* v, Tp* e, GhostRule<Tp> gr
 
 template <class T, class Tp>
 struct Engine : EngineBase {
-    int stage_smem = 0, tail_smem = 0;
-
-    int init(sw_ctx* ctx) {
-        stage_smem = 8 * (STAGE_TX + 8) * (STAGE_TY + 3) * (int)sizeof(T);
-        tail_smem = 12 * (TAIL_TX + 8) * (TAIL_TY + 4) * (int)sizeof(T);
-        CK(cudaFuncSetAttribute(rk_stage_kernel<T, Tp, STAGE_TX, STAGE_TY, STAGE_NT>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, stage_smem));
-        CK(cudaFuncSetAttribute(tail_kernel<T, Tp, TAIL_TX, TAIL_TY, TAIL_NT>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, tail_smem));
-        return SW_OK;
-    }
+    int init(sw_ctx*) { return SW_OK; }
 
     GhostRule<Tp> rule(sw_ctx* ctx) const {
         GhostRule<Tp> r;
@@ -210,6 +270,110 @@ struct Engine : EngineBase {
     static int ring_blocks(const Geom& g, int nt) {
         int n = Ring::u_count(g.ep, g.N, g.M) + Ring::v_count(g.N);
         return std::min(RING_BLOCKS_MAX, (n + nt - 1) / nt);
+    }
+
+    template <bool PER, bool FIRST, bool LAST>
+    static void stage_launch(const StageArgs<T, Tp>& a, int nblk, cudaStream_t s) {
+        rk_stage_kernel<T, Tp, PER, FIRST, LAST, STAGE_TY><<<nblk, 128, 0, s>>>(a);
+    }
+    static void stage_dispatch(const StageArgs<T, Tp>& a, bool per, bool first, bool last, int nblk, cudaStream_t s) {
+        if (per) {
+            if (first) stage_launch<true, true, false>(a, nblk, s);
+            else if (last) stage_launch<true, false, true>(a, nblk, s);
+            else stage_launch<true, false, false>(a, nblk, s);
+        } else {
+            if (first) stage_launch<false, true, false>(a, nblk, s);
+            else if (last) stage_launch<false, false, true>(a, nblk, s);
+            else stage_launch<false, false, false>(a, nblk, s);
+        }
+    }
+    template <bool PER, bool FIRST, bool LAST>
+    static int stage_tma_launch(sw_ctx* ctx, const StageArgs<T, Tp>& a, const StageMaps& mp) {
+        constexpr int TY = STAGE_TMA_TY, K = STAGE_TMA_K, S = STAGE_TMA_S;
+        auto kern = rk_stage_tma<T, Tp, PER, FIRST, LAST, TY, K, S>;
+        constexpr int smem = stage_tma_smem<T, Tp, FIRST, LAST, K, S>();
+        static int occ = -1;   // per instantiation
+        if (occ < 0) {
+            if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return -1;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 160, smem) != cudaSuccess || occ < 1) return -1;
+        }
+        const Geom& g = a.g;
+        const int ntiles = ((g.N + BAND - 1) / BAND) * ((g.M + TY - 1) / TY);
+        const int npersist = std::min(ntiles, ctx->nsm * occ);
+        const int nring = std::min(RING_BLOCKS_MAX, (Ring::u_count(g.ep, g.N, g.M) + Ring::v_count(g.N) + 159) / 160);
+        kern<<<npersist + nring, 160, smem, ctx->stream>>>(a, mp, npersist, ctx->sched);
+        return 0;
+    }
+    static int stage_tma_dispatch(sw_ctx* ctx, const StageArgs<T, Tp>& a, const StageMaps& mp, bool per, bool first,
+                                  bool last) {
+        if (per) {
+            if (first) return stage_tma_launch<true, true, false>(ctx, a, mp);
+            if (last) return stage_tma_launch<true, false, true>(ctx, a, mp);
+            return stage_tma_launch<true, false, false>(ctx, a, mp);
+        }
+        if (first) return stage_tma_launch<false, true, false>(ctx, a, mp);
+        if (last) return stage_tma_launch<false, false, true>(ctx, a, mp);
+        return stage_tma_launch<false, false, false>(ctx, a, mp);
+    }
+
+    template <bool PER, bool FIRST, bool LAST>
+    static int stage2_launch(sw_ctx* ctx, const StageArgs<T, Tp>& a, const StageMaps2& mp) {
+        if constexpr (std::is_same<T, float>::value && std::is_same<Tp, float>::value) {
+            constexpr int TY = STAGE2_TY, K = STAGE2_K, S = STAGE2_S;
+            auto kern = rk_stage_f2<PER, FIRST, LAST, TY, K, S>;
+            constexpr int smem = stage2_smem<FIRST, LAST, K, S>();
+            static int occ = -1;
+            if (occ < 0) {
+                if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return -1;
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 160, smem) != cudaSuccess || occ < 1) return -1;
+            }
+            const Geom& g = a.g;
+            const int ntiles = ((g.N + BAND2 - 1) / BAND2) * ((g.M + TY - 1) / TY);
+            const int npersist = std::min(ntiles, ctx->nsm * occ);
+            const int nring = std::min(RING_BLOCKS_MAX, (Ring::u_count(g.ep, g.N, g.M) + Ring::v_count(g.N) + 159) / 160);
+            kern<<<npersist + nring, 160, smem, ctx->stream>>>(a, mp, npersist, ctx->sched);
+            return 0;
+        } else {
+            return -1;
+        }
+    }
+    static int stage2_dispatch(sw_ctx* ctx, const StageArgs<T, Tp>& a, const StageMaps2& mp, bool per, bool first,
+                               bool last) {
+        if (per) {
+            if (first) return stage2_launch<true, true, false>(ctx, a, mp);
+            if (last) return stage2_launch<true, false, true>(ctx, a, mp);
+            return stage2_launch<true, false, false>(ctx, a, mp);
+        }
+        if (first) return stage2_launch<false, true, false>(ctx, a, mp);
+        if (last) return stage2_launch<false, false, true>(ctx, a, mp);
+        return stage2_launch<false, false, false>(ctx, a, mp);
+    }
+
+    template <bool PER, int DRAG, bool SMAG>
+    static void tail_launch(const TailArgs<T, Tp>& a, int nblk, cudaStream_t s) {
+        tail_kernel<T, Tp, PER, DRAG, SMAG, TAIL_TY><<<nblk, 128, 0, s>>>(a);
+    }
+    template <bool PER>
+    static void tail_dispatch2(const TailArgs<T, Tp>& a, int drag, bool smag, int nblk, cudaStream_t s) {
+        if (smag) {
+            if (drag == SW_DRAG_QUADRATIC) tail_launch<PER, SW_DRAG_QUADRATIC, true>(a, nblk, s);
+            else if (drag == SW_DRAG_LINEAR) tail_launch<PER, SW_DRAG_LINEAR, true>(a, nblk, s);
+            else tail_launch<PER, SW_DRAG_NONE, true>(a, nblk, s);
+        } else {
+            if (drag == SW_DRAG_QUADRATIC) tail_launch<PER, SW_DRAG_QUADRATIC, false>(a, nblk, s);
+            else if (drag == SW_DRAG_LINEAR) tail_launch<PER, SW_DRAG_LINEAR, false>(a, nblk, s);
+            else tail_launch<PER, SW_DRAG_NONE, false>(a, nblk, s);
+        }
+    }
+    template <bool PER>
+    static void tracer_dispatch2(const TracerArgs<T, Tp>& a, bool um_is_u, bool cons, dim3 grid, cudaStream_t s) {
+        if (um_is_u) {
+            if (cons) tracer_kernel<T, Tp, PER, true, true><<<grid, 128, 0, s>>>(a);
+            else tracer_kernel<T, Tp, PER, true, false><<<grid, 128, 0, s>>>(a);
+        } else {
+            if (cons) tracer_kernel<T, Tp, PER, false, true><<<grid, 128, 0, s>>>(a);
+            else tracer_kernel<T, Tp, PER, false, false><<<grid, 128, 0, s>>>(a);
+        }
     }
 
     int ghost_state(sw_ctx* ctx) override {
@@ -231,20 +395,21 @@ struct Engine : EngineBase {
         T Fyt = c.seasonal_wind_y ? (T)std::sin(c.omegaFy * (double)ctx->t) : one;
 
         // ------------------------------------------------ RK stages (:55-78)
-        const int ntx = (g.N + STAGE_TX - 1) / STAGE_TX, nty = (g.M + STAGE_TY - 1) / STAGE_TY;
-        const int nblk = ntx * nty + ring_blocks(g, STAGE_NT);
+        const int nsx = (g.N + STRIP - 1) / STRIP, nsy = (g.M + STAGE_TY - 1) / STAGE_TY;
+        const int nring = ring_blocks(g, 128);
+        const int nblk = (nsx * nsy + 3) / 4 + nring;
         for (int k = 1; k <= c.RKo; k++) {
             StageArgs<T, Tp> a;
-            a.g = g; a.ntx = ntx; a.nty = nty;
+            a.g = g; a.nsx = nsx; a.nsy = nsy; a.nring_blocks = nring;
             const Fields3& in = (k == 1) ? X : ((k % 2 == 0) ? ctx->A : ctx->B);
             Fields3& out1 = (k % 2 == 1) ? ctx->A : ctx->B;
             a.u1 = (const Tp*)in.u; a.v1 = (const Tp*)in.v; a.e1 = (const Tp*)in.e;
             a.uX = (const Tp*)X.u; a.vX = (const Tp*)X.v; a.eX = (const Tp*)X.e;
             a.u0i = (const Tp*)ctx->Acc.u; a.v0i = (const Tp*)ctx->Acc.v; a.e0i = (const Tp*)ctx->Acc.e;
-            a.first = (k == 1); a.last = (k == c.RKo);
-            if (!a.last) { a.u1o = (Tp*)out1.u; a.v1o = (Tp*)out1.v; a.e1o = (Tp*)out1.e; }
+            const bool first = (k == 1), last = (k == c.RKo);
+            if (!last) { a.u1o = (Tp*)out1.u; a.v1o = (Tp*)out1.v; a.e1o = (Tp*)out1.e; }
             else { a.u1o = a.v1o = a.e1o = nullptr; }
-            if (a.last) {
+            if (last) {
                 // the final X0: u, v to Acc when the tail follows, else straight into
                 // the new state; eta always into the new state (the tail keeps eta)
                 a.u0o = (Tp*)(tail_now ? ctx->Acc.u : Y.u);
@@ -260,30 +425,48 @@ struct Engine : EngineBase {
             a.Fxt = Fxt; a.Fyt = Fyt;
             a.gr = rule(ctx);
             a.st = ctx->dst;
-            int rc = launch(ctx, 0, [&] {
-                rk_stage_kernel<T, Tp, STAGE_TX, STAGE_TY, STAGE_NT>
-                    <<<nblk, STAGE_NT, stage_smem, ctx->stream>>>(a);
-            });
+            int rc;
+            constexpr bool F32 = std::is_same<T, float>::value && std::is_same<Tp, float>::value;
+            if (ctx->use_tma && F32 && ctx->packed) {
+                StageMaps2 mp;
+                mp.in_u = ctx->tmaps[in.u].in2; mp.in_v = ctx->tmaps[in.v].in2; mp.in_e = ctx->tmaps[in.e].in2;
+                mp.x_u = ctx->tmaps[X.u].x2; mp.x_v = ctx->tmaps[X.v].x2; mp.x_e = ctx->tmaps[X.e].x2;
+                mp.a_u = ctx->tmaps[ctx->Acc.u].x2; mp.a_v = ctx->tmaps[ctx->Acc.v].x2; mp.a_e = ctx->tmaps[ctx->Acc.e].x2;
+                int lr = 0;
+                rc = launch(ctx, 0, [&] { lr = stage2_dispatch(ctx, a, mp, g.ep != 0, first, last); });
+                if (!rc && lr) rc = fail(ctx, SW_ERR_CUDA, "packed stage kernel could not be configured");
+            } else if (ctx->use_tma) {
+                StageMaps mp;
+                mp.in_u = ctx->tmaps[in.u].in; mp.in_v = ctx->tmaps[in.v].in; mp.in_e = ctx->tmaps[in.e].in;
+                mp.x_u = ctx->tmaps[X.u].x; mp.x_v = ctx->tmaps[X.v].x; mp.x_e = ctx->tmaps[X.e].x;
+                mp.a_u = ctx->tmaps[ctx->Acc.u].x; mp.a_v = ctx->tmaps[ctx->Acc.v].x; mp.a_e = ctx->tmaps[ctx->Acc.e].x;
+                int lr = 0;
+                rc = launch(ctx, 0, [&] { lr = stage_tma_dispatch(ctx, a, mp, g.ep != 0, first, last); });
+                if (!rc && lr) rc = fail(ctx, SW_ERR_CUDA, "TMA stage kernel could not be configured");
+            } else {
+                rc = launch(ctx, 0, [&] { stage_dispatch(a, g.ep != 0, first, last, nblk, ctx->stream); });
+            }
             if (rc) return rc;
         }
 
         // -------------------------------------- drag + diffusion (:216-221)
         if (tail_now) {
             TailArgs<T, Tp> a;
-            const int tx = (g.N + TAIL_TX - 1) / TAIL_TX, ty = (g.M + TAIL_TY - 1) / TAIL_TY;
-            a.g = g; a.ntx = tx; a.nty = ty;
+            const int nsx = (g.N + STRIP - 1) / STRIP, nsy = (g.M + TAIL_TY - 1) / TAIL_TY;
+            const int nring = ring_blocks(g, 128);
+            a.g = g; a.nsx = nsx; a.nsy = nsy; a.nring_blocks = nring;
             a.u0 = (const Tp*)ctx->Acc.u; a.v0 = (const Tp*)ctx->Acc.v; a.e0 = (const Tp*)Y.e;
             a.uo = (Tp*)Y.u; a.vo = (Tp*)Y.v;
             a.H = sf<T>(ctx->H);
-            a.drag = c.bottom_drag;
-            a.smag = (c.diffusion == SW_DIFF_SMAGORINSKY);
             a.cD = (T)c.cD; a.rD = (T)c.rD; a.cSmag = (T)c.cSmag; a.nuB = (T)c.nuB;
             a.Dt_diff = (Tp)c.Dt_diff;
             a.gr = rule(ctx);
             a.st = ctx->dst;
-            int nb = tx * ty + ring_blocks(g, TAIL_NT);
+            const int nb = (nsx * nsy + 3) / 4 + nring;
+            const bool smag = (c.diffusion == SW_DIFF_SMAGORINSKY);
             int rc = launch(ctx, 1, [&] {
-                tail_kernel<T, Tp, TAIL_TX, TAIL_TY, TAIL_NT><<<nb, TAIL_NT, tail_smem, ctx->stream>>>(a);
+                if (g.ep) tail_dispatch2<true>(a, c.bottom_drag, smag, nb, ctx->stream);
+                else tail_dispatch2<false>(a, c.bottom_drag, smag, nb, ctx->stream);
             });
             if (rc) return rc;
         }
@@ -303,18 +486,19 @@ struct Engine : EngineBase {
                 a.g = g;
                 a.u = (const Tp*)Y.u; a.v = (const Tp*)Y.v;
                 a.um = (const T*)ctx->um; a.vm = (const T*)ctx->vm;
-                a.um_is_u = (c.nadvstep == 1);
+                const bool um_is_u = (c.nadvstep == 1);
                 a.sst = (const Tp*)ctx->sst[ctx->sp];
                 a.sst_o = (Tp*)ctx->sst[1 - ctx->sp];
                 a.dtadvu = (T)c.dtadvu; a.dtadvv = (T)c.dtadvv;
                 a.half_dtadvu = (T)c.half_dtadvu; a.half_dtadvv = (T)c.half_dtadvv;
-                a.consumption = c.tracer_consumption;
                 a.jSST = (T)c.jSST; a.SSTmin = (T)c.SSTmin;
                 a.gr = rule(ctx);
                 a.st = ctx->dst;
-                long long n = (long long)g.N * g.M;
-                int nb = (int)std::min<long long>((n + 255) / 256, 148 * 16);
-                int rc = launch(ctx, 2, [&] { tracer_kernel<T, Tp><<<nb, 256, 0, ctx->stream>>>(a); });
+                dim3 grid((g.N + 127) / 128, std::min(g.M, 4096));
+                int rc = launch(ctx, 2, [&] {
+                    if (g.ep) tracer_dispatch2<true>(a, um_is_u, c.tracer_consumption != 0, grid, ctx->stream);
+                    else tracer_dispatch2<false>(a, um_is_u, c.tracer_consumption != 0, grid, ctx->stream);
+                });
                 if (rc) return rc;
                 ctx->sp = 1 - ctx->sp;
             }
@@ -528,6 +712,8 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
         void* p = nullptr;
         if ((rc = alloc(&p, sizeof(DevStatus)))) return rc;
         ctx->dst = static_cast<DevStatus*>(p);
+        if ((rc = alloc(&p, sizeof(TileSched)))) return rc;
+        ctx->sched = static_cast<TileSched*>(p);
     }
     CK(cudaMallocHost(&ctx->hst, sizeof(DevStatus)));
     std::memset(ctx->hst, 0, sizeof(DevStatus));
@@ -538,6 +724,27 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
     if ((rc = upload_static(ctx, ctx->Fy, st->Fy, N, M - 1, 0, 1))) return rc;
     if ((rc = upload_static(ctx, ctx->H, st->H, N + 2, M + 2, -1, -1))) return rc;
 
+    {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, dev);
+        const char* env = getenv("SWB200_TMA");
+        bool want = !(env && env[0] == '0');
+        bool ok = want && encode_fn() != nullptr;
+        for (Fields3* f : {&ctx->S[0], &ctx->S[1], &ctx->A, &ctx->B, &ctx->Acc})
+            for (void* p : {f->u, f->v, f->e}) {
+                if (!ok) break;
+                sw_ctx::Maps mp;
+                ok = make_map(&mp.in, p, ctx->tpsz, g.P, g.R, BOXW_IN, STAGE_TMA_K) &&
+                     make_map(&mp.x, p, ctx->tpsz, g.P, g.R, BOXW_X, STAGE_TMA_K) &&
+                     make_map(&mp.in2, p, ctx->tpsz, g.P, g.R, BOXW_IN2, STAGE2_K) &&
+                     make_map(&mp.x2, p, ctx->tpsz, g.P, g.R, BOXW_X2, STAGE2_K);
+                ctx->tmaps[p] = mp;
+            }
+        ctx->use_tma = ok;
+        const char* envp = getenv("SWB200_PACKED");
+        ctx->packed = (envp && envp[0] == '1');
+    }
     if (cfg->T == SW_FLOAT32 && cfg->Tprog == SW_FLOAT32) {
         auto* e = new Engine<float, float>(); ctx->eng.reset(e); if ((rc = e->init(ctx))) return rc;
     } else if (cfg->T == SW_FLOAT64 && cfg->Tprog == SW_FLOAT64) {
@@ -559,6 +766,7 @@ int sw_set_state(sw_ctx* ctx, const void* u, const void* v, const void* eta, con
     if ((rc = copy_in(ctx, ctx->S[0].e, eta, shape_e(ctx->g)))) return rc;
     if ((rc = copy_in(ctx, ctx->sst[0], sst, shape_s(ctx->g)))) return rc;
     CK(cudaMemsetAsync(ctx->dst, 0, sizeof(DevStatus), ctx->stream));
+    CK(cudaMemsetAsync(ctx->sched, 0, sizeof(TileSched), ctx->stream));
     // ghost_points!(u,v,eta) opens every step (src/time_integration.jl:48); it is
     // idempotent after the first, so it is applied once here
     if ((rc = ctx->eng->ghost_state(ctx))) return rc;

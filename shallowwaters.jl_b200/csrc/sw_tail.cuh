@@ -7,223 +7,226 @@
 //   add_drag_diff_tendencies!  (src/diffusion.jl:221-251)
 //   ghost_points_uv!           (src/ghost_points.jl:202-216)
 // writing u, v out of place.  Intermediates follow the reference's arrays and
-// operation order; positions in T-cell/face coordinates:
-//   Lu(F,b) = ∇²u at u-points, Lv(a,G) at v-points           (src/gradients.jl:29-42)
-//   DSq(F,G) = (dudy + dvdx)² at corners; DT(a,b) = (dudx + dvdy)² at T-cells
-//   ν(a,b) = cSmag·sqrt(Ixy(DSq) + DT); νq = Ixy(ν) at corners (src/diffusion.jl:68-111)
+// operation order, at T-cell (a,b), u-point (F,b), v-point (a,G), corner (F,G):
+//   Lu(F,b) = ∇²u, Lv(a,G) = ∇²v                          (src/gradients.jl:29-42)
+//   DSq(F,G) = (dudy + dvdx)², DT(a,b) = (dudx + dvdy)²    (src/diffusion.jl:68-111)
+//   ν(a,b) = cSmag·sqrt(Ixy(DSq) + DT),  νq(F,G) = Ixy(ν)
 //   S11(a,b) = ν·∂xLu, S22(a,b) = ν·∂yLv, S12(F,G) = νq·∂yLu, S21(F,G) = νq·∂xLv
-//   LLu1 = ∂xS11, LLu2 = ∂yS12, LLv1 = ∂xS21, LLv2 = ∂yS22
-// Tile TX x TY with a 2-cell halo: device columns [x0, x0+TX+8), rows
-// [y0, y0+TY+4), local (lx, ly) = (x - x0 + 4, y - y0 + 2).
+//   LLu1 = ∂xS11, LLu2 = ∂yS12, LLv1 = ∂xS21, LLv2 = ∂yS22  (src/diffusion.jl:126-183)
+//   Bu = cD·Ix(sqrtKE)·u / Ix(h), Bv = cD·Iy(sqrtKE)·v / Iy(h) (src/bottom_drag.jl:20-76)
+// Execution as in sw_stage.cuh: one warp per 28-column strip, lanes 2..29
+// produce output, rows streamed bottom-up with a register window; iteration r
+// consumes input row r+2 and writes output row r.
 #pragma once
 #include "sw_common.cuh"
 #include "sw_ghost.cuh"
+#include "sw_stage.cuh"
 
 namespace swb {
 
 template <class T, class Tp>
 struct TailArgs {
     Geom g;
-    int ntx, nty;
+    int nsx, nsy, nring_blocks;
     const Tp* u0; const Tp* v0; const Tp* e0;   // X0 after ghost points
     Tp* uo; Tp* vo;                             // new u, v
     SField<T> H;
-    int drag;        // enum sw_bottom_drag
-    int smag;        // 1 Smagorinsky, 0 constant
     T cD, rD, cSmag, nuB;
     Tp Dt_diff;
     GhostRule<Tp> gr;
     DevStatus* st;
 };
 
-template <class T, class Tp, int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT)
+// untouched halo cells keep u0 (and so do their ghost copies)
+template <class T, class Tp>
+__device__ void tail_ring(const TailArgs<T, Tp>& A, int k0, int kstride) {
+    const Geom& g = A.g;
+    const int nu = Ring::u_count(g.ep, g.N, g.M), nv = Ring::v_count(g.N);
+    for (int k = k0; k < nu + nv; k += kstride) {
+        if (k < nu) {
+            int F, b;
+            Ring::u_at(k, g.ep, g.N, g.M, F, b);
+            Tp x = A.u0[g.idx(F, b)];
+            A.uo[g.idx(F, b)] = x;
+            A.gr.u(A.uo, g, F, b, x);
+        } else {
+            int a, G;
+            Ring::v_at(k - nu, g.N, g.M, a, G);
+            Tp x = A.v0[g.idx(a, G)];
+            A.vo[g.idx(a, G)] = x;
+            A.gr.v(A.vo, g, a, G, x);
+        }
+    }
+}
+
+// DRAG: enum sw_bottom_drag; SMAG: Smagorinsky (else constant νB)
+template <class T, class Tp, bool PER, int DRAG, bool SMAG, int TY>
+__global__ void __launch_bounds__(128)
 tail_kernel(TailArgs<T, Tp> A) {
     if (A.st->stop) return;
     const Geom& g = A.g;
-    const int ntiles = A.ntx * A.nty;
-
-    // untouched halo cells keep u0 (and so do their ghost copies)
-    if ((int)blockIdx.x >= ntiles) {
-        const int nu = Ring::u_count(g.ep, g.N, g.M), nv = Ring::v_count(g.N);
-        for (int k = ((int)blockIdx.x - ntiles) * NT + threadIdx.x; k < nu + nv;
-             k += ((int)gridDim.x - ntiles) * NT) {
-            if (k < nu) {
-                int F, b;
-                Ring::u_at(k, g.ep, g.N, g.M, F, b);
-                Tp x = A.u0[g.idx(F, b)];
-                A.uo[g.idx(F, b)] = x;
-                A.gr.u(A.uo, g, F, b, x);
-            } else {
-                int a, G;
-                Ring::v_at(k - nu, g.N, g.M, a, G);
-                Tp x = A.v0[g.idx(a, G)];
-                A.vo[g.idx(a, G)] = x;
-                A.gr.v(A.vo, g, a, G, x);
-            }
-        }
+    const int nstrips = A.nsx * A.nsy;
+    const int nstrip_blocks = (nstrips + 3) / 4;
+    if ((int)blockIdx.x >= nstrip_blocks) {
+        tail_ring(A, ((int)blockIdx.x - nstrip_blocks) * 128 + threadIdx.x, A.nring_blocks * 128);
         return;
     }
-
-    constexpr int SW = TX + 8, SH = TY + 4, SZ = SW * SH;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* su = reinterpret_cast<T*>(smem_raw);
-    T* sv = su + SZ;
-    T* sh = sv + SZ;       // h = eta0 + H
-    T* sLu = sh + SZ;
-    T* sLv = sLu + SZ;
-    T* sDSq = sLv + SZ;
-    T* sNu = sDSq + SZ;    // DT, then ν in place
-    T* sKE = sNu + SZ;     // sqrtKE
-    T* sS11 = sKE + SZ;
-    T* sS22 = sS11 + SZ;
-    T* sS12 = sS22 + SZ;
-    T* sS21 = sS12 + SZ;
-#define S_(arr, lx, ly) arr[(ly) * SW + (lx)]
-
-    const int x0 = ((int)blockIdx.x % A.ntx) * TX;
-    const int y0 = ((int)blockIdx.x / A.ntx) * TY;
-    const int tid = threadIdx.x;
+    const int w = (int)blockIdx.x * 4 + (int)(threadIdx.x >> 5);
+    if (w >= nstrips) return;
+    const int lane = threadIdx.x & 31;
+    const int sx = w % A.nsx, sy = w / A.nsx;
+    const int c = sx * STRIP + lane - 2;
+    const int y0 = sy * TY;
+    const int N = g.N, M = g.M, P = g.P;
+    const bool out_lane = lane >= 2 && lane < 2 + STRIP;
+    const bool col_u = out_lane && c >= (PER ? 0 : 1) && c < N;
+    const bool col_a = out_lane && c >= 0 && c < N;
+    const bool gx_u = PER && (c <= 1 || c >= N - 2);
+    const bool gx_v = c <= 1 || c >= N - 2;
+    constexpr bool QUAD = (DRAG == SW_DRAG_QUADRATIC);
     const T half = T(0.5), q4 = T(0.25);
+    const int cb = c + COL0;
+    auto ofs = [&](int y) { return (y + ROW0) * P + cb; };
 
-    for (int k = tid; k < SZ; k += NT) {
-        int ly = k / SW, lx = k - ly * SW;
-        int row = y0 + ly, col = x0 + lx;
-        T uu = T(0), vv = T(0), hh = T(0);
-        if (row < g.R && col < g.P) {
-            long gi = (long)row * g.P + col;
-            uu = cvt<T>(A.u0[gi]);
-            vv = cvt<T>(A.v0[gi]);
-            if (A.drag == SW_DRAG_QUADRATIC) hh = cvt<T>(A.e0[gi]) + A.H.at(col - COL0, row - ROW0);
-        }
-        su[k] = uu; sv[k] = vv; sh[k] = hh;
-    }
-    __syncthreads();
+    // window: index 0 = row r, 1 = r+1, 2 = r+2 (inputs); older rows kept explicitly
+    auto ldrow = [&](int y, T& uu, T& vv, T& hh) {
+        uu = cvt<T>(A.u0[ofs(y)]);
+        vv = cvt<T>(A.v0[ofs(y)]);
+        if (QUAD) hh = cvt<T>(A.e0[ofs(y)]) + A.H.at(c, y);
+        else hh = T(0);
+    };
+    int r = y0 - 3;
+    const int ra = max(r, -2), rb = max(r + 1, -2);
+    T u_r, v_r, h_r, u_r1, v_r1, h_r1;
+    ldrow(ra, u_r, v_r, h_r);
+    ldrow(rb, u_r1, v_r1, h_r1);
+    T ul_r1 = shup(u_r1), ur_r1 = shdn(u_r1), vl_r1 = shup(v_r1), vr_r1 = shdn(v_r1), hl_r1 = shup(h_r1);
+    T hl_r = shup(h_r);
+    T h_rm1 = T(0);
+    // derived windows
+    T DSq_r1 = T(0), DSqR_r1 = T(0);
+    T nu_r = T(0), nul_r = T(0);
+    T Lu_r = T(0), Lv_r = T(0);
+    T S11_r = T(0), S11l_r = T(0), S12_r = T(0), S21_r = T(0), S21r_r = T(0), S22_rm1 = T(0);
+    T sKE_rm1 = T(0), sKE_r = T(0), sKEl_r = T(0);
 
-    // Lu, Lv over lx in [3,TX+4], ly in [1,TY+2]; DT over the same T-cells;
-    // DSq over corners lx in [3,TX+5], ly in [1,TY+3]; sqrtKE over lx in [3,TX+3], ly in [1,TY+1]
-    {
-        constexpr int W1 = TX + 2, H1 = TY + 2;
-        for (int k = tid; k < W1 * H1; k += NT) {
-            int ly = 1 + k / W1, lx = 3 + k % W1;
-            T c = S_(su, lx, ly);
-            S_(sLu, lx, ly) = ((S_(su, lx - 1, ly) - c) + (S_(su, lx + 1, ly) - c)) +
-                              ((S_(su, lx, ly - 1) - c) + (S_(su, lx, ly + 1) - c));
-            c = S_(sv, lx, ly);
-            S_(sLv, lx, ly) = ((S_(sv, lx - 1, ly) - c) + (S_(sv, lx + 1, ly) - c)) +
-                              ((S_(sv, lx, ly - 1) - c) + (S_(sv, lx, ly + 1) - c));
-            if (A.smag) {
-                T dudx = S_(su, lx + 1, ly) - S_(su, lx, ly);      // ∂x!(dudx, u) at T-cell
-                T dvdy = S_(sv, lx, ly + 1) - S_(sv, lx, ly);      // ∂y!(dvdy, v) at T-cell
-                T s = dudx + dvdy;
-                S_(sNu, lx, ly) = s * s;                          // DT
-            }
-        }
-        if (A.smag) {
-            constexpr int W2 = TX + 3, H2 = TY + 3;
-            for (int k = tid; k < W2 * H2; k += NT) {
-                int ly = 1 + k / W2, lx = 3 + k % W2;
-                T dudy = S_(su, lx, ly) - S_(su, lx, ly - 1);
-                T dvdx = S_(sv, lx, ly) - S_(sv, lx - 1, ly);
-                T s = dudy + dvdx;
-                S_(sDSq, lx, ly) = s * s;                         // DS_q
-            }
-        }
-        if (A.drag == SW_DRAG_QUADRATIC) {
-            constexpr int W3 = TX + 1, H3 = TY + 1;
-            for (int k = tid; k < W3 * H3; k += NT) {
-                int ly = 1 + k / W3, lx = 3 + k % W3;
-                T uR = S_(su, lx + 1, ly), uL = S_(su, lx, ly);
-                T vT = S_(sv, lx, ly + 1), vB = S_(sv, lx, ly);
-                T KEu = half * (uR * uR + uL * uL);
-                T KEv = half * (vT * vT + vB * vB);
-                S_(sKE, lx, ly) = sqrt(KEu + KEv);                // src/bottom_drag.jl:46-50
-            }
-        }
-    }
-    __syncthreads();
+    // software pipeline: at iteration r, row r+2 is consumed while rows r+3
+    // and r+4 are in flight
+    T u_r2 = cvt<T>(A.u0[ofs(r + 2)]), v_r2 = cvt<T>(A.v0[ofs(r + 2)]);
+    T h_r2 = QUAD ? cvt<T>(A.e0[ofs(r + 2)]) + A.H.at(c, r + 2) : T(0);
+    Tp pu1 = A.u0[ofs(r + 3)], pv1 = A.v0[ofs(r + 3)], pe1 = QUAD ? A.e0[ofs(r + 3)] : Tp(0);
+    T pH1 = QUAD ? A.H.at(c, r + 3) : T(0);
+    Tp pu2 = A.u0[ofs(r + 4)], pv2 = A.v0[ofs(r + 4)], pe2 = QUAD ? A.e0[ofs(r + 4)] : Tp(0);
+    T pH2 = QUAD ? A.H.at(c, r + 4) : T(0);
 
-    // ν = cSmag·sqrt(DS + DT) with DS = Ixy(DS_q), over lx in [3,TX+4], ly in [1,TY+2]
-    if (A.smag) {
-        constexpr int W1 = TX + 2, H1 = TY + 2;
-        for (int k = tid; k < W1 * H1; k += NT) {
-            int ly = 1 + k / W1, lx = 3 + k % W1;
-            T DS = q4 * (S_(sDSq, lx, ly) + S_(sDSq, lx + 1, ly)) + q4 * (S_(sDSq, lx, ly + 1) + S_(sDSq, lx + 1, ly + 1));
-            S_(sNu, lx, ly) = A.cSmag * sqrt(DS + S_(sNu, lx, ly));
+SWB_ROW_UNROLL
+    for (; r < y0 + TY; r++) {
+        if (r > y0 - 3) {
+            u_r2 = cvt<T>(pu1); v_r2 = cvt<T>(pv1);
+            h_r2 = QUAD ? cvt<T>(pe1) + pH1 : T(0);
+            pu1 = pu2; pv1 = pv2; pe1 = pe2; pH1 = pH2;
+            const int o4 = ofs(r + 4);
+            pu2 = A.u0[o4]; pv2 = A.v0[o4];
+            if (QUAD) { pe2 = A.e0[o4]; pH2 = A.H.at(c, r + 4); }
         }
-        __syncthreads();
-    }
+        const T ul_r2 = shup(u_r2), ur_r2 = shdn(u_r2), vl_r2 = shup(v_r2), vr_r2 = shdn(v_r2);
+        const T hl_r2 = QUAD ? shup(h_r2) : T(0);
+        const bool out_row = r >= y0 && r < M;
+        Tp U0 = Tp(0), V0 = Tp(0);
+        if (std::is_same<T, Tp>::value) { U0 = cvt<Tp>(u_r); V0 = cvt<Tp>(v_r); }
+        else if (out_row && out_lane) { U0 = A.u0[ofs(r)]; V0 = A.v0[ofs(r)]; }
 
-    // S11(a,b): lx in [3,TX+3], ly in [2,TY+2);  S22(a,b): lx in [4,TX+4), ly in [1,TY+2)
-    // S12(F,G): lx in [4,TX+4), ly in [2,TY+2];  S21(F,G): lx in [4,TX+4], ly in [2,TY+2)
-    {
-        constexpr int W = TX + 1, Hh = TY + 1;
-        for (int k = tid; k < W * Hh; k += NT) {
-            int ly = 1 + k / W, lx = 3 + k % W;       // lx in [3,TX+3], ly in [1,TY+1]
-            // S11 at T-cell (lx, ly+1): ν(a,b)·(Lu(a+1,b) - Lu(a,b))
-            {
-                int l2 = ly + 1;
-                T d = S_(sLu, lx + 1, l2) - S_(sLu, lx, l2);
-                S_(sS11, lx, l2) = (A.smag ? S_(sNu, lx, l2) : A.nuB) * d;
-            }
-            // S22 at T-cell (lx+1, ly): ν(a,b)·(Lv(a,b+1) - Lv(a,b))
-            if (lx < TX + 3) {
-                int l1 = lx + 1;
-                T d = S_(sLv, l1, ly + 1) - S_(sLv, l1, ly);
-                S_(sS22, l1, ly) = (A.smag ? S_(sNu, l1, ly) : A.nuB) * d;
-            }
-            // corners (lx+1, ly+1): νq = Ixy(ν)
-            int cx = lx + 1, cy = ly + 1;
-            T nq = A.nuB;
-            if (A.smag)
-                nq = q4 * (S_(sNu, cx - 1, cy - 1) + S_(sNu, cx, cy - 1)) + q4 * (S_(sNu, cx - 1, cy) + S_(sNu, cx, cy));
-            if (cx < TX + 4) S_(sS12, cx, cy) = nq * (S_(sLu, cx, cy) - S_(sLu, cx, cy - 1));
-            if (cy < TY + 2) S_(sS21, cx, cy) = nq * (S_(sLv, cx, cy) - S_(sLv, cx - 1, cy));
+        // ∇² at row r+1 (∇²!: ((u[i,j+1]-c)+(u[i+2,j+1]-c)) + ((u[i+1,j]-c)+(u[i+1,j+2]-c)))
+        T Lu_r1, Lv_r1;
+        {
+            T cc = u_r1;
+            Lu_r1 = ((ul_r1 - cc) + (ur_r1 - cc)) + ((u_r - cc) + (u_r2 - cc));
+            cc = v_r1;
+            Lv_r1 = ((vl_r1 - cc) + (vr_r1 - cc)) + ((v_r - cc) + (v_r2 - cc));
         }
-    }
-    __syncthreads();
+        const T Lur_r1 = shdn(Lu_r1), Lvl_r1 = shup(Lv_r1);
 
-    for (int k = tid; k < TX * TY; k += NT) {
-        int ly = 2 + k / TX, lx = 4 + k % TX;
-        int x = x0 + lx - 4, y = y0 + ly - 2;
-        if (g.u_in(x, y)) {
-            T Bu;
-            if (A.drag == SW_DRAG_QUADRATIC) {
-                T ke = half * (S_(sKE, lx, ly) + S_(sKE, lx - 1, ly));      // sqrtKE_u = Ix!(sqrtKE)
-                T hu = half * (S_(sh, lx, ly) + S_(sh, lx - 1, ly));        // h_u = Ix!(h)
-                Bu = A.cD * ke * S_(su, lx, ly) / hu;                       // src/bottom_drag.jl:60-64
-            } else if (A.drag == SW_DRAG_LINEAR) {
-                Bu = A.rD * S_(su, lx, ly);
-            } else {
-                Bu = T(0);
-            }
-            T LLu1 = S_(sS11, lx, ly) - S_(sS11, lx - 1, ly);
-            T LLu2 = S_(sS12, lx, ly + 1) - S_(sS12, lx, ly);
-            long gi = g.idx(x, y);
-            Tp nu_ = A.u0[gi] + A.Dt_diff * (cvt<Tp>(Bu) + cvt<Tp>(LLu1) + cvt<Tp>(LLu2));
-            A.uo[gi] = nu_;
-            A.gr.u(A.uo, g, x, y, nu_);
+        // viscosity ν at T-row r+1 and νq at corner row r+1
+        T nu_r1, nuq_r1;
+        if (SMAG) {
+            T s = (u_r2 - u_r1) + (v_r2 - vl_r2);          // dudy + dvdx at corner (c, r+2)
+            const T DSq_r2 = s * s;
+            const T DSqR_r2 = shdn(DSq_r2);
+            const T DS = q4 * (DSq_r1 + DSqR_r1) + q4 * (DSq_r2 + DSqR_r2);
+            s = (ur_r1 - u_r1) + (v_r2 - v_r1);            // dudx + dvdy at T-cell (c, r+1)
+            const T DT = s * s;
+            nu_r1 = A.cSmag * sqrt(DS + DT);
+            const T nul_r1 = shup(nu_r1);
+            nuq_r1 = q4 * (nul_r + nu_r) + q4 * (nul_r1 + nu_r1);
+            DSq_r1 = DSq_r2; DSqR_r1 = DSqR_r2;
+            nul_r = nul_r1;
+        } else {
+            nu_r1 = A.nuB;
+            nuq_r1 = A.nuB;
         }
-        if (g.v_in(x, y)) {
-            T Bv;
-            if (A.drag == SW_DRAG_QUADRATIC) {
-                T ke = half * (S_(sKE, lx, ly) + S_(sKE, lx, ly - 1));      // sqrtKE_v = Iy!(sqrtKE)
-                T hv = half * (S_(sh, lx, ly) + S_(sh, lx, ly - 1));
-                Bv = A.cD * ke * S_(sv, lx, ly) / hv;                       // src/bottom_drag.jl:71-75
-            } else if (A.drag == SW_DRAG_LINEAR) {
-                Bv = A.rD * S_(sv, lx, ly);
-            } else {
-                Bv = T(0);
-            }
-            T LLv1 = S_(sS21, lx + 1, ly) - S_(sS21, lx, ly);
-            T LLv2 = S_(sS22, lx, ly) - S_(sS22, lx, ly - 1);
-            long gi = g.idx(x, y);
-            Tp nv_ = A.v0[gi] + A.Dt_diff * (cvt<Tp>(Bv) + cvt<Tp>(LLv1) + cvt<Tp>(LLv2));
-            A.vo[gi] = nv_;
-            A.gr.v(A.vo, g, x, y, nv_);
+        const T S11_r1 = nu_r1 * (Lur_r1 - Lu_r1);       // at T-cell (c, r+1)
+        const T S11l_r1 = shup(S11_r1);
+        const T S12_r1 = nuq_r1 * (Lu_r1 - Lu_r);         // at corner (c, r+1)
+        const T S21_r1 = nuq_r1 * (Lv_r1 - Lvl_r1);       // at corner (c, r+1)
+        const T S21r_r1 = shdn(S21_r1);
+        const T S22_r = nu_r * (Lv_r1 - Lv_r);            // at T-cell (c, r)
+
+        T sKE_r1 = T(0), sKEl_r1 = T(0);
+        if (QUAD) {
+            const T KEu = half * (ur_r1 * ur_r1 + u_r1 * u_r1);
+            const T KEv = half * (v_r2 * v_r2 + v_r1 * v_r1);
+            sKE_r1 = sqrt(KEu + KEv);
+            sKEl_r1 = shup(sKE_r1);
         }
+
+        if (out_row) {
+            if (col_u) {
+                T Bu;
+                if (QUAD) {
+                    T ke = half * (sKE_r + sKEl_r);
+                    T hu = half * (h_r + hl_r);
+                    Bu = A.cD * ke * u_r / hu;
+                } else if (DRAG == SW_DRAG_LINEAR) {
+                    Bu = A.rD * u_r;
+                } else {
+                    Bu = T(0);
+                }
+                const T LLu1 = S11_r - S11l_r;
+                const T LLu2 = S12_r1 - S12_r;
+                Tp val = U0 + A.Dt_diff * (cvt<Tp>(Bu) + cvt<Tp>(LLu1) + cvt<Tp>(LLu2));
+                A.uo[ofs(r)] = val;
+                if (gx_u || (!PER && (r <= 1 || r >= M - 2))) A.gr.u(A.uo, g, c, r, val);
+            }
+            if (col_a && r >= 1) {
+                T Bv;
+                if (QUAD) {
+                    T ke = half * (sKE_r + sKE_rm1);
+                    T hv = half * (h_r + h_rm1);
+                    Bv = A.cD * ke * v_r / hv;
+                } else if (DRAG == SW_DRAG_LINEAR) {
+                    Bv = A.rD * v_r;
+                } else {
+                    Bv = T(0);
+                }
+                const T LLv1 = S21r_r - S21_r;
+                const T LLv2 = S22_r - S22_rm1;
+                Tp val = V0 + A.Dt_diff * (cvt<Tp>(Bv) + cvt<Tp>(LLv1) + cvt<Tp>(LLv2));
+                A.vo[ofs(r)] = val;
+                if (gx_v) A.gr.v(A.vo, g, c, r, val);
+            }
+        }
+
+        // slide
+        h_rm1 = h_r;
+        u_r = u_r1; v_r = v_r1; h_r = h_r1; hl_r = hl_r1;
+        u_r1 = u_r2; v_r1 = v_r2; h_r1 = h_r2; hl_r1 = hl_r2;
+        ul_r1 = ul_r2; ur_r1 = ur_r2; vl_r1 = vl_r2; vr_r1 = vr_r2;
+        nu_r = nu_r1;
+        Lu_r = Lu_r1; Lv_r = Lv_r1;
+        S11_r = S11_r1; S11l_r = S11l_r1; S12_r = S12_r1; S21_r = S21_r1; S21r_r = S21r_r1;
+        S22_rm1 = S22_r;
+        sKE_rm1 = sKE_r; sKE_r = sKE_r1; sKEl_r = sKEl_r1;
     }
-#undef S_
 }
 
 }  // namespace swb

@@ -23,121 +23,121 @@ struct TracerArgs {
     Geom g;
     const Tp* u; const Tp* v;       // u0, v0 after the tail (converted to T on load)
     const T* um; const T* vm;       // mid-point velocities (T); may alias u, v (see um_is_u)
-    int um_is_u;                    // nadvstep == 1: um, vm are u, v of this step
     const Tp* sst; Tp* sst_o;
     T dtadvu, dtadvv, half_dtadvu, half_dtadvv;
-    int consumption;
     T jSST, SSTmin;
     GhostRule<Tp> gr;
     DevStatus* st;
 };
 
-struct Clip { long long k; };
-
+// Julia's Int(floor(x)); NaN, Inf and indices no array can take are flagged
 template <class T>
-__device__ inline long long jfloor(T x, int& bad) {
-    double d = (double)x;
-    if (!(fabs(d) < 9.2e18)) { bad = 1; return 0; }
-    return (long long)floor(d);
+__device__ __forceinline__ int ifloor(T x, int& bad) {
+    if (!(fabs(x) < T(1.0e9))) { bad = 1; return 0; }
+    return (int)floor(x);
 }
 
-// clip (src/tracer_advection.jl:211-223) and wrap (:227-240)
-template <class T>
-__device__ inline long long clip_idx(long long xyi, long long ij, T xy, long long mn, long long h1, T& x0) {
-    long long xyis = xyi + ij + h1;
-    if (xyis < 1 + h1) { x0 = T(0); return 1 + h1; }
-    if (xyis > mn - 1) { x0 = T(1); return mn - 1; }
-    x0 = xy - (T)(double)xyi;
-    return xyis;
-}
-template <class T>
-__device__ inline long long wrap_idx(long long xyi, long long ij, T xy, long long mn, long long h1, long long h2, T& x0) {
-    long long xyis = xyi + ij + h1;
-    x0 = xy - (T)(double)xyi;
-    if (xyis < 1 + h1) return xyis + mn - h1 - h2;
-    if (xyis > mn - 1) return xyis - mn + h1 + h2;
-    return xyis;
-}
 // bilin (src/tracer_advection.jl:243-246)
 template <class T>
-__device__ inline T bilin(T f00, T f10, T f01, T f11, T x, T y) {
+__device__ __forceinline__ T bilin(T f00, T f10, T f01, T f11, T x, T y) {
     const T one = T(1);
     return f00 * (one - x) * (one - y) + f10 * x * (one - y) + f01 * (one - x) * y + f11 * x * y;
 }
 
-template <class T, class Tp>
-__global__ void tracer_kernel(TracerArgs<T, Tp> A) {
+// Lower-left index and relative coordinate along one axis.  clip and wrap
+// (src/tracer_advection.jl:211-240) written for an offset k0 = xi + i (the
+// departure cell relative to the arrival cell i): the reference's index is
+// in range for k0 in [lo, hi]; clip pins to lo/hi with coordinate 0/1, wrap
+// shifts by n (one period) and keeps xy - xi.
+template <class T, bool WRAP>
+__device__ __forceinline__ int axis(int k0, int xi, T xy, int lo, int hi, int n, T& x0) {
+    if (WRAP) {
+        x0 = xy - (T)xi;
+        if (k0 < lo) return k0 + n;
+        if (k0 > hi) return k0 - n;
+        return k0;
+    } else {
+        if (k0 < lo) { x0 = T(0); return lo; }
+        if (k0 > hi) { x0 = T(1); return hi; }
+        x0 = xy - (T)xi;
+        return k0;
+    }
+}
+
+// 2-D launch: x over columns, y over rows (grid-stride in y)
+template <class T, class Tp, bool PER, bool UM_IS_U, bool CONS>
+__global__ void __launch_bounds__(128)
+tracer_kernel(TracerArgs<T, Tp> A) {
     if (A.st->stop) return;
     const Geom& g = A.g;
-    const int N = g.N, M = g.M, ep = g.ep;
-    const int nux = ep ? N : N - 1;
+    const int N = g.N, M = g.M;
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= N) return;
+    const T half = T(0.5);
     int bad = 0;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)N * M;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int a = (int)(t % N), b = (int)(t / N);
-        const long long i = a + 1, j = b + 1;            // Julia indices of xd[i,j]
-        const T half = T(0.5);
-        auto U = [&](int F, int bb) { return cvt<T>(A.u[g.idx(F, bb)]); };
-        auto V = [&](int aa, int G) { return cvt<T>(A.v[g.idx(aa, G)]); };
-        auto UM = [&](int F, int bb) { return A.um_is_u ? cvt<T>(A.u[g.idx(F, bb)]) : A.um[g.idx(F, bb)]; };
-        auto VM = [&](int aa, int G) { return A.um_is_u ? cvt<T>(A.v[g.idx(aa, G)]) : A.vm[g.idx(aa, G)]; };
-
-        // u_T = Ix!(u), v_T = Iy!(v) at the T-cell; backtraj! at half step (:75-76, :96-124)
-        T uT = half * (U(a + 1, b) + U(a, b));
-        T vT = half * (V(a, b + 1) + V(a, b));
+    const int P = g.P;
+    const bool gx = a == 0 || a == N - 1;
+    // element (x, y) of a field sits at (y + ROW0) * P + x + COL0
+    auto at = [&](int x, int y) { return (y + ROW0) * P + x + COL0; };
+    for (int b = blockIdx.y; b < M; b += gridDim.y) {
+        // departure!: u_T = Ix!(u), v_T = Iy!(v); backtraj! at half step (:75-76, :96-124)
+        const int o = at(a, b);
+        const T uT = half * (cvt<T>(A.u[o + 1]) + cvt<T>(A.u[o]));
+        const T vT = half * (cvt<T>(A.v[o + P]) + cvt<T>(A.v[o]));
         T xd = (-A.half_dtadvu) * uT;
         T yd = (-A.half_dtadvv) * vT;
-
-        // interp_uv!(uinterp, um_T, xd, yd): u case, muv = nux+3, nuv = M+4 (:130-176)
+        int xi = ifloor(xd, bad), yi = ifloor(yd, bad);
         T ui, vi;
-        {
-            long long xi = jfloor(xd, bad), yi = jfloor(yd, bad);
+        {   // interp_uv!(uinterp, um_T, ...): um_T at T-cell F0 is ½(um(F0+1) + um(F0)) (:130-176)
             T x0, y0;
-            long long muv = nux + 3, nuv = M + 4;
-            long long k = ep ? wrap_idx(xi, i, xd, muv, 1 + ep, 1, x0) : clip_idx(xi, i, xd, muv, 1 + ep, x0);
-            long long l = clip_idx(yi, j, yd, nuv, 2, y0);
-            if (k < 1 || k + 1 > muv || l < 1 || l + 1 > nuv) { bad = 1; k = min(max(k, 1LL), muv - 1); l = min(max(l, 1LL), nuv - 1); }
-            // um_T[k,l] = 0.5*(um[k+1,l] + um[k,l]), um[k,l] at (F = k-2-ep, b = l-3)
-            auto umT = [&](long long kk, long long ll) {
-                int F = (int)kk - 2 - ep, bb = (int)ll - 3;
-                return half * (UM(F + 1, bb) + UM(F, bb));
-            };
-            ui = bilin(umT(k, l), umT(k + 1, l), umT(k, l + 1), umT(k + 1, l + 1), x0, y0);
+            int F0 = axis<T, PER>(xi + a, xi, xd, 0, N - 1, N, x0);
+            const int b0 = axis<T, false>(yi + b, yi, yd, 0, M, 0, y0);
+            if (F0 < -2 || F0 > N - 1) { bad = 1; F0 = 0; }
+            const int k = at(F0, b0);
+            T m00, m10, m20, m01, m11, m21;
+            if (UM_IS_U) {
+                m00 = cvt<T>(A.u[k]); m10 = cvt<T>(A.u[k + 1]); m20 = cvt<T>(A.u[k + 2]);
+                m01 = cvt<T>(A.u[k + P]); m11 = cvt<T>(A.u[k + P + 1]); m21 = cvt<T>(A.u[k + P + 2]);
+            } else {
+                m00 = A.um[k]; m10 = A.um[k + 1]; m20 = A.um[k + 2];
+                m01 = A.um[k + P]; m11 = A.um[k + P + 1]; m21 = A.um[k + P + 2];
+            }
+            ui = bilin(half * (m10 + m00), half * (m20 + m10), half * (m11 + m01), half * (m21 + m11), x0, y0);
         }
-        {
-            long long xi = jfloor(xd, bad), yi = jfloor(yd, bad);
+        {   // interp_uv!(vinterp, vm_T, ...): vm_T at T-row G0 is ½(vm(G0+1) + vm(G0))
             T x0, y0;
-            long long muv = N + 4, nuv = M + 2;
-            long long k = ep ? wrap_idx(xi, i, xd, muv, 2, 2, x0) : clip_idx(xi, i, xd, muv, 2, x0);
-            long long l = clip_idx(yi, j, yd, nuv, 1, y0);
-            if (k < 1 || k + 1 > muv || l < 1 || l + 1 > nuv) { bad = 1; k = min(max(k, 1LL), muv - 1); l = min(max(l, 1LL), nuv - 1); }
-            // vm_T[k,l] = 0.5*(vm[k,l+1] + vm[k,l]), vm[k,l] at (a = k-3, G = l-2)
-            auto vmT = [&](long long kk, long long ll) {
-                int aa = (int)kk - 3, G = (int)ll - 2;
-                return half * (VM(aa, G + 1) + VM(aa, G));
-            };
-            vi = bilin(vmT(k, l), vmT(k + 1, l), vmT(k, l + 1), vmT(k + 1, l + 1), x0, y0);
+            int a0 = axis<T, PER>(xi + a, xi, xd, 0, N, N, x0);
+            const int G0 = axis<T, false>(yi + b, yi, yd, 0, M - 1, 0, y0);
+            if (a0 < -2 || a0 > N) { bad = 1; a0 = 0; }
+            const int k = at(a0, G0);
+            T m00, m01, m02, m10, m11, m12;
+            if (UM_IS_U) {
+                m00 = cvt<T>(A.v[k]); m01 = cvt<T>(A.v[k + P]); m02 = cvt<T>(A.v[k + 2 * P]);
+                m10 = cvt<T>(A.v[k + 1]); m11 = cvt<T>(A.v[k + P + 1]); m12 = cvt<T>(A.v[k + 2 * P + 1]);
+            } else {
+                m00 = A.vm[k]; m01 = A.vm[k + P]; m02 = A.vm[k + 2 * P];
+                m10 = A.vm[k + 1]; m11 = A.vm[k + P + 1]; m12 = A.vm[k + 2 * P + 1];
+            }
+            vi = bilin(half * (m01 + m00), half * (m11 + m10), half * (m02 + m01), half * (m12 + m11), x0, y0);
         }
         // backtraj! at full step (:83-84)
         xd = (-A.dtadvu) * ui;
         yd = (-A.dtadvv) * vi;
-
-        // adv_sst! (:179-206): m = N+2, n = M, halo 1 in x, 0 in y
+        xi = ifloor(xd, bad);
+        yi = ifloor(yd, bad);
         T s;
-        {
-            long long xi = jfloor(xd, bad), yi = jfloor(yd, bad);
+        {   // adv_sst! (:179-206)
             T x0, y0;
-            long long m = N + 2, n = M;
-            long long k = ep ? wrap_idx(xi, i, xd, m, 1, 1, x0) : clip_idx(xi, i, xd, m, 1, x0);
-            long long l = clip_idx(yi, j, yd, n, 0, y0);
-            if (k < 1 || k + 1 > m || l < 1 || l + 1 > n) { bad = 1; k = min(max(k, 1LL), m - 1); l = min(max(l, 1LL), n - 1); }
-            auto S = [&](long long kk, long long ll) { return cvt<T>(A.sst[g.idx((int)kk - 2, (int)ll - 1)]); };
-            s = bilin(S(k, l), S(k + 1, l), S(k, l + 1), S(k + 1, l + 1), x0, y0);
+            int a0 = axis<T, PER>(xi + a, xi, xd, 0, N - 1, N, x0);
+            const int b0 = axis<T, false>(yi + b, yi, yd, 0, M - 2, 0, y0);
+            if (a0 < -1 || a0 > N - 1) { bad = 1; a0 = 0; }
+            const int k = at(a0, b0);
+            s = bilin(cvt<T>(A.sst[k]), cvt<T>(A.sst[k + 1]), cvt<T>(A.sst[k + P]), cvt<T>(A.sst[k + P + 1]), x0, y0);
         }
-        if (A.consumption) s += A.jSST * (A.SSTmin - s);   // tracer_consumption! (:262-275)
-        Tp out = cvt<Tp>(s);
-        A.sst_o[g.idx(a, b)] = out;
-        A.gr.sst(A.sst_o, g, a, b, out);                   // ghost_points_sst! (:40)
+        if (CONS) s += A.jSST * (A.SSTmin - s);              // tracer_consumption! (:262-275)
+        const Tp out = cvt<Tp>(s);
+        A.sst_o[o] = out;
+        if (gx) A.gr.sst(A.sst_o, g, a, b, out);             // ghost_points_sst! (:40)
     }
     if (bad) {   // the reference throws here; halt the device-side loop
         atomicCAS(&A.st->error, 0, (int)SW_ERR_DEPARTURE);
