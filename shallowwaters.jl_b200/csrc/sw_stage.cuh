@@ -339,8 +339,184 @@ __host__ __device__ constexpr int stage_tma_smem() {
     return S * StageSlot<Tp, FIRST, LAST, K>::BYTES + 2 * S * 8 + S * 4;
 }
 
+// One tile (band x TY rows) of the consumer warps of rk_stage_tma.  EDGE is
+// false for warps none of whose output cells is near a boundary: then every
+// output lane writes, nothing is a ghost source and the row loop is unrolled.
+// Returns false if a wait timed out.
+template <class T, class Tp, bool PER, bool FIRST, bool LAST, int TY, int K, int S, bool EDGE>
+__device__ __forceinline__ bool stage_tile(const StageArgs<T, Tp>& A, const Tp* ring, uint64_t* full, uint64_t* empty,
+                                           uint32_t gbase, int cx0, int y0, int warp, int lane) {
+    using SL = StageSlot<Tp, FIRST, LAST, K>;
+    constexpr int NCH = (TY + 3 + K - 1) / K;
+    const Geom& g = A.g;
+    const int N = g.N, M = g.M;
+    const T half = T(0.5), o12 = T(1.0 / 12.0);
+    const int P = g.P;
+    const int sc_in = warp * STRIP + lane + 2;     // column inside the input box
+    const int sc_x = warp * STRIP + lane - 2;      // column inside the X/X0 box (output lanes)
+    const bool out_lane = lane >= 2 && lane < 2 + STRIP;
+    const int Hsy = A.H.sy, fqsy = A.fq.sy, Fxsy = A.Fx.sy, Fysy = A.Fy.sy;
+    const int c = cx0 + warp * STRIP + lane - 2;
+    const bool col_u = EDGE ? out_lane && c >= (PER ? 0 : 1) && c < N : out_lane;
+    const bool col_a = EDGE ? out_lane && c >= 0 && c < N : out_lane;
+    const bool gx_u = EDGE && PER && (c <= 1 || c >= N - 2);
+    const bool gx_v = EDGE && (c <= 1 || c >= N - 2);
+    const bool gx_e = EDGE && (c == 0 || c == N - 1);
+    const bool wrap = EDGE && PER && c == -1;
+    const bool qc_wrap = EDGE && PER && c == 0;
+    const int cb = c + COL0;
+
+    auto slot_ptr = [&](int j) { return ring + ((gbase + j) % S) * SL::ELEMS; };
+    auto wait_chunk = [&](int j) { return mbar_wait(&full[(gbase + j) % S], ((gbase + j) / S) & 1, A.st); };
+    auto release = [&](int j) {
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[(gbase + j) % S]);
+    };
+
+    // static fields: lane pointers at the row of first use, one row ahead in registers
+    int r = y0 - 2;
+    const T* __restrict__ pH = A.H.p + (r + 1 + ROW0) * Hsy + cb * A.H.sx;
+    const T* __restrict__ pfq = A.fq.p + (r + 1 + ROW0) * fqsy + cb * A.fq.sx;
+    const T* __restrict__ pFx = A.Fx.p + (r + ROW0) * Fxsy + cb * A.Fx.sx;
+    const T* __restrict__ pFy = A.Fy.p + (r + ROW0) * Fysy + cb * A.Fy.sx;
+    T nH = *pH, nfq = *pfq, nFx = *pFx, nFy = *pFy;
+
+    const Tp* pin = slot_ptr(0) + sc_in;        // input row 0 of the tile
+    T u_r = cvt<T>(pin[SL::U]), v_r = cvt<T>(pin[SL::V]), e_r = cvt<T>(pin[SL::E]);
+    Tp Xu_r = pin[SL::U], Xv_r = pin[SL::V], Xe_r = pin[SL::E];   // raw row r (X of the first stage)
+    T h_r = e_r + A.H.at(c, r);
+    T hl_r = shup(h_r), ur_r = shdn(u_r);
+    T U_r = u_r * (half * (h_r + hl_r));
+    T Ur_r = shdn(U_r);
+    T V_r = T(0), Vl_r = T(0), q_r = T(0), ql_r = T(0), qr_r = T(0);
+    T p_rm1 = T(0), qhu_part = T(0);
+    T uN_r = T(0), hN_r = T(0), hNm1_r = T(0);
+    if (wrap) {
+        uN_r = cvt<T>(A.u1[g.idx(N, r)]);
+        hN_r = cvt<T>(A.e1[g.idx(N, r)]) + A.H.at(N, r);
+        hNm1_r = cvt<T>(A.e1[g.idx(N - 1, r)]) + A.H.at(N - 1, r);
+    }
+    const Tp* px = slot_ptr(0) + sc_x;          // X/X0 row 0 of the tile
+    int nrel = 0;
+
+#pragma unroll
+    for (int i = 0; i < TY + 2; i++, r++) {
+        // next input row (index i+1): new slot at a chunk boundary
+        const int kin = i + 1;
+        if (kin % K == 0) {
+            if (!wait_chunk(kin / K)) return false;
+            pin = slot_ptr(kin / K) + sc_in;
+        } else {
+            pin += BOXW_IN;
+        }
+        const Tp rawu = pin[SL::U], rawv = pin[SL::V], rawe = pin[SL::E];
+        const T fq = nfq, H1 = nH, Fxr = nFx, Fyr = nFy;
+        pH += Hsy; pfq += fqsy; pFx += Fxsy; pFy += Fysy;
+        nH = *pH; nfq = *pfq; nFx = *pFx; nFy = *pFy;
+        // X/X0 row (index i)
+        if (i > 0) {
+            if (i % K == 0) px = slot_ptr(i / K) + sc_x;
+            else px += BOXW_X;
+        }
+
+        const T u_r1 = cvt<T>(rawu), v_r1 = cvt<T>(rawv), e_r1 = cvt<T>(rawe);
+        const T h_r1 = e_r1 + H1;                                 // thickness! (src/rhs.jl:131-139)
+        const T hl_r1 = shup(h_r1), vl_r1 = shup(v_r1), ur_r1 = shdn(u_r1);
+
+        T q_r1;
+        T uN_r1 = T(0), hN_r1 = T(0), hNm1_r1 = T(0);
+        if (wrap) {
+            uN_r1 = cvt<T>(A.u1[g.idx(N, r + 1)]);
+            hN_r1 = cvt<T>(A.e1[g.idx(N, r + 1)]) + A.H.at(N, r + 1);
+            hNm1_r1 = cvt<T>(A.e1[g.idx(N - 1, r + 1)]) + A.H.at(N - 1, r + 1);
+            const T vN = cvt<T>(A.v1[g.idx(N, r + 1)]), vNm1 = cvt<T>(A.v1[g.idx(N - 1, r + 1)]);
+            q_r1 = pv_q<T>(fq, vN, vNm1, uN_r1, uN_r, hNm1_r, hN_r, hNm1_r1, hN_r1);
+        } else {
+            q_r1 = pv_q<T>(fq, v_r1, vl_r1, u_r1, u_r, hl_r, h_r, hl_r1, h_r1);
+        }
+        const T ql_r1 = shup(q_r1), qr_r1 = shdn(q_r1);
+        const T U_r1 = u_r1 * (half * (h_r1 + hl_r1));
+        const T V_r1 = v_r1 * (half * (h_r1 + h_r));
+        const T Ur_r1 = shdn(U_r1), Vl_r1 = shup(V_r1);
+        const T KEu = half * (ur_r * ur_r + u_r * u_r);
+        const T KEv = half * (v_r1 * v_r1 + v_r * v_r);
+        const T p_r = half * (KEu + KEv) + A.g_ * e_r;
+        const T pl_r = shup(p_r);
+        const T s = q_r + q_r1;
+        const T qa = o12 * (s + qr_r1);
+        const T qb = o12 * (s + ql_r1);
+        const T qc = qc_wrap ? o12 * (s + ql_r) : o12 * (q_r + ql_r + q_r1);
+        const T qd = o12 * (s + qr_r);
+        const T qbr = shdn(qb), qcr = shdn(qc);
+
+        if (i >= 2 && (!EDGE || r < M)) {
+            const int o = (r + ROW0) * P + cb;
+            if (col_u) {
+                const T qhv = qa * V_r1 + qb * Vl_r1 + qc * Vl_r + qd * V_r;
+                const T dpdx = p_r - pl_r;
+                const Tp du = (cvt<Tp>(qhv) - cvt<Tp>(dpdx)) + cvt<Tp>(A.Fxt * Fxr);
+                const Tp X = FIRST ? Xu_r : (SL::LOAD_X ? px[SL::XU] : Tp(0));
+                const bool gs = EDGE && (gx_u || (!PER && (r <= 1 || r >= M - 2)));
+                if (!LAST) {
+                    const Tp x1 = X + A.b * du;
+                    A.u1o[o] = x1;
+                    if (gs) A.gr.u(A.u1o, g, c, r, x1);
+                }
+                const Tp x0 = (FIRST ? X : px[SL::AU]) + A.a * du;
+                A.u0o[o] = x0;
+                if (LAST && gs) A.gr.u(A.u0o, g, c, r, x0);
+            }
+            if (col_a) {
+                if (!EDGE || r >= 1) {
+                    const T qhu = qhu_part + qcr * Ur_r + qd * U_r;
+                    const T dpdy = p_r - p_rm1;
+                    const Tp dv = -(cvt<Tp>(qhu) + cvt<Tp>(dpdy)) + cvt<Tp>(A.Fyt * Fyr);
+                    const Tp X = FIRST ? Xv_r : (SL::LOAD_X ? px[SL::XV] : Tp(0));
+                    if (!LAST) {
+                        const Tp x1 = X + A.b * dv;
+                        A.v1o[o] = x1;
+                        if (gx_v) A.gr.v(A.v1o, g, c, r, x1);
+                    }
+                    const Tp x0 = (FIRST ? X : px[SL::AV]) + A.a * dv;
+                    A.v0o[o] = x0;
+                    if (LAST && gx_v) A.gr.v(A.v0o, g, c, r, x0);
+                }
+                const T dUdx = Ur_r - U_r;
+                const T dVdy = V_r1 - V_r;
+                const Tp de = -(cvt<Tp>(dUdx) + cvt<Tp>(dVdy));
+                const Tp X = FIRST ? Xe_r : (SL::LOAD_X ? px[SL::XW] : Tp(0));
+                const bool gs = EDGE && (gx_e || r == 0 || r == M - 1);
+                if (!LAST) {
+                    const Tp x1 = X + A.b * de;
+                    A.e1o[o] = x1;
+                    if (gs) A.gr.eta(A.e1o, g, c, r, x1);
+                }
+                const Tp x0 = (FIRST ? X : px[SL::AW]) + A.a * de;
+                A.e0o[o] = x0;
+                if (LAST && gs) A.gr.eta(A.e0o, g, c, r, x0);
+            }
+        }
+        // chunk i/K is done once its last X row (and so all its input rows) was used
+        if (i % K == K - 1) { release(i / K); nrel++; }
+
+        qhu_part = qa * U_r + qbr * Ur_r;
+        u_r = u_r1; v_r = v_r1; e_r = e_r1; h_r = h_r1; hl_r = hl_r1; ur_r = ur_r1;
+        q_r = q_r1; ql_r = ql_r1; qr_r = qr_r1;
+        U_r = U_r1; Ur_r = Ur_r1;
+        V_r = V_r1; Vl_r = Vl_r1;
+        p_rm1 = p_r;
+        uN_r = uN_r1; hN_r = hN_r1; hNm1_r = hNm1_r1;
+        Xu_r = rawu; Xv_r = rawv; Xe_r = rawe;
+    }
+    for (int j = nrel; j < NCH; j++) release(j);
+    return true;
+}
+
+#ifndef SWB_TMA_MINB
+#define SWB_TMA_MINB 6     // resident blocks per SM the register budget is sized for
+#endif
 template <class T, class Tp, bool PER, bool FIRST, bool LAST, int TY, int K, int S>
-__global__ void __launch_bounds__(160)
+__global__ void __launch_bounds__(160, SWB_TMA_MINB)
 rk_stage_tma(const __grid_constant__ StageArgs<T, Tp> A, const __grid_constant__ StageMaps MP, int npersist,
              TileSched* sched) {
     using SL = StageSlot<Tp, FIRST, LAST, K>;
@@ -432,171 +608,19 @@ rk_stage_tma(const __grid_constant__ StageArgs<T, Tp> A, const __grid_constant__
     }
 
     // -------------------------------------------------------------- consumers
-    const T half = T(0.5), o12 = T(1.0 / 12.0);
-    const int P = g.P;
-    const int sc_in = warp * STRIP + lane + 2;     // column inside the input box
-    const int sc_x = warp * STRIP + lane - 2;      // column inside the X/X0 box (output lanes)
-    const bool out_lane = lane >= 2 && lane < 2 + STRIP;
-    const int Hsy = A.H.sy, fqsy = A.fq.sy, Fxsy = A.Fx.sy, Fysy = A.Fy.sy;
-    uint32_t gbase = 0;                            // global chunk counter at the tile start
-
-    for (;; gbase += NCH) {
+    for (uint32_t gbase = 0;; gbase += NCH) {
         if (!mbar_wait(&full[gbase % S], (gbase / S) & 1, A.st)) return;
         const int t = slot_tile[gbase % S];
         if (t < 0) return;
         const int cx0 = (t % nbx) * BAND, y0 = (t / nbx) * TY;
-        const int c = cx0 + warp * STRIP + lane - 2;
-        const bool col_u = out_lane && c >= (PER ? 0 : 1) && c < N;
-        const bool col_a = out_lane && c >= 0 && c < N;
-        const bool gx_u = PER && (c <= 1 || c >= N - 2);
-        const bool gx_v = c <= 1 || c >= N - 2;
-        const bool gx_e = c == 0 || c == N - 1;
-        const bool wrap = PER && c == -1;
-        const bool qc_wrap = PER && c == 0;
-        const int cb = c + COL0;
-
-        auto slot_ptr = [&](int j) { return ring + ((gbase + j) % S) * SL::ELEMS; };
-        auto wait_chunk = [&](int j) { return mbar_wait(&full[(gbase + j) % S], ((gbase + j) / S) & 1, A.st); };
-        auto release = [&](int j) {
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&empty[(gbase + j) % S]);
-        };
-
-        // static fields: lane pointers at the row of first use, one row ahead in registers
-        int r = y0 - 2;
-        const T* __restrict__ pH = A.H.p + (r + 1 + ROW0) * Hsy + cb * A.H.sx;
-        const T* __restrict__ pfq = A.fq.p + (r + 1 + ROW0) * fqsy + cb * A.fq.sx;
-        const T* __restrict__ pFx = A.Fx.p + (r + ROW0) * Fxsy + cb * A.Fx.sx;
-        const T* __restrict__ pFy = A.Fy.p + (r + ROW0) * Fysy + cb * A.Fy.sx;
-        T nH = *pH, nfq = *pfq, nFx = *pFx, nFy = *pFy;
-
-        const Tp* pin = slot_ptr(0) + sc_in;        // input row 0 of the tile
-        T u_r = cvt<T>(pin[SL::U]), v_r = cvt<T>(pin[SL::V]), e_r = cvt<T>(pin[SL::E]);
-        Tp Xu_r = pin[SL::U], Xv_r = pin[SL::V], Xe_r = pin[SL::E];   // raw row r (X of the first stage)
-        T h_r = e_r + A.H.at(c, r);
-        T hl_r = shup(h_r), ur_r = shdn(u_r);
-        T U_r = u_r * (half * (h_r + hl_r));
-        T Ur_r = shdn(U_r);
-        T V_r = T(0), Vl_r = T(0), q_r = T(0), ql_r = T(0), qr_r = T(0);
-        T p_rm1 = T(0), qhu_part = T(0);
-        T uN_r = T(0), hN_r = T(0), hNm1_r = T(0);
-        if (wrap) {
-            uN_r = cvt<T>(A.u1[g.idx(N, r)]);
-            hN_r = cvt<T>(A.e1[g.idx(N, r)]) + A.H.at(N, r);
-            hNm1_r = cvt<T>(A.e1[g.idx(N - 1, r)]) + A.H.at(N - 1, r);
-        }
-        const Tp* px = slot_ptr(0) + sc_x;          // X/X0 row 0 of the tile
-        int nrel = 0;
-
-        for (int i = 0; i < TY + 2; i++, r++) {
-            // next input row (index i+1): new slot at a chunk boundary
-            const int kin = i + 1;
-            if (kin % K == 0) {
-                if (!wait_chunk(kin / K)) return;
-                pin = slot_ptr(kin / K) + sc_in;
-            } else {
-                pin += BOXW_IN;
-            }
-            const Tp rawu = pin[SL::U], rawv = pin[SL::V], rawe = pin[SL::E];
-            const T fq = nfq, H1 = nH, Fxr = nFx, Fyr = nFy;
-            pH += Hsy; pfq += fqsy; pFx += Fxsy; pFy += Fysy;
-            nH = *pH; nfq = *pfq; nFx = *pFx; nFy = *pFy;
-            // X/X0 row (index i)
-            if (i > 0) {
-                if (i % K == 0) px = slot_ptr(i / K) + sc_x;
-                else px += BOXW_X;
-            }
-
-            const T u_r1 = cvt<T>(rawu), v_r1 = cvt<T>(rawv), e_r1 = cvt<T>(rawe);
-            const T h_r1 = e_r1 + H1;                                 // thickness! (src/rhs.jl:131-139)
-            const T hl_r1 = shup(h_r1), vl_r1 = shup(v_r1), ur_r1 = shdn(u_r1);
-
-            T q_r1;
-            T uN_r1 = T(0), hN_r1 = T(0), hNm1_r1 = T(0);
-            if (wrap) {
-                uN_r1 = cvt<T>(A.u1[g.idx(N, r + 1)]);
-                hN_r1 = cvt<T>(A.e1[g.idx(N, r + 1)]) + A.H.at(N, r + 1);
-                hNm1_r1 = cvt<T>(A.e1[g.idx(N - 1, r + 1)]) + A.H.at(N - 1, r + 1);
-                const T vN = cvt<T>(A.v1[g.idx(N, r + 1)]), vNm1 = cvt<T>(A.v1[g.idx(N - 1, r + 1)]);
-                q_r1 = pv_q<T>(fq, vN, vNm1, uN_r1, uN_r, hNm1_r, hN_r, hNm1_r1, hN_r1);
-            } else {
-                q_r1 = pv_q<T>(fq, v_r1, vl_r1, u_r1, u_r, hl_r, h_r, hl_r1, h_r1);
-            }
-            const T ql_r1 = shup(q_r1), qr_r1 = shdn(q_r1);
-            const T U_r1 = u_r1 * (half * (h_r1 + hl_r1));
-            const T V_r1 = v_r1 * (half * (h_r1 + h_r));
-            const T Ur_r1 = shdn(U_r1), Vl_r1 = shup(V_r1);
-            const T KEu = half * (ur_r * ur_r + u_r * u_r);
-            const T KEv = half * (v_r1 * v_r1 + v_r * v_r);
-            const T p_r = half * (KEu + KEv) + A.g_ * e_r;
-            const T pl_r = shup(p_r);
-            const T s = q_r + q_r1;
-            const T qa = o12 * (s + qr_r1);
-            const T qb = o12 * (s + ql_r1);
-            const T qc = qc_wrap ? o12 * (s + ql_r) : o12 * (q_r + ql_r + q_r1);
-            const T qd = o12 * (s + qr_r);
-            const T qbr = shdn(qb), qcr = shdn(qc);
-
-            if (i >= 2 && r < M) {
-                const int o = (r + ROW0) * P + cb;
-                if (col_u) {
-                    const T qhv = qa * V_r1 + qb * Vl_r1 + qc * Vl_r + qd * V_r;
-                    const T dpdx = p_r - pl_r;
-                    const Tp du = (cvt<Tp>(qhv) - cvt<Tp>(dpdx)) + cvt<Tp>(A.Fxt * Fxr);
-                    const Tp X = FIRST ? Xu_r : (SL::LOAD_X ? px[SL::XU] : Tp(0));
-                    const bool gs = gx_u || (!PER && (r <= 1 || r >= M - 2));
-                    if (!LAST) {
-                        const Tp x1 = X + A.b * du;
-                        A.u1o[o] = x1;
-                        if (gs) A.gr.u(A.u1o, g, c, r, x1);
-                    }
-                    const Tp x0 = (FIRST ? X : px[SL::AU]) + A.a * du;
-                    A.u0o[o] = x0;
-                    if (LAST && gs) A.gr.u(A.u0o, g, c, r, x0);
-                }
-                if (col_a) {
-                    if (r >= 1) {
-                        const T qhu = qhu_part + qcr * Ur_r + qd * U_r;
-                        const T dpdy = p_r - p_rm1;
-                        const Tp dv = -(cvt<Tp>(qhu) + cvt<Tp>(dpdy)) + cvt<Tp>(A.Fyt * Fyr);
-                        const Tp X = FIRST ? Xv_r : (SL::LOAD_X ? px[SL::XV] : Tp(0));
-                        if (!LAST) {
-                            const Tp x1 = X + A.b * dv;
-                            A.v1o[o] = x1;
-                            if (gx_v) A.gr.v(A.v1o, g, c, r, x1);
-                        }
-                        const Tp x0 = (FIRST ? X : px[SL::AV]) + A.a * dv;
-                        A.v0o[o] = x0;
-                        if (LAST && gx_v) A.gr.v(A.v0o, g, c, r, x0);
-                    }
-                    const T dUdx = Ur_r - U_r;
-                    const T dVdy = V_r1 - V_r;
-                    const Tp de = -(cvt<Tp>(dUdx) + cvt<Tp>(dVdy));
-                    const Tp X = FIRST ? Xe_r : (SL::LOAD_X ? px[SL::XW] : Tp(0));
-                    const bool gs = gx_e || r == 0 || r == M - 1;
-                    if (!LAST) {
-                        const Tp x1 = X + A.b * de;
-                        A.e1o[o] = x1;
-                        if (gs) A.gr.eta(A.e1o, g, c, r, x1);
-                    }
-                    const Tp x0 = (FIRST ? X : px[SL::AW]) + A.a * de;
-                    A.e0o[o] = x0;
-                    if (LAST && gs) A.gr.eta(A.e0o, g, c, r, x0);
-                }
-            }
-            // chunk i/K is done once its last X row (and so all its input rows) was used
-            if (i % K == K - 1) { release(i / K); nrel++; }
-
-            qhu_part = qa * U_r + qbr * Ur_r;
-            u_r = u_r1; v_r = v_r1; e_r = e_r1; h_r = h_r1; hl_r = hl_r1; ur_r = ur_r1;
-            q_r = q_r1; ql_r = ql_r1; qr_r = qr_r1;
-            U_r = U_r1; Ur_r = Ur_r1;
-            V_r = V_r1; Vl_r = Vl_r1;
-            p_rm1 = p_r;
-            uN_r = uN_r1; hN_r = hN_r1; hNm1_r = hNm1_r1;
-            Xu_r = rawu; Xv_r = rawv; Xe_r = rawe;
-        }
-        for (int j = nrel; j < NCH; j++) release(j);
+        // Warp-uniform: does any output cell of this warp need edge handling
+        // (ghost sources, the periodic q wrap, columns beyond N, rows near the
+        // y boundaries)?  Interior warps run without any of those tests.
+        const int cw = cx0 + warp * STRIP;               // column of output lane 2
+        const bool edge = cw <= 1 || cw + STRIP - 1 >= N - 2 || y0 <= 1 || y0 + TY - 1 >= M - 2;
+        const bool ok = edge ? stage_tile<T, Tp, PER, FIRST, LAST, TY, K, S, true>(A, ring, full, empty, gbase, cx0, y0, warp, lane)
+                             : stage_tile<T, Tp, PER, FIRST, LAST, TY, K, S, false>(A, ring, full, empty, gbase, cx0, y0, warp, lane);
+        if (!ok) return;
     }
 }
 
