@@ -203,6 +203,12 @@ int sw_diagnostics(sw_ctx* ctx, sw_diag* out);
  * of that size is written between steps (outside the timed intervals). */
 int sw_run_profiled(sw_ctx* ctx, int64_t nsteps, int64_t l2_flush_bytes,
                     sw_profile* prof, sw_status* status);
+/* sw_run with one CUDA-event interval per time step; when l2_flush_bytes > 0
+ * a buffer of that size is written between steps (outside the intervals).
+ * *step_ms_total is the sum of the intervals.  Steps run as on sw_run (from
+ * CUDA graphs where possible).  No reference counterpart (measurement). */
+int sw_run_timed(sw_ctx* ctx, int64_t nsteps, int64_t l2_flush_bytes,
+                 double* step_ms_total, sw_status* status);
 /* Number of CUDA kernel launches the library has issued on this context. */
 int64_t sw_kernel_launches(const sw_ctx* ctx);
 void sw_destroy(sw_ctx* ctx);

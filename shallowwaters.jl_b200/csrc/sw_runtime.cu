@@ -73,7 +73,8 @@ struct Fields3 { void* u = nullptr; void* v = nullptr; void* e = nullptr; };
 struct sw_ctx;
 struct EngineBase {
     virtual ~EngineBase() = default;
-    virtual int step(sw_ctx* ctx, long long i) = 0;
+    virtual int step(sw_ctx* ctx, long long i) = 0;          // one time step, without the NaN check
+    virtual int nan_check(sw_ctx* ctx, long long i) = 0;     // the check of step i (state before it)
     virtual int ghost_state(sw_ctx* ctx) = 0;
 };
 
@@ -97,6 +98,11 @@ struct sw_ctx {
     std::map<const void*, Maps> tmaps;
     bool use_tma = false;
     bool packed = false;          // FP32x2 stage kernel for Float32 (opt-in: SWB200_PACKED=1)
+    // CUDA graphs of one time step, keyed by the buffer parities and the
+    // sub-steps that are due (see step_key); off with SWB200_GRAPHS=0
+    bool use_graphs = true;
+    struct StepGraph { cudaGraphExec_t exec = nullptr; long long launches = 0; bool flips_sp = false; };
+    std::map<unsigned, StepGraph> graphs;
     int nsm = 148;
     DevStatus* dst = nullptr;     // device status
     DevStatus* hst = nullptr;     // pinned host mirror
@@ -504,15 +510,18 @@ struct Engine : EngineBase {
             }
         }
 
-        // ------------------------------------------- NaN check (:232-237)
-        if ((i % c.nout) == 0) {
-            int rc = launch(ctx, 4, [&] {
-                nan_check_kernel<Tp><<<148, 256, 0, ctx->stream>>>(g, (const Tp*)X.u, (const Tp*)X.v, (const Tp*)X.e,
-                                                                  (const Tp*)ctx->sst[ctx->sp], i, ctx->dst);
-            });
-            if (rc) return rc;
-        }
         return SW_OK;
+    }
+
+    // NaN check of step i (src/time_integration.jl:232-237): u, v, eta before
+    // the step (still S[p]) and sst after it
+    int nan_check(sw_ctx* ctx, long long i) override {
+        const Geom& g = ctx->g;
+        const Fields3& X = ctx->S[ctx->p];
+        return launch(ctx, 4, [&] {
+            nan_check_kernel<Tp><<<148, 256, 0, ctx->stream>>>(g, (const Tp*)X.u, (const Tp*)X.v, (const Tp*)X.e,
+                                                              (const Tp*)ctx->sst[ctx->sp], i, ctx->dst);
+        });
     }
 };
 
@@ -599,17 +608,66 @@ int copy_out(sw_ctx* ctx, void* host, const void* dev, HostShape s) {
     return SW_OK;
 }
 
+// What a step launches, beyond the fixed buffers: the state and tracer
+// parities and which sub-steps are due.  Steps with equal keys launch the same
+// kernels with the same arguments (the seasonal wind factors excepted, which
+// is why those runs are not graphed).
+unsigned step_key(const sw_ctx* ctx, long long i) {
+    const sw_config& c = ctx->cfg;
+    const bool tail_now = (i % c.nstep_diff) == 0;
+    const bool tracer_now = c.tracer_advection && (i % c.nadvstep) == 0;
+    const bool copy_now = c.tracer_advection && c.nadvstep > 1 && ((i + c.nadvstep_half) % c.nadvstep) == 0;
+    return (unsigned)ctx->p | (unsigned)ctx->sp << 1 | (unsigned)tail_now << 2 | (unsigned)tracer_now << 3 |
+           (unsigned)copy_now << 4;
+}
+
+// One time step: replayed from a CUDA graph when possible, captured on first use.
+int do_step(sw_ctx* ctx, long long i) {
+    const sw_config& c = ctx->cfg;
+    if (!ctx->use_graphs || ctx->prof || c.seasonal_wind_x || c.seasonal_wind_y) return ctx->eng->step(ctx, i);
+    const unsigned key = step_key(ctx, i);
+    auto it = ctx->graphs.find(key);
+    if (it == ctx->graphs.end()) {
+        const long long t0 = ctx->t, l0 = ctx->launches;
+        const int sp0 = ctx->sp;
+        CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = ctx->eng->step(ctx, i);
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+        sw_ctx::StepGraph sg;
+        sg.launches = ctx->launches - l0;
+        sg.flips_sp = ctx->sp != sp0;
+        ctx->t = t0; ctx->launches = l0; ctx->sp = sp0;
+        if (!rc && e == cudaSuccess) e = cudaGraphInstantiate(&sg.exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        if (rc) return rc;
+        if (e != cudaSuccess) {
+            // capture is an optimisation: run this context without graphs
+            (void)cudaGetLastError();
+            ctx->use_graphs = false;
+            return ctx->eng->step(ctx, i);
+        }
+        it = ctx->graphs.emplace(key, sg).first;
+    }
+    CK(cudaGraphLaunch(it->second.exec, ctx->stream));
+    ctx->launches += it->second.launches;
+    ctx->t += c.dtint;
+    if (it->second.flips_sp) ctx->sp = 1 - ctx->sp;
+    return SW_OK;
+}
+
 int run_steps(sw_ctx* ctx, long long nsteps, sw_status* status) {
     const sw_config& c = ctx->cfg;
     long long done = 0;
     int code = SW_OK;
     for (long long s = 0; s < nsteps; s++) {
         long long i = ctx->step + 1;
-        int rc = ctx->eng->step(ctx, i);
+        int rc = do_step(ctx, i);
         if (rc) return rc;
         done++;
         bool check = (i % c.nout) == 0;
         if (check) {
+            if ((rc = ctx->eng->nan_check(ctx, i))) return rc;
             CK(cudaMemcpyAsync(ctx->hst, ctx->dst, sizeof(DevStatus), cudaMemcpyDeviceToHost, ctx->stream));
             CK(cudaStreamSynchronize(ctx->stream));
             if (ctx->hst->error) {
@@ -659,6 +717,7 @@ int64_t sw_kernel_launches(const sw_ctx* ctx) { return ctx ? ctx->launches : 0; 
 void sw_destroy(sw_ctx* ctx) {
     if (!ctx) return;
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second.exec);
     for (void* p : ctx->allocs) cudaFree(p);
     if (ctx->hst) cudaFreeHost(ctx->hst);
     for (auto e : ctx->evpool) cudaEventDestroy(e);
@@ -742,6 +801,8 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
                 ctx->tmaps[p] = mp;
             }
         ctx->use_tma = ok;
+        const char* envg = getenv("SWB200_GRAPHS");
+        ctx->use_graphs = !(envg && envg[0] == '0');
         const char* envp = getenv("SWB200_PACKED");
         ctx->packed = (envp && envp[0] == '1');
     }
@@ -791,17 +852,17 @@ int sw_run(sw_ctx* ctx, int64_t nsteps, sw_status* status) {
     return run_steps(ctx, nsteps, status);
 }
 
-int sw_run_profiled(sw_ctx* ctx, int64_t nsteps, int64_t l2_flush_bytes, sw_profile* prof, sw_status* status) {
-    if (!ctx || !prof || nsteps < 0) return SW_ERR_ARG;
-    std::memset(prof, 0, sizeof(*prof));
+// Per-step CUDA-event intervals around run_steps(ctx, 1), with an optional L2
+// flush between steps outside the intervals.  Shared by the two timed runs.
+static int run_timed_steps(sw_ctx* ctx, int64_t nsteps, int64_t l2_flush_bytes, double* step_ms_total,
+                           long long* done_out) {
     if (l2_flush_bytes > 0 && (size_t)l2_flush_bytes > ctx->flush_bytes) {
         if (ctx->flush) cudaFree(ctx->flush);
+        ctx->flush = nullptr;
+        ctx->flush_bytes = 0;
         CK(cudaMalloc(&ctx->flush, (size_t)l2_flush_bytes));
         ctx->flush_bytes = (size_t)l2_flush_bytes;
     }
-    ctx->prof = true;
-    ctx->marks.clear();
-    ctx->evnext = 0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> steps;
     int code = SW_OK;
     long long done = 0;
@@ -816,13 +877,40 @@ int sw_run_profiled(sw_ctx* ctx, int64_t nsteps, int64_t l2_flush_bytes, sw_prof
         done += st1.steps_done;
         if (code) break;
     }
-    ctx->prof = false;
     CK(cudaStreamSynchronize(ctx->stream));
+    *step_ms_total = 0;
     for (auto& pr : steps) {
         float ms = 0;
         cudaEventElapsedTime(&ms, pr.first, pr.second);
-        prof->step_ms_total += ms;
+        *step_ms_total += ms;
     }
+    *done_out = done;
+    return code;
+}
+
+int sw_run_timed(sw_ctx* ctx, int64_t nsteps, int64_t l2_flush_bytes, double* step_ms_total, sw_status* status) {
+    if (!ctx || !step_ms_total || nsteps < 0) return SW_ERR_ARG;
+    ctx->evnext = 0;
+    long long done = 0;
+    const int code = run_timed_steps(ctx, nsteps, l2_flush_bytes, step_ms_total, &done);
+    if (status) {
+        status->steps_done = done;
+        status->step = ctx->step;
+        status->code = code;
+        status->nan_step = code == SW_NAN_DETECTED ? ctx->step : -1;
+    }
+    return code;
+}
+
+int sw_run_profiled(sw_ctx* ctx, int64_t nsteps, int64_t l2_flush_bytes, sw_profile* prof, sw_status* status) {
+    if (!ctx || !prof || nsteps < 0) return SW_ERR_ARG;
+    std::memset(prof, 0, sizeof(*prof));
+    ctx->prof = true;
+    ctx->marks.clear();
+    ctx->evnext = 0;
+    long long done = 0;
+    const int code = run_timed_steps(ctx, nsteps, l2_flush_bytes, &prof->step_ms_total, &done);
+    ctx->prof = false;
     for (auto& m : ctx->marks) {
         float ms = 0;
         cudaEventElapsedTime(&ms, m.a, m.b);

@@ -71,6 +71,14 @@ class Model:
             abi.check(self.lib, rc, self.ctx)
         return prof, st
 
+    def run_timed(self, nsteps: int, l2_flush_bytes: int = 0):
+        """Run nsteps steps as sw_run does; returns (sum of per-step device ms, status)."""
+        ms, st = C.c_double(0.0), abi.SwStatus()
+        rc = self.lib.sw_run_timed(self.ctx, int(nsteps), int(l2_flush_bytes), C.byref(ms), C.byref(st))
+        if rc not in (abi.SW_OK, abi.SW_NAN_DETECTED):
+            abi.check(self.lib, rc, self.ctx)
+        return ms.value, st
+
     def diagnostics(self) -> abi.SwDiag:
         d = abi.SwDiag()
         abi.check(self.lib, self.lib.sw_diagnostics(self.ctx, C.byref(d)), self.ctx)

@@ -144,3 +144,23 @@ def test_kernel_launch_count():
     m.run(10)
     # 4 stages + tail + tracer per step, plus NaN checks every nout steps
     assert m.kernel_launches - n0 >= 60
+
+
+def test_graph_replay_equals_direct_launches(monkeypatch):
+    """Steps replayed from CUDA graphs equal steps launched one kernel at a
+    time, over enough steps to use every graph key (parities, tracer and
+    diffusion sub-steps)."""
+    P = Parameter(nx=40, Ndays=0.5, Uadv=2.0, nstep_diff=3, diffusion="Smagorinsky")
+    S = model_setup(P)
+    Prog = initial_conditions(P.Tprog, S, **seeded_inputs(S, 5))
+    out = []
+    for graphs in ("1", "0"):
+        monkeypatch.setenv("SWB200_GRAPHS", graphs)
+        m = Model(S)
+        m.set_state(Prog)
+        st = m.run(37)
+        assert st.code == 0
+        out.append(m.get_state())
+        m.close()
+    for x, y, name in zip(out[0], out[1], ("u", "v", "η", "sst")):
+        assert_bitwise(x, y, name)
