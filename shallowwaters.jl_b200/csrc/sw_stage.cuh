@@ -339,6 +339,13 @@ __host__ __device__ constexpr int stage_tma_smem() {
     return S * StageSlot<Tp, FIRST, LAST, K>::BYTES + 2 * S * 8 + S * 4;
 }
 
+#ifndef SWB_TMA_UNROLL
+#define SWB_TMA_UNROLL 2        // row-loop unroll of interior warps (code size vs. scheduling)
+#endif
+#ifndef SWB_TMA_UNROLL_EDGE
+#define SWB_TMA_UNROLL_EDGE 1   // edge warps are few: keep their code small
+#endif
+constexpr int TMA_UNROLL = SWB_TMA_UNROLL, TMA_UNROLL_EDGE = SWB_TMA_UNROLL_EDGE;
 // One tile (band x TY rows) of the consumer warps of rk_stage_tma.  EDGE is
 // false for warps none of whose output cells is near a boundary: then every
 // output lane writes, nothing is a ghost source and the row loop is unrolled.
@@ -399,7 +406,7 @@ __device__ __forceinline__ bool stage_tile(const StageArgs<T, Tp>& A, const Tp* 
     const Tp* px = slot_ptr(0) + sc_x;          // X/X0 row 0 of the tile
     int nrel = 0;
 
-#pragma unroll
+#pragma unroll (EDGE ? TMA_UNROLL_EDGE : TMA_UNROLL)
     for (int i = 0; i < TY + 2; i++, r++) {
         // next input row (index i+1): new slot at a chunk boundary
         const int kin = i + 1;
