@@ -31,6 +31,7 @@
 #include "sw_ghost.cuh"
 #include "sw_stage.cuh"
 #include "sw_stage2.cuh"
+#include "sw_ssp.cuh"
 #include "sw_tail.cuh"
 #include "sw_tracer.cuh"
 
@@ -87,6 +88,7 @@ struct sw_ctx {
     int device = 0;
     std::vector<void*> allocs;
     Fields3 S[2], A, B, Acc;
+    Fields3 C;                 // third stage buffer of the SSP schemes
     void* sst[2] = {nullptr, nullptr};
     void* um = nullptr; void* vm = nullptr;
     void* flush = nullptr; size_t flush_bytes = 0;
@@ -390,6 +392,103 @@ struct Engine : EngineBase {
         });
     }
 
+    // ---------------------------------------------- SSP schemes (:80-196)
+    template <bool PER, int MODE, bool FINAL>
+    static void ssp_launch(sw_ctx* ctx, const SspArgs<T, Tp>& a) {
+        const Geom& g = a.g;
+        const int nb = (a.nsx * a.nsy + 3) / 4 + a.nring_blocks;
+        ssp_momentum_kernel<T, Tp, PER, MODE, FINAL, STAGE_TY><<<nb, 128, 0, ctx->stream>>>(a);
+    }
+    template <int MODE, bool FINAL>
+    int ssp_stage(sw_ctx* ctx, const SspArgs<T, Tp>& a) {
+        int rc = launch(ctx, 0, [&] {
+            if (a.g.ep) ssp_launch<true, MODE, FINAL>(ctx, a);
+            else ssp_launch<false, MODE, FINAL>(ctx, a);
+        });
+        if (rc) return rc;
+        return launch(ctx, 0, [&] {
+            dim3 grid((a.g.N + 255) / 256, a.g.M);
+            ssp_continuity_kernel<T, Tp, MODE, FINAL><<<grid, 256, 0, ctx->stream>>>(a);
+        });
+    }
+    // The stages of SSPRK2 / SSPRK3 / 4SSPRK3.  X is the state at the step
+    // start; the final u0, v0 go to Acc when the tail follows (else to Y), the
+    // final eta0 to Y.  Stage buffers rotate through A, B, C avoiding the
+    // current input and the SSPRK3 snapshot u0 (src/time_integration.jl:148-152),
+    // which starts as the state: u0 equals u at every step start.
+    int ssp_stages(sw_ctx* ctx, Fields3& X, Fields3& Y, bool tail_now, T Fxt, T Fyt) {
+        const sw_config& c = ctx->cfg;
+        const Geom& g = ctx->g;
+        Fields3 fin;
+        fin.u = tail_now ? ctx->Acc.u : Y.u;
+        fin.v = tail_now ? ctx->Acc.v : Y.v;
+        fin.e = Y.e;
+        const Fields3* pool[3] = {&ctx->A, &ctx->B, &ctx->C};
+        const Fields3* cur = &X;
+        const Fields3* snap = &X;
+
+        SspArgs<T, Tp> a;
+        a.g = g;
+        a.nsx = (g.N + STRIP - 1) / STRIP; a.nsy = (g.M + STAGE_TY - 1) / STAGE_TY;
+        a.nring_blocks = ring_blocks(g, 128);
+        a.uS = (const Tp*)X.u; a.vS = (const Tp*)X.v; a.eS = (const Tp*)X.e;
+        a.ufo = a.vfo = a.efo = nullptr;
+        a.H = sf<T>(ctx->H); a.fq = sf<T>(ctx->fq); a.Fx = sf<T>(ctx->Fx); a.Fy = sf<T>(ctx->Fy);
+        a.g_ = (T)c.g; a.Fxt = Fxt; a.Fyt = Fyt;
+        a.k.half = (Tp)0.5;
+        a.k.kna = (Tp)c.ssp_kna; a.k.knb = (Tp)c.ssp_knb;
+        a.gr = rule(ctx);
+        a.st = ctx->dst;
+
+        int first = 1, last = 0;
+        if (c.time_scheme == SW_SSPRK2) { first = 1; last = c.RKs; }
+        else if (c.time_scheme == SW_SSPRK3) { first = 2; last = c.ssp_s + 1; }
+        else { first = 1; last = 4; }
+        auto free_buf = [&](const Fields3* busy) {
+            for (const Fields3* f : pool)
+                if (f != cur && f != snap && f != busy) return f;
+            return (const Fields3*)nullptr;
+        };
+        for (int rki = first; rki <= last; rki++) {
+            const bool is_last = rki == last;
+            // the other schemes' last u1 is the final state itself; SSPRK2 keeps
+            // u1 and writes the final combination beside it
+            const bool to_fin = is_last && c.time_scheme != SW_SSPRK2;
+            const bool combo = (c.time_scheme == SW_SSPRK2 && is_last) ||
+                               (c.time_scheme == SW_4SSPRK3 && rki == 3);
+            const Fields3* out = to_fin ? &fin : free_buf(nullptr);
+            const Fields3* cmb = nullptr;
+            if (combo) cmb = is_last ? &fin : free_buf(out);
+            if (!out || (combo && !cmb)) return fail(ctx, SW_ERR_ARG, "no free SSP stage buffer");
+            a.u1 = (const Tp*)cur->u; a.v1 = (const Tp*)cur->v; a.e1 = (const Tp*)cur->e;
+            a.uZ = (const Tp*)snap->u; a.vZ = (const Tp*)snap->v; a.eZ = (const Tp*)snap->e;
+            a.u1o = (Tp*)out->u; a.v1o = (Tp*)out->v; a.e1o = (Tp*)out->e;
+            if (combo) {
+                a.ufo = (Tp*)cmb->u; a.vfo = (Tp*)cmb->v; a.efo = (Tp*)cmb->e;
+                if (c.time_scheme == SW_SSPRK2) {                // (:107-109)
+                    a.k.fa = (Tp)(1.0 / c.RKs); a.k.fb = (Tp)((double)(c.RKs - 1) / c.RKs);
+                } else {                                         // (:186-191)
+                    a.k.fa = (Tp)(2.0 / 3.0); a.k.fb = (Tp)(1.0 / 3.0);
+                }
+            }
+            int rc;
+            if (c.time_scheme == SW_SSPRK2) {
+                a.k.x = (Tp)c.Dt_Ds;
+                rc = combo ? ssp_stage<SSP_AXB, true>(ctx, a) : ssp_stage<SSP_AXB, false>(ctx, a);
+            } else if (c.time_scheme == SW_SSPRK3) {
+                if (rki == c.ssp_kn) { a.k.x = (Tp)c.ssp_Dt_Dnc; rc = ssp_stage<SSP_KN, false>(ctx, a); }
+                else { a.k.x = (Tp)c.ssp_Dt_Dn; rc = ssp_stage<SSP_AXB, false>(ctx, a); }
+            } else {
+                a.k.x = (Tp)c.Dt_D;
+                rc = combo ? ssp_stage<SSP_4, true>(ctx, a) : ssp_stage<SSP_4, false>(ctx, a);
+            }
+            if (rc) return rc;
+            if (c.time_scheme == SW_SSPRK3 && rki == c.ssp_mn) snap = out;   // u0 = u1 (:148-152)
+            cur = combo ? cmb : out;
+        }
+        return SW_OK;
+    }
+
     int step(sw_ctx* ctx, long long i) override {
         const sw_config& c = ctx->cfg;
         const Geom& g = ctx->g;
@@ -404,6 +503,9 @@ struct Engine : EngineBase {
         const int nsx = (g.N + STRIP - 1) / STRIP, nsy = (g.M + STAGE_TY - 1) / STAGE_TY;
         const int nring = ring_blocks(g, 128);
         const int nblk = (nsx * nsy + 3) / 4 + nring;
+        if (c.time_scheme != SW_RK) {
+            if (int rc = ssp_stages(ctx, X, Y, tail_now, Fxt, Fyt)) return rc;
+        } else {
         for (int k = 1; k <= c.RKo; k++) {
             StageArgs<T, Tp> a;
             a.g = g; a.nsx = nsx; a.nsy = nsy; a.nring_blocks = nring;
@@ -453,6 +555,8 @@ struct Engine : EngineBase {
                 rc = launch(ctx, 0, [&] { stage_dispatch(a, g.ep != 0, first, last, nblk, ctx->stream); });
             }
             if (rc) return rc;
+        }
+
         }
 
         // -------------------------------------- drag + diffusion (:216-221)
@@ -536,8 +640,13 @@ int check_config(const sw_config* c, std::string& why) {
     }
     if (!fmt_size(c->T) || !fmt_size(c->Tprog) || !fmt_size(c->Tcomm)) { why = "unknown number format"; return SW_ERR_ARG; }
     if (c->nstep_diff < 1 || c->nadvstep < 1 || c->nout < 1 || c->dtint < 1) { why = "step counts must be >= 1"; return SW_ERR_ARG; }
-    if (c->time_scheme != SW_RK) { why = "time_scheme other than RK not built yet"; return SW_ERR_UNSUPPORTED; }
-    if (c->RKo < 2 || c->RKo > 4) { why = "RKo must be 2, 3 or 4"; return SW_ERR_ARG; }
+    if (c->time_scheme < SW_RK || c->time_scheme > SW_4SSPRK3) { why = "unknown time_scheme"; return SW_ERR_ARG; }
+    if (c->time_scheme == SW_SSPRK2 && c->RKs < 2) { why = "SSPRK2 needs RKs >= 2"; return SW_ERR_ARG; }
+    if (c->time_scheme == SW_SSPRK3 && (c->ssp_s < 2 || c->ssp_kn < 2 || c->ssp_kn > c->ssp_s + 1)) {
+        why = "inconsistent SSPRK3 coefficients";
+        return SW_ERR_ARG;
+    }
+    if (c->time_scheme == SW_RK && (c->RKo < 2 || c->RKo > 4)) { why = "RKo must be 2, 3 or 4"; return SW_ERR_ARG; }
     if (c->dynamics != SW_NONLINEAR) { why = "linear dynamics not built yet"; return SW_ERR_UNSUPPORTED; }
     if (c->adv_scheme != SW_ARAKAWA_HSU) { why = "Sadourny advection not built yet"; return SW_ERR_UNSUPPORTED; }
     if (c->nstep_advcor != 0) { why = "nstep_advcor > 0 not built yet"; return SW_ERR_UNSUPPORTED; }
@@ -760,6 +869,9 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
     const size_t fb = ctx->nelem * ctx->tpsz;
     for (Fields3* f : {&ctx->S[0], &ctx->S[1], &ctx->A, &ctx->B, &ctx->Acc})
         for (void** p : {&f->u, &f->v, &f->e})
+            if ((rc = alloc(p, fb))) return rc;
+    if (cfg->time_scheme != SW_RK)
+        for (void** p : {&ctx->C.u, &ctx->C.v, &ctx->C.e})
             if ((rc = alloc(p, fb))) return rc;
     if ((rc = alloc(&ctx->sst[0], fb))) return rc;
     if ((rc = alloc(&ctx->sst[1], fb))) return rc;

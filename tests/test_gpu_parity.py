@@ -62,6 +62,16 @@ CASES = {
     "odd_37_nonperiodic": dict(nx=37, bc="nonperiodic", diffusion="Smagorinsky"),
     "wide_130": dict(nx=130, L_ratio=4, Ndays=0.2),
     "square_64_nonperiodic": dict(nx=64, L_ratio=1, bc="nonperiodic", Ndays=0.2),
+    # semi-implicit strong-stability-preserving schemes (src/time_integration.jl:80-196)
+    "ssprk2_s3": dict(time_scheme="SSPRK2", RKs=3, cfl=1.2),
+    "ssprk2_s2_smag": dict(time_scheme="SSPRK2", RKs=2, cfl=0.7, diffusion="Smagorinsky"),
+    "ssprk3_n2": dict(time_scheme="SSPRK3", RKn=2, cfl=1.2),
+    "ssprk3_n3_nonperiodic": dict(time_scheme="SSPRK3", RKn=3, cfl=2.5, bc="nonperiodic"),
+    "4ssprk3": dict(time_scheme="4SSPRK3", cfl=1.0),
+    "4ssprk3_nonperiodic_f64": dict(time_scheme="4SSPRK3", bc="nonperiodic", diffusion="Smagorinsky",
+                                    T=np.float64),
+    "ssprk3_mixed_f32_f64": dict(time_scheme="SSPRK3", RKn=2, T=np.float32, Tprog=np.float64),
+    "ssprk2_tcomm_float16": dict(time_scheme="SSPRK2", RKs=3, Tcomm=np.float16, α=0.5, bc="nonperiodic"),
 }
 
 
