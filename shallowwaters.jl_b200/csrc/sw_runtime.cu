@@ -32,6 +32,7 @@
 #include "sw_stage.cuh"
 #include "sw_stage2.cuh"
 #include "sw_ssp.cuh"
+#include "sw_diag.cuh"
 #include "sw_tail.cuh"
 #include "sw_tracer.cuh"
 
@@ -76,6 +77,7 @@ struct EngineBase {
     virtual ~EngineBase() = default;
     virtual int step(sw_ctx* ctx, long long i) = 0;          // one time step, without the NaN check
     virtual int nan_check(sw_ctx* ctx, long long i) = 0;     // the check of step i (state before it)
+    virtual int diagnostics(sw_ctx* ctx, sw_diag* out) = 0;
     virtual int ghost_state(sw_ctx* ctx) = 0;
 };
 
@@ -107,6 +109,7 @@ struct sw_ctx {
     std::map<unsigned, StepGraph> graphs;
     int nsm = 148;
     DevStatus* dst = nullptr;     // device status
+    DiagPartial* diag = nullptr;  // DIAG_BLOCKS partials + the result (allocated on first use)
     DevStatus* hst = nullptr;     // pinned host mirror
     int p = 0;                    // state parity
     int sp = 0;                   // tracer parity
@@ -267,6 +270,17 @@ __global__ void ghost_state_kernel(Geom g, Tp* u, Tp* v, Tp* e, GhostRule<Tp> gr
 template <class T, class Tp>
 struct Engine : EngineBase {
     int init(sw_ctx*) { return SW_OK; }
+
+    // continuity! variant and its fields (src/continuity.jl:3-49); the forcing
+    // factor Fetat = T(sin(omega_Feta*t)) at the step's model time
+    template <class Args>
+    void set_cont(sw_ctx* ctx, Args& a) const {
+        const sw_config& c = ctx->cfg;
+        a.cont = c.surface_relax ? 1 : c.surface_forcing ? 2 : 0;
+        a.eref = sf<T>(ctx->eref); a.Feta = sf<T>(ctx->Feta);
+        a.gamma = (T)c.gamma;
+        a.Fetat = c.surface_forcing ? (T)std::sin(c.omegaFeta * (double)ctx->t) : T(0);
+    }
 
     GhostRule<Tp> rule(sw_ctx* ctx) const {
         GhostRule<Tp> r;
@@ -435,6 +449,7 @@ struct Engine : EngineBase {
         a.ufo = a.vfo = a.efo = nullptr;
         a.H = sf<T>(ctx->H); a.fq = sf<T>(ctx->fq); a.Fx = sf<T>(ctx->Fx); a.Fy = sf<T>(ctx->Fy);
         a.g_ = (T)c.g; a.Fxt = Fxt; a.Fyt = Fyt;
+        set_cont(ctx, a);
         a.k.half = (Tp)0.5;
         a.k.kna = (Tp)c.ssp_kna; a.k.knb = (Tp)c.ssp_knb;
         a.gr = rule(ctx);
@@ -531,11 +546,12 @@ struct Engine : EngineBase {
             a.b = (k < c.RKo) ? (Tp)c.RKbDt[k - 1] : Tp(0);
             a.g_ = (T)c.g;
             a.Fxt = Fxt; a.Fyt = Fyt;
+            set_cont(ctx, a);
             a.gr = rule(ctx);
             a.st = ctx->dst;
             int rc;
             constexpr bool F32 = std::is_same<T, float>::value && std::is_same<Tp, float>::value;
-            if (ctx->use_tma && F32 && ctx->packed) {
+            if (ctx->use_tma && F32 && ctx->packed && a.cont == 0) {
                 StageMaps2 mp;
                 mp.in_u = ctx->tmaps[in.u].in2; mp.in_v = ctx->tmaps[in.v].in2; mp.in_e = ctx->tmaps[in.e].in2;
                 mp.x_u = ctx->tmaps[X.u].x2; mp.x_v = ctx->tmaps[X.v].x2; mp.x_e = ctx->tmaps[X.e].x2;
@@ -543,7 +559,7 @@ struct Engine : EngineBase {
                 int lr = 0;
                 rc = launch(ctx, 0, [&] { lr = stage2_dispatch(ctx, a, mp, g.ep != 0, first, last); });
                 if (!rc && lr) rc = fail(ctx, SW_ERR_CUDA, "packed stage kernel could not be configured");
-            } else if (ctx->use_tma) {
+            } else if (ctx->use_tma && a.cont == 0) {
                 StageMaps mp;
                 mp.in_u = ctx->tmaps[in.u].in; mp.in_v = ctx->tmaps[in.v].in; mp.in_e = ctx->tmaps[in.e].in;
                 mp.x_u = ctx->tmaps[X.u].x; mp.x_v = ctx->tmaps[X.v].x; mp.x_e = ctx->tmaps[X.e].x;
@@ -617,6 +633,29 @@ struct Engine : EngineBase {
         return SW_OK;
     }
 
+    int diagnostics(sw_ctx* ctx, sw_diag* out) override {
+        if (!ctx->diag) {
+            CK(cudaMalloc(&ctx->diag, (DIAG_BLOCKS + 1) * sizeof(DiagPartial)));
+            ctx->allocs.push_back(ctx->diag);
+        }
+        const Fields3& X = ctx->S[ctx->p];
+        int rc = launch(ctx, 5, [&] {
+            diag_partial_kernel<T, Tp><<<DIAG_BLOCKS, DIAG_THREADS, 0, ctx->stream>>>(
+                ctx->g, (const Tp*)X.u, (const Tp*)X.v, (const Tp*)X.e, (const Tp*)ctx->sst[ctx->sp], sf<T>(ctx->H),
+                ctx->cfg.g, ctx->diag);
+            diag_final_kernel<<<1, 32, 0, ctx->stream>>>(ctx->diag, DIAG_BLOCKS, ctx->diag + DIAG_BLOCKS);
+        });
+        if (rc) return rc;
+        DiagPartial r;
+        CK(cudaMemcpyAsync(&r, ctx->diag + DIAG_BLOCKS, sizeof(r), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        out->mass = r.mass;
+        out->energy = r.energy;
+        out->max_speed = r.max_speed;
+        out->nan_count = (int64_t)r.nan_count;
+        return SW_OK;
+    }
+
     // NaN check of step i (src/time_integration.jl:232-237): u, v, eta before
     // the step (still S[p]) and sst after it
     int nan_check(sw_ctx* ctx, long long i) override {
@@ -650,7 +689,7 @@ int check_config(const sw_config* c, std::string& why) {
     if (c->dynamics != SW_NONLINEAR) { why = "linear dynamics not built yet"; return SW_ERR_UNSUPPORTED; }
     if (c->adv_scheme != SW_ARAKAWA_HSU) { why = "Sadourny advection not built yet"; return SW_ERR_UNSUPPORTED; }
     if (c->nstep_advcor != 0) { why = "nstep_advcor > 0 not built yet"; return SW_ERR_UNSUPPORTED; }
-    if (c->surface_relax || c->surface_forcing) { why = "surface relaxation/forcing not built yet"; return SW_ERR_UNSUPPORTED; }
+    if (c->surface_relax && c->surface_forcing) { why = "surface_relax and surface_forcing are exclusive"; return SW_ERR_ARG; }
     if (c->storage != SW_STORE_NATIVE) { why = "16-bit storage not built yet"; return SW_ERR_UNSUPPORTED; }
     bool ok = (c->T == SW_FLOAT32 && c->Tprog == SW_FLOAT32) || (c->T == SW_FLOAT64 && c->Tprog == SW_FLOAT64) ||
               (c->T == SW_FLOAT32 && c->Tprog == SW_FLOAT64);
@@ -733,7 +772,8 @@ unsigned step_key(const sw_ctx* ctx, long long i) {
 // One time step: replayed from a CUDA graph when possible, captured on first use.
 int do_step(sw_ctx* ctx, long long i) {
     const sw_config& c = ctx->cfg;
-    if (!ctx->use_graphs || ctx->prof || c.seasonal_wind_x || c.seasonal_wind_y) return ctx->eng->step(ctx, i);
+    if (!ctx->use_graphs || ctx->prof || c.seasonal_wind_x || c.seasonal_wind_y || c.surface_forcing)
+        return ctx->eng->step(ctx, i);
     const unsigned key = step_key(ctx, i);
     auto it = ctx->graphs.find(key);
     if (it == ctx->graphs.end()) {
@@ -894,6 +934,14 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
     if ((rc = upload_static(ctx, ctx->Fx, st->Fx, nux, M, 1 - g.ep, 0))) return rc;
     if ((rc = upload_static(ctx, ctx->Fy, st->Fy, N, M - 1, 0, 1))) return rc;
     if ((rc = upload_static(ctx, ctx->H, st->H, N + 2, M + 2, -1, -1))) return rc;
+    if (cfg->surface_relax) {
+        if (!st->eta_ref) return fail(ctx, SW_ERR_ARG, "surface_relax needs eta_ref");
+        if ((rc = upload_static(ctx, ctx->eref, st->eta_ref, N, M, 0, 0))) return rc;
+    }
+    if (cfg->surface_forcing) {
+        if (!st->Feta) return fail(ctx, SW_ERR_ARG, "surface_forcing needs Feta");
+        if ((rc = upload_static(ctx, ctx->Feta, st->Feta, N, M, 0, 0))) return rc;
+    }
 
     {
         int dev = 0;
@@ -1041,7 +1089,7 @@ int sw_run_profiled(sw_ctx* ctx, int64_t nsteps, int64_t l2_flush_bytes, sw_prof
 
 int sw_diagnostics(sw_ctx* ctx, sw_diag* out) {
     if (!ctx || !out) return SW_ERR_ARG;
-    return fail(ctx, SW_ERR_UNSUPPORTED, "sw_diagnostics not built yet");
+    return ctx->eng->diagnostics(ctx, out);
 }
 
 int sw_time_integration(const sw_config* cfg, const sw_static* st, void* u, void* v, void* eta, void* sst,

@@ -60,6 +60,9 @@ struct SspArgs {
     Tp* ufo; Tp* vfo; Tp* efo;                   // combination fa*u + fb*u1 (COMBO only)
     SField<T> H, fq, Fx, Fy;
     T g_, Fxt, Fyt;
+    int cont;                                    // continuity! variant, as StageArgs::cont
+    SField<T> eref, Feta;
+    T gamma, Fetat;
     SspCoef<Tp> k;
     GhostRule<Tp> gr;
     DevStatus* st;
@@ -242,7 +245,8 @@ ssp_continuity_kernel(SspArgs<T, Tp> A) {
     const T Vb1 = cvt<T>(A.v1o[g.idx(a, b + 1)]) * (half * (h(a, b + 1) + hc));
     const T dUdx = Ua1 - Ua;
     const T dVdy = Vb1 - Vb;
-    const Tp de = -(cvt<Tp>(dUdx) + cvt<Tp>(dVdy));               // continuity_itself! (:52-68)
+    const Tp de = deta_of<T, Tp>(A.cont, dUdx, dVdy, cvt<T>(A.e1[g.idx(a, b)]), A.eref, A.Feta, A.gamma, A.Fetat,
+                                 a, b);                              // src/continuity.jl:3-68
     const int o = g.idx(a, b);
     const Tp z = (MODE == SSP_KN) ? A.eZ[o] : Tp(0);
     const Tp st = COMBO ? A.eS[o] : Tp(0);

@@ -46,9 +46,26 @@ struct StageArgs {
     Tp a, b;                            // RKaΔt[k], RKbΔt[k] (Tprog)
     T g_;                               // gravity (T)
     T Fxt, Fyt;                         // seasonal factors (1 if off)
+    // continuity! variant (src/continuity.jl:3-49): 0 plain, 1 surface
+    // relaxation gamma*(eta_ref - eta), 2 surface forcing Fetat*Feta.  Only the
+    // streaming kernel implements 1 and 2.
+    int cont;
+    SField<T> eref, Feta;
+    T gamma, Fetat;
     GhostRule<Tp> gr;
     DevStatus* st;
 };
+
+// deta at the T-cell (c, r) from the flux divergences: continuity_itself!,
+// continuity_surf_relax!, continuity_forcing! (src/continuity.jl:3-68)
+template <class T, class Tp>
+__device__ __forceinline__ Tp deta_of(int cont, T dUdx, T dVdy, T eta, const SField<T>& eref, const SField<T>& Feta,
+                                      T gamma, T Fetat, int c, int r) {
+    const Tp de = -(cvt<Tp>(dUdx) + cvt<Tp>(dVdy));
+    if (cont == 1) return de + cvt<Tp>(gamma * (eref.at(c, r) - eta));
+    if (cont == 2) return de + cvt<Tp>(Fetat * Feta.at(c, r));
+    return de;
+}
 
 // q at the corner (F, G): PV! (src/PV_advection.jl:2-18) with h_q = Ixy!(h)
 // (src/interpolations.jl:33-45), dvdx = ∂x!(v), dudy = ∂y!(u)
@@ -264,7 +281,7 @@ SWB_ROW_UNROLL
                 // deta at (a=c, b=r): continuity_itself! (src/continuity.jl:52-68)
                 const T dUdx = Ur_r - U_r;
                 const T dVdy = V_r1 - V_r;
-                const Tp de = -(cvt<Tp>(dUdx) + cvt<Tp>(dVdy));
+                const Tp de = deta_of<T, Tp>(A.cont, dUdx, dVdy, e_r, A.eref, A.Feta, A.gamma, A.Fetat, c, r);
                 const Tp X = (FIRST && SAME) ? cvt<Tp>(e_r) : Xe_;
                 const bool gs = gx_e || r == 0 || r == M - 1;
                 if (!LAST) {

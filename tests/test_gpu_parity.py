@@ -72,6 +72,11 @@ CASES = {
                                     T=np.float64),
     "ssprk3_mixed_f32_f64": dict(time_scheme="SSPRK3", RKn=2, T=np.float32, Tprog=np.float64),
     "ssprk2_tcomm_float16": dict(time_scheme="SSPRK2", RKs=3, Tcomm=np.float16, α=0.5, bc="nonperiodic"),
+    # continuity! variants (src/continuity.jl:3-49)
+    "surface_relax": dict(surface_relax=True),
+    "surface_forcing_nonperiodic": dict(surface_forcing=True, bc="nonperiodic"),
+    "ssprk2_surface_relax": dict(time_scheme="SSPRK2", RKs=3, cfl=1.2, surface_relax=True),
+    "4ssprk3_surface_forcing": dict(time_scheme="4SSPRK3", surface_forcing=True),
 }
 
 
@@ -174,3 +179,29 @@ def test_graph_replay_equals_direct_launches(monkeypatch):
         m.close()
     for x, y, name in zip(out[0], out[1], ("u", "v", "η", "sst")):
         assert_bitwise(x, y, name)
+
+
+def test_diagnostics_fp64_reductions():
+    """sw_diagnostics: FP64 mass, energy, max speed and NaN count of the
+    current state, against numpy in double on the downloaded state."""
+    P = Parameter(nx=40, Ndays=0.2, Uadv=1000, bc="nonperiodic", topography="seamount")
+    S = model_setup(P)
+    m = Model(S)
+    m.set_state(initial_conditions(P.Tprog, S, **seeded_inputs(S, 7)))
+    m.run(25)
+    d = m.diagnostics()
+    u, v, e, sst = (np.asarray(a, dtype=np.float64) for a in m.get_state())
+    G = S.grid
+    N, M, ep = G.nx, G.ny, G.ep
+    eta = e[1:M + 1, 1:N + 1]
+    H = np.asarray(S.forcing.H, dtype=np.float64)[1:M + 1, 1:N + 1]
+    # ([j][i] arrays) u at face F, row b: u[b + 2, F + 1 + ep]; v at column a, face G: v[G + 1, a + 2]
+    uu = u[2:M + 2, 1 + ep:N + 2 + ep]
+    vv = v[1:M + 2, 2:N + 2]
+    energy = np.sum(0.5 * (eta + H) * (0.5 * (uu[:, :-1] ** 2 + uu[:, 1:] ** 2) + 0.5 * (vv[:-1] ** 2 + vv[1:] ** 2))
+                    + 0.5 * float(S.parameters.g) * eta ** 2)
+    assert uu.shape == (M, N + 1) and vv.shape == (M + 1, N)
+    np.testing.assert_allclose(d.mass, eta.sum(), rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(d.energy, energy, rtol=1e-12)
+    assert d.max_speed == max(np.abs(uu[:, :-1]).max(), np.abs(vv[:-1]).max())
+    assert d.nan_count == 0
