@@ -199,6 +199,21 @@ int sw_run(sw_ctx* ctx, int64_t nsteps, sw_status* status);
 int sw_get_state(sw_ctx* ctx, void* u, void* v, void* eta, void* sst);
 /* FP64 reductions over the current state. */
 int sw_diagnostics(sw_ctx* ctx, sw_diag* out);
+/* sw_diagnostics for callers that cannot allocate device memory (for example
+ * a host whose pool allocator owns the GPU's memory, or a time loop that must
+ * not be stalled by the device-wide synchronisation of cudaMalloc/cudaFree).
+ * No counterpart in the reference.  The fields are the caller's DEVICE
+ * buffers in the host-array layout and shapes above (u, v, eta, sst in Tprog,
+ * H in T); only cfg->nx, ny, periodic, T, Tprog and g are read.  Reduction
+ * scratch is a fixed array inside the library, so it allocates nothing and
+ * accepts at most 16,777,216 cells (nx*ny), returning SW_ERR_ARG beyond that.
+ * The first call on a device looks up that array (make it before any stream
+ * capture); calls whose kernels overlap on one device share the array and
+ * race.  Runs on `stream` (a cudaStream_t, NULL for the default stream) and
+ * returns after the result has reached *out. */
+int sw_diagnostics_noalloc(const sw_config* cfg, const void* u, const void* v,
+                           const void* eta, const void* sst, const void* H,
+                           void* stream, sw_diag* out);
 /* sw_run with per-kernel CUDA-event timing; when l2_flush_bytes > 0 a buffer
  * of that size is written between steps (outside the timed intervals). */
 int sw_run_profiled(sw_ctx* ctx, int64_t nsteps, int64_t l2_flush_bytes,
