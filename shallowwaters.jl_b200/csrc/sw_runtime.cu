@@ -32,6 +32,7 @@
 #include "sw_stage.cuh"
 #include "sw_stage2.cuh"
 #include "sw_ssp.cuh"
+#include "sw_linear.cuh"
 #include "sw_diag.cuh"
 #include "sw_tail.cuh"
 #include "sw_tracer.cuh"
@@ -410,8 +411,49 @@ struct Engine : EngineBase {
     template <bool PER, int MODE, bool FINAL>
     static void ssp_launch(sw_ctx* ctx, const SspArgs<T, Tp>& a) {
         const Geom& g = a.g;
+        if (ctx->cfg.dynamics == SW_LINEAR) {
+            const int ncb = (int)(((long long)g.N * g.M + 255) / 256);
+            const SspArgs<T, Tp> b = ring256(a);
+            lin_ssp_momentum_kernel<T, Tp, PER, MODE, FINAL><<<ncb + b.nring_blocks, 256, 0, ctx->stream>>>(
+                b, linear_rhs(ctx, a.u1, a.v1, a.e1, a.Fxt, a.Fyt), ncb);
+            return;
+        }
         const int nb = (a.nsx * a.nsy + 3) / 4 + a.nring_blocks;
         ssp_momentum_kernel<T, Tp, PER, MODE, FINAL, STAGE_TY><<<nb, 128, 0, ctx->stream>>>(a);
+    }
+    // the point-wise linear kernels run their ring with 256 threads per block
+    template <class Args>
+    static Args ring256(const Args& a) {
+        Args b = a;
+        b.nring_blocks = ring_blocks(a.g, 256);
+        return b;
+    }
+    static LinearRhs<T, Tp> linear_rhs(sw_ctx* ctx, const Tp* u, const Tp* v, const Tp* e, T Fxt, T Fyt) {
+        LinearRhs<T, Tp> L;
+        L.g = ctx->g;
+        L.u = u; L.v = v; L.e = e;
+        L.fu = sf<T>(ctx->fu); L.fv = sf<T>(ctx->fv); L.Fx = sf<T>(ctx->Fx); L.Fy = sf<T>(ctx->Fy);
+        L.g_ = (T)ctx->cfg.g; L.Fxt = Fxt; L.Fyt = Fyt;
+        return L;
+    }
+    template <bool PER, bool FIRST, bool LAST>
+    static void lin_rk_launch(sw_ctx* ctx, const StageArgs<T, Tp>& a) {
+        const Geom& g = a.g;
+        const int ncb = (int)(((long long)g.N * g.M + 255) / 256);
+        const StageArgs<T, Tp> b = ring256(a);
+        lin_rk_stage_kernel<T, Tp, PER, FIRST, LAST><<<ncb + b.nring_blocks, 256, 0, ctx->stream>>>(
+            b, linear_rhs(ctx, a.u1, a.v1, a.e1, a.Fxt, a.Fyt), ncb);
+    }
+    static void lin_rk_dispatch(sw_ctx* ctx, const StageArgs<T, Tp>& a, bool per, bool first, bool last) {
+        if (per) {
+            if (first) lin_rk_launch<true, true, false>(ctx, a);
+            else if (last) lin_rk_launch<true, false, true>(ctx, a);
+            else lin_rk_launch<true, false, false>(ctx, a);
+        } else {
+            if (first) lin_rk_launch<false, true, false>(ctx, a);
+            else if (last) lin_rk_launch<false, false, true>(ctx, a);
+            else lin_rk_launch<false, false, false>(ctx, a);
+        }
     }
     template <int MODE, bool FINAL>
     int ssp_stage(sw_ctx* ctx, const SspArgs<T, Tp>& a) {
@@ -551,7 +593,9 @@ struct Engine : EngineBase {
             a.st = ctx->dst;
             int rc;
             constexpr bool F32 = std::is_same<T, float>::value && std::is_same<Tp, float>::value;
-            if (ctx->use_tma && F32 && ctx->packed && a.cont == 0) {
+            if (c.dynamics == SW_LINEAR) {
+                rc = launch(ctx, 0, [&] { lin_rk_dispatch(ctx, a, g.ep != 0, first, last); });
+            } else if (ctx->use_tma && F32 && ctx->packed && a.cont == 0) {
                 StageMaps2 mp;
                 mp.in_u = ctx->tmaps[in.u].in2; mp.in_v = ctx->tmaps[in.v].in2; mp.in_e = ctx->tmaps[in.e].in2;
                 mp.x_u = ctx->tmaps[X.u].x2; mp.x_v = ctx->tmaps[X.v].x2; mp.x_e = ctx->tmaps[X.e].x2;
@@ -686,9 +730,9 @@ int check_config(const sw_config* c, std::string& why) {
         return SW_ERR_ARG;
     }
     if (c->time_scheme == SW_RK && (c->RKo < 2 || c->RKo > 4)) { why = "RKo must be 2, 3 or 4"; return SW_ERR_ARG; }
-    if (c->dynamics != SW_NONLINEAR) { why = "linear dynamics not built yet"; return SW_ERR_UNSUPPORTED; }
+    if (c->dynamics != SW_NONLINEAR && c->dynamics != SW_LINEAR) { why = "unknown dynamics"; return SW_ERR_ARG; }
     if (c->adv_scheme != SW_ARAKAWA_HSU) { why = "Sadourny advection not built yet"; return SW_ERR_UNSUPPORTED; }
-    if (c->nstep_advcor != 0) { why = "nstep_advcor > 0 not built yet"; return SW_ERR_UNSUPPORTED; }
+    if (c->dynamics == SW_NONLINEAR && c->nstep_advcor != 0) { why = "nstep_advcor > 0 not built yet"; return SW_ERR_UNSUPPORTED; }
     if (c->surface_relax && c->surface_forcing) { why = "surface_relax and surface_forcing are exclusive"; return SW_ERR_ARG; }
     if (c->storage != SW_STORE_NATIVE) { why = "16-bit storage not built yet"; return SW_ERR_UNSUPPORTED; }
     bool ok = (c->T == SW_FLOAT32 && c->Tprog == SW_FLOAT32) || (c->T == SW_FLOAT64 && c->Tprog == SW_FLOAT64) ||
@@ -934,6 +978,11 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
     if ((rc = upload_static(ctx, ctx->Fx, st->Fx, nux, M, 1 - g.ep, 0))) return rc;
     if ((rc = upload_static(ctx, ctx->Fy, st->Fy, N, M - 1, 0, 1))) return rc;
     if ((rc = upload_static(ctx, ctx->H, st->H, N + 2, M + 2, -1, -1))) return rc;
+    if (cfg->dynamics == SW_LINEAR) {
+        if (!st->f_u || !st->f_v) return fail(ctx, SW_ERR_ARG, "linear dynamics needs f_u and f_v");
+        if ((rc = upload_static(ctx, ctx->fu, st->f_u, nux, M, 1 - g.ep, 0))) return rc;
+        if ((rc = upload_static(ctx, ctx->fv, st->f_v, N, M - 1, 0, 1))) return rc;
+    }
     if (cfg->surface_relax) {
         if (!st->eta_ref) return fail(ctx, SW_ERR_ARG, "surface_relax needs eta_ref");
         if ((rc = upload_static(ctx, ctx->eref, st->eta_ref, N, M, 0, 0))) return rc;

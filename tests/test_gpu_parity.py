@@ -77,6 +77,14 @@ CASES = {
     "surface_forcing_nonperiodic": dict(surface_forcing=True, bc="nonperiodic"),
     "ssprk2_surface_relax": dict(time_scheme="SSPRK2", RKs=3, cfl=1.2, surface_relax=True),
     "4ssprk3_surface_forcing": dict(time_scheme="4SSPRK3", surface_forcing=True),
+    # linear dynamics (src/rhs.jl:59-86); with RK, continuity! sees the never-computed U = V = 0
+    "linear": dict(dynamics="linear"),
+    "linear_nonperiodic_relax": dict(dynamics="linear", bc="nonperiodic", surface_relax=True),
+    "linear_rk3_mixed_f32_f64": dict(dynamics="linear", RKo=3, cfl=0.6, T=np.float32, Tprog=np.float64),
+    "linear_advcor_ignored": dict(dynamics="linear", nstep_advcor=2),
+    "linear_ssprk2": dict(dynamics="linear", time_scheme="SSPRK2", cfl=0.7),
+    "linear_4ssprk3_nonperiodic_f64": dict(dynamics="linear", time_scheme="4SSPRK3", bc="nonperiodic",
+                                           T=np.float64),
 }
 
 
