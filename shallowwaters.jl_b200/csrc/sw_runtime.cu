@@ -278,6 +278,7 @@ struct Engine : EngineBase {
     void set_cont(sw_ctx* ctx, Args& a) const {
         const sw_config& c = ctx->cfg;
         a.cont = c.surface_relax ? 1 : c.surface_forcing ? 2 : 0;
+        a.sadourny = c.adv_scheme == SW_SADOURNY;
         a.eref = sf<T>(ctx->eref); a.Feta = sf<T>(ctx->Feta);
         a.gamma = (T)c.gamma;
         a.Fetat = c.surface_forcing ? (T)std::sin(c.omegaFeta * (double)ctx->t) : T(0);
@@ -595,7 +596,7 @@ struct Engine : EngineBase {
             constexpr bool F32 = std::is_same<T, float>::value && std::is_same<Tp, float>::value;
             if (c.dynamics == SW_LINEAR) {
                 rc = launch(ctx, 0, [&] { lin_rk_dispatch(ctx, a, g.ep != 0, first, last); });
-            } else if (ctx->use_tma && F32 && ctx->packed && a.cont == 0) {
+            } else if (ctx->use_tma && F32 && ctx->packed && a.cont == 0 && !a.sadourny) {
                 StageMaps2 mp;
                 mp.in_u = ctx->tmaps[in.u].in2; mp.in_v = ctx->tmaps[in.v].in2; mp.in_e = ctx->tmaps[in.e].in2;
                 mp.x_u = ctx->tmaps[X.u].x2; mp.x_v = ctx->tmaps[X.v].x2; mp.x_e = ctx->tmaps[X.e].x2;
@@ -603,7 +604,7 @@ struct Engine : EngineBase {
                 int lr = 0;
                 rc = launch(ctx, 0, [&] { lr = stage2_dispatch(ctx, a, mp, g.ep != 0, first, last); });
                 if (!rc && lr) rc = fail(ctx, SW_ERR_CUDA, "packed stage kernel could not be configured");
-            } else if (ctx->use_tma && a.cont == 0) {
+            } else if (ctx->use_tma && a.cont == 0 && !a.sadourny) {
                 StageMaps mp;
                 mp.in_u = ctx->tmaps[in.u].in; mp.in_v = ctx->tmaps[in.v].in; mp.in_e = ctx->tmaps[in.e].in;
                 mp.x_u = ctx->tmaps[X.u].x; mp.x_v = ctx->tmaps[X.v].x; mp.x_e = ctx->tmaps[X.e].x;
@@ -731,7 +732,7 @@ int check_config(const sw_config* c, std::string& why) {
     }
     if (c->time_scheme == SW_RK && (c->RKo < 2 || c->RKo > 4)) { why = "RKo must be 2, 3 or 4"; return SW_ERR_ARG; }
     if (c->dynamics != SW_NONLINEAR && c->dynamics != SW_LINEAR) { why = "unknown dynamics"; return SW_ERR_ARG; }
-    if (c->adv_scheme != SW_ARAKAWA_HSU) { why = "Sadourny advection not built yet"; return SW_ERR_UNSUPPORTED; }
+    if (c->adv_scheme != SW_ARAKAWA_HSU && c->adv_scheme != SW_SADOURNY) { why = "unknown adv_scheme"; return SW_ERR_ARG; }
     if (c->dynamics == SW_NONLINEAR && c->nstep_advcor != 0) { why = "nstep_advcor > 0 not built yet"; return SW_ERR_UNSUPPORTED; }
     if (c->surface_relax && c->surface_forcing) { why = "surface_relax and surface_forcing are exclusive"; return SW_ERR_ARG; }
     if (c->storage != SW_STORE_NATIVE) { why = "16-bit storage not built yet"; return SW_ERR_UNSUPPORTED; }

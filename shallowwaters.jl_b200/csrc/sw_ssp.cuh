@@ -61,6 +61,7 @@ struct SspArgs {
     SField<T> H, fq, Fx, Fy;
     T g_, Fxt, Fyt;
     int cont;                                    // continuity! variant, as StageArgs::cont
+    int sadourny;                                // PV_Sadourny!, as StageArgs::sadourny
     SField<T> eref, Feta;
     T gamma, Fetat;
     SspCoef<Tp> k;
@@ -139,7 +140,7 @@ ssp_momentum_kernel(SspArgs<T, Tp> A) {
     T U_r = u_r * (half * (h_r + hl_r));
     T Ur_r = shdn(U_r);
     T V_r = T(0), Vl_r = T(0), q_r = T(0), ql_r = T(0), qr_r = T(0);
-    T p_rm1 = T(0), qhu_part = T(0);
+    T p_rm1 = T(0), qhu_part = T(0), sad_part = T(0);
     T uN_r = T(0), hN_r = T(0), hNm1_r = T(0);
     if (wrap) {
         uN_r = cvt<T>(A.u1[g.idx(N, r)]);
@@ -183,7 +184,8 @@ ssp_momentum_kernel(SspArgs<T, Tp> A) {
         if (r >= y0 && r < M) {
             const int o = row(r) + cb;
             if (col_u) {                                            // momentum_u! (src/rhs.jl:218-245)
-                const T qhv = qa * V_r1 + qb * Vl_r1 + qc * Vl_r + qd * V_r;
+                const T qhv = A.sadourny ? sadourny_qhv(q_r, q_r1, V_r, Vl_r, V_r1, Vl_r1)
+                                         : qa * V_r1 + qb * Vl_r1 + qc * Vl_r + qd * V_r;
                 const T dpdx = p_r - pl_r;
                 const Tp du = (cvt<Tp>(qhv) - cvt<Tp>(dpdx)) + cvt<Tp>(A.Fxt * A.Fx.at(c, r));
                 const Tp z = (MODE == SSP_KN) ? A.uZ[o] : Tp(0);
@@ -199,7 +201,8 @@ ssp_momentum_kernel(SspArgs<T, Tp> A) {
                 }
             }
             if (col_a && r >= 1) {                                  // momentum_v! (src/rhs.jl:248-274)
-                const T qhu = qhu_part + qcr * Ur_r + qd * U_r;
+                const T qhu = A.sadourny ? (half * (qr_r + q_r)) * (sad_part + T(0.25) * (U_r + Ur_r))
+                                             : qhu_part + qcr * Ur_r + qd * U_r;
                 const T dpdy = p_r - p_rm1;
                 const Tp dv = -(cvt<Tp>(qhu) + cvt<Tp>(dpdy)) + cvt<Tp>(A.Fyt * A.Fy.at(c, r));
                 const Tp z = (MODE == SSP_KN) ? A.vZ[o] : Tp(0);
@@ -216,6 +219,7 @@ ssp_momentum_kernel(SspArgs<T, Tp> A) {
         }
 
         qhu_part = qa * U_r + qbr * Ur_r;
+        sad_part = T(0.25) * (U_r + Ur_r);
         u_r = u_r1; v_r = v_r1; e_r = e_r1; h_r = h_r1; hl_r = hl_r1; ur_r = ur_r1;
         q_r = q_r1; ql_r = ql_r1; qr_r = qr_r1;
         U_r = U_r1; Ur_r = Ur_r1;

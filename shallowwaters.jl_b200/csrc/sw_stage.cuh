@@ -52,6 +52,7 @@ struct StageArgs {
     int cont;
     SField<T> eref, Feta;
     T gamma, Fetat;
+    int sadourny;                       // 1: PV_Sadourny! instead of PV_ArakawaHsu! (streaming kernel only)
     GhostRule<Tp> gr;
     DevStatus* st;
 };
@@ -65,6 +66,16 @@ __device__ __forceinline__ Tp deta_of(int cont, T dUdx, T dVdy, T eta, const SFi
     if (cont == 1) return de + cvt<Tp>(gamma * (eref.at(c, r) - eta));
     if (cont == 2) return de + cvt<Tp>(Fetat * Feta.at(c, r));
     return de;
+}
+
+// PV_Sadourny! at the u-point (F, b) (src/PV_advection.jl:31-59):
+// Iy!(q) * Ixy!(V) with q at the corners (F, b), (F, b+1) and V at
+// (F-1, b), (F, b), (F-1, b+1), (F, b+1).  The v-point form Ix!(q) * Ixy!(U)
+// is written inline where its lower half, carried from the previous row, is.
+template <class T>
+__device__ __forceinline__ T sadourny_qhv(T q_b, T q_b1, T V_b, T Vl_b, T V_b1, T Vl_b1) {
+    const T half = T(0.5), q4 = T(0.25);
+    return (half * (q_b1 + q_b)) * (q4 * (Vl_b + V_b) + q4 * (Vl_b1 + V_b1));
 }
 
 // q at the corner (F, G): PV! (src/PV_advection.jl:2-18) with h_q = Ixy!(h)
@@ -170,7 +181,7 @@ rk_stage_kernel(StageArgs<T, Tp> A) {
     T U_r = u_r * (half * (h_r + hl_r));
     T Ur_r = shdn(U_r);
     T V_r = T(0), Vl_r = T(0), q_r = T(0), ql_r = T(0), qr_r = T(0);
-    T p_rm1 = T(0), qhu_part = T(0);
+    T p_rm1 = T(0), qhu_part = T(0), sad_part = T(0);
     T uN_r = T(0), hN_r = T(0), hNm1_r = T(0);
     if (wrap) {
         uN_r = cvt<T>(A.u1[g.idx(N, r)]);
@@ -248,7 +259,8 @@ SWB_ROW_UNROLL
         if (r >= y0 && r < M) {
             // du at (F=c, b=r): momentum_u! (src/rhs.jl:218-245) with qhv (PV_ArakawaHsu!, :63-75)
             if (col_u) {
-                const T qhv = qa * V_r1 + qb * Vl_r1 + qc * Vl_r + qd * V_r;
+                const T qhv = A.sadourny ? sadourny_qhv(q_r, q_r1, V_r, Vl_r, V_r1, Vl_r1)
+                                         : qa * V_r1 + qb * Vl_r1 + qc * Vl_r + qd * V_r;
                 const T dpdx = p_r - pl_r;
                 const Tp du = (cvt<Tp>(qhv) - cvt<Tp>(dpdx)) + cvt<Tp>(A.Fxt * A.Fx.at(c, r));
                 const Tp X = (FIRST && SAME) ? cvt<Tp>(u_r) : Xu_;
@@ -265,7 +277,8 @@ SWB_ROW_UNROLL
             if (col_a) {
                 // dv at (a=c, G=r): momentum_v! (:248-274) with qhu (:77-83)
                 if (r >= 1) {
-                    const T qhu = qhu_part + qcr * Ur_r + qd * U_r;
+                    const T qhu = A.sadourny ? (half * (qr_r + q_r)) * (sad_part + T(0.25) * (U_r + Ur_r))
+                                             : qhu_part + qcr * Ur_r + qd * U_r;
                     const T dpdy = p_r - p_rm1;
                     const Tp dv = -(cvt<Tp>(qhu) + cvt<Tp>(dpdy)) + cvt<Tp>(A.Fyt * A.Fy.at(c, r));
                     const Tp X = (FIRST && SAME) ? cvt<Tp>(v_r) : Xv_;
@@ -298,6 +311,7 @@ SWB_ROW_UNROLL
         // ---- slide the window; the first two products of qhu at G = r+1
         // (qα(c,r)·U(c,r) + qβ(c+1,r)·U(c+1,r)) are formed now, in the same order
         qhu_part = qa * U_r + qbr * Ur_r;
+        sad_part = T(0.25) * (U_r + Ur_r);
         u_r = u_r1; v_r = v_r1; e_r = e_r1; h_r = h_r1; hl_r = hl_r1; ur_r = ur_r1;
         q_r = q_r1; ql_r = ql_r1; qr_r = qr_r1;
         U_r = U_r1; Ur_r = Ur_r1;

@@ -85,6 +85,11 @@ CASES = {
     "linear_ssprk2": dict(dynamics="linear", time_scheme="SSPRK2", cfl=0.7),
     "linear_4ssprk3_nonperiodic_f64": dict(dynamics="linear", time_scheme="4SSPRK3", bc="nonperiodic",
                                            T=np.float64),
+    # Sadourny's enstrophy-conserving PV advection (src/PV_advection.jl:31-59)
+    "sadourny": dict(adv_scheme="Sadourny"),
+    "sadourny_nonperiodic_smag": dict(adv_scheme="Sadourny", bc="nonperiodic", diffusion="Smagorinsky"),
+    "sadourny_mixed_f32_f64": dict(adv_scheme="Sadourny", T=np.float32, Tprog=np.float64),
+    "sadourny_ssprk3_f64": dict(adv_scheme="Sadourny", time_scheme="SSPRK3", RKn=2, cfl=1.2, T=np.float64),
 }
 
 
