@@ -33,6 +33,7 @@
 #include "sw_stage2.cuh"
 #include "sw_ssp.cuh"
 #include "sw_linear.cuh"
+#include "sw_advcor.cuh"
 #include "sw_diag.cuh"
 #include "sw_tail.cuh"
 #include "sw_tracer.cuh"
@@ -79,6 +80,7 @@ struct EngineBase {
     virtual int step(sw_ctx* ctx, long long i) = 0;          // one time step, without the NaN check
     virtual int nan_check(sw_ctx* ctx, long long i) = 0;     // the check of step i (state before it)
     virtual int diagnostics(sw_ctx* ctx, sw_diag* out) = 0;
+    virtual int prologue(sw_ctx* ctx) = 0;                   // work of time_integration before its loop
     virtual int ghost_state(sw_ctx* ctx) = 0;
 };
 
@@ -92,6 +94,9 @@ struct sw_ctx {
     std::vector<void*> allocs;
     Fields3 S[2], A, B, Acc;
     Fields3 C;                 // third stage buffer of the SSP schemes
+    void* qS = nullptr;        // nstep_advcor > 0: stored q, KEu, KEv (type T, sw_advcor.cuh)
+    void* KEuS = nullptr;
+    void* KEvS = nullptr;
     void* sst[2] = {nullptr, nullptr};
     void* um = nullptr; void* vm = nullptr;
     void* flush = nullptr; size_t flush_bytes = 0;
@@ -279,6 +284,7 @@ struct Engine : EngineBase {
         const sw_config& c = ctx->cfg;
         a.cont = c.surface_relax ? 1 : c.surface_forcing ? 2 : 0;
         a.sadourny = c.adv_scheme == SW_SADOURNY;
+        a.qS = (const T*)ctx->qS; a.KEuS = (const T*)ctx->KEuS; a.KEvS = (const T*)ctx->KEvS;
         a.eref = sf<T>(ctx->eref); a.Feta = sf<T>(ctx->Feta);
         a.gamma = (T)c.gamma;
         a.Fetat = c.surface_forcing ? (T)std::sin(c.omegaFeta * (double)ctx->t) : T(0);
@@ -596,7 +602,7 @@ struct Engine : EngineBase {
             constexpr bool F32 = std::is_same<T, float>::value && std::is_same<Tp, float>::value;
             if (c.dynamics == SW_LINEAR) {
                 rc = launch(ctx, 0, [&] { lin_rk_dispatch(ctx, a, g.ep != 0, first, last); });
-            } else if (ctx->use_tma && F32 && ctx->packed && a.cont == 0 && !a.sadourny) {
+            } else if (ctx->use_tma && F32 && ctx->packed && a.cont == 0 && !a.sadourny && !a.qS) {
                 StageMaps2 mp;
                 mp.in_u = ctx->tmaps[in.u].in2; mp.in_v = ctx->tmaps[in.v].in2; mp.in_e = ctx->tmaps[in.e].in2;
                 mp.x_u = ctx->tmaps[X.u].x2; mp.x_v = ctx->tmaps[X.v].x2; mp.x_e = ctx->tmaps[X.e].x2;
@@ -604,7 +610,7 @@ struct Engine : EngineBase {
                 int lr = 0;
                 rc = launch(ctx, 0, [&] { lr = stage2_dispatch(ctx, a, mp, g.ep != 0, first, last); });
                 if (!rc && lr) rc = fail(ctx, SW_ERR_CUDA, "packed stage kernel could not be configured");
-            } else if (ctx->use_tma && a.cont == 0 && !a.sadourny) {
+            } else if (ctx->use_tma && a.cont == 0 && !a.sadourny && !a.qS) {
                 StageMaps mp;
                 mp.in_u = ctx->tmaps[in.u].in; mp.in_v = ctx->tmaps[in.v].in; mp.in_e = ctx->tmaps[in.e].in;
                 mp.x_u = ctx->tmaps[X.u].x; mp.x_v = ctx->tmaps[X.v].x; mp.x_e = ctx->tmaps[X.e].x;
@@ -618,6 +624,13 @@ struct Engine : EngineBase {
             if (rc) return rc;
         }
 
+        }
+
+        // ---------------------- advection/Coriolis refresh (:208-211)
+        if (ctx->qS && (i % c.nstep_advcor) == 0) {
+            const void* u0 = tail_now ? ctx->Acc.u : Y.u;
+            const void* v0 = tail_now ? ctx->Acc.v : Y.v;
+            if (int rc = advcor_refresh(ctx, u0, v0, Y.e, false)) return rc;
         }
 
         // -------------------------------------- drag + diffusion (:216-221)
@@ -640,6 +653,9 @@ struct Engine : EngineBase {
                 else tail_dispatch2<false>(a, c.bottom_drag, smag, nb, ctx->stream);
             });
             if (rc) return rc;
+            // bottom_drag_quadratic! leaves its KEu, KEv (of u0) for the next stages
+            if (ctx->qS && c.bottom_drag == SW_DRAG_QUADRATIC)
+                if ((rc = advcor_refresh(ctx, ctx->Acc.u, ctx->Acc.v, Y.e, true))) return rc;
         }
         ctx->t += c.dtint;
 
@@ -676,6 +692,33 @@ struct Engine : EngineBase {
         }
 
         return SW_OK;
+    }
+
+    // advection/Coriolis refresh (nstep_advcor > 0) from u, v, eta with valid
+    // ghosts; KE only after a quadratic-drag tail (sw_advcor.cuh)
+    int advcor_refresh(sw_ctx* ctx, const void* u, const void* v, const void* e, bool ke_only) {
+        const Geom& g = ctx->g;
+        dim3 grid((g.N + 4 + 255) / 256, g.M + 2);
+        return launch(ctx, 3, [&] {
+            auto args = [&](auto kern) {
+                kern<<<grid, 256, 0, ctx->stream>>>(g, (const Tp*)u, (const Tp*)v, (const Tp*)e, sf<T>(ctx->H),
+                                                    sf<T>(ctx->fq), (T*)ctx->qS, (T*)ctx->KEuS, (T*)ctx->KEvS);
+            };
+            if (g.ep) {
+                if (ke_only) args(advcor_refresh_kernel<T, Tp, true, true>);
+                else args(advcor_refresh_kernel<T, Tp, true, false>);
+            } else {
+                if (ke_only) args(advcor_refresh_kernel<T, Tp, false, true>);
+                else args(advcor_refresh_kernel<T, Tp, false, false>);
+            }
+        });
+    }
+    // the prologue of time_integration (src/time_integration.jl:20-31): the
+    // advection/Coriolis terms of the initial state
+    int prologue(sw_ctx* ctx) override {
+        if (!ctx->qS) return SW_OK;
+        const Fields3& X = ctx->S[ctx->p];
+        return advcor_refresh(ctx, X.u, X.v, X.e, false);
     }
 
     int diagnostics(sw_ctx* ctx, sw_diag* out) override {
@@ -733,7 +776,7 @@ int check_config(const sw_config* c, std::string& why) {
     if (c->time_scheme == SW_RK && (c->RKo < 2 || c->RKo > 4)) { why = "RKo must be 2, 3 or 4"; return SW_ERR_ARG; }
     if (c->dynamics != SW_NONLINEAR && c->dynamics != SW_LINEAR) { why = "unknown dynamics"; return SW_ERR_ARG; }
     if (c->adv_scheme != SW_ARAKAWA_HSU && c->adv_scheme != SW_SADOURNY) { why = "unknown adv_scheme"; return SW_ERR_ARG; }
-    if (c->dynamics == SW_NONLINEAR && c->nstep_advcor != 0) { why = "nstep_advcor > 0 not built yet"; return SW_ERR_UNSUPPORTED; }
+    if (c->nstep_advcor < 0) { why = "nstep_advcor must be >= 0"; return SW_ERR_ARG; }
     if (c->surface_relax && c->surface_forcing) { why = "surface_relax and surface_forcing are exclusive"; return SW_ERR_ARG; }
     if (c->storage != SW_STORE_NATIVE) { why = "16-bit storage not built yet"; return SW_ERR_UNSUPPORTED; }
     bool ok = (c->T == SW_FLOAT32 && c->Tprog == SW_FLOAT32) || (c->T == SW_FLOAT64 && c->Tprog == SW_FLOAT64) ||
@@ -810,8 +853,9 @@ unsigned step_key(const sw_ctx* ctx, long long i) {
     const bool tail_now = (i % c.nstep_diff) == 0;
     const bool tracer_now = c.tracer_advection && (i % c.nadvstep) == 0;
     const bool copy_now = c.tracer_advection && c.nadvstep > 1 && ((i + c.nadvstep_half) % c.nadvstep) == 0;
+    const bool refresh_now = c.nstep_advcor > 0 && (i % c.nstep_advcor) == 0;
     return (unsigned)ctx->p | (unsigned)ctx->sp << 1 | (unsigned)tail_now << 2 | (unsigned)tracer_now << 3 |
-           (unsigned)copy_now << 4;
+           (unsigned)copy_now << 4 | (unsigned)refresh_now << 5;
 }
 
 // One time step: replayed from a CUDA graph when possible, captured on first use.
@@ -958,6 +1002,9 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
     if (cfg->time_scheme != SW_RK)
         for (void** p : {&ctx->C.u, &ctx->C.v, &ctx->C.e})
             if ((rc = alloc(p, fb))) return rc;
+    if (cfg->dynamics == SW_NONLINEAR && cfg->nstep_advcor > 0)
+        for (void** p : {&ctx->qS, &ctx->KEuS, &ctx->KEvS})
+            if ((rc = alloc(p, ctx->nelem * ctx->tsz))) return rc;
     if ((rc = alloc(&ctx->sst[0], fb))) return rc;
     if ((rc = alloc(&ctx->sst[1], fb))) return rc;
     if (cfg->tracer_advection && cfg->nadvstep > 1) {
@@ -1038,6 +1085,9 @@ int sw_set_state(sw_ctx* ctx, const void* u, const void* v, const void* eta, con
     if ((rc = copy_in(ctx, ctx->sst[0], sst, shape_s(ctx->g)))) return rc;
     CK(cudaMemsetAsync(ctx->dst, 0, sizeof(DevStatus), ctx->stream));
     CK(cudaMemsetAsync(ctx->sched, 0, sizeof(TileSched), ctx->stream));
+    // the prologue reads the state as given, before any ghost point copy
+    // (src/time_integration.jl:20-31)
+    if ((rc = ctx->eng->prologue(ctx))) return rc;
     // ghost_points!(u,v,eta) opens every step (src/time_integration.jl:48); it is
     // idempotent after the first, so it is applied once here
     if ((rc = ctx->eng->ghost_state(ctx))) return rc;

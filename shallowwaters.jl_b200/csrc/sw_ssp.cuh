@@ -62,6 +62,7 @@ struct SspArgs {
     T g_, Fxt, Fyt;
     int cont;                                    // continuity! variant, as StageArgs::cont
     int sadourny;                                // PV_Sadourny!, as StageArgs::sadourny
+    const T* qS; const T* KEuS; const T* KEvS;   // stored advection/Coriolis terms, as StageArgs
     SField<T> eref, Feta;
     T gamma, Fetat;
     SspCoef<Tp> k;
@@ -157,7 +158,9 @@ ssp_momentum_kernel(SspArgs<T, Tp> A) {
         T q_r1;                                                     // PV! (src/PV_advection.jl:2-18)
         const T fq = A.fq.at(c, r + 1);
         T uN_r1 = T(0), hN_r1 = T(0), hNm1_r1 = T(0);
-        if (wrap) {
+        if (A.qS) {
+            q_r1 = A.qS[g.idx(c, r + 1)];                          // stored at the last refresh
+        } else if (wrap) {
             uN_r1 = cvt<T>(A.u1[g.idx(N, r + 1)]);
             hN_r1 = cvt<T>(A.e1[g.idx(N, r + 1)]) + A.H.at(N, r + 1);
             hNm1_r1 = cvt<T>(A.e1[g.idx(N - 1, r + 1)]) + A.H.at(N - 1, r + 1);
@@ -170,8 +173,8 @@ ssp_momentum_kernel(SspArgs<T, Tp> A) {
         const T U_r1 = u_r1 * (half * (h_r1 + hl_r1));              // Uflux!/Vflux! (src/rhs.jl:277-304)
         const T V_r1 = v_r1 * (half * (h_r1 + h_r));
         const T Ur_r1 = shdn(U_r1), Vl_r1 = shup(V_r1);
-        const T KEu = half * (ur_r * ur_r + u_r * u_r);             // bernoulli! (src/rhs.jl:162-180)
-        const T KEv = half * (v_r1 * v_r1 + v_r * v_r);
+        const T KEu = A.qS ? A.KEuS[g.idx(c, r)] : half * (ur_r * ur_r + u_r * u_r);             // bernoulli! (src/rhs.jl:162-180)
+        const T KEv = A.qS ? A.KEvS[g.idx(c, r)] : half * (v_r1 * v_r1 + v_r * v_r);
         const T p_r = half * (KEu + KEv) + A.g_ * e_r;
         const T pl_r = shup(p_r);
         const T s = q_r + q_r1;                                     // AHα..δ (src/PV_advection.jl:88-146)

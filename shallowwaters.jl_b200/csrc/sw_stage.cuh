@@ -53,6 +53,9 @@ struct StageArgs {
     SField<T> eref, Feta;
     T gamma, Fetat;
     int sadourny;                       // 1: PV_Sadourny! instead of PV_ArakawaHsu! (streaming kernel only)
+    // nstep_advcor > 0: q and KEu, KEv of the last refresh (sw_advcor.cuh),
+    // null otherwise (streaming kernel only)
+    const T* qS; const T* KEuS; const T* KEvS;
     GhostRule<Tp> gr;
     DevStatus* st;
 };
@@ -226,7 +229,9 @@ SWB_ROW_UNROLL
         T q_r1;
         const T fq = pfq[(r + 1 + ROW0) * fqsy];
         T uN_r1 = T(0), hN_r1 = T(0), hNm1_r1 = T(0);
-        if (wrap) {
+        if (A.qS) {
+            q_r1 = A.qS[g.idx(c, r + 1)];                          // stored at the last refresh
+        } else if (wrap) {
             uN_r1 = cvt<T>(A.u1[g.idx(N, r + 1)]);
             hN_r1 = cvt<T>(A.e1[g.idx(N, r + 1)]) + A.H.at(N, r + 1);
             hNm1_r1 = cvt<T>(A.e1[g.idx(N - 1, r + 1)]) + A.H.at(N - 1, r + 1);
@@ -243,8 +248,8 @@ SWB_ROW_UNROLL
         const T Ur_r1 = shdn(U_r1), Vl_r1 = shup(V_r1);
 
         // ---- p(c, r) = ½(KEu + KEv) + gη   (bernoulli!, src/rhs.jl:162-180)
-        const T KEu = half * (ur_r * ur_r + u_r * u_r);
-        const T KEv = half * (v_r1 * v_r1 + v_r * v_r);
+        const T KEu = A.qS ? A.KEuS[g.idx(c, r)] : half * (ur_r * ur_r + u_r * u_r);
+        const T KEv = A.qS ? A.KEvS[g.idx(c, r)] : half * (v_r1 * v_r1 + v_r * v_r);
         const T p_r = half * (KEu + KEv) + A.g_ * e_r;
         const T pl_r = shup(p_r);
 

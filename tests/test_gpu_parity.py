@@ -90,6 +90,15 @@ CASES = {
     "sadourny_nonperiodic_smag": dict(adv_scheme="Sadourny", bc="nonperiodic", diffusion="Smagorinsky"),
     "sadourny_mixed_f32_f64": dict(adv_scheme="Sadourny", T=np.float32, Tprog=np.float64),
     "sadourny_ssprk3_f64": dict(adv_scheme="Sadourny", time_scheme="SSPRK3", RKn=2, cfl=1.2, T=np.float64),
+    # advection/Coriolis terms refreshed every nstep_advcor steps (src/time_integration.jl:208-211)
+    "advcor_1": dict(nstep_advcor=1),
+    "advcor_2_smag": dict(nstep_advcor=2, diffusion="Smagorinsky"),
+    "advcor_3_nonperiodic_nstep_diff_2": dict(nstep_advcor=3, nstep_diff=2, bc="nonperiodic"),
+    "advcor_2_linear_drag": dict(nstep_advcor=2, bottom_drag="linear"),
+    "advcor_2_sadourny_f64": dict(nstep_advcor=2, adv_scheme="Sadourny", T=np.float64),
+    "advcor_ssprk2": dict(time_scheme="SSPRK2", RKs=3, cfl=1.2, nstep_advcor=1),
+    "advcor_ssprk3_n3_nonperiodic": dict(time_scheme="SSPRK3", RKn=3, cfl=2.5, nstep_advcor=1, bc="nonperiodic"),
+    "advcor_2_mixed_f32_f64": dict(nstep_advcor=2, T=np.float32, Tprog=np.float64),
 }
 
 
