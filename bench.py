@@ -284,20 +284,29 @@ def main():
     cfg = abi.make_config(S, nt=args.steps)
     static = abi.StaticFields(S)
     status = abi.SwStatus()
-    barrier()
-    t0 = time.perf_counter()
-    rc = lib.sw_time_integration(C.byref(cfg), static.ptr(), *abi.state_ptrs(*pinned), C.byref(status))
-    t_e2e = time.perf_counter() - t0
-    barrier()
-    if rc != 0:
-        raise SystemExit(f"sw_time_integration failed: {rc}")
-    t_e2e = allmax(t_e2e)
+
+    def e2e_call(c):
+        for dst, src in zip(pinned, Prog):      # the call overwrites its buffers: restore the inputs (untimed)
+            dst[...] = src
+        barrier()
+        t0 = time.perf_counter()
+        rc = lib.sw_time_integration(C.byref(c), static.ptr(), *abi.state_ptrs(*pinned), C.byref(status))
+        dt = time.perf_counter() - t0
+        barrier()
+        if rc != 0:
+            raise SystemExit(f"sw_time_integration failed: {rc}")
+        return dt
+
+    # one untimed call of W steps (first-use costs of the process), then the
+    # median of three timed calls of K steps
+    e2e_call(abi.make_config(S, nt=max(args.warmup, 1)))
+    t_e2e = allmax(statistics.median(e2e_call(cfg) for _ in range(3)))
     state_bytes = sum(a.nbytes for a in pinned)
     static_bytes = sum(a.nbytes for a in static.arrays.values())
     e2e = {"value": args.gpus * cells * args.steps / t_e2e, "unit": UNIT,
            "h2d_bytes_per_step": (state_bytes + static_bytes) / args.steps,
            "d2h_bytes_per_step": state_bytes / args.steps,
-           "call": "sw_time_integration (create + upload + run + download + destroy)"}
+           "call": "sw_time_integration (create + upload + run + download + destroy), median of 3 after 1 warm-up call"}
 
     cpu = None
     if rank == 0 and args.gpus == 1 and not args.no_cpu:

@@ -46,7 +46,7 @@ namespace {
 #define SWB_STAGE_TY 32
 #endif
 #ifndef SWB_TAIL_TY
-#define SWB_TAIL_TY 16
+#define SWB_TAIL_TY 32
 #endif
 constexpr int STAGE_TY = SWB_STAGE_TY;  // rows per warp strip of the stage kernel
 constexpr int TAIL_TY = SWB_TAIL_TY;    // rows per warp strip of the tail kernel

@@ -59,9 +59,12 @@ __device__ void tail_ring(const TailArgs<T, Tp>& A, int k0, int kstride) {
     }
 }
 
+#ifndef SWB_TAIL_MINB
+#define SWB_TAIL_MINB 1    // resident blocks per SM the register budget is sized for
+#endif
 // DRAG: enum sw_bottom_drag; SMAG: Smagorinsky (else constant νB)
 template <class T, class Tp, bool PER, int DRAG, bool SMAG, int TY>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, SWB_TAIL_MINB)
 tail_kernel(TailArgs<T, Tp> A) {
     if (A.st->stop) return;
     const Geom& g = A.g;
