@@ -58,6 +58,39 @@ struct SField {
     __device__ __forceinline__ T at(int x, int y) const { return p[(y + ROW0) * sy + (x + COL0) * sx]; }
 };
 
+// Julia's Float16 as a compute type: every +, -, *, / and sqrt is evaluated in
+// Float32 and rounded once to binary16 (what Julia does for Float16 values);
+// conversions from Float32 and Float64 round directly, ties to even.
+struct jf16 {
+    __half h;
+    jf16() = default;
+    __host__ __device__ explicit jf16(float x) : h(__float2half_rn(x)) {}
+    __host__ __device__ explicit jf16(double x) : h(__double2half(x)) {}
+    __host__ __device__ explicit jf16(int x) : h(__double2half((double)x)) {}
+    __host__ __device__ explicit operator float() const { return __half2float(h); }
+    __host__ __device__ explicit operator double() const { return (double)__half2float(h); }
+    __host__ __device__ explicit operator int() const { return (int)__half2float(h); }
+    // found by argument-dependent lookup only, so float and double calls are untouched
+    friend __device__ inline jf16 sqrt(jf16 a) { return jf16(sqrtf(float(a))); }
+    friend __device__ inline jf16 floor(jf16 a) { return jf16(floorf(float(a))); }
+    friend __device__ inline jf16 fabs(jf16 a) { return jf16(fabsf(float(a))); }
+};
+static_assert(sizeof(jf16) == 2, "jf16 must have the layout of binary16");
+__host__ __device__ inline jf16 operator+(jf16 a, jf16 b) { return jf16(float(a) + float(b)); }
+__host__ __device__ inline jf16 operator-(jf16 a, jf16 b) { return jf16(float(a) - float(b)); }
+__host__ __device__ inline jf16 operator*(jf16 a, jf16 b) { return jf16(float(a) * float(b)); }
+__host__ __device__ inline jf16 operator/(jf16 a, jf16 b) { return jf16(float(a) / float(b)); }
+__host__ __device__ inline jf16 operator-(jf16 a) { return jf16(-float(a)); }
+__host__ __device__ inline jf16& operator+=(jf16& a, jf16 b) { return a = a + b; }
+__host__ __device__ inline jf16& operator-=(jf16& a, jf16 b) { return a = a - b; }
+__host__ __device__ inline jf16& operator*=(jf16& a, jf16 b) { return a = a * b; }
+__host__ __device__ inline bool operator<(jf16 a, jf16 b) { return float(a) < float(b); }
+__host__ __device__ inline bool operator>(jf16 a, jf16 b) { return float(a) > float(b); }
+__host__ __device__ inline bool operator<=(jf16 a, jf16 b) { return float(a) <= float(b); }
+__host__ __device__ inline bool operator>=(jf16 a, jf16 b) { return float(a) >= float(b); }
+__host__ __device__ inline bool operator==(jf16 a, jf16 b) { return float(a) == float(b); }
+__host__ __device__ inline bool operator!=(jf16 a, jf16 b) { return float(a) != float(b); }
+
 // number conversion (Julia's T(x))
 template <class To, class From>
 __host__ __device__ inline To cvt(From x) { return static_cast<To>(x); }

@@ -317,8 +317,13 @@ struct Engine : EngineBase {
             else stage_launch<false, false, false>(a, nblk, s);
         }
     }
+    // the TMA stage kernel serves Float32/Float64 compute; Float16 compute runs streaming
+    static constexpr bool TMA_TYPES = !std::is_same<T, jf16>::value && !std::is_same<Tp, jf16>::value;
     template <bool PER, bool FIRST, bool LAST>
     static int stage_tma_launch(sw_ctx* ctx, const StageArgs<T, Tp>& a, const StageMaps& mp) {
+      if constexpr (!TMA_TYPES) {
+        return -1;
+      } else {
         constexpr int TY = STAGE_TMA_TY, K = STAGE_TMA_K, S = STAGE_TMA_S;
         auto kern = rk_stage_tma<T, Tp, PER, FIRST, LAST, TY, K, S>;
         constexpr int smem = stage_tma_smem<T, Tp, FIRST, LAST, K, S>();
@@ -333,6 +338,7 @@ struct Engine : EngineBase {
         const int nring = std::min(RING_BLOCKS_MAX, (Ring::u_count(g.ep, g.N, g.M) + Ring::v_count(g.N) + 159) / 160);
         kern<<<npersist + nring, 160, smem, ctx->stream>>>(a, mp, npersist, ctx->sched);
         return 0;
+      }
     }
     static int stage_tma_dispatch(sw_ctx* ctx, const StageArgs<T, Tp>& a, const StageMaps& mp, bool per, bool first,
                                   bool last) {
@@ -610,7 +616,7 @@ struct Engine : EngineBase {
                 int lr = 0;
                 rc = launch(ctx, 0, [&] { lr = stage2_dispatch(ctx, a, mp, g.ep != 0, first, last); });
                 if (!rc && lr) rc = fail(ctx, SW_ERR_CUDA, "packed stage kernel could not be configured");
-            } else if (ctx->use_tma && a.cont == 0 && !a.sadourny && !a.qS) {
+            } else if (TMA_TYPES && ctx->use_tma && a.cont == 0 && !a.sadourny && !a.qS) {
                 StageMaps mp;
                 mp.in_u = ctx->tmaps[in.u].in; mp.in_v = ctx->tmaps[in.v].in; mp.in_e = ctx->tmaps[in.e].in;
                 mp.x_u = ctx->tmaps[X.u].x; mp.x_v = ctx->tmaps[X.v].x; mp.x_e = ctx->tmaps[X.e].x;
@@ -780,7 +786,8 @@ int check_config(const sw_config* c, std::string& why) {
     if (c->surface_relax && c->surface_forcing) { why = "surface_relax and surface_forcing are exclusive"; return SW_ERR_ARG; }
     if (c->storage != SW_STORE_NATIVE) { why = "16-bit storage not built yet"; return SW_ERR_UNSUPPORTED; }
     bool ok = (c->T == SW_FLOAT32 && c->Tprog == SW_FLOAT32) || (c->T == SW_FLOAT64 && c->Tprog == SW_FLOAT64) ||
-              (c->T == SW_FLOAT32 && c->Tprog == SW_FLOAT64);
+              (c->T == SW_FLOAT32 && c->Tprog == SW_FLOAT64) || (c->T == SW_FLOAT16 && c->Tprog == SW_FLOAT32) ||
+              (c->T == SW_FLOAT16 && c->Tprog == SW_FLOAT16);
     if (!ok) { why = "(T, Tprog) pair not built"; return SW_ERR_UNSUPPORTED; }
     return SW_OK;
 }
@@ -1067,8 +1074,12 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
         auto* e = new Engine<float, float>(); ctx->eng.reset(e); if ((rc = e->init(ctx))) return rc;
     } else if (cfg->T == SW_FLOAT64 && cfg->Tprog == SW_FLOAT64) {
         auto* e = new Engine<double, double>(); ctx->eng.reset(e); if ((rc = e->init(ctx))) return rc;
-    } else {
+    } else if (cfg->T == SW_FLOAT32 && cfg->Tprog == SW_FLOAT64) {
         auto* e = new Engine<float, double>(); ctx->eng.reset(e); if ((rc = e->init(ctx))) return rc;
+    } else if (cfg->T == SW_FLOAT16 && cfg->Tprog == SW_FLOAT32) {
+        auto* e = new Engine<jf16, float>(); ctx->eng.reset(e); if ((rc = e->init(ctx))) return rc;
+    } else {
+        auto* e = new Engine<jf16, jf16>(); ctx->eng.reset(e); if ((rc = e->init(ctx))) return rc;
     }
     CK(cudaStreamSynchronize(ctx->stream));
     *out = holder.release();

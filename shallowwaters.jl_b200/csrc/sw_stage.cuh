@@ -96,6 +96,8 @@ template <class T>
 __device__ __forceinline__ T shup(T x) { return __shfl_up_sync(0xffffffffu, x, 1); }
 template <class T>
 __device__ __forceinline__ T shdn(T x) { return __shfl_down_sync(0xffffffffu, x, 1); }
+__device__ __forceinline__ jf16 shup(jf16 x) { jf16 r; r.h = __shfl_up_sync(0xffffffffu, x.h, 1); return r; }
+__device__ __forceinline__ jf16 shdn(jf16 x) { jf16 r; r.h = __shfl_down_sync(0xffffffffu, x.h, 1); return r; }
 
 // Ring: untouched halo cells of X1' / X0 (see sw_ghost.cuh)
 template <class T, class Tp>

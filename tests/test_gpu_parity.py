@@ -99,6 +99,15 @@ CASES = {
     "advcor_ssprk2": dict(time_scheme="SSPRK2", RKs=3, cfl=1.2, nstep_advcor=1),
     "advcor_ssprk3_n3_nonperiodic": dict(time_scheme="SSPRK3", RKn=3, cfl=2.5, nstep_advcor=1, bc="nonperiodic"),
     "advcor_2_mixed_f32_f64": dict(nstep_advcor=2, T=np.float32, Tprog=np.float64),
+    # Float16 compute with Julia's Float16 arithmetic (test/runtests.jl:37)
+    "float16_T_f32_prog": dict(T=np.float16, Tprog=np.float32),
+    "float16_all": dict(T=np.float16, Tprog=np.float16),
+    "float16_nonperiodic_smag": dict(T=np.float16, Tprog=np.float32, bc="nonperiodic", diffusion="Smagorinsky",
+                                     topography="seamount"),
+    "float16_ssprk2_advcor": dict(T=np.float16, Tprog=np.float32, time_scheme="SSPRK2", RKs=3, cfl=1.2,
+                                  nstep_advcor=1),
+    "float16_tracer_every_30_linear_drag": dict(T=np.float16, Tprog=np.float32, Uadv=2.0, Ndays=1,
+                                                bottom_drag="linear"),
 }
 
 
