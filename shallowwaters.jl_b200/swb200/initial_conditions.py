@@ -193,13 +193,16 @@ def initial_conditions(Tprog, S: ModelSetup, *, u0=None, v0=None, η0=None, sst0
     ``u0, v0, η0, sst0`` optionally replace the interior fields (no halo, in
     Float64 or Tprog) before they are rounded to Tprog and the halo is added;
     this is how seeded synthetic inputs enter, since the reference has no hook
-    for custom initial states.  ``initial_cond == "ncfile"`` (NetCDF restart)
-    is not supported by this host.
+    for custom initial states.  ``initial_cond == "ncfile"`` reads u, v, η (and
+    sst with ``sst_initial == "restart"``) from a previous run's NetCDF output
+    (src/initial_conditions.jl:39-120,144-150; ``output.read_restart``).
     """
     P, G = S.parameters, S.grid
-    if P.initial_cond != "rest" and u0 is None:
-        raise NotImplementedError("initial_cond='ncfile' (NetCDF restart) is not supported; "
-                                  "pass the restart fields as u0, v0, η0, sst0")
+    if P.initial_cond == "ncfile" and u0 is None:
+        from .output import read_restart
+        u0, v0, η0, sst_r = read_restart(S)
+        if sst0 is None and sst_r is not None:
+            sst0 = sst_r
     u = np.zeros((G.nuy, G.nux)) if u0 is None else np.asarray(u0)
     v = np.zeros((G.nvy, G.nvx)) if v0 is None else np.asarray(v0)
     η = np.zeros((G.ny, G.nx)) if η0 is None else np.asarray(η0)

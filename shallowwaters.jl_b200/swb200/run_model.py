@@ -64,7 +64,51 @@ def run_model(T=np.float32, P: Parameter | None = None, **kwargs) -> PrognosticV
         P = P.replace(**kwargs)
     S = model_setup(P)
     Prog = initial_conditions(P.Tprog, S, **init)
-    out, status = time_integration(Prog, S, storage=storage, storage_scale_uv=scale)
+    if P.output:
+        out, status = _time_integration_with_output(Prog, S, storage=storage, storage_scale_uv=scale)
+    else:
+        out, status = time_integration(Prog, S, storage=storage, storage_scale_uv=scale)
     if status.code == abi.SW_NAN_DETECTED:
         print(f" NaNs detected at time step {status.nan_step}")
     return out
+
+
+def _time_integration_with_output(Prog: PrognosticVars, S: ModelSetup, *, storage="native",
+                                  storage_scale_uv=1024.0):
+    """The time loop with output_nc! every nout steps (src/time_integration.jl:41,233):
+    the state stays on the GPU and is read back only for the frames."""
+    from .model import Model
+    from .output import NcFiles
+    G = S.grid
+    nc = NcFiles(S)
+    m = Model(S, storage=storage, storage_scale_uv=storage_scale_uv)
+    try:
+        m.set_state(Prog)
+        state = m.get_state()
+        nc.write(0, state, state)                       # output_nc!(0, ...) of the initial state
+        i = 0
+        status = abi.SwStatus()
+        while i < G.nt:
+            n = min(G.nout - i % G.nout, G.nt - i)
+            if (i + n) % G.nout == 0:
+                # the frame needs the state one step before it for du, dv, dη
+                if n > 1:
+                    status = m.run(n - 1)
+                    if status.code != abi.SW_OK:
+                        break
+                before = m.get_state()
+                status = m.run(1)
+                if status.code != abi.SW_OK:
+                    break
+                i += n
+                nc.write(i, m.get_state(), before)
+            else:
+                status = m.run(n)
+                if status.code != abi.SW_OK:
+                    break
+                i += n
+        u, v, η, sst = m.get_state()
+    finally:
+        nc.close()
+        m.close()
+    return PrognosticVars(*remove_halo(u, v, η, sst, S)), status

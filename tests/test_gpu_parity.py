@@ -236,3 +236,38 @@ def test_diagnostics_fp64_reductions():
     np.testing.assert_allclose(d.energy, energy, rtol=1e-12)
     assert d.max_speed == max(np.abs(uu[:, :-1]).max(), np.abs(vv[:-1]).max())
     assert d.nan_count == 0
+
+
+def test_output_frames_match_oracle(tmp_path):
+    """run_model(output=true): each frame is the state after step k*nout, the
+    du frame the change over that step (src/output.jl:63-133)."""
+    import os
+    from scipy.io import netcdf_file
+    from swb200.initial_conditions import remove_halo
+    P = Parameter(nx=40, Ndays=0.3, Uadv=1000, output=True, outpath=str(tmp_path), output_dt=1,
+                  output_vars=["u", "η", "sst", "du"])
+    S = model_setup(P)
+    init = seeded_inputs(S, 8)
+    out = run_model(P, **init)
+    nout, nt = S.grid.nout, S.grid.nt
+    path = os.path.join(str(tmp_path), "run0000")
+
+    def frames(name):
+        with netcdf_file(os.path.join(path, name + ".nc"), "r", mmap=False) as nc:
+            return np.array(nc.variables[name][:], dtype=np.float32), np.array(nc.variables["t"][:], dtype=np.int64)
+
+    u, t = frames("u")
+    du, _ = frames("du")
+    assert len(t) == nt // nout + 1
+    np.testing.assert_array_equal(t, np.arange(len(t)) * nout * S.grid.dtint)
+    o = O.Oracle(S)
+    o.set_state(initial_conditions(P.Tprog, S, **init))
+    k = 2
+    o.run(k * nout - 1)
+    before = remove_halo(*o.get_state(), S)[0].astype(np.float32)
+    o.run(1)
+    after = remove_halo(*o.get_state(), S)[0].astype(np.float32)
+    assert_bitwise(u[k], after, "u frame")
+    assert_bitwise(du[k], after - before, "du frame")
+    if nt % nout == 0:
+        assert_bitwise(u[-1], out.u.astype(np.float32), "last frame")
