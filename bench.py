@@ -165,6 +165,38 @@ def cpu_run(S, Prog, threads, target_s, max_steps):
 
 
 # --------------------------------------------------------------- main
+def bench_ensemble(args, rank, world, barrier, allmax):
+    """Aggregate cell-updates/s of a seeded ensemble of uneven members (nx in
+    {64..256}, L_ratio 1-2, periodic / nonperiodic), sharded over the ranks and
+    run ``--threads`` at a time per GPU, next to the same members run one at a
+    time (N = 1 only).  Each rank's span is taken between device
+    synchronisations; the job time is the maximum over ranks."""
+    from swb200.ensemble import COLUMNS, c4_members, member_cost, run_ensemble, run_local
+    members = c4_members(args.members, seed=2024, Ndays=args.days)
+    costs = [member_cost(m) for m in members]
+    run_local(c4_members(2, seed=1, Ndays=0.05), threads=2)          # warm-up: module load, graphs
+    barrier()
+    table, secs = run_ensemble(members, threads=args.threads, costs=costs)
+    barrier()
+    t = allmax(secs)
+    value = sum(costs) / t
+    seq = None
+    if world == 1:
+        t0 = time.perf_counter()
+        run_local(members, threads=1)
+        seq = sum(costs) / (time.perf_counter() - t0)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "ensemble cell-updates/s", "value": value, "unit": UNIT, "n_gpus": world,
+            "higher_is_better": True, "scaling": "strong", "dtype": "f32", "data": "synthetic (seeded members)",
+            "config": {"workload": f"{len(members)} members, nx in {{64..256}}, L_ratio 1-2, periodic/nonperiodic, "
+                                   f"{args.days} days each", "members_per_gpu_at_once": args.threads,
+                       "cell_updates": int(sum(costs)), "parallelism": f"members sharded over {world} GPU(s)"},
+            "seconds": t, "sequential_value": seq,
+            "nan_members": int((table[:, COLUMNS.index("nan_count")] > 0).sum())}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -174,6 +206,11 @@ def main():
     ap.add_argument("--nx", type=int, default=2048)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="channel", choices=["channel", "ensemble"],
+                    help="channel: the 2048x1024 headline run; ensemble: seeded members of uneven size")
+    ap.add_argument("--members", type=int, default=256)
+    ap.add_argument("--days", type=float, default=1.0, help="model days per ensemble member")
+    ap.add_argument("--threads", type=int, default=8, help="members run at once per GPU")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -240,6 +277,9 @@ def main():
         t = torch.tensor([x], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
+
+    if args.workload == "ensemble":
+        return bench_ensemble(args, rank, world, barrier, allmax)
 
     Prog = make_state(S, rng)
     m = Model(S)

@@ -179,16 +179,15 @@ constexpr int STAGE_TMA_TY = SWB_TMA_TY, STAGE_TMA_K = SWB_TMA_K, STAGE_TMA_S = 
 constexpr int STAGE2_TY = SWB_S2_TY, STAGE2_K = SWB_S2_K, STAGE2_S = SWB_S2_S;
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
-        tried = true;
+    // looked up once, thread-safely (contexts may be created from several threads)
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
         void* p = nullptr;
         cudaDriverEntryPointQueryResult q;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }
+            return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+    }();
     return fn;
 }
 
@@ -327,11 +326,15 @@ struct Engine : EngineBase {
         constexpr int TY = STAGE_TMA_TY, K = STAGE_TMA_K, S = STAGE_TMA_S;
         auto kern = rk_stage_tma<T, Tp, PER, FIRST, LAST, TY, K, S>;
         constexpr int smem = stage_tma_smem<T, Tp, FIRST, LAST, K, S>();
-        static int occ = -1;   // per instantiation
-        if (occ < 0) {
-            if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return -1;
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 160, smem) != cudaSuccess || occ < 1) return -1;
-        }
+        // per instantiation, set up once and thread-safely
+        static const int occ = [&] {
+            int o = -1;
+            if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, 160, smem) != cudaSuccess)
+                o = -1;
+            return o;
+        }();
+        if (occ < 1) return -1;
         const Geom& g = a.g;
         const int ntiles = ((g.N + BAND - 1) / BAND) * ((g.M + TY - 1) / TY);
         const int npersist = std::min(ntiles, ctx->nsm * occ);
@@ -358,11 +361,14 @@ struct Engine : EngineBase {
             constexpr int TY = STAGE2_TY, K = STAGE2_K, S = STAGE2_S;
             auto kern = rk_stage_f2<PER, FIRST, LAST, TY, K, S>;
             constexpr int smem = stage2_smem<FIRST, LAST, K, S>();
-            static int occ = -1;
-            if (occ < 0) {
-                if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return -1;
-                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 160, smem) != cudaSuccess || occ < 1) return -1;
-            }
+            static const int occ = [&] {
+                int o = -1;
+                if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
+                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, 160, smem) != cudaSuccess)
+                    o = -1;
+                return o;
+            }();
+            if (occ < 1) return -1;
             const Geom& g = a.g;
             const int ntiles = ((g.N + BAND2 - 1) / BAND2) * ((g.M + TY - 1) / TY);
             const int npersist = std::min(ntiles, ctx->nsm * occ);

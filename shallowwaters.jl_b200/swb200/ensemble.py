@@ -1,0 +1,132 @@
+"""Ensembles of independent model runs, sharded over GPUs.
+
+Members share nothing: each is a full run_model (its own grid, forcing, time
+step and step count).  Members are therefore dealt out whole, with no data
+exchange during the run.
+
+* Across GPUs: one process per GPU (torch.distributed).  Every rank computes
+  the same greedy longest-first assignment of members by their cost
+  nx*ny*nt and runs its own share.  A single FP64 all-reduce of the
+  per-member diagnostics table (mass, energy, max speed, NaN count, steps) at
+  the end is the only collective.
+* On one GPU: several members run at once.  Each member is a libswb200 context
+  with its own CUDA stream, driven from its own host thread (the library call
+  releases the GIL).  Small grids that cannot fill the GPU alone then overlap.
+
+``c4_members`` builds the seeded ensemble of uneven sizes used for
+measurements: nx in {64, 96, 128, 192, 256}, L_ratio in {1, 2}, bc alternating
+periodic / nonperiodic free-slip, Fx0 ~ U(0.05, 0.2) Pa and seeded eta noise
+sigma = 0.01 m per member.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import time
+from dataclasses import dataclass, field
+from typing import Callable, Dict, List, Optional
+
+import numpy as np
+
+COLUMNS = ("mass", "energy", "max_speed", "nan_count", "steps", "cells")
+
+
+@dataclass
+class Member:
+    """One ensemble member: Parameter keyword arguments and its noise seed."""
+    index: int
+    kwargs: Dict = field(default_factory=dict)
+    seed: int = 0
+
+
+def c4_members(n: int = 256, seed: int = 2024, Ndays: float = 30.0, **extra) -> List[Member]:
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        nx = int(rng.choice([64, 96, 128, 192, 256]))
+        L_ratio = int(rng.choice([1, 2]))
+        kw = dict(nx=nx, L_ratio=L_ratio, Ndays=Ndays, Fx0=float(rng.uniform(0.05, 0.2)),
+                  bc="periodic" if k % 2 == 0 else "nonperiodic", α=0.0)
+        kw.update(extra)
+        out.append(Member(k, kw, int(rng.integers(0, 2**31 - 1))))
+    return out
+
+
+def member_setup(m: Member):
+    """Parameter, ModelSetup and the seeded initial state of a member."""
+    from . import Parameter, initial_conditions, model_setup
+    P = Parameter(**m.kwargs)
+    S = model_setup(P)
+    rng = np.random.default_rng(m.seed)
+    η0 = rng.normal(0.0, 0.01, size=(S.grid.ny, S.grid.nx))
+    return P, S, initial_conditions(P.Tprog, S, η0=η0)
+
+
+def member_cost(m: Member) -> int:
+    """nx * ny * nt: the member's cell updates."""
+    from . import Parameter, model_setup
+    S = model_setup(Parameter(**m.kwargs))
+    return S.grid.nx * S.grid.ny * S.grid.nt
+
+
+def partition(costs: List[int], nranks: int) -> List[List[int]]:
+    """Greedy longest-processing-time assignment: members by decreasing cost,
+    each to the least loaded rank (lowest rank on ties).  Deterministic, so
+    every rank derives the same assignment without communicating."""
+    load = [0] * nranks
+    parts: List[List[int]] = [[] for _ in range(nranks)]
+    for i in sorted(range(len(costs)), key=lambda k: (-costs[k], k)):
+        r = min(range(nranks), key=lambda q: (load[q], q))
+        parts[r].append(i)
+        load[r] += costs[i]
+    return [sorted(p) for p in parts]
+
+
+def run_member(m: Member) -> np.ndarray:
+    """Run one member to its end on the current GPU; returns its row of COLUMNS."""
+    from .model import Model
+    P, S, Prog = member_setup(m)
+    with Model(S) as model:
+        model.set_state(Prog)
+        st = model.run(S.grid.nt)
+        d = model.diagnostics()
+    return np.array([d.mass, d.energy, d.max_speed, d.nan_count, st.steps_done, S.grid.nx * S.grid.ny],
+                    dtype=np.float64)
+
+
+def run_local(members: List[Member], threads: int = 8,
+              runner: Callable[[Member], np.ndarray] = run_member) -> Dict[int, np.ndarray]:
+    """Run members on this process's GPU, ``threads`` at a time."""
+    if threads <= 1:
+        return {m.index: runner(m) for m in members}
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+        futs = {m.index: ex.submit(runner, m) for m in members}
+        return {k: f.result() for k, f in futs.items()}
+
+
+def run_ensemble(members: List[Member], *, threads: int = 8, costs: Optional[List[int]] = None,
+                 runner: Callable[[Member], np.ndarray] = run_member):
+    """Run an ensemble over all ranks of the default process group (or alone).
+
+    Returns ``(table, seconds)``: the (len(members), len(COLUMNS)) FP64 table of
+    every member's diagnostics, identical on all ranks, and this rank's time.
+    """
+    import torch
+    import torch.distributed as dist
+    dist_on = dist.is_available() and dist.is_initialized()
+    rank, world = (dist.get_rank(), dist.get_world_size()) if dist_on else (0, 1)
+    if costs is None:
+        costs = [member_cost(m) for m in members]
+    mine = [members[i] for i in partition(costs, world)[rank]]
+    t0 = time.perf_counter()
+    local = run_local(mine, threads, runner)
+    seconds = time.perf_counter() - t0
+    table = np.zeros((len(members), len(COLUMNS)), dtype=np.float64)
+    pos = {m.index: k for k, m in enumerate(members)}
+    for idx, row in local.items():
+        table[pos[idx]] = row
+    if dist_on and world > 1:
+        dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+        t = torch.from_numpy(table).to(dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)      # each row is non-zero on exactly one rank
+        table = t.cpu().numpy()
+    return table, seconds
