@@ -44,22 +44,13 @@ STEP_BYTES_PER_CELL = 264
 
 
 def workload_params(nx=2048, seed=1234):
-    rng = np.random.default_rng(seed)
-    Fx0 = float(rng.uniform(0.08, 0.16))
-    kw = dict(nx=nx, L_ratio=2, bc="periodic", wind_forcing_x="channel", Fx0=Fx0, topography="flat", H=500,
-              g=10, cfl=1, time_scheme="RK", RKo=4, adv_scheme="ArakawaHsu", diffusion="Smagorinsky",
-              bottom_drag="quadratic", tracer_advection=True, Uadv=1000, Ndays=100)
-    return kw, rng
+    from swb200.precision import channel_params
+    return channel_params(nx, seed)
 
 
 def make_state(S, rng):
-    from swb200 import initial_conditions
-    G = S.grid
-    eta = rng.normal(0.0, 0.01, (G.ny, G.nx))
-    i = np.arange(G.nx)[None, :]
-    j = np.arange(G.ny)[:, None]
-    sst = np.where(((i // 10) + (j // 10)) % 2 == 0, 1.0, -1.0)
-    return initial_conditions(S.parameters.Tprog, S, η0=eta, sst0=sst)
+    from swb200.precision import channel_state
+    return channel_state(S, rng)
 
 
 # ------------------------------------------------------------------ clocks
@@ -211,6 +202,8 @@ def main():
     ap.add_argument("--members", type=int, default=256)
     ap.add_argument("--days", type=float, default=1.0, help="model days per ensemble member")
     ap.add_argument("--threads", type=int, default=8, help="members run at once per GPU")
+    ap.add_argument("--form", default="fp32", choices=["fp32", "bf16", "f16"],
+                    help="state storage between steps: plain FP32 or compensated 16-bit pairs (u, v scaled by 2^10)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -226,7 +219,7 @@ def main():
     cells = G.nx * G.ny
     config = {"workload": f"periodic wind-driven channel {G.nx}x{G.ny}, RK4, Arakawa-Hsu, Smagorinsky, "
                           f"quadratic drag, tracer every step",
-              "nx": G.nx, "ny": G.ny, "dtint_s": G.dtint, "form": "fp32",
+              "nx": G.nx, "ny": G.ny, "dtint_s": G.dtint, "form": args.form,
               "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{args.gpus}",
               "step_launch": "one CUDA graph per time step"}
     base = {"metric": METRIC, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -282,7 +275,8 @@ def main():
         return bench_ensemble(args, rank, world, barrier, allmax)
 
     Prog = make_state(S, rng)
-    m = Model(S)
+    storage = {"fp32": "native", "bf16": "bf16", "f16": "f16"}[args.form]
+    m = Model(S, storage=storage)
     m.set_state(Prog)
     m.run(args.warmup)
 
@@ -321,7 +315,7 @@ def main():
         dst[...] = src
     import ctypes as C
     lib = abi.load_library()
-    cfg = abi.make_config(S, nt=args.steps)
+    cfg = abi.make_config(S, nt=args.steps, storage=storage)
     static = abi.StaticFields(S)
     status = abi.SwStatus()
 
@@ -339,7 +333,7 @@ def main():
 
     # one untimed call of W steps (first-use costs of the process), then the
     # median of three timed calls of K steps
-    e2e_call(abi.make_config(S, nt=max(args.warmup, 1)))
+    e2e_call(abi.make_config(S, nt=max(args.warmup, 1), storage=storage))
     t_e2e = allmax(statistics.median(e2e_call(cfg) for _ in range(3)))
     state_bytes = sum(a.nbytes for a in pinned)
     static_bytes = sum(a.nbytes for a in static.arrays.values())

@@ -34,6 +34,7 @@
 #include "sw_ssp.cuh"
 #include "sw_linear.cuh"
 #include "sw_advcor.cuh"
+#include "sw_storage.cuh"
 #include "sw_diag.cuh"
 #include "sw_tail.cuh"
 #include "sw_tracer.cuh"
@@ -81,6 +82,7 @@ struct EngineBase {
     virtual int nan_check(sw_ctx* ctx, long long i) = 0;     // the check of step i (state before it)
     virtual int diagnostics(sw_ctx* ctx, sw_diag* out) = 0;
     virtual int prologue(sw_ctx* ctx) = 0;                   // work of time_integration before its loop
+    virtual int store_round_state(sw_ctx* ctx) = 0;          // 16-bit storage form of the current state
     virtual int ghost_state(sw_ctx* ctx) = 0;
 };
 
@@ -231,34 +233,44 @@ int launch(sw_ctx* ctx, int kind, F&& f) {
     return SW_OK;
 }
 
-// ghost points on every source cell of u, v, eta (used once on an uploaded state)
+// ghost points of u, v, eta: the rule of every cell whose value some halo cell
+// copies (the source cells of sw_ghost.cuh) and of the untouched ring cells,
+// enumerated directly so the launch touches only the domain's edges
 template <class Tp>
 __global__ void ghost_state_kernel(Geom g, Tp* u, Tp* v, Tp* e, GhostRule<Tp> gr) {
     const int N = g.N, M = g.M, ep = g.ep;
-    long long nu_in = (long long)(ep ? N : N - 1) * M, nv_in = (long long)N * (M - 1), ne = (long long)N * M;
-    long long nur = Ring::u_count(ep, N, M), nvr = Ring::v_count(N);
-    long long tot = nu_in + nv_in + ne + nur + nvr;
+    const int nux = ep ? N : N - 1;
+    // u sources: periodic columns F in {0, 1, N-2, N-1}; nonperiodic rows b in {0, 1, M-2, M-1}
+    const long long nus = ep ? 4LL * M : 4LL * nux;
+    const long long nvs = 4LL * (M - 1);                   // v: columns a in {0, 1, N-2, N-1}, G in [1, M)
+    const long long nes = 2LL * N + 2LL * (M - 2);         // eta: the perimeter of the T-cells
+    const long long nur = Ring::u_count(ep, N, M), nvr = Ring::v_count(N);
+    const long long tot = nus + nvs + nes + nur + nvr;
+    auto edge4 = [](int k, int n) { return k < 2 ? k : n - 4 + k; };   // 0, 1, n-2, n-1
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < tot; k += (long long)gridDim.x * blockDim.x) {
         long long r = k;
-        if (r < nu_in) {
-            int w = ep ? N : N - 1;
-            int F = (int)(r % w) + (1 - ep), b = (int)(r / w);
+        if (r < nus) {
+            int F, b;
+            if (ep) { F = edge4((int)(r / M), N); b = (int)(r % M); }
+            else { b = edge4((int)(r / nux), M); F = (int)(r % nux) + 1; }
             gr.u(u, g, F, b, u[g.idx(F, b)]);
             continue;
         }
-        r -= nu_in;
-        if (r < nv_in) {
-            int a = (int)(r % N), G = (int)(r / N) + 1;
+        r -= nus;
+        if (r < nvs) {
+            const int a = edge4((int)(r / (M - 1)), N), G = (int)(r % (M - 1)) + 1;
             gr.v(v, g, a, G, v[g.idx(a, G)]);
             continue;
         }
-        r -= nv_in;
-        if (r < ne) {
-            int a = (int)(r % N), b = (int)(r / N);
+        r -= nvs;
+        if (r < nes) {
+            int a, b;
+            if (r < 2LL * N) { a = (int)(r % N); b = r < N ? 0 : M - 1; }
+            else { const int q = (int)(r - 2LL * N); a = q < M - 2 ? 0 : N - 1; b = q % (M - 2) + 1; }
             gr.eta(e, g, a, b, e[g.idx(a, b)]);
             continue;
         }
-        r -= ne;
+        r -= nes;
         if (r < nur) {
             int F, b;
             Ring::u_at((int)r, ep, N, M, F, b);
@@ -703,7 +715,36 @@ struct Engine : EngineBase {
             }
         }
 
+        // ------------------------------- 16-bit storage form (sw_storage.cuh)
+        if (c.storage != SW_STORE_NATIVE)
+            if (int rc = store_round(ctx, Y)) return rc;
         return SW_OK;
+    }
+
+    // rounds the state F (and the current tracer) to the 16-bit storage form
+    // in place, then re-applies the ghost rules to the rounded interior
+    int store_round(sw_ctx* ctx, const Fields3& F) {
+        if constexpr (std::is_same<T, float>::value && std::is_same<Tp, float>::value) {
+            const sw_config& c = ctx->cfg;
+            const float s = (float)c.storage_scale_uv, inv = 1.0f / s;
+            int rc = launch(ctx, 5, [&] {
+                auto args = [&](auto kern) {
+                    kern<<<4 * ctx->nsm, 256, 0, ctx->stream>>>((float*)F.u, (float*)F.v, (float*)F.e,
+                                                                  (float*)ctx->sst[ctx->sp], (long long)ctx->nelem, s, inv);
+                };
+                if (c.storage == SW_STORE_BF16) args(store_round_kernel<__nv_bfloat16>);
+                else args(store_round_kernel<__half>);
+            });
+            if (rc) return rc;
+            return launch(ctx, 5, [&] {
+                ghost_state_kernel<Tp><<<148, 256, 0, ctx->stream>>>(ctx->g, (Tp*)F.u, (Tp*)F.v, (Tp*)F.e, rule(ctx));
+            });
+        } else {
+            return fail(ctx, SW_ERR_UNSUPPORTED, "16-bit storage needs T = Tprog = Float32");
+        }
+    }
+    int store_round_state(sw_ctx* ctx) override {
+        return ctx->cfg.storage == SW_STORE_NATIVE ? SW_OK : store_round(ctx, ctx->S[ctx->p]);
     }
 
     // advection/Coriolis refresh (nstep_advcor > 0) from u, v, eta with valid
@@ -790,7 +831,18 @@ int check_config(const sw_config* c, std::string& why) {
     if (c->adv_scheme != SW_ARAKAWA_HSU && c->adv_scheme != SW_SADOURNY) { why = "unknown adv_scheme"; return SW_ERR_ARG; }
     if (c->nstep_advcor < 0) { why = "nstep_advcor must be >= 0"; return SW_ERR_ARG; }
     if (c->surface_relax && c->surface_forcing) { why = "surface_relax and surface_forcing are exclusive"; return SW_ERR_ARG; }
-    if (c->storage != SW_STORE_NATIVE) { why = "16-bit storage not built yet"; return SW_ERR_UNSUPPORTED; }
+    if (c->storage != SW_STORE_NATIVE && c->storage != SW_STORE_BF16 && c->storage != SW_STORE_F16) {
+        why = "unknown storage";
+        return SW_ERR_ARG;
+    }
+    if (c->storage != SW_STORE_NATIVE) {
+        const double s = c->storage_scale_uv;
+        int ex = 0;
+        if (!(s > 0) || std::frexp(s, &ex) != 0.5 || c->T != SW_FLOAT32 || c->Tprog != SW_FLOAT32) {
+            why = "16-bit storage needs T = Tprog = Float32 and a power-of-two storage_scale_uv";
+            return SW_ERR_ARG;
+        }
+    }
     bool ok = (c->T == SW_FLOAT32 && c->Tprog == SW_FLOAT32) || (c->T == SW_FLOAT64 && c->Tprog == SW_FLOAT64) ||
               (c->T == SW_FLOAT32 && c->Tprog == SW_FLOAT64) || (c->T == SW_FLOAT16 && c->Tprog == SW_FLOAT32) ||
               (c->T == SW_FLOAT16 && c->Tprog == SW_FLOAT16);
@@ -1108,6 +1160,7 @@ int sw_set_state(sw_ctx* ctx, const void* u, const void* v, const void* eta, con
     // ghost_points!(u,v,eta) opens every step (src/time_integration.jl:48); it is
     // idempotent after the first, so it is applied once here
     if ((rc = ctx->eng->ghost_state(ctx))) return rc;
+    if ((rc = ctx->eng->store_round_state(ctx))) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
     return SW_OK;
 }
