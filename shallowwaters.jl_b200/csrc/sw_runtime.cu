@@ -330,13 +330,13 @@ struct Engine : EngineBase {
     }
     // the TMA stage kernel serves Float32/Float64 compute; Float16 compute runs streaming
     static constexpr bool TMA_TYPES = !std::is_same<T, jf16>::value && !std::is_same<Tp, jf16>::value;
-    template <bool PER, bool FIRST, bool LAST>
+    template <bool PER, bool FIRST, bool LAST, bool ROWF>
     static int stage_tma_launch(sw_ctx* ctx, const StageArgs<T, Tp>& a, const StageMaps& mp) {
       if constexpr (!TMA_TYPES) {
         return -1;
       } else {
         constexpr int TY = STAGE_TMA_TY, K = STAGE_TMA_K, S = STAGE_TMA_S;
-        auto kern = rk_stage_tma<T, Tp, PER, FIRST, LAST, TY, K, S>;
+        auto kern = rk_stage_tma<T, Tp, PER, FIRST, LAST, TY, K, S, ROWF>;
         constexpr int smem = stage_tma_smem<T, Tp, FIRST, LAST, K, S>();
         // per instantiation, set up once and thread-safely
         static const int occ = [&] {
@@ -357,14 +357,23 @@ struct Engine : EngineBase {
     }
     static int stage_tma_dispatch(sw_ctx* ctx, const StageArgs<T, Tp>& a, const StageMaps& mp, bool per, bool first,
                                   bool last) {
+        // static fields constant along x (flat bottom, beta-plane f, zonal winds):
+        // the kernel variant that broadcasts their rows by warp shuffles
+        const bool rowf = a.H.sx == 0 && a.fq.sx == 0 && a.Fx.sx == 0 && a.Fy.sx == 0;
+        if (rowf) return stage_tma_pick<true>(ctx, a, mp, per, first, last);
+        return stage_tma_pick<false>(ctx, a, mp, per, first, last);
+    }
+    template <bool ROWF>
+    static int stage_tma_pick(sw_ctx* ctx, const StageArgs<T, Tp>& a, const StageMaps& mp, bool per, bool first,
+                              bool last) {
         if (per) {
-            if (first) return stage_tma_launch<true, true, false>(ctx, a, mp);
-            if (last) return stage_tma_launch<true, false, true>(ctx, a, mp);
-            return stage_tma_launch<true, false, false>(ctx, a, mp);
+            if (first) return stage_tma_launch<true, true, false, ROWF>(ctx, a, mp);
+            if (last) return stage_tma_launch<true, false, true, ROWF>(ctx, a, mp);
+            return stage_tma_launch<true, false, false, ROWF>(ctx, a, mp);
         }
-        if (first) return stage_tma_launch<false, true, false>(ctx, a, mp);
-        if (last) return stage_tma_launch<false, false, true>(ctx, a, mp);
-        return stage_tma_launch<false, false, false>(ctx, a, mp);
+        if (first) return stage_tma_launch<false, true, false, ROWF>(ctx, a, mp);
+        if (last) return stage_tma_launch<false, false, true, ROWF>(ctx, a, mp);
+        return stage_tma_launch<false, false, false, ROWF>(ctx, a, mp);
     }
 
     template <bool PER, bool FIRST, bool LAST>

@@ -388,7 +388,7 @@ constexpr int TMA_UNROLL = SWB_TMA_UNROLL, TMA_UNROLL_EDGE = SWB_TMA_UNROLL_EDGE
 // false for warps none of whose output cells is near a boundary: then every
 // output lane writes, nothing is a ghost source and the row loop is unrolled.
 // Returns false if a wait timed out.
-template <class T, class Tp, bool PER, bool FIRST, bool LAST, int TY, int K, int S, bool EDGE>
+template <class T, class Tp, bool PER, bool FIRST, bool LAST, int TY, int K, int S, bool EDGE, bool ROWF>
 __device__ __forceinline__ bool stage_tile(const StageArgs<T, Tp>& A, const Tp* ring, uint64_t* full, uint64_t* empty,
                                            uint32_t gbase, int cx0, int y0, int warp, int lane) {
     using SL = StageSlot<Tp, FIRST, LAST, K>;
@@ -418,18 +418,27 @@ __device__ __forceinline__ bool stage_tile(const StageArgs<T, Tp>& A, const Tp* 
         if (lane == 0) mbar_arrive(&empty[(gbase + j) % S]);
     };
 
-    // static fields: lane pointers at the row of first use, one row ahead in registers
+    // static fields.  ROWF (all four constant along x): lane k holds row
+    // y0-2+k of each, broadcast to the row being computed by warp shuffles.
+    // Otherwise lane pointers at the row of first use, one row ahead in registers.
     int r = y0 - 2;
+    static_assert(TY + 3 <= 32, "a tile's static rows must fit in one warp");
+    T tH = T(0), tfq = T(0), tFx = T(0), tFy = T(0);
+    if (ROWF) {
+        const int ry = y0 - 2 + (lane < TY + 3 ? lane : TY + 2) + ROW0;
+        tH = A.H.p[ry * Hsy]; tfq = A.fq.p[ry * fqsy]; tFx = A.Fx.p[ry * Fxsy]; tFy = A.Fy.p[ry * Fysy];
+    }
     const T* __restrict__ pH = A.H.p + (r + 1 + ROW0) * Hsy + cb * A.H.sx;
     const T* __restrict__ pfq = A.fq.p + (r + 1 + ROW0) * fqsy + cb * A.fq.sx;
     const T* __restrict__ pFx = A.Fx.p + (r + ROW0) * Fxsy + cb * A.Fx.sx;
     const T* __restrict__ pFy = A.Fy.p + (r + ROW0) * Fysy + cb * A.Fy.sx;
-    T nH = *pH, nfq = *pfq, nFx = *pFx, nFy = *pFy;
+    T nH = T(0), nfq = T(0), nFx = T(0), nFy = T(0);
+    if (!ROWF) { nH = *pH; nfq = *pfq; nFx = *pFx; nFy = *pFy; }
 
     const Tp* pin = slot_ptr(0) + sc_in;        // input row 0 of the tile
     T u_r = cvt<T>(pin[SL::U]), v_r = cvt<T>(pin[SL::V]), e_r = cvt<T>(pin[SL::E]);
     Tp Xu_r = pin[SL::U], Xv_r = pin[SL::V], Xe_r = pin[SL::E];   // raw row r (X of the first stage)
-    T h_r = e_r + A.H.at(c, r);
+    T h_r = e_r + (ROWF ? __shfl_sync(0xffffffffu, tH, 0) : A.H.at(c, r));
     T hl_r = shup(h_r), ur_r = shdn(u_r);
     T U_r = u_r * (half * (h_r + hl_r));
     T Ur_r = shdn(U_r);
@@ -455,9 +464,15 @@ __device__ __forceinline__ bool stage_tile(const StageArgs<T, Tp>& A, const Tp* 
             pin += BOXW_IN;
         }
         const Tp rawu = pin[SL::U], rawv = pin[SL::V], rawe = pin[SL::E];
-        const T fq = nfq, H1 = nH, Fxr = nFx, Fyr = nFy;
-        pH += Hsy; pfq += fqsy; pFx += Fxsy; pFy += Fysy;
-        nH = *pH; nfq = *pfq; nFx = *pFx; nFy = *pFy;
+        T fq, H1, Fxr, Fyr;
+        if (ROWF) {          // rows r+1 (H, f_q) and r (Fx, Fy) of the tile's lane table
+            fq = __shfl_sync(0xffffffffu, tfq, i + 1); H1 = __shfl_sync(0xffffffffu, tH, i + 1);
+            Fxr = __shfl_sync(0xffffffffu, tFx, i); Fyr = __shfl_sync(0xffffffffu, tFy, i);
+        } else {
+            fq = nfq; H1 = nH; Fxr = nFx; Fyr = nFy;
+            pH += Hsy; pfq += fqsy; pFx += Fxsy; pFy += Fysy;
+            nH = *pH; nfq = *pfq; nFx = *pFx; nFy = *pFy;
+        }
         // X/X0 row (index i)
         if (i > 0) {
             if (i % K == 0) px = slot_ptr(i / K) + sc_x;
@@ -560,7 +575,7 @@ __device__ __forceinline__ bool stage_tile(const StageArgs<T, Tp>& A, const Tp* 
 #ifndef SWB_TMA_MINB
 #define SWB_TMA_MINB 6     // resident blocks per SM the register budget is sized for
 #endif
-template <class T, class Tp, bool PER, bool FIRST, bool LAST, int TY, int K, int S>
+template <class T, class Tp, bool PER, bool FIRST, bool LAST, int TY, int K, int S, bool ROWF>
 __global__ void __launch_bounds__(160, SWB_TMA_MINB)
 rk_stage_tma(const __grid_constant__ StageArgs<T, Tp> A, const __grid_constant__ StageMaps MP, int npersist,
              TileSched* sched) {
@@ -663,8 +678,8 @@ rk_stage_tma(const __grid_constant__ StageArgs<T, Tp> A, const __grid_constant__
         // y boundaries)?  Interior warps run without any of those tests.
         const int cw = cx0 + warp * STRIP;               // column of output lane 2
         const bool edge = cw <= 1 || cw + STRIP - 1 >= N - 2 || y0 <= 1 || y0 + TY - 1 >= M - 2;
-        const bool ok = edge ? stage_tile<T, Tp, PER, FIRST, LAST, TY, K, S, true>(A, ring, full, empty, gbase, cx0, y0, warp, lane)
-                             : stage_tile<T, Tp, PER, FIRST, LAST, TY, K, S, false>(A, ring, full, empty, gbase, cx0, y0, warp, lane);
+        const bool ok = edge ? stage_tile<T, Tp, PER, FIRST, LAST, TY, K, S, true, ROWF>(A, ring, full, empty, gbase, cx0, y0, warp, lane)
+                             : stage_tile<T, Tp, PER, FIRST, LAST, TY, K, S, false, ROWF>(A, ring, full, empty, gbase, cx0, y0, warp, lane);
         if (!ok) return;
     }
 }
