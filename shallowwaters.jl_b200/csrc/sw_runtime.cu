@@ -50,7 +50,14 @@ namespace {
 #define SWB_TAIL_TY 32
 #endif
 constexpr int STAGE_TY = SWB_STAGE_TY;  // rows per warp strip of the stage kernel
-constexpr int TAIL_TY = SWB_TAIL_TY;    // rows per warp strip of the tail kernel
+constexpr int TAIL_TY = SWB_TAIL_TY;
+#ifndef SWB_TAIL_TMA_TY
+#define SWB_TAIL_TMA_TY 24
+#endif
+#ifndef SWB_TAIL_TMA_S
+#define SWB_TAIL_TMA_S 4
+#endif
+constexpr int TAIL_TMA_TY = SWB_TAIL_TMA_TY, TAIL_TMA_S = SWB_TAIL_TMA_S;    // rows per warp strip of the tail kernel
 constexpr int PADX = 72, PADY = 44;     // column/row padding: strips read up to TY+3 rows and 30 columns past the edge
 constexpr int RING_BLOCKS_MAX = 32;
 
@@ -110,6 +117,7 @@ struct sw_ctx {
     std::map<const void*, Maps> tmaps;
     bool use_tma = false;
     bool packed = false;          // FP32x2 stage kernel for Float32 (opt-in: SWB200_PACKED=1)
+    bool tail_tma = false;        // TMA-fed tail for Float32 (opt-in: SWB200_TAIL_TMA=1; measured slower)
     // CUDA graphs of one time step, keyed by the buffer parities and the
     // sub-steps that are due (see step_key); off with SWB200_GRAPHS=0
     bool use_graphs = true;
@@ -416,6 +424,43 @@ struct Engine : EngineBase {
     static void tail_launch(const TailArgs<T, Tp>& a, int nblk, cudaStream_t s) {
         tail_kernel<T, Tp, PER, DRAG, SMAG, TAIL_TY><<<nblk, 128, 0, s>>>(a);
     }
+    // TMA-fed tail (Float32): returns -1 if it cannot be configured
+    template <bool PER, int DRAG, bool SMAG, bool ROWH>
+    static int tail_tma_launch(sw_ctx* ctx, const TailArgs<T, Tp>& a, const TailMaps& mp) {
+        if constexpr (std::is_same<T, float>::value && std::is_same<Tp, float>::value) {
+            constexpr int TY = TAIL_TMA_TY, K = STAGE_TMA_K, S = TAIL_TMA_S;
+            constexpr bool QUAD = DRAG == SW_DRAG_QUADRATIC;
+            auto kern = tail_tma<PER, DRAG, SMAG, TY, K, S, ROWH>;
+            constexpr int smem = tail_tma_smem<K, S, QUAD>();
+            static const int occ = [&] {
+                int o = -1;
+                if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
+                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, 160, smem) != cudaSuccess)
+                    o = -1;
+                return o;
+            }();
+            if (occ < 1) return -1;
+            const Geom& g = a.g;
+            const int ntiles = ((g.N + BAND - 1) / BAND) * ((g.M + TY - 1) / TY);
+            const int npersist = std::min(ntiles, ctx->nsm * occ);
+            const int nring = std::min(RING_BLOCKS_MAX, (Ring::u_count(g.ep, g.N, g.M) + Ring::v_count(g.N) + 159) / 160);
+            kern<<<npersist + nring, 160, smem, ctx->stream>>>(a, mp, npersist, ctx->sched);
+            return 0;
+        } else {
+            return -1;
+        }
+    }
+    template <bool PER, bool ROWH>
+    static int tail_tma_dispatch(sw_ctx* ctx, const TailArgs<T, Tp>& a, const TailMaps& mp, int drag, bool smag) {
+        if (smag) {
+            if (drag == SW_DRAG_QUADRATIC) return tail_tma_launch<PER, SW_DRAG_QUADRATIC, true, ROWH>(ctx, a, mp);
+            if (drag == SW_DRAG_LINEAR) return tail_tma_launch<PER, SW_DRAG_LINEAR, true, true>(ctx, a, mp);
+            return tail_tma_launch<PER, SW_DRAG_NONE, true, true>(ctx, a, mp);
+        }
+        if (drag == SW_DRAG_QUADRATIC) return tail_tma_launch<PER, SW_DRAG_QUADRATIC, false, ROWH>(ctx, a, mp);
+        if (drag == SW_DRAG_LINEAR) return tail_tma_launch<PER, SW_DRAG_LINEAR, false, true>(ctx, a, mp);
+        return tail_tma_launch<PER, SW_DRAG_NONE, false, true>(ctx, a, mp);
+    }
     template <bool PER>
     static void tail_dispatch2(const TailArgs<T, Tp>& a, int drag, bool smag, int nblk, cudaStream_t s) {
         if (smag) {
@@ -681,10 +726,26 @@ struct Engine : EngineBase {
             a.st = ctx->dst;
             const int nb = (nsx * nsy + 3) / 4 + nring;
             const bool smag = (c.diffusion == SW_DIFF_SMAGORINSKY);
-            int rc = launch(ctx, 1, [&] {
-                if (g.ep) tail_dispatch2<true>(a, c.bottom_drag, smag, nb, ctx->stream);
-                else tail_dispatch2<false>(a, c.bottom_drag, smag, nb, ctx->stream);
-            });
+            constexpr bool F32 = std::is_same<T, float>::value && std::is_same<Tp, float>::value;
+            int rc;
+            if (F32 && ctx->use_tma && ctx->tail_tma) {
+                TailMaps mp;
+                mp.u = ctx->tmaps[ctx->Acc.u].in; mp.v = ctx->tmaps[ctx->Acc.v].in; mp.e = ctx->tmaps[Y.e].in;
+                const bool rowh = ctx->H.sx == 0;
+                int lr = 0;
+                rc = launch(ctx, 1, [&] {
+                    if (g.ep) lr = rowh ? tail_tma_dispatch<true, true>(ctx, a, mp, c.bottom_drag, smag)
+                                        : tail_tma_dispatch<true, false>(ctx, a, mp, c.bottom_drag, smag);
+                    else lr = rowh ? tail_tma_dispatch<false, true>(ctx, a, mp, c.bottom_drag, smag)
+                                   : tail_tma_dispatch<false, false>(ctx, a, mp, c.bottom_drag, smag);
+                });
+                if (!rc && lr) rc = fail(ctx, SW_ERR_CUDA, "TMA tail kernel could not be configured");
+            } else {
+                rc = launch(ctx, 1, [&] {
+                    if (g.ep) tail_dispatch2<true>(a, c.bottom_drag, smag, nb, ctx->stream);
+                    else tail_dispatch2<false>(a, c.bottom_drag, smag, nb, ctx->stream);
+                });
+            }
             if (rc) return rc;
             // bottom_drag_quadratic! leaves its KEu, KEv (of u0) for the next stages
             if (ctx->qS && c.bottom_drag == SW_DRAG_QUADRATIC)
@@ -1132,6 +1193,8 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
                 ctx->tmaps[p] = mp;
             }
         ctx->use_tma = ok;
+        const char* envt = getenv("SWB200_TAIL_TMA");
+        ctx->tail_tma = (envt && envt[0] == '1');
         const char* envg = getenv("SWB200_GRAPHS");
         ctx->use_graphs = !(envg && envg[0] == '0');
         const char* envp = getenv("SWB200_PACKED");
