@@ -226,7 +226,15 @@ int sw_run_timed(sw_ctx* ctx, int64_t nsteps, int64_t l2_flush_bytes,
                  double* step_ms_total, sw_status* status);
 /* Number of CUDA kernel launches the library has issued on this context. */
 int64_t sw_kernel_launches(const sw_ctx* ctx);
+/* Ends a context.  Its device blocks are kept by the library for reuse by
+ * later contexts of the same sizes (up to 16 GiB in all), so repeated drop-in
+ * calls do not pay for cudaMalloc/cudaFree; sw_trim_memory frees them.  No
+ * reference counterpart (the reference's preallocate! arrays are freed by
+ * Julia's garbage collector). */
 void sw_destroy(sw_ctx* ctx);
+/* Returns every device and pinned block kept for reuse to CUDA.  Call it with
+ * no context in use. */
+int sw_trim_memory(void);
 
 const char* sw_strerror(int code);
 const char* sw_last_error(const sw_ctx* ctx);

@@ -23,6 +23,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -82,6 +83,74 @@ struct Fields3 { void* u = nullptr; void* v = nullptr; void* e = nullptr; };
 
 }  // namespace
 
+// Device and pinned blocks released by sw_destroy are kept for reuse by later
+// contexts of the same sizes: a drop-in call (create, run, destroy) then costs
+// no cudaMalloc/cudaFree after the first, which are slow and, for cudaFree,
+// erratic (milliseconds to a second).  At most CACHE_LIMIT bytes of device
+// memory are held; sw_trim_memory returns them all.
+namespace {
+struct BlockCache {
+    std::mutex mu;
+    std::multimap<std::pair<int, size_t>, void*> dev;   // (device, bytes) -> block
+    std::multimap<size_t, void*> pinned;
+    size_t cached = 0;
+};
+BlockCache& block_cache() {
+    static BlockCache* c = new BlockCache();   // never destroyed: may be used during process exit
+    return *c;
+}
+constexpr size_t CACHE_LIMIT = size_t(16) << 30;
+
+cudaError_t cached_malloc(void** p, size_t bytes) {
+    int d = 0;
+    cudaGetDevice(&d);
+    {
+        BlockCache& c = block_cache();
+        std::lock_guard<std::mutex> lock(c.mu);
+        auto it = c.dev.find({d, bytes});
+        if (it != c.dev.end()) {
+            *p = it->second;
+            c.dev.erase(it);
+            c.cached -= bytes;
+            return cudaSuccess;
+        }
+    }
+    return cudaMalloc(p, bytes);
+}
+void cached_free(void* p, size_t bytes) {
+    int d = 0;
+    cudaGetDevice(&d);
+    {
+        BlockCache& c = block_cache();
+        std::lock_guard<std::mutex> lock(c.mu);
+        if (c.cached + bytes <= CACHE_LIMIT) {
+            c.dev.insert({{d, bytes}, p});
+            c.cached += bytes;
+            return;
+        }
+    }
+    cudaFree(p);
+}
+cudaError_t cached_malloc_host(void** p, size_t bytes) {
+    {
+        BlockCache& c = block_cache();
+        std::lock_guard<std::mutex> lock(c.mu);
+        auto it = c.pinned.find(bytes);
+        if (it != c.pinned.end()) {
+            *p = it->second;
+            c.pinned.erase(it);
+            return cudaSuccess;
+        }
+    }
+    return cudaMallocHost(p, bytes);
+}
+void cached_free_host(void* p, size_t bytes) {
+    BlockCache& c = block_cache();
+    std::lock_guard<std::mutex> lock(c.mu);
+    c.pinned.insert({bytes, p});
+}
+}  // namespace
+
 struct sw_ctx;
 struct EngineBase {
     virtual ~EngineBase() = default;
@@ -100,7 +169,7 @@ struct sw_ctx {
     size_t tsz = 0, tpsz = 0;  // sizeof(T), sizeof(Tprog)
     cudaStream_t stream = nullptr;
     int device = 0;
-    std::vector<void*> allocs;
+    std::vector<std::pair<void*, size_t>> allocs;   // device blocks and their sizes (cached_malloc)
     Fields3 S[2], A, B, Acc;
     Fields3 C;                 // third stage buffer of the SSP schemes
     void* qS = nullptr;        // nstep_advcor > 0: stored q, KEu, KEv (type T, sw_advcor.cuh)
@@ -846,8 +915,9 @@ struct Engine : EngineBase {
 
     int diagnostics(sw_ctx* ctx, sw_diag* out) override {
         if (!ctx->diag) {
-            CK(cudaMalloc(&ctx->diag, (DIAG_BLOCKS + 1) * sizeof(DiagPartial)));
-            ctx->allocs.push_back(ctx->diag);
+            const size_t bytes = (DIAG_BLOCKS + 1) * sizeof(DiagPartial);
+            CK(cached_malloc((void**)&ctx->diag, bytes));
+            ctx->allocs.push_back({ctx->diag, bytes});
         }
         const Fields3& X = ctx->S[ctx->p];
         int rc = launch(ctx, 5, [&] {
@@ -953,8 +1023,8 @@ int upload_static(sw_ctx* ctx, sw_ctx::SF& out, const void* host, int w, int h, 
             std::memcpy(&buf[((size_t)(hy0 + j + ROW0) * g.P + (hx0 + COL0)) * ts], el(0, j), ts * (size_t)w);
         out.sx = 1; out.sy = g.P;
     }
-    CK(cudaMalloc(&out.p, buf.size()));
-    ctx->allocs.push_back(out.p);
+    CK(cached_malloc(&out.p, buf.size()));
+    ctx->allocs.push_back({out.p, buf.size()});
     CK(cudaMemcpy(out.p, buf.data(), buf.size(), cudaMemcpyHostToDevice));
     return SW_OK;
 }
@@ -1087,12 +1157,30 @@ const char* sw_last_error(const sw_ctx* ctx) { return ctx ? ctx->err.c_str() : "
 
 int64_t sw_kernel_launches(const sw_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+int sw_trim_memory(void) {
+    BlockCache& c = block_cache();
+    std::lock_guard<std::mutex> lock(c.mu);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    for (auto& kv : c.dev) {
+        cudaSetDevice(kv.first.first);
+        cudaFree(kv.second);
+    }
+    cudaSetDevice(cur);
+    for (auto& kv : c.pinned) cudaFreeHost(kv.second);
+    c.dev.clear();
+    c.pinned.clear();
+    c.cached = 0;
+    return SW_OK;
+}
+
 void sw_destroy(sw_ctx* ctx) {
     if (!ctx) return;
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second.exec);
-    for (void* p : ctx->allocs) cudaFree(p);
-    if (ctx->hst) cudaFreeHost(ctx->hst);
+    for (auto& a : ctx->allocs) cached_free(a.first, a.second);
+    if (ctx->hst) cached_free_host(ctx->hst, sizeof(DevStatus));
+    if (ctx->flush) cudaFree(ctx->flush);
     for (auto e : ctx->evpool) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -1125,8 +1213,8 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
     CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
 
     auto alloc = [&](void** p, size_t bytes) -> int {
-        CK(cudaMalloc(p, bytes));
-        ctx->allocs.push_back(*p);
+        CK(cached_malloc(p, bytes));
+        ctx->allocs.push_back({*p, bytes});
         CK(cudaMemsetAsync(*p, 0, bytes, ctx->stream));
         return SW_OK;
     };
@@ -1153,7 +1241,7 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
         if ((rc = alloc(&p, sizeof(TileSched)))) return rc;
         ctx->sched = static_cast<TileSched*>(p);
     }
-    CK(cudaMallocHost(&ctx->hst, sizeof(DevStatus)));
+    CK(cached_malloc_host((void**)&ctx->hst, sizeof(DevStatus)));
     std::memset(ctx->hst, 0, sizeof(DevStatus));
 
     const int N = g.N, M = g.M, nux = g.ep ? N : N - 1;
@@ -1182,14 +1270,16 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
         const char* env = getenv("SWB200_TMA");
         bool want = !(env && env[0] == '0');
         bool ok = want && encode_fn() != nullptr;
+        const char* envp = getenv("SWB200_PACKED");
+        ctx->packed = (envp && envp[0] == '1');
         for (Fields3* f : {&ctx->S[0], &ctx->S[1], &ctx->A, &ctx->B, &ctx->Acc})
             for (void* p : {f->u, f->v, f->e}) {
                 if (!ok) break;
                 sw_ctx::Maps mp;
                 ok = make_map(&mp.in, p, ctx->tpsz, g.P, g.R, BOXW_IN, STAGE_TMA_K) &&
                      make_map(&mp.x, p, ctx->tpsz, g.P, g.R, BOXW_X, STAGE_TMA_K) &&
-                     make_map(&mp.in2, p, ctx->tpsz, g.P, g.R, BOXW_IN2, STAGE2_K) &&
-                     make_map(&mp.x2, p, ctx->tpsz, g.P, g.R, BOXW_X2, STAGE2_K);
+                     (!ctx->packed || (make_map(&mp.in2, p, ctx->tpsz, g.P, g.R, BOXW_IN2, STAGE2_K) &&
+                                       make_map(&mp.x2, p, ctx->tpsz, g.P, g.R, BOXW_X2, STAGE2_K)));
                 ctx->tmaps[p] = mp;
             }
         ctx->use_tma = ok;
@@ -1197,8 +1287,6 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
         ctx->tail_tma = (envt && envt[0] == '1');
         const char* envg = getenv("SWB200_GRAPHS");
         ctx->use_graphs = !(envg && envg[0] == '0');
-        const char* envp = getenv("SWB200_PACKED");
-        ctx->packed = (envp && envp[0] == '1');
     }
     if (cfg->T == SW_FLOAT32 && cfg->Tprog == SW_FLOAT32) {
         auto* e = new Engine<float, float>(); ctx->eng.reset(e); if ((rc = e->init(ctx))) return rc;

@@ -184,6 +184,7 @@ EXPORTS = {
     "sw_run_timed": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.POINTER(C.c_double), C.c_void_p]),
     "sw_diagnostics_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.c_void_p, C.c_void_p]),
+    "sw_trim_memory": (C.c_int, []),
     "sw_kernel_launches": (C.c_int64, [C.c_void_p]),
     "sw_destroy": (None, [C.c_void_p]),
     "sw_strerror": (C.c_char_p, [C.c_int]),

@@ -319,3 +319,29 @@ def test_storage_form_is_a_rounded_fp32_step(form, bc):
         m.run(1)
         for x, y, name in zip(m.get_state(), ref, ("u", "v", "η", "sst")):
             assert_bitwise(x, y, f"{name} after {k} steps ({form})")
+
+
+def test_contexts_reuse_memory_and_trim():
+    """Destroyed contexts leave their blocks to the next context of the same
+    shape (zeroed again at creation); sw_trim_memory returns them to CUDA."""
+    from swb200 import abi
+    P = Parameter(nx=40, Ndays=0.2, Uadv=1000)
+    S = model_setup(P)
+    Prog = initial_conditions(P.Tprog, S, **seeded_inputs(S, 13))
+    states = []
+    for _ in range(2):
+        m = Model(S)
+        m.set_state(Prog)
+        m.run(7)
+        states.append(m.get_state())
+        m.close()
+    for x, y, name in zip(states[0], states[1], ("u", "v", "η", "sst")):
+        assert_bitwise(x, y, name)
+    lib = abi.load_library()
+    assert lib.sw_trim_memory() == abi.SW_OK
+    m = Model(S)
+    m.set_state(Prog)
+    m.run(7)
+    for x, y, name in zip(m.get_state(), states[0], ("u", "v", "η", "sst")):
+        assert_bitwise(x, y, name)
+    m.close()
