@@ -361,11 +361,15 @@ template <class Tp, bool FIRST, bool LAST, int K>
 struct StageSlot {
     static constexpr bool LOAD_X = !FIRST && !LAST;   // X read for the b update
     static constexpr bool LOAD_A = !FIRST;            // X0 read for the a update
-    static constexpr int IN = K * BOXW_IN;
-    static constexpr int XE = K * BOXW_X;
+    // each box region starts on a 128-byte boundary; the copies fill K rows of
+    // the box width densely and the rest of a region is padding
+    static constexpr int ALIGN = int(128 / sizeof(Tp));
+    static constexpr int IN = (K * BOXW_IN + ALIGN - 1) / ALIGN * ALIGN;    // region strides (elements)
+    static constexpr int XE = (K * BOXW_X + ALIGN - 1) / ALIGN * ALIGN;
     static constexpr int NX = (LOAD_X ? 3 : 0) + (LOAD_A ? 3 : 0);
-    static constexpr int ELEMS = 3 * IN + NX * XE;
-    static constexpr uint32_t BYTES = ELEMS * sizeof(Tp);
+    static constexpr int ELEMS = 3 * IN + NX * XE;                          // slot stride (elements)
+    static constexpr uint32_t BYTES = ELEMS * sizeof(Tp);                   // slot size
+    static constexpr uint32_t TX_BYTES = (3 * K * BOXW_IN + NX * K * BOXW_X) * sizeof(Tp);   // bytes copied
     static constexpr int U = 0, V = IN, E = 2 * IN;
     static constexpr int XU = 3 * IN, XV = XU + XE, XW = XV + XE;
     static constexpr int AU = 3 * IN + (LOAD_X ? 3 * XE : 0), AV = AU + XE, AW = AV + XE;
@@ -637,7 +641,7 @@ rk_stage_tma(const __grid_constant__ StageArgs<T, Tp> A, const __grid_constant__
                 const int slot = gc % S;
                 if (!acquire(slot)) { ok = false; break; }
                 slot_tile[slot] = t;
-                mbar_arrive_expect_tx(&full[slot], SL::BYTES);
+                mbar_arrive_expect_tx(&full[slot], SL::TX_BYTES);
                 Tp* b = ring + slot * SL::ELEMS;
                 const int yd = y0 - 2 + j * K + ROW0;
                 tma_load_2d(b + SL::U, &MP.in_u, cx0, yd, &full[slot]);

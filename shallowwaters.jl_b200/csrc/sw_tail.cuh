@@ -254,9 +254,10 @@ struct TailMaps {
 
 template <int K, int S, bool QUAD>
 struct TailSlot {
-    static constexpr int IN = K * BOXW_IN;
+    static constexpr int IN = (K * BOXW_IN + 31) / 32 * 32;          // region stride: 128-byte multiples
     static constexpr int ELEMS = (QUAD ? 3 : 2) * IN;
     static constexpr uint32_t BYTES = ELEMS * sizeof(float);
+    static constexpr uint32_t TX_BYTES = (QUAD ? 3 : 2) * K * BOXW_IN * sizeof(float);   // bytes copied
     static constexpr int U = 0, V = IN, E = 2 * IN;
     static_assert((IN * sizeof(float)) % 128 == 0, "TMA destinations need 128-B alignment");
 };
@@ -327,7 +328,7 @@ tail_tma(const __grid_constant__ TailArgs<float, float> A, const __grid_constant
                 const int slot = gc % S;
                 if (!acquire(slot)) { ok = false; break; }
                 slot_tile[slot] = t;
-                mbar_arrive_expect_tx(&full[slot], SL::BYTES);
+                mbar_arrive_expect_tx(&full[slot], SL::TX_BYTES);
                 float* b = ring + slot * SL::ELEMS;
                 const int yd = y0 - 3 + j * K + ROW0;
                 tma_load_2d(b + SL::U, &MP.u, cx0, yd, &full[slot]);
