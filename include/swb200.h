@@ -236,6 +236,28 @@ void sw_destroy(sw_ctx* ctx);
  * no context in use. */
 int sw_trim_memory(void);
 
+/* Ensembles advanced together: n members, each with its own config and static
+ * fields (any grid size and parameters), advanced with one kernel launch per
+ * sub-step for all members that share the boundary type and options.  Members
+ * must be Float32, RK, nonlinear, nstep_diff = 1, without nstep_advcor,
+ * seasonal wind or surface forcing (else SW_ERR_UNSUPPORTED).  Every member
+ * computes exactly what a lone context computes.  No reference counterpart
+ * (an ensemble there is a loop of run_model calls). */
+typedef struct sw_batch sw_batch;
+int sw_batch_create(int32_t n, const sw_config* cfgs, const sw_static* statics, sw_batch** out);
+/* Upload member m's state (as sw_set_state); resets the batch to step 0. */
+int sw_batch_set_state(sw_batch* b, int32_t member, const void* u, const void* v,
+                       const void* eta, const void* sst);
+/* Advance up to nsteps global steps; a member stops after its own nt steps (or
+ * a NaN stop).  statuses: n entries, the member's steps done and code. */
+int sw_batch_run(sw_batch* b, int64_t nsteps, sw_status* statuses);
+int sw_batch_get_state(sw_batch* b, int32_t member, void* u, void* v, void* eta, void* sst);
+int64_t sw_batch_launches(const sw_batch* b);
+/* Member m's context (owned by the batch: do not destroy it), e.g. for
+ * sw_diagnostics after a run. */
+sw_ctx* sw_batch_member(sw_batch* b, int32_t member);
+void sw_batch_destroy(sw_batch* b);
+
 const char* sw_strerror(int code);
 const char* sw_last_error(const sw_ctx* ctx);
 int sw_abi_version(void);

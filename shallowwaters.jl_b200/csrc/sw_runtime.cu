@@ -36,6 +36,7 @@
 #include "sw_linear.cuh"
 #include "sw_advcor.cuh"
 #include "sw_storage.cuh"
+#include "sw_batch.cuh"
 #include "sw_diag.cuh"
 #include "sw_tail.cuh"
 #include "sw_tracer.cuh"
@@ -700,6 +701,82 @@ struct Engine : EngineBase {
         return SW_OK;
     }
 
+    // The arguments of RK stage k for a step from the state S[p]: stage k reads
+    // S[p] (k = 1) or the stage buffer A/B and writes the other one; the
+    // accumulator X0 lives in Acc; the last stage puts u, v in Acc when the tail
+    // follows (else in S[1-p]) and eta in S[1-p].
+    StageArgs<T, Tp> stage_args(sw_ctx* ctx, int k, int p, bool tail_now, T Fxt, T Fyt) const {
+        const sw_config& c = ctx->cfg;
+        const Geom& g = ctx->g;
+        const Fields3& X = ctx->S[p];
+        const Fields3& Y = ctx->S[1 - p];
+        StageArgs<T, Tp> a;
+        a.g = g;
+        a.nsx = (g.N + STRIP - 1) / STRIP; a.nsy = (g.M + STAGE_TY - 1) / STAGE_TY;
+        a.nring_blocks = ring_blocks(g, 128);
+        const Fields3& in = (k == 1) ? X : ((k % 2 == 0) ? ctx->A : ctx->B);
+        const Fields3& out1 = (k % 2 == 1) ? ctx->A : ctx->B;
+        a.u1 = (const Tp*)in.u; a.v1 = (const Tp*)in.v; a.e1 = (const Tp*)in.e;
+        a.uX = (const Tp*)X.u; a.vX = (const Tp*)X.v; a.eX = (const Tp*)X.e;
+        a.u0i = (const Tp*)ctx->Acc.u; a.v0i = (const Tp*)ctx->Acc.v; a.e0i = (const Tp*)ctx->Acc.e;
+        const bool last = (k == c.RKo);
+        if (!last) { a.u1o = (Tp*)out1.u; a.v1o = (Tp*)out1.v; a.e1o = (Tp*)out1.e; }
+        else { a.u1o = a.v1o = a.e1o = nullptr; }
+        if (last) {
+            // the final X0: u, v to Acc when the tail follows, else straight into
+            // the new state; eta always into the new state (the tail keeps eta)
+            a.u0o = (Tp*)(tail_now ? ctx->Acc.u : Y.u);
+            a.v0o = (Tp*)(tail_now ? ctx->Acc.v : Y.v);
+            a.e0o = (Tp*)Y.e;
+        } else {
+            a.u0o = (Tp*)ctx->Acc.u; a.v0o = (Tp*)ctx->Acc.v; a.e0o = (Tp*)ctx->Acc.e;
+        }
+        a.H = sf<T>(ctx->H); a.fq = sf<T>(ctx->fq); a.Fx = sf<T>(ctx->Fx); a.Fy = sf<T>(ctx->Fy);
+        a.a = (Tp)c.RKaDt[k - 1];
+        a.b = (k < c.RKo) ? (Tp)c.RKbDt[k - 1] : Tp(0);
+        a.g_ = (T)c.g;
+        a.Fxt = Fxt; a.Fyt = Fyt;
+        set_cont(ctx, a);
+        a.gr = rule(ctx);
+        a.st = ctx->dst;
+        return a;
+    }
+    // The tail's arguments for a step from S[p]: u0, v0 in Acc, eta0 in S[1-p]
+    TailArgs<T, Tp> tail_args(sw_ctx* ctx, int p) const {
+        const sw_config& c = ctx->cfg;
+        const Geom& g = ctx->g;
+        const Fields3& Y = ctx->S[1 - p];
+        TailArgs<T, Tp> a;
+        a.g = g;
+        a.nsx = (g.N + STRIP - 1) / STRIP; a.nsy = (g.M + TAIL_TY - 1) / TAIL_TY;
+        a.nring_blocks = ring_blocks(g, 128);
+        a.u0 = (const Tp*)ctx->Acc.u; a.v0 = (const Tp*)ctx->Acc.v; a.e0 = (const Tp*)Y.e;
+        a.uo = (Tp*)Y.u; a.vo = (Tp*)Y.v;
+        a.H = sf<T>(ctx->H);
+        a.cD = (T)c.cD; a.rD = (T)c.rD; a.cSmag = (T)c.cSmag; a.nuB = (T)c.nuB;
+        a.Dt_diff = (Tp)c.Dt_diff;
+        a.gr = rule(ctx);
+        a.st = ctx->dst;
+        return a;
+    }
+    // The tracer's arguments for a step from S[p], reading sst[sp] and writing sst[1-sp]
+    TracerArgs<T, Tp> tracer_args(sw_ctx* ctx, int p, int sp) const {
+        const sw_config& c = ctx->cfg;
+        const Fields3& Y = ctx->S[1 - p];
+        TracerArgs<T, Tp> a;
+        a.g = ctx->g;
+        a.u = (const Tp*)Y.u; a.v = (const Tp*)Y.v;
+        a.um = (const T*)ctx->um; a.vm = (const T*)ctx->vm;
+        a.sst = (const Tp*)ctx->sst[sp];
+        a.sst_o = (Tp*)ctx->sst[1 - sp];
+        a.dtadvu = (T)c.dtadvu; a.dtadvv = (T)c.dtadvv;
+        a.half_dtadvu = (T)c.half_dtadvu; a.half_dtadvv = (T)c.half_dtadvv;
+        a.jSST = (T)c.jSST; a.SSTmin = (T)c.SSTmin;
+        a.gr = rule(ctx);
+        a.st = ctx->dst;
+        return a;
+    }
+
     int step(sw_ctx* ctx, long long i) override {
         const sw_config& c = ctx->cfg;
         const Geom& g = ctx->g;
@@ -718,33 +795,9 @@ struct Engine : EngineBase {
             if (int rc = ssp_stages(ctx, X, Y, tail_now, Fxt, Fyt)) return rc;
         } else {
         for (int k = 1; k <= c.RKo; k++) {
-            StageArgs<T, Tp> a;
-            a.g = g; a.nsx = nsx; a.nsy = nsy; a.nring_blocks = nring;
+            StageArgs<T, Tp> a = stage_args(ctx, k, ctx->p, tail_now, Fxt, Fyt);
             const Fields3& in = (k == 1) ? X : ((k % 2 == 0) ? ctx->A : ctx->B);
-            Fields3& out1 = (k % 2 == 1) ? ctx->A : ctx->B;
-            a.u1 = (const Tp*)in.u; a.v1 = (const Tp*)in.v; a.e1 = (const Tp*)in.e;
-            a.uX = (const Tp*)X.u; a.vX = (const Tp*)X.v; a.eX = (const Tp*)X.e;
-            a.u0i = (const Tp*)ctx->Acc.u; a.v0i = (const Tp*)ctx->Acc.v; a.e0i = (const Tp*)ctx->Acc.e;
             const bool first = (k == 1), last = (k == c.RKo);
-            if (!last) { a.u1o = (Tp*)out1.u; a.v1o = (Tp*)out1.v; a.e1o = (Tp*)out1.e; }
-            else { a.u1o = a.v1o = a.e1o = nullptr; }
-            if (last) {
-                // the final X0: u, v to Acc when the tail follows, else straight into
-                // the new state; eta always into the new state (the tail keeps eta)
-                a.u0o = (Tp*)(tail_now ? ctx->Acc.u : Y.u);
-                a.v0o = (Tp*)(tail_now ? ctx->Acc.v : Y.v);
-                a.e0o = (Tp*)Y.e;
-            } else {
-                a.u0o = (Tp*)ctx->Acc.u; a.v0o = (Tp*)ctx->Acc.v; a.e0o = (Tp*)ctx->Acc.e;
-            }
-            a.H = sf<T>(ctx->H); a.fq = sf<T>(ctx->fq); a.Fx = sf<T>(ctx->Fx); a.Fy = sf<T>(ctx->Fy);
-            a.a = (Tp)c.RKaDt[k - 1];
-            a.b = (k < c.RKo) ? (Tp)c.RKbDt[k - 1] : Tp(0);
-            a.g_ = (T)c.g;
-            a.Fxt = Fxt; a.Fyt = Fyt;
-            set_cont(ctx, a);
-            a.gr = rule(ctx);
-            a.st = ctx->dst;
             int rc;
             constexpr bool F32 = std::is_same<T, float>::value && std::is_same<Tp, float>::value;
             if (c.dynamics == SW_LINEAR) {
@@ -782,18 +835,8 @@ struct Engine : EngineBase {
 
         // -------------------------------------- drag + diffusion (:216-221)
         if (tail_now) {
-            TailArgs<T, Tp> a;
-            const int nsx = (g.N + STRIP - 1) / STRIP, nsy = (g.M + TAIL_TY - 1) / TAIL_TY;
-            const int nring = ring_blocks(g, 128);
-            a.g = g; a.nsx = nsx; a.nsy = nsy; a.nring_blocks = nring;
-            a.u0 = (const Tp*)ctx->Acc.u; a.v0 = (const Tp*)ctx->Acc.v; a.e0 = (const Tp*)Y.e;
-            a.uo = (Tp*)Y.u; a.vo = (Tp*)Y.v;
-            a.H = sf<T>(ctx->H);
-            a.cD = (T)c.cD; a.rD = (T)c.rD; a.cSmag = (T)c.cSmag; a.nuB = (T)c.nuB;
-            a.Dt_diff = (Tp)c.Dt_diff;
-            a.gr = rule(ctx);
-            a.st = ctx->dst;
-            const int nb = (nsx * nsy + 3) / 4 + nring;
+            TailArgs<T, Tp> a = tail_args(ctx, ctx->p);
+            const int nb = (a.nsx * a.nsy + 3) / 4 + a.nring_blocks;
             const bool smag = (c.diffusion == SW_DIFF_SMAGORINSKY);
             constexpr bool F32 = std::is_same<T, float>::value && std::is_same<Tp, float>::value;
             int rc;
@@ -832,18 +875,8 @@ struct Engine : EngineBase {
                 if (rc) return rc;
             }
             if ((i % c.nadvstep) == 0) {
-                TracerArgs<T, Tp> a;
-                a.g = g;
-                a.u = (const Tp*)Y.u; a.v = (const Tp*)Y.v;
-                a.um = (const T*)ctx->um; a.vm = (const T*)ctx->vm;
+                TracerArgs<T, Tp> a = tracer_args(ctx, ctx->p, ctx->sp);
                 const bool um_is_u = (c.nadvstep == 1);
-                a.sst = (const Tp*)ctx->sst[ctx->sp];
-                a.sst_o = (Tp*)ctx->sst[1 - ctx->sp];
-                a.dtadvu = (T)c.dtadvu; a.dtadvv = (T)c.dtadvv;
-                a.half_dtadvu = (T)c.half_dtadvu; a.half_dtadvv = (T)c.half_dtadvv;
-                a.jSST = (T)c.jSST; a.SSTmin = (T)c.SSTmin;
-                a.gr = rule(ctx);
-                a.st = ctx->dst;
                 dim3 grid((g.N + 127) / 128, std::min(g.M, 4096));
                 int rc = launch(ctx, 2, [&] {
                     if (g.ep) tracer_dispatch2<true>(a, um_is_u, c.tracer_consumption != 0, grid, ctx->stream);
@@ -1146,6 +1179,191 @@ int run_steps(sw_ctx* ctx, long long nsteps, sw_status* status) {
 
 }  // namespace
 
+// ======================================================================= batches
+// An ensemble advanced with one launch per sub-step for all members that share
+// the boundary type and options (sw_batch.cuh).  Each member is a full context
+// (its buffers, static fields and state); the batch adds the device tables of
+// every member's kernel arguments.
+struct BatchGroup {
+    int per = 1, rko = 4, drag = 0;
+    bool smag = false, um_is_u = true, cons = false, tracer_any = false;
+    std::vector<int> idx;                      // member indices
+    StageArgs<float, float>* stage[2][4] = {};  // per parity of X, per stage
+    TailArgs<float, float>* tail[2] = {};
+    TracerArgs<float, float>* tracer[2] = {};   // 2n entries: k odd, then k even
+    BatchCopy* copy[2] = {};
+    BatchNan* nan[2] = {};                      // 2n entries: even, then odd tracer count
+    BatchMember* memb = nullptr;
+    int *b_stage = nullptr, *b_tail = nullptr, *b_tracer = nullptr, *nbx_tracer = nullptr, *b_copy = nullptr,
+        *b_nan = nullptr;
+    int n_stage = 0, n_tail = 0, n_tracer = 0, n_copy = 0, n_nan = 0;
+};
+
+struct sw_batch {
+    std::vector<sw_ctx*> mem;
+    std::vector<BatchGroup> groups;
+    std::vector<std::pair<void*, size_t>> tables;
+    cudaStream_t stream = nullptr;
+    long long step = 0, max_nt = 0;
+    long long launches = 0;
+    std::string err;
+};
+
+namespace {
+
+template <class V>
+int upload_table(sw_batch* b, const std::vector<V>& host, V** dev) {
+    const size_t bytes = host.size() * sizeof(V);
+    void* p = nullptr;
+    if (cached_malloc(&p, bytes) != cudaSuccess) return SW_ERR_NOMEM;
+    b->tables.push_back({p, bytes});
+    if (cudaMemcpyAsync(p, host.data(), bytes, cudaMemcpyHostToDevice, b->stream) != cudaSuccess) return SW_ERR_CUDA;
+    *dev = static_cast<V*>(p);
+    return SW_OK;
+}
+
+std::vector<int> prefix(const std::vector<int>& counts) {
+    std::vector<int> o(counts.size() + 1, 0);
+    for (size_t k = 0; k < counts.size(); k++) o[k + 1] = o[k] + counts[k];
+    return o;
+}
+
+int batch_check(const sw_config& c, std::string& why) {
+    if (c.T != SW_FLOAT32 || c.Tprog != SW_FLOAT32) why = "batched members compute in Float32";
+    else if (c.time_scheme != SW_RK) why = "batched members use the RK schemes";
+    else if (c.dynamics != SW_NONLINEAR || c.nstep_advcor != 0) why = "batched members use nonlinear dynamics without nstep_advcor";
+    else if (c.nstep_diff != 1) why = "batched members apply drag and diffusion every step (nstep_diff = 1)";
+    else if (c.seasonal_wind_x || c.seasonal_wind_y || c.surface_forcing) why = "batched members have no time-dependent forcing";
+    else if (c.storage != SW_STORE_NATIVE) why = "batched members keep the native state storage";
+    else return SW_OK;
+    return SW_ERR_UNSUPPORTED;
+}
+
+int batch_build(sw_batch* b) {
+    using E = Engine<float, float>;
+    std::map<std::vector<int>, int> key_group;
+    for (int m = 0; m < (int)b->mem.size(); m++) {
+        const sw_config& c = b->mem[m]->cfg;
+        const std::vector<int> key = {c.periodic != 0, c.nadvstep == 1 || !c.tracer_advection, c.RKo,
+                                      c.bottom_drag, c.diffusion, c.tracer_consumption};
+        auto it = key_group.find(key);
+        if (it == key_group.end()) {
+            it = key_group.emplace(key, (int)b->groups.size()).first;
+            BatchGroup gr;
+            gr.per = c.periodic != 0;
+            gr.um_is_u = key[1] != 0;
+            gr.rko = c.RKo;
+            gr.drag = c.bottom_drag;
+            gr.smag = c.diffusion == SW_DIFF_SMAGORINSKY;
+            gr.cons = c.tracer_consumption != 0;
+            b->groups.push_back(gr);
+        }
+        b->groups[it->second].idx.push_back(m);
+    }
+    for (BatchGroup& gr : b->groups) {
+        const int n = (int)gr.idx.size();
+        std::vector<int> cs, ct, ctr, nbx, cc, cn;
+        std::vector<BatchMember> mems;
+        for (int m : gr.idx) {
+            sw_ctx* ctx = b->mem[m];
+            const Geom& g = ctx->g;
+            const sw_config& c = ctx->cfg;
+            E* e = dynamic_cast<E*>(ctx->eng.get());
+            const StageArgs<float, float> s1 = e->stage_args(ctx, 1, 0, true, 1.f, 1.f);
+            const TailArgs<float, float> t0 = e->tail_args(ctx, 0);
+            cs.push_back((s1.nsx * s1.nsy + 3) / 4 + s1.nring_blocks);
+            ct.push_back((t0.nsx * t0.nsy + 3) / 4 + t0.nring_blocks);
+            const int bx = (g.N + 127) / 128, gy = std::min(g.M, 256);
+            nbx.push_back(bx);
+            ctr.push_back(bx * gy);
+            cc.push_back(16);
+            cn.push_back(8);
+            BatchMember bm;
+            bm.nt = c.nt; bm.tracer = c.tracer_advection; bm.nadvstep = c.nadvstep;
+            bm.nadvstep_half = c.nadvstep_half; bm.nout = c.nout; bm.cells = g.N * g.M;
+            mems.push_back(bm);
+            gr.tracer_any = gr.tracer_any || c.tracer_advection;
+            b->max_nt = std::max(b->max_nt, (long long)c.nt);
+        }
+        int rc;
+        for (int p = 0; p < 2; p++) {
+            for (int k = 1; k <= gr.rko; k++) {
+                std::vector<StageArgs<float, float>> v;
+                for (int m : gr.idx)
+                    v.push_back(dynamic_cast<E*>(b->mem[m]->eng.get())->stage_args(b->mem[m], k, p, true, 1.f, 1.f));
+                if ((rc = upload_table(b, v, &gr.stage[p][k - 1]))) return rc;
+            }
+            std::vector<TailArgs<float, float>> vt;
+            std::vector<TracerArgs<float, float>> vr(2 * n);
+            std::vector<BatchCopy> vc;
+            std::vector<BatchNan> vn(2 * n);
+            for (int q = 0; q < n; q++) {
+                sw_ctx* ctx = b->mem[gr.idx[q]];
+                E* e = dynamic_cast<E*>(ctx->eng.get());
+                vt.push_back(e->tail_args(ctx, p));
+                vr[q] = e->tracer_args(ctx, p, 0);          // k odd: sst[0] -> sst[1]
+                vr[n + q] = e->tracer_args(ctx, p, 1);      // k even: sst[1] -> sst[0]
+                const Fields3& X = ctx->S[p];
+                const Fields3& Y = ctx->S[1 - p];
+                vc.push_back(BatchCopy{(const float*)Y.u, (const float*)Y.v, (float*)ctx->um, (float*)ctx->vm,
+                                       (long long)ctx->nelem, ctx->dst});
+                for (int par = 0; par < 2; par++)
+                    vn[par * n + q] = BatchNan{ctx->g, (const float*)X.u, (const float*)X.v, (const float*)X.e,
+                                               (const float*)ctx->sst[par], ctx->dst};
+            }
+            if ((rc = upload_table(b, vt, &gr.tail[p]))) return rc;
+            if ((rc = upload_table(b, vr, &gr.tracer[p]))) return rc;
+            if ((rc = upload_table(b, vc, &gr.copy[p]))) return rc;
+            if ((rc = upload_table(b, vn, &gr.nan[p]))) return rc;
+        }
+        const std::vector<int> ps = prefix(cs), pt = prefix(ct), ptr = prefix(ctr), pc = prefix(cc), pn = prefix(cn);
+        gr.n_stage = ps.back(); gr.n_tail = pt.back(); gr.n_tracer = ptr.back(); gr.n_copy = pc.back(); gr.n_nan = pn.back();
+        if ((rc = upload_table(b, ps, &gr.b_stage)) || (rc = upload_table(b, pt, &gr.b_tail)) ||
+            (rc = upload_table(b, ptr, &gr.b_tracer)) || (rc = upload_table(b, nbx, &gr.nbx_tracer)) ||
+            (rc = upload_table(b, pc, &gr.b_copy)) || (rc = upload_table(b, pn, &gr.b_nan)) ||
+            (rc = upload_table(b, mems, &gr.memb)))
+            return rc;
+    }
+    return cudaStreamSynchronize(b->stream) == cudaSuccess ? SW_OK : SW_ERR_CUDA;
+}
+
+template <bool PER>
+void batch_group_step(sw_batch* b, const BatchGroup& gr, long long i) {
+    const int p = (int)((i - 1) % 2), n = (int)gr.idx.size();
+    cudaStream_t s = b->stream;
+    for (int k = 1; k <= gr.rko; k++) {
+        const StageArgs<float, float>* a = gr.stage[p][k - 1];
+        if (k == 1) rk_stage_batch<float, float, PER, true, false, STAGE_TY><<<gr.n_stage, 128, 0, s>>>(a, gr.b_stage, n, gr.memb, i);
+        else if (k == gr.rko) rk_stage_batch<float, float, PER, false, true, STAGE_TY><<<gr.n_stage, 128, 0, s>>>(a, gr.b_stage, n, gr.memb, i);
+        else rk_stage_batch<float, float, PER, false, false, STAGE_TY><<<gr.n_stage, 128, 0, s>>>(a, gr.b_stage, n, gr.memb, i);
+    }
+    auto tail = [&](auto kern) { kern<<<gr.n_tail, 128, 0, s>>>(gr.tail[p], gr.b_tail, n, gr.memb, i); };
+    if (gr.smag) {
+        if (gr.drag == SW_DRAG_QUADRATIC) tail(tail_batch<float, float, PER, SW_DRAG_QUADRATIC, true, TAIL_TY>);
+        else if (gr.drag == SW_DRAG_LINEAR) tail(tail_batch<float, float, PER, SW_DRAG_LINEAR, true, TAIL_TY>);
+        else tail(tail_batch<float, float, PER, SW_DRAG_NONE, true, TAIL_TY>);
+    } else {
+        if (gr.drag == SW_DRAG_QUADRATIC) tail(tail_batch<float, float, PER, SW_DRAG_QUADRATIC, false, TAIL_TY>);
+        else if (gr.drag == SW_DRAG_LINEAR) tail(tail_batch<float, float, PER, SW_DRAG_LINEAR, false, TAIL_TY>);
+        else tail(tail_batch<float, float, PER, SW_DRAG_NONE, false, TAIL_TY>);
+    }
+    b->launches += gr.rko + 1;
+    if (gr.tracer_any) {
+        if (!gr.um_is_u) {
+            copy_batch<<<gr.n_copy, 256, 0, s>>>(gr.copy[p], gr.b_copy, n, gr.memb, i);
+            b->launches++;
+        }
+        auto tr = [&](auto kern) { kern<<<gr.n_tracer, 128, 0, s>>>(gr.tracer[p], gr.b_tracer, gr.nbx_tracer, n, gr.memb, i); };
+        if (gr.um_is_u) { if (gr.cons) tr(tracer_batch<float, float, PER, true, true>); else tr(tracer_batch<float, float, PER, true, false>); }
+        else { if (gr.cons) tr(tracer_batch<float, float, PER, false, true>); else tr(tracer_batch<float, float, PER, false, false>); }
+        b->launches++;
+    }
+    nan_batch<<<gr.n_nan, 256, 0, s>>>(gr.nan[p], gr.b_nan, n, gr.memb, i);
+    b->launches++;
+}
+
+}  // namespace
+
 // ======================================================================= C ABI
 extern "C" {
 
@@ -1156,6 +1374,112 @@ const char* sw_strerror(int code) { return err_name(code); }
 const char* sw_last_error(const sw_ctx* ctx) { return ctx ? ctx->err.c_str() : ""; }
 
 int64_t sw_kernel_launches(const sw_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int sw_batch_create(int32_t n, const sw_config* cfgs, const sw_static* statics, sw_batch** out) {
+    if (n < 1 || !cfgs || !statics || !out) return SW_ERR_ARG;
+    *out = nullptr;
+    std::string why;
+    for (int m = 0; m < n; m++) {
+        const int rc = batch_check(cfgs[m], why);
+        if (rc) {
+            fprintf(stderr, "swb200: batch member %d: %s\n", m, why.c_str());
+            return rc;
+        }
+    }
+    std::unique_ptr<sw_batch> b(new sw_batch());
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return SW_ERR_CUDA;
+    for (int m = 0; m < n; m++) {
+        sw_ctx* ctx = nullptr;
+        const int rc = sw_create(&cfgs[m], &statics[m], &ctx);
+        if (rc) {
+            sw_batch_destroy(b.release());
+            return rc;
+        }
+        b->mem.push_back(ctx);
+    }
+    if (const int rc = batch_build(b.get())) {
+        sw_batch_destroy(b.release());
+        return rc;
+    }
+    *out = b.release();
+    return SW_OK;
+}
+
+int sw_batch_set_state(sw_batch* b, int32_t member, const void* u, const void* v, const void* eta, const void* sst) {
+    if (!b || member < 0 || member >= (int)b->mem.size()) return SW_ERR_ARG;
+    const int rc = sw_set_state(b->mem[member], u, v, eta, sst);
+    if (rc) return rc;
+    b->step = 0;
+    return SW_OK;
+}
+
+int sw_batch_run(sw_batch* b, int64_t nsteps, sw_status* statuses) {
+    if (!b || nsteps < 0) return SW_ERR_ARG;
+    for (sw_ctx* ctx : b->mem)          // states uploaded on the members' own streams
+        if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return SW_ERR_CUDA;
+    const long long until = std::min(b->max_nt, b->step + (long long)nsteps);
+    for (long long i = b->step + 1; i <= until; i++) {
+        for (const BatchGroup& gr : b->groups) {
+            if (gr.per) batch_group_step<true>(b, gr, i);
+            else batch_group_step<false>(b, gr, i);
+        }
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) {
+        b->err = std::string("batch run: ") + cudaGetErrorString(e);
+        return SW_ERR_CUDA;
+    }
+    b->step = until;
+    int code = SW_OK;
+    for (int m = 0; m < (int)b->mem.size(); m++) {
+        sw_ctx* ctx = b->mem[m];
+        DevStatus ds;
+        if (cudaMemcpy(&ds, ctx->dst, sizeof(ds), cudaMemcpyDeviceToHost) != cudaSuccess) return SW_ERR_CUDA;
+        long long done = std::min(b->step, (long long)ctx->cfg.nt);
+        int mc = SW_OK;
+        if (ds.error) {
+            mc = ds.error;
+        } else if (ds.stop) {
+            mc = SW_NAN_DETECTED;
+            done = ds.nan_step;
+        }
+        // the member's state: before the failing step on a NaN stop, else after its last step
+        const long long last = mc == SW_NAN_DETECTED ? done - 1 : done;
+        ctx->p = (int)(last % 2);
+        ctx->sp = ctx->cfg.tracer_advection ? (int)((done / ctx->cfg.nadvstep) % 2) : 0;
+        ctx->step = done;
+        if (statuses) {
+            statuses[m].steps_done = done;
+            statuses[m].step = done;
+            statuses[m].nan_step = mc == SW_NAN_DETECTED ? done : -1;
+            statuses[m].code = mc;
+            statuses[m].reserved = 0;
+        }
+        if (mc && !code) code = mc;
+    }
+    return code;
+}
+
+int sw_batch_get_state(sw_batch* b, int32_t member, void* u, void* v, void* eta, void* sst) {
+    if (!b || member < 0 || member >= (int)b->mem.size()) return SW_ERR_ARG;
+    return sw_get_state(b->mem[member], u, v, eta, sst);
+}
+
+int64_t sw_batch_launches(const sw_batch* b) { return b ? b->launches : 0; }
+
+sw_ctx* sw_batch_member(sw_batch* b, int32_t member) {
+    return (b && member >= 0 && member < (int)b->mem.size()) ? b->mem[member] : nullptr;
+}
+
+void sw_batch_destroy(sw_batch* b) {
+    if (!b) return;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    for (auto& t : b->tables) cached_free(t.first, t.second);
+    for (sw_ctx* ctx : b->mem) sw_destroy(ctx);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
 
 int sw_trim_memory(void) {
     BlockCache& c = block_cache();

@@ -136,18 +136,18 @@ __device__ void stage_ring(const StageArgs<T, Tp>& A, bool first, bool last, int
     }
 }
 
+// The streaming stage for block bx of its grid (strip blocks, then ring blocks).
 template <class T, class Tp, bool PER, bool FIRST, bool LAST, int TY>
-__global__ void __launch_bounds__(128)
-rk_stage_kernel(StageArgs<T, Tp> A) {
+__device__ __forceinline__ void rk_stage_body(const StageArgs<T, Tp>& A, int bx) {
     if (A.st->stop) return;
     const Geom& g = A.g;
     const int nstrips = A.nsx * A.nsy;
     const int nstrip_blocks = (nstrips + 3) / 4;
-    if ((int)blockIdx.x >= nstrip_blocks) {
-        stage_ring(A, FIRST, LAST, ((int)blockIdx.x - nstrip_blocks) * 128 + threadIdx.x, A.nring_blocks * 128);
+    if (bx >= nstrip_blocks) {
+        stage_ring(A, FIRST, LAST, (bx - nstrip_blocks) * 128 + threadIdx.x, A.nring_blocks * 128);
         return;
     }
-    const int w = (int)blockIdx.x * 4 + (int)(threadIdx.x >> 5);
+    const int w = bx * 4 + (int)(threadIdx.x >> 5);
     if (w >= nstrips) return;                 // whole warp leaves together
     const int lane = threadIdx.x & 31;
     const int sx = w % A.nsx, sy = w / A.nsx;
@@ -328,6 +328,12 @@ SWB_ROW_UNROLL
     }
 }
 
+
+template <class T, class Tp, bool PER, bool FIRST, bool LAST, int TY>
+__global__ void __launch_bounds__(128)
+rk_stage_kernel(StageArgs<T, Tp> A) {
+    rk_stage_body<T, Tp, PER, FIRST, LAST, TY>(A, (int)blockIdx.x);
+}
 
 // ===========================================================================
 // TMA-fed variant.  Persistent blocks of 4 consumer warps (one 28-column strip

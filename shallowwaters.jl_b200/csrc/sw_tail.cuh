@@ -64,18 +64,18 @@ __device__ void tail_ring(const TailArgs<T, Tp>& A, int k0, int kstride) {
 #define SWB_TAIL_MINB 1    // resident blocks per SM the register budget is sized for
 #endif
 // DRAG: enum sw_bottom_drag; SMAG: Smagorinsky (else constant νB)
+// The streaming tail for block bx of its grid (strip blocks, then ring blocks).
 template <class T, class Tp, bool PER, int DRAG, bool SMAG, int TY>
-__global__ void __launch_bounds__(128, SWB_TAIL_MINB)
-tail_kernel(TailArgs<T, Tp> A) {
+__device__ __forceinline__ void tail_body(const TailArgs<T, Tp>& A, int bx) {
     if (A.st->stop) return;
     const Geom& g = A.g;
     const int nstrips = A.nsx * A.nsy;
     const int nstrip_blocks = (nstrips + 3) / 4;
-    if ((int)blockIdx.x >= nstrip_blocks) {
-        tail_ring(A, ((int)blockIdx.x - nstrip_blocks) * 128 + threadIdx.x, A.nring_blocks * 128);
+    if (bx >= nstrip_blocks) {
+        tail_ring(A, (bx - nstrip_blocks) * 128 + threadIdx.x, A.nring_blocks * 128);
         return;
     }
-    const int w = (int)blockIdx.x * 4 + (int)(threadIdx.x >> 5);
+    const int w = bx * 4 + (int)(threadIdx.x >> 5);
     if (w >= nstrips) return;
     const int lane = threadIdx.x & 31;
     const int sx = w % A.nsx, sy = w / A.nsx;
@@ -233,6 +233,12 @@ SWB_ROW_UNROLL
     }
 }
 
+
+template <class T, class Tp, bool PER, int DRAG, bool SMAG, int TY>
+__global__ void __launch_bounds__(128, SWB_TAIL_MINB)
+tail_kernel(TailArgs<T, Tp> A) {
+    tail_body<T, Tp, PER, DRAG, SMAG, TY>(A, (int)blockIdx.x);
+}
 
 // ===========================================================================
 // TMA-fed tail.  Same arithmetic and order as tail_kernel; the rows of u0, v0

@@ -65,13 +65,13 @@ __device__ __forceinline__ int axis(int k0, int xi, T xy, int lo, int hi, int n,
 }
 
 // 2-D launch: x over columns, y over rows (grid-stride in y)
+// The tracer for column block bx and rows by, by + gy, ... (128 threads).
 template <class T, class Tp, bool PER, bool UM_IS_U, bool CONS>
-__global__ void __launch_bounds__(128)
-tracer_kernel(TracerArgs<T, Tp> A) {
+__device__ __forceinline__ void tracer_body(const TracerArgs<T, Tp>& A, int bx, int by, int gy) {
     if (A.st->stop) return;
     const Geom& g = A.g;
     const int N = g.N, M = g.M;
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    const int a = bx * 128 + threadIdx.x;
     if (a >= N) return;
     const T half = T(0.5);
     int bad = 0;
@@ -79,7 +79,7 @@ tracer_kernel(TracerArgs<T, Tp> A) {
     const bool gx = a == 0 || a == N - 1;
     // element (x, y) of a field sits at (y + ROW0) * P + x + COL0
     auto at = [&](int x, int y) { return (y + ROW0) * P + x + COL0; };
-    for (int b = blockIdx.y; b < M; b += gridDim.y) {
+    for (int b = by; b < M; b += gy) {
         // departure!: u_T = Ix!(u), v_T = Iy!(v); backtraj! at half step (:75-76, :96-124)
         const int o = at(a, b);
         const T uT = half * (cvt<T>(A.u[o + 1]) + cvt<T>(A.u[o]));
@@ -143,6 +143,12 @@ tracer_kernel(TracerArgs<T, Tp> A) {
         atomicCAS(&A.st->error, 0, (int)SW_ERR_DEPARTURE);
         atomicExch(&A.st->stop, 1);
     }
+}
+
+template <class T, class Tp, bool PER, bool UM_IS_U, bool CONS>
+__global__ void __launch_bounds__(128)
+tracer_kernel(TracerArgs<T, Tp> A) {
+    tracer_body<T, Tp, PER, UM_IS_U, CONS>(A, (int)blockIdx.x, (int)blockIdx.y, (int)gridDim.y);
 }
 
 // um, vm = u0, v0 converted to T (src/tracer_advection.jl:12-17), over whole buffers

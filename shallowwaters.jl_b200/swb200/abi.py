@@ -185,6 +185,13 @@ EXPORTS = {
     "sw_diagnostics_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.c_void_p, C.c_void_p]),
     "sw_trim_memory": (C.c_int, []),
+    "sw_batch_create": (C.c_int, [C.c_int32, C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "sw_batch_set_state": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "sw_batch_run": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p]),
+    "sw_batch_get_state": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "sw_batch_launches": (C.c_int64, [C.c_void_p]),
+    "sw_batch_member": (C.c_void_p, [C.c_void_p, C.c_int32]),
+    "sw_batch_destroy": (None, [C.c_void_p]),
     "sw_kernel_launches": (C.c_int64, [C.c_void_p]),
     "sw_destroy": (None, [C.c_void_p]),
     "sw_strerror": (C.c_char_p, [C.c_int]),

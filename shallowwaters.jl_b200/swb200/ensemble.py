@@ -9,9 +9,11 @@ exchange during the run.
   nx*ny*nt and runs its own share.  A single FP64 all-reduce of the
   per-member diagnostics table (mass, energy, max speed, NaN count, steps) at
   the end is the only collective.
-* On one GPU: several members run at once.  Each member is a libswb200 context
-  with its own CUDA stream, driven from its own host thread (the library call
-  releases the GIL).  Small grids that cannot fill the GPU alone then overlap.
+* On one GPU, either as a batch (``run_batched``, sw_batch_*): one kernel
+  launch per sub-step advances every member that shares the boundary type and
+  options, so many small grids fill the GPU together; or several members at
+  once, each a libswb200 context with its own CUDA stream driven from its own
+  host thread (``run_local``; the library call releases the GIL).
 
 ``c4_members`` builds the seeded ensemble of uneven sizes used for
 measurements: nx in {64, 96, 128, 192, 256}, L_ratio in {1, 2}, bc alternating
@@ -93,6 +95,45 @@ def run_member(m: Member) -> np.ndarray:
                     dtype=np.float64)
 
 
+def run_batched(members: List[Member], lib=None, return_states: bool = False):
+    """Run members as one batch (sw_batch_*): one launch per sub-step for all
+    members sharing the boundary type and options.  Returns {index: row of
+    COLUMNS} (and the final states without halo when ``return_states``)."""
+    import ctypes as C
+    from . import abi
+    from .initial_conditions import remove_halo
+    lib = lib or abi.load_library()
+    setups = [member_setup(m) for m in members]
+    cfgs = (abi.SwConfig * len(members))(*[abi.make_config(S) for _, S, _ in setups])
+    statics = [abi.StaticFields(S) for _, S, _ in setups]
+    sts = (abi.SwStatic * len(members))(*[st.struct for st in statics])
+    b = C.c_void_p()
+    abi.check(lib, lib.sw_batch_create(len(members), cfgs, sts, C.byref(b)))
+    try:
+        states = []
+        for k, (P, S, Prog) in enumerate(setups):
+            arrs = [np.ascontiguousarray(a, dtype=P.Tprog) for a in Prog]
+            states.append(arrs)
+            abi.check(lib, lib.sw_batch_set_state(b, k, *abi.state_ptrs(*arrs)))
+        status = (abi.SwStatus * len(members))()
+        rc = lib.sw_batch_run(b, 1 << 62, status)
+        if rc not in (abi.SW_OK, abi.SW_NAN_DETECTED):
+            abi.check(lib, rc)
+        out, fin = {}, {}
+        for k, (m, (P, S, _)) in enumerate(zip(members, setups)):
+            d = abi.SwDiag()
+            abi.check(lib, lib.sw_diagnostics(lib.sw_batch_member(b, k), C.byref(d)))
+            out[m.index] = np.array([d.mass, d.energy, d.max_speed, d.nan_count, status[k].steps_done,
+                                     S.grid.nx * S.grid.ny], dtype=np.float64)
+            if return_states:
+                arrs = [np.empty_like(a) for a in states[k]]
+                abi.check(lib, lib.sw_batch_get_state(b, k, *abi.state_ptrs(*arrs)))
+                fin[m.index] = remove_halo(*arrs, S)
+    finally:
+        lib.sw_batch_destroy(b)
+    return (out, fin) if return_states else out
+
+
 def run_local(members: List[Member], threads: int = 8,
               runner: Callable[[Member], np.ndarray] = run_member) -> Dict[int, np.ndarray]:
     """Run members on this process's GPU, ``threads`` at a time."""
@@ -104,7 +145,7 @@ def run_local(members: List[Member], threads: int = 8,
 
 
 def run_ensemble(members: List[Member], *, threads: int = 8, costs: Optional[List[int]] = None,
-                 runner: Callable[[Member], np.ndarray] = run_member):
+                 runner: Callable[[Member], np.ndarray] = run_member, batched: bool = False):
     """Run an ensemble over all ranks of the default process group (or alone).
 
     Returns ``(table, seconds)``: the (len(members), len(COLUMNS)) FP64 table of
@@ -118,7 +159,7 @@ def run_ensemble(members: List[Member], *, threads: int = 8, costs: Optional[Lis
         costs = [member_cost(m) for m in members]
     mine = [members[i] for i in partition(costs, world)[rank]]
     t0 = time.perf_counter()
-    local = run_local(mine, threads, runner)
+    local = run_batched(mine) if batched and mine else run_local(mine, threads, runner)
     seconds = time.perf_counter() - t0
     table = np.zeros((len(members), len(COLUMNS)), dtype=np.float64)
     pos = {m.index: k for k, m in enumerate(members)}
