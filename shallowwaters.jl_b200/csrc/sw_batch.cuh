@@ -14,7 +14,9 @@
 //   um/vm copy    (i + nadvstep_half) % nadvstep == 0
 //   NaN check     i % nout == 0
 // The bodies are those of the single-model kernels (rk_stage_body, tail_body,
-// tracer_body), so every member computes exactly what it computes alone.
+// tracer_body), so every member computes exactly what it computes alone.  The
+// kernels read i from device memory and batch_advance moves it on, so the
+// launches of a step can be replayed from a CUDA graph.
 #pragma once
 #include "sw_stage.cuh"
 #include "sw_tail.cuh"
@@ -51,7 +53,8 @@ __device__ __forceinline__ void load_args(Args& dst, const Args* __restrict__ sr
 template <class T, class Tp, bool PER, bool FIRST, bool LAST, int TY>
 __global__ void __launch_bounds__(128)
 rk_stage_batch(const StageArgs<T, Tp>* __restrict__ args, const int* __restrict__ block0, int n,
-               const BatchMember* __restrict__ mem, long long i) {
+               const BatchMember* __restrict__ mem, const long long* __restrict__ istep) {
+    const long long i = *istep;
     __shared__ __align__(16) StageArgs<T, Tp> A;
     const int m = batch_member(block0, n, (int)blockIdx.x);
     if (i > mem[m].nt) return;
@@ -63,7 +66,8 @@ rk_stage_batch(const StageArgs<T, Tp>* __restrict__ args, const int* __restrict_
 template <class T, class Tp, bool PER, int DRAG, bool SMAG, int TY>
 __global__ void __launch_bounds__(128)
 tail_batch(const TailArgs<T, Tp>* __restrict__ args, const int* __restrict__ block0, int n,
-           const BatchMember* __restrict__ mem, long long i) {
+           const BatchMember* __restrict__ mem, const long long* __restrict__ istep) {
+    const long long i = *istep;
     __shared__ __align__(16) TailArgs<T, Tp> A;
     const int m = batch_member(block0, n, (int)blockIdx.x);
     if (i > mem[m].nt) return;
@@ -77,7 +81,8 @@ tail_batch(const TailArgs<T, Tp>* __restrict__ args, const int* __restrict__ blo
 template <class T, class Tp, bool PER, bool UM_IS_U, bool CONS>
 __global__ void __launch_bounds__(128)
 tracer_batch(const TracerArgs<T, Tp>* __restrict__ args, const int* __restrict__ block0, const int* __restrict__ nbx,
-             int n, const BatchMember* __restrict__ mem, long long i) {
+             int n, const BatchMember* __restrict__ mem, const long long* __restrict__ istep) {
+    const long long i = *istep;
     __shared__ __align__(16) TracerArgs<T, Tp> A;
     const int m = batch_member(block0, n, (int)blockIdx.x);
     const BatchMember& me = mem[m];
@@ -98,7 +103,8 @@ struct BatchCopy {     // um, vm = u0, v0 of a member (tracer with nadvstep > 1)
 
 __global__ void __launch_bounds__(256)
 copy_batch(const BatchCopy* __restrict__ args, const int* __restrict__ block0, int n,
-           const BatchMember* __restrict__ mem, long long i) {
+           const BatchMember* __restrict__ mem, const long long* __restrict__ istep) {
+    const long long i = *istep;
     const int m = batch_member(block0, n, (int)blockIdx.x);
     const BatchMember& me = mem[m];
     if (i > me.nt || !me.tracer || me.nadvstep <= 1 || ((i + me.nadvstep_half) % me.nadvstep) != 0) return;
@@ -120,7 +126,8 @@ struct BatchNan {      // nan_check_kernel's operands for one member and tracer 
 // args: per member, [m] for an even number of tracer steps so far, [n + m] for odd
 __global__ void __launch_bounds__(256)
 nan_batch(const BatchNan* __restrict__ args, const int* __restrict__ block0, int n,
-          const BatchMember* __restrict__ mem, long long i) {
+          const BatchMember* __restrict__ mem, const long long* __restrict__ istep) {
+    const long long i = *istep;
     const int m = batch_member(block0, n, (int)blockIdx.x);
     const BatchMember& me = mem[m];
     if (i > me.nt || (i % me.nout) != 0) return;
@@ -149,6 +156,11 @@ nan_batch(const BatchNan* __restrict__ args, const int* __restrict__ block0, int
         atomicCAS(&a.st->stop, 0, 1);
         a.st->nan_step = i;
     }
+}
+
+// the global step i of the next replay
+__global__ void batch_advance(long long* istep) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *istep += 1;
 }
 
 }  // namespace swb

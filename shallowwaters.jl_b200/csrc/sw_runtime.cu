@@ -1183,7 +1183,10 @@ int run_steps(sw_ctx* ctx, long long nsteps, sw_status* status) {
 // An ensemble advanced with one launch per sub-step for all members that share
 // the boundary type and options (sw_batch.cuh).  Each member is a full context
 // (its buffers, static fields and state); the batch adds the device tables of
-// every member's kernel arguments.
+// every member's kernel arguments.  A global step is replayed from one of two
+// CUDA graphs (by the parity of the step): each group's launches run on a
+// stream of its own, forked from and joined back to the batch stream, and a
+// last one-thread kernel moves the device-side step counter on.
 struct BatchGroup {
     int per = 1, rko = 4, drag = 0;
     bool smag = false, um_is_u = true, cons = false, tracer_any = false;
@@ -1204,8 +1207,12 @@ struct sw_batch {
     std::vector<BatchGroup> groups;
     std::vector<std::pair<void*, size_t>> tables;
     cudaStream_t stream = nullptr;
+    std::vector<cudaStream_t> gstreams;        // one per group
+    std::vector<cudaEvent_t> events;           // fork, then one join per group
+    long long* d_step = nullptr;               // the global step the next replay runs
+    cudaGraphExec_t graph[2] = {};             // global steps i with (i - 1) % 2 == 0, 1
     long long step = 0, max_nt = 0;
-    long long launches = 0;
+    long long launches = 0, launches_per_step[2] = {};
     std::string err;
 };
 
@@ -1324,13 +1331,26 @@ int batch_build(sw_batch* b) {
             (rc = upload_table(b, mems, &gr.memb)))
             return rc;
     }
+    if (const int rc = upload_table(b, std::vector<long long>{1}, &b->d_step)) return rc;
+    for (size_t g = 0; g <= b->groups.size(); g++) {
+        cudaEvent_t ev;
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return SW_ERR_CUDA;
+        b->events.push_back(ev);
+        if (g == b->groups.size()) break;
+        cudaStream_t st;
+        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return SW_ERR_CUDA;
+        b->gstreams.push_back(st);
+    }
     return cudaStreamSynchronize(b->stream) == cudaSuccess ? SW_OK : SW_ERR_CUDA;
 }
 
+// the launches of group gr for a global step of parity p (the step read from
+// b->d_step), on stream s; returns how many
 template <bool PER>
-void batch_group_step(sw_batch* b, const BatchGroup& gr, long long i) {
-    const int p = (int)((i - 1) % 2), n = (int)gr.idx.size();
-    cudaStream_t s = b->stream;
+int batch_group_step(sw_batch* b, const BatchGroup& gr, int p, cudaStream_t s) {
+    const int n = (int)gr.idx.size();
+    const long long* i = b->d_step;
+    int launches = 0;
     for (int k = 1; k <= gr.rko; k++) {
         const StageArgs<float, float>* a = gr.stage[p][k - 1];
         if (k == 1) rk_stage_batch<float, float, PER, true, false, STAGE_TY><<<gr.n_stage, 128, 0, s>>>(a, gr.b_stage, n, gr.memb, i);
@@ -1347,19 +1367,52 @@ void batch_group_step(sw_batch* b, const BatchGroup& gr, long long i) {
         else if (gr.drag == SW_DRAG_LINEAR) tail(tail_batch<float, float, PER, SW_DRAG_LINEAR, false, TAIL_TY>);
         else tail(tail_batch<float, float, PER, SW_DRAG_NONE, false, TAIL_TY>);
     }
-    b->launches += gr.rko + 1;
+    launches += gr.rko + 1;
     if (gr.tracer_any) {
         if (!gr.um_is_u) {
             copy_batch<<<gr.n_copy, 256, 0, s>>>(gr.copy[p], gr.b_copy, n, gr.memb, i);
-            b->launches++;
+            launches++;
         }
         auto tr = [&](auto kern) { kern<<<gr.n_tracer, 128, 0, s>>>(gr.tracer[p], gr.b_tracer, gr.nbx_tracer, n, gr.memb, i); };
         if (gr.um_is_u) { if (gr.cons) tr(tracer_batch<float, float, PER, true, true>); else tr(tracer_batch<float, float, PER, true, false>); }
         else { if (gr.cons) tr(tracer_batch<float, float, PER, false, true>); else tr(tracer_batch<float, float, PER, false, false>); }
-        b->launches++;
+        launches++;
     }
     nan_batch<<<gr.n_nan, 256, 0, s>>>(gr.nan[p], gr.b_nan, n, gr.memb, i);
-    b->launches++;
+    return launches + 1;
+}
+
+// captures the graph of a global step of parity p: fork to the group streams,
+// each group's launches, join, then batch_advance
+int batch_graph(sw_batch* b, int p) {
+    cudaStream_t s = b->stream;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return SW_ERR_CUDA;
+    int launches = 0;
+    cudaError_t e = cudaEventRecord(b->events[0], s);
+    for (size_t g = 0; g < b->groups.size() && e == cudaSuccess; g++) {
+        const BatchGroup& gr = b->groups[g];
+        cudaStream_t gs = b->gstreams[g];
+        if ((e = cudaStreamWaitEvent(gs, b->events[0], 0)) != cudaSuccess) break;
+        launches += gr.per ? batch_group_step<true>(b, gr, p, gs) : batch_group_step<false>(b, gr, p, gs);
+        if ((e = cudaEventRecord(b->events[g + 1], gs)) != cudaSuccess) break;
+        e = cudaStreamWaitEvent(s, b->events[g + 1], 0);
+    }
+    if (e == cudaSuccess) {
+        batch_advance<<<1, 32, 0, s>>>(b->d_step);
+        launches++;
+        e = cudaGetLastError();
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(s, &graph);
+    if (e == cudaSuccess) e = ec;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&b->graph[p], graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        b->err = std::string("batch graph: ") + cudaGetErrorString(e);
+        return SW_ERR_CUDA;
+    }
+    b->launches_per_step[p] = launches;
+    return SW_OK;
 }
 
 }  // namespace
@@ -1417,14 +1470,19 @@ int sw_batch_run(sw_batch* b, int64_t nsteps, sw_status* statuses) {
     if (!b || nsteps < 0) return SW_ERR_ARG;
     for (sw_ctx* ctx : b->mem)          // states uploaded on the members' own streams
         if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return SW_ERR_CUDA;
+    for (int p = 0; p < 2; p++)
+        if (!b->graph[p])
+            if (const int rc = batch_graph(b, p)) return rc;
     const long long until = std::min(b->max_nt, b->step + (long long)nsteps);
-    for (long long i = b->step + 1; i <= until; i++) {
-        for (const BatchGroup& gr : b->groups) {
-            if (gr.per) batch_group_step<true>(b, gr, i);
-            else batch_group_step<false>(b, gr, i);
-        }
+    const long long next = b->step + 1;
+    cudaError_t e = cudaMemcpyAsync(b->d_step, &next, sizeof(next), cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    for (long long i = next; i <= until && e == cudaSuccess; i++) {
+        const int p = (int)((i - 1) % 2);
+        e = cudaGraphLaunch(b->graph[p], b->stream);
+        b->launches += b->launches_per_step[p];
     }
-    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
     if (e != cudaSuccess) {
         b->err = std::string("batch run: ") + cudaGetErrorString(e);
@@ -1475,6 +1533,10 @@ sw_ctx* sw_batch_member(sw_batch* b, int32_t member) {
 void sw_batch_destroy(sw_batch* b) {
     if (!b) return;
     if (b->stream) cudaStreamSynchronize(b->stream);
+    for (cudaGraphExec_t g : b->graph)
+        if (g) cudaGraphExecDestroy(g);
+    for (cudaEvent_t ev : b->events) cudaEventDestroy(ev);
+    for (cudaStream_t st : b->gstreams) cudaStreamDestroy(st);
     for (auto& t : b->tables) cached_free(t.first, t.second);
     for (sw_ctx* ctx : b->mem) sw_destroy(ctx);
     if (b->stream) cudaStreamDestroy(b->stream);
