@@ -194,6 +194,45 @@ def bench_ensemble(args, rank, world, barrier, allmax):
     return 0
 
 
+def bench_adjoint(args):
+    """Gradient of the twin experiment's eta misfit (512 x 256 periodic channel,
+    RK4, Arakawa-Hsu, Smagorinsky, quadratic drag; observations from a run
+    with the wind perturbed by eight seeded Fourier modes): device time of
+    the adjoint's forward sweep plus reverse sweep against the time loop's own
+    forward run over the same window, both on the GPU."""
+    import numpy as np
+    from swb200 import Model
+    from swb200.adjoint import gradient, twin
+    T = {"f64": np.float64, "f32": np.float32}[args.adj_dtype]
+    n = args.adj_steps
+    S, Prog, obs, dFx = twin(nx=args.adj_nx, nsteps=n, T=T)
+    nc = args.checkpoints or n
+    gradient(S, Prog, obs, 4, ncheckpoints=4)                              # warm-up
+    with Model(S) as m:
+        m.set_state(Prog)
+        m.run(4)
+        m.set_state(Prog)
+        fwd_ms, st = m.run_timed(n)
+    t0 = time.perf_counter()
+    r = gradient(S, Prog, obs, n, ncheckpoints=nc)
+    wall = time.perf_counter() - t0
+    st_ = r.stats
+    adj_ms = st_.forward_ms + st_.reverse_ms
+    G = S.grid
+    print(json.dumps({
+        "metric": "adjoint cost / forward cost", "value": adj_ms / fwd_ms, "unit": "x", "n_gpus": 1,
+        "higher_is_better": False, "dtype": args.adj_dtype, "data": "synthetic (seeded twin experiment)",
+        "config": {"workload": f"twin experiment {G.nx}x{G.ny} periodic channel, RK4, Arakawa-Hsu, Smagorinsky, "
+                               f"quadratic drag, {n} steps, J = sum (eta_T - eta_obs)^2, gradient w.r.t. u0, v0, "
+                               f"eta0 and Fx", "checkpoints": st_.checkpoints},
+        "forward_ms": fwd_ms, "adjoint_forward_sweep_ms": st_.forward_ms, "adjoint_reverse_sweep_ms": st_.reverse_ms,
+        "adjoint_wall_s": wall, "forward_steps": st_.forward_steps, "adjoint_steps": st_.adjoint_steps,
+        "launches_per_adjoint_step": st_.launches_per_adjoint_step,
+        "launches_per_forward_step": st_.launches_per_forward_step,
+        "J": r.J, "dJ_along_dFx": float(np.sum(r.Fx * dFx))}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -203,8 +242,13 @@ def main():
     ap.add_argument("--nx", type=int, default=2048)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="channel", choices=["channel", "ensemble"],
-                    help="channel: the 2048x1024 headline run; ensemble: seeded members of uneven size")
+    ap.add_argument("--workload", default="channel", choices=["channel", "ensemble", "adjoint"],
+                    help="channel: the 2048x1024 headline run; ensemble: seeded members of uneven size; "
+                         "adjoint: the gradient of the 512x256 twin experiment")
+    ap.add_argument("--adj-steps", type=int, default=2000)
+    ap.add_argument("--adj-nx", type=int, default=512)
+    ap.add_argument("--adj-dtype", default="f64", choices=["f64", "f32"])
+    ap.add_argument("--checkpoints", type=int, default=0, help="adjoint checkpoint slots (0: one per step)")
     ap.add_argument("--members", type=int, default=256)
     ap.add_argument("--days", type=float, default=1.0, help="model days per ensemble member")
     ap.add_argument("--threads", type=int, default=8, help="members run at once per GPU")
@@ -279,6 +323,8 @@ def main():
 
     if args.workload == "ensemble":
         return bench_ensemble(args, rank, world, barrier, allmax)
+    if args.workload == "adjoint":
+        return bench_adjoint(args) if rank == 0 else 0
 
     Prog = make_state(S, rng)
     storage = {"fp32": "native", "bf16": "bf16", "f16": "f16"}[args.form]

@@ -258,6 +258,41 @@ int64_t sw_batch_launches(const sw_batch* b);
 sw_ctx* sw_batch_member(sw_batch* b, int32_t member);
 void sw_batch_destroy(sw_batch* b);
 
+/* Reverse-mode gradient (adjoint) of an eta misfit through the time loop:
+ *   J = sum over the interior i <= nx, j <= ny of (eta(i+1, j+1) after
+ *       nsteps steps - eta_obs(i, j))^2
+ * differentiated with respect to the initial state (u, v, eta with their
+ * halos, shapes above) and the wind forcing Fx (nux x M).  Replaces the
+ * ForwardDiff/ChainRules route of the Julia ecosystem, which the reference
+ * cannot take (its number types are restricted to AbstractFloat), so it has no
+ * counterpart in the reference; the forward model it differentiates is
+ * src/time_integration.jl:45-78,204-233.  Supported: T = Tprog = Tcomm in
+ * Float32 or Float64, RK2/3/4, nonlinear dynamics, Arakawa-Hsu, nstep_advcor =
+ * 0, nstep_diff = 1, any drag and diffusion, either boundary, no time-dependent
+ * forcing (else SW_ERR_UNSUPPORTED).  The tracer is passive and plays no part.
+ * Inputs and outputs are HOST buffers in T: u, v, eta the initial state,
+ * eta_obs nx x ny; g_u, g_v, g_eta (state shapes), g_Fx and eta_final (the eta
+ * after nsteps, with halo) may be NULL.  ncheckpoints >= nsteps keeps every
+ * step state on the device; fewer slots recompute states with the binomial
+ * checkpoint schedule.  The derivative of sqrt at 0 (drag and Smagorinsky at
+ * rest) is taken as 0.  Gradients are summed with atomics, so repeated calls
+ * agree to rounding, not bit for bit.  stats may be NULL. */
+typedef struct sw_adjoint_stats {
+    double forward_ms;                 /* device time of the first forward sweep      */
+    double reverse_ms;                 /* device time of the reverse sweep            */
+    int64_t forward_steps;             /* steps advanced, recomputation included      */
+    int64_t adjoint_steps;             /* adjoint steps (= nsteps)                    */
+    int32_t checkpoints;               /* state slots used                            */
+    int32_t launches_per_forward_step;
+    int32_t launches_per_adjoint_step;
+    int32_t reserved;
+} sw_adjoint_stats;
+int sw_adjoint_run(const sw_config* cfg, const sw_static* st,
+                   const void* u, const void* v, const void* eta, const void* eta_obs,
+                   int64_t nsteps, int32_t ncheckpoints, double* J,
+                   void* g_u, void* g_v, void* g_eta, void* g_Fx, void* eta_final,
+                   sw_adjoint_stats* stats);
+
 const char* sw_strerror(int code);
 const char* sw_last_error(const sw_ctx* ctx);
 int sw_abi_version(void);

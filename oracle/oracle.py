@@ -47,6 +47,9 @@ def lib():
         L.oracle_destroy.argtypes = [C.c_void_p]
         L.oracle_set_threads.argtypes = [C.c_int]
         L.oracle_set_threads.restype = C.c_int
+        L.oracle_jvp.argtypes = [C.c_void_p, C.c_void_p] + [C.c_void_p] * 8 + [C.c_int64, C.POINTER(C.c_double),
+                                                                                 C.POINTER(C.c_double)]
+        L.oracle_jvp.restype = C.c_int
         _lib = L
     return _lib
 
@@ -116,3 +119,32 @@ def run_model(T=np.float32, P=None, *, nsteps=None, **kwargs):
     o.set_state(Prog)
     st = o.run(S.grid.nt if nsteps is None else nsteps)
     return PrognosticVars(*remove_halo(*o.get_state(), S)), st
+
+
+def jvp(S, Prog, eta_obs, nsteps, du=None, dv=None, deta=None, dFx=None):
+    """(J, dJ) with J = sum over the interior of (eta after nsteps - eta_obs)^2
+    and dJ its directional derivative along (du, dv, deta, dFx) (state shapes
+    with halo, dFx (nuy, nux); None is zero), from the restated loop run with
+    forward-mode dual numbers.  Float64 setups only."""
+    cfg = abi.make_config(S, nt=nsteps)
+    st = abi.StaticFields(S)
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in list(Prog)[:3]]
+    dirs = [None if d is None else np.ascontiguousarray(d, dtype=np.float64) for d in (du, dv, deta, dFx)]
+    obs = np.ascontiguousarray(eta_obs, dtype=np.float64)
+    J, dJ = C.c_double(), C.c_double()
+    ptr = lambda a: None if a is None else a.ctypes.data  # noqa: E731
+    rc = lib().oracle_jvp(C.byref(cfg), st.ptr(), *[a.ctypes.data for a in arrs], *[ptr(d) for d in dirs],
+                          obs.ctypes.data, int(nsteps), C.byref(J), C.byref(dJ))
+    if rc:
+        raise RuntimeError(f"oracle_jvp failed ({rc}): {lib().oracle_last_error(None).decode()}")
+    return J.value, dJ.value
+
+
+def cost(S, Prog, eta_obs, nsteps):
+    """J = sum over the interior of (eta after nsteps - eta_obs)^2 from the
+    restated loop in S's number type (summed in float64)."""
+    o = Oracle(S)
+    o.set_state(Prog)
+    o.run(nsteps)
+    e = remove_halo(*o.get_state(), S)[2].astype(np.float64)
+    return float(np.sum((e - np.asarray(eta_obs, np.float64)) ** 2))

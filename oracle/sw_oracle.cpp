@@ -174,4 +174,50 @@ int oracle_time_integration(const sw_config* cfg, const sw_static* st, void* u, 
     return rc;
 }
 
+
+// Directional derivative of J = sum over the interior of (eta after nsteps -
+// eta_obs)^2 along (du, dv, deta, dFx), by running the restated time loop
+// with the forward-mode Dual number type (value and derivative carried
+// together; sqrt'(0) = 0).  This is the check of the library's adjoint
+// (sw_adjoint_run): <gradient, direction> must equal *dJ.  cfg must be
+// Float64 (T = Tprog); static fields and the state are double arrays in the
+// swb200.h shapes, eta_obs is nx x ny.  du, dv, deta, dFx may be NULL (zero).
+int oracle_jvp(const sw_config* cfg, const sw_static* st, const double* u, const double* v, const double* eta,
+               const double* du, const double* dv, const double* deta, const double* dFx,
+               const double* eta_obs, int64_t nsteps, double* J, double* dJ) {
+    try {
+        if (!cfg || !st || !u || !v || !eta || !eta_obs || !J || !dJ) return SW_ERR_ARG;
+        if (cfg->T != SW_FLOAT64 || cfg->Tprog != SW_FLOAT64) return SW_ERR_ARG;
+        sw_static none{};
+        Model<Dual, Dual> M(*cfg, none);
+        auto fill = [](Arr<Dual>& a, const void* p, const double* d) {
+            if (!p) return;
+            const double* x = static_cast<const double*>(p);
+            for (size_t k = 0; k < a.size(); k++) a[k] = Dual(x[k], d ? d[k] : 0.0);
+        };
+        fill(M.f_q, st->f_q, nullptr); fill(M.f_u, st->f_u, nullptr); fill(M.f_v, st->f_v, nullptr);
+        fill(M.Fx, st->Fx, dFx); fill(M.Fy, st->Fy, nullptr); fill(M.H, st->H, nullptr);
+        fill(M.eta_ref, st->eta_ref, nullptr); fill(M.Feta, st->Feta, nullptr);
+        fill(M.u, u, du); fill(M.v, v, dv); fill(M.eta, eta, deta);
+        M.step = 0;
+        M.t = 0;
+        M.prologue();
+        int64_t nan_step = -1;
+        M.run(nsteps, &nan_step);
+        if (nan_step >= 0) return SW_NAN_DETECTED;
+        Dual s(0.0, 0.0);
+        for (int j = 1; j <= M.ny; j++)
+            for (int i = 1; i <= M.nx; i++) {
+                const Dual d = M.eta(i + 1, j + 1) - Dual(eta_obs[(size_t)(i - 1) + (size_t)(j - 1) * M.nx], 0.0);
+                s = s + d * d;
+            }
+        *J = s.v;
+        *dJ = s.d;
+        return SW_OK;
+    } catch (std::exception& e) {
+        g_err = e.what();
+        return SW_ERR_ARG;
+    }
+}
+
 }  // extern "C"

@@ -1,0 +1,1206 @@
+// sw_adjoint.cu -- reverse-mode gradient of an eta misfit through the time loop.
+//
+//   J = sum over the interior of (eta after nsteps - eta_obs)^2
+//
+// differentiated with respect to the initial state (u, v, eta with their
+// halos) and the wind forcing Fx.  The forward model is the RK branch of
+// time_integration (src/time_integration.jl:45-78 and the tail :204-233) with
+// nonlinear dynamics, Arakawa-Hsu PV advection, quadratic / linear / no bottom
+// drag and Smagorinsky / constant biharmonic diffusion, periodic or
+// nonperiodic boundaries.  The tracer is passive (it never feeds back into
+// u, v, eta), so it plays no part in J.
+//
+// Layout: every field is kept in the reference's own array shape (Julia
+// (i, j), x fastest, 1-based, no padding), one device array per reference
+// array, so each kernel below is the reference pass it cites and its adjoint.
+// Forward passes recompute the reference's intermediate arrays exactly (same
+// operation order; built with --fmad=false), so the recomputed forward state
+// is bit-identical with the time loop's.  Each reverse pass is the transpose
+// of one forward pass written in scatter form: for every output point it adds
+// (output adjoint) x (partial derivative) into the adjoints of the inputs it
+// read, with atomicAdd where several outputs share an input.  The summation
+// order of those atomics is not fixed, so gradients agree between runs to
+// rounding, not bit for bit.
+//
+// sqrt at zero (quadratic drag sqrt(KEu + KEv), src/bottom_drag.jl:48, and
+// the Smagorinsky coefficient sqrt(DS + DT), src/diffusion.jl:106): the
+// derivative is taken as 0 there, which is the derivative of the |u|u forms
+// at rest.
+//
+// Time window: the step states are kept in device memory at checkpoints;
+// with fewer checkpoint slots than steps, the reverse sweep recomputes the
+// missing states from the nearest checkpoint with the binomial schedule
+// (Griewank and Walther, "Algorithm 799: Revolve", ACM TOMS 26 (2000)).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "swb200.h"
+
+namespace swa {
+
+#ifdef SWA_HOST_CHECK
+#define SWA_BOUNDS
+#endif
+#ifdef SWA_BOUNDS
+// host check build: every array access outside its reference shape is counted
+// (and redirected to a scratch element) instead of being performed
+extern long long swa_bounds_failures;
+#endif
+
+template <class T>
+struct A2 {
+    T* d = nullptr;
+    int m = 0, n = 0;
+    __host__ __device__ __forceinline__ T& operator()(int i, int j) const {
+#if defined(SWA_BOUNDS) && !defined(__CUDA_ARCH__)
+        if (i < 1 || i > m || j < 1 || j > n || !d) {
+            static T scratch;
+            if (swa_bounds_failures++ < 8) fprintf(stderr, "swa: (%d, %d) outside %d x %d\n", i, j, m, n);
+            return scratch;
+        }
+#endif
+        return d[(i - 1) + (long long)(j - 1) * m];
+    }
+    size_t size() const { return (size_t)m * (size_t)n; }
+};
+
+template <class T>
+__host__ __device__ __forceinline__ void add(T& r, T x) {
+#ifdef __CUDA_ARCH__
+    atomicAdd(&r, x);
+#else
+    r += x;
+#endif
+}
+
+template <class T>
+__host__ __device__ __forceinline__ T sqrt_(T x) {
+#ifdef __CUDA_ARCH__
+    return sqrt(x);
+#else
+    return std::sqrt(x);
+#endif
+}
+
+// one thread per point (i, j) of an m x n range, 1-based
+template <class F>
+__global__ void __launch_bounds__(256) for2d(int m, int n, F f) {
+    const int i = (int)(blockIdx.x * 32 + threadIdx.x) + 1;
+    const int j = (int)(blockIdx.y * 8 + threadIdx.y) + 1;
+    if (i <= m && j <= n) f(i, j);
+}
+
+template <class F>
+__global__ void __launch_bounds__(256) for1d(long long n, F f) {
+    for (long long k = blockIdx.x * 256LL + threadIdx.x; k < n; k += (long long)gridDim.x * 256LL) f(k);
+}
+
+// Issues the passes on a stream (or, in the host check build, runs them in
+// loops on the host).
+struct Launcher {
+    cudaStream_t s;
+    bool host = false;
+    int launches = 0;
+    template <class F>
+    void d2(int m, int n, F f) {
+        if (host) {
+            for (int j = 1; j <= n; j++)
+                for (int i = 1; i <= m; i++) f(i, j);
+        } else {
+            dim3 g((unsigned)((m + 31) / 32), (unsigned)((n + 7) / 8)), b(32, 8);
+            for2d<<<g, b, 0, s>>>(m, n, f);
+        }
+        launches++;
+    }
+    template <class F>
+    void d1(long long n, F f) {
+        if (host) {
+            for (long long k = 0; k < n; k++) f(k);
+        } else {
+            const long long nb = std::min<long long>((n + 255) / 256, 148LL * 16);
+            for1d<<<(unsigned)std::max<long long>(nb, 1), 256, 0, s>>>(n, f);
+        }
+        launches++;
+    }
+    void zero(void* p, size_t bytes) {
+        if (host) std::memset(p, 0, bytes);
+        else cudaMemsetAsync(p, 0, bytes, s);
+    }
+    void copy(void* dst, const void* src, size_t bytes) {
+        if (host) std::memcpy(dst, src, bytes);
+        else cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, s);
+    }
+};
+
+// the three prognostic fields of one state, contiguous in one block
+template <class T>
+struct State {
+    A2<T> u, v, e;
+    T* base = nullptr;
+    size_t elems = 0;
+};
+
+template <class T>
+struct Work {
+    int nx, ny, nux, nuy, nvx, nvy, ep, rko;
+    T g, cD, rD, cSmag, nuB, Dt_diff, oma;   // oma = 1 - alpha (Tprog = T)
+    T RKa[4], RKb[3];
+    int drag, diff;
+    // static fields
+    A2<T> H, f_q, Fx, Fy;
+    // states
+    State<T> X;                 // the state being advanced (in / out of a step)
+    State<T> Ys[4];             // stage inputs after their ghost points; Ys[0] = ghosted start state
+    State<T> Z;                 // RK result after ghost points = the tail's input
+    State<T> Xb, acc, Yb[2];    // adjoints: of the step output / input, of the stage inputs
+    // stage intermediates (src/preallocate.jl:70-152, 227-254)
+    A2<T> hu, hv, hq, U, V, q, qa, qb, qc, qd, p;
+    // their adjoints
+    A2<T> bU, bV, bp, bqa, bqb, bqc, bqd, bq, bhu, bhv, bhq;
+    // tail intermediates (src/preallocate.jl:193-222, 259-338)
+    A2<T> thu, thv, sKE, sKEu, sKEv, Bu, Bv, Lu, Lv, dLudx, dLudy, dLvdx, dLvdy, sDT, sDS, DSq, rS, nuS, nuSq, S11,
+        S12, S21, S22;
+    A2<T> bBu, bBv, bS11, bS12, bS21, bS22, bnuS, bnuSq, bdLudx, bdLudy, bdLvdx, bdLvdy, bLu, bLv, bsKE, bsKEu,
+        bsKEv, bthu, bthv, bDS, bDT, bDSq;
+    A2<T> bFx;                  // gradient with respect to Fx
+    T* stage_adj = nullptr; size_t stage_adj_elems = 0;   // bU..bhq, one block (zeroed per stage)
+    T* tail_adj = nullptr; size_t tail_adj_elems = 0;     // bBu..bDSq, one block (zeroed per step)
+};
+
+// ------------------------------------------------------------ ghost points
+// ghost_points! (src/ghost_points.jl:182-199) on u, v (and eta); with uv_only
+// only ghost_points_uv! (:202-216).  Two launches: eta's y-halo rows copy the
+// x-halo columns written by the first (src/ghost_points.jl:119-133).
+template <class T>
+void ghost(Launcher& L, const Work<T>& w, const State<T>& s, bool uv_only) {
+    const A2<T> u = s.u, v = s.v, e = s.e;
+    const int ep = w.ep;
+    const T c = w.oma;
+    const int nmax = std::max(std::max(u.m, u.n), std::max(std::max(v.m, v.n), std::max(e.m, e.n)));
+    L.d1(nmax, [=] __host__ __device__(long long k) {
+        const int t = (int)k + 1;
+        if (ep) {
+            if (t <= u.n) { const int m = u.m; u(1, t) = u(m - 3, t); u(2, t) = u(m - 2, t); u(m - 1, t) = u(3, t); u(m, t) = u(4, t); }
+            if (t <= v.n) { const int m = v.m; v(1, t) = v(m - 3, t); v(2, t) = v(m - 2, t); v(m - 1, t) = v(3, t); v(m, t) = v(4, t); }
+            if (!uv_only && t <= e.n) { const int m = e.m; e(1, t) = e(m - 1, t); e(m, t) = e(2, t); }
+        } else {
+            if (t <= u.m) { const int n = u.n; u(t, 1) = c * u(t, 4); u(t, 2) = c * u(t, 3); u(t, n - 1) = c * u(t, n - 2); u(t, n) = c * u(t, n - 3); }
+            if (t <= v.n) { const int m = v.m; v(1, t) = c * v(4, t); v(2, t) = c * v(3, t); v(m - 1, t) = c * v(m - 2, t); v(m, t) = c * v(m - 3, t); }
+            if (!uv_only && t <= e.n) { const int m = e.m; e(1, t) = e(2, t); e(m, t) = e(m - 1, t); }
+        }
+    });
+    if (uv_only) return;
+    L.d1(e.m, [=] __host__ __device__(long long k) {
+        const int i = (int)k + 1, n = e.n;
+        e(i, 1) = e(i, 2);
+        e(i, n) = e(i, n - 1);
+    });
+}
+
+// transpose of ghost(): each halo adjoint is added onto its source and cleared
+template <class T>
+void ghostT(Launcher& L, const Work<T>& w, const State<T>& s, bool uv_only) {
+    const A2<T> u = s.u, v = s.v, e = s.e;
+    const int ep = w.ep;
+    const T c = w.oma;
+    const T zero = T(0);
+    if (!uv_only)
+        L.d1(e.m, [=] __host__ __device__(long long k) {
+            const int i = (int)k + 1, n = e.n;
+            e(i, 2) += e(i, 1); e(i, 1) = zero;
+            e(i, n - 1) += e(i, n); e(i, n) = zero;
+        });
+    const int nmax = std::max(std::max(u.m, u.n), std::max(std::max(v.m, v.n), std::max(e.m, e.n)));
+    L.d1(nmax, [=] __host__ __device__(long long k) {
+        const int t = (int)k + 1;
+        if (ep) {
+            if (t <= u.n) {
+                const int m = u.m;
+                u(m - 3, t) += u(1, t); u(m - 2, t) += u(2, t); u(3, t) += u(m - 1, t); u(4, t) += u(m, t);
+                u(1, t) = zero; u(2, t) = zero; u(m - 1, t) = zero; u(m, t) = zero;
+            }
+            if (t <= v.n) {
+                const int m = v.m;
+                v(m - 3, t) += v(1, t); v(m - 2, t) += v(2, t); v(3, t) += v(m - 1, t); v(4, t) += v(m, t);
+                v(1, t) = zero; v(2, t) = zero; v(m - 1, t) = zero; v(m, t) = zero;
+            }
+            if (!uv_only && t <= e.n) {
+                const int m = e.m;
+                e(m - 1, t) += e(1, t); e(2, t) += e(m, t); e(1, t) = zero; e(m, t) = zero;
+            }
+        } else {
+            if (t <= u.m) {
+                const int n = u.n;
+                u(t, 4) += c * u(t, 1); u(t, 3) += c * u(t, 2); u(t, n - 2) += c * u(t, n - 1); u(t, n - 3) += c * u(t, n);
+                u(t, 1) = zero; u(t, 2) = zero; u(t, n - 1) = zero; u(t, n) = zero;
+            }
+            if (t <= v.n) {
+                const int m = v.m;
+                v(4, t) += c * v(1, t); v(3, t) += c * v(2, t); v(m - 2, t) += c * v(m - 1, t); v(m - 3, t) += c * v(m, t);
+                v(1, t) = zero; v(2, t) = zero; v(m - 1, t) = zero; v(m, t) = zero;
+            }
+            if (!uv_only && t <= e.n) {
+                const int m = e.m;
+                e(2, t) += e(1, t); e(m - 1, t) += e(m, t); e(1, t) = zero; e(m, t) = zero;
+            }
+        }
+    });
+}
+
+// ------------------------------------------------------------ RK stage, forward
+// rhs_nonlinear! without the momentum write (src/rhs.jl:24-51): thickness!,
+// Ix!/Iy!/Ixy! of h, UVfluxes! (:307-324), PV! (src/PV_advection.jl:2-18),
+// AHα..δ! (src/PV_advection.jl:88-146) and bernoulli! (src/rhs.jl:162-180).
+template <class T>
+void stage_fwd(Launcher& L, const Work<T>& w, const State<T>& Y) {
+    const A2<T> u = Y.u, v = Y.v, e = Y.e, H = w.H, f_q = w.f_q;
+    const A2<T> hu = w.hu, hv = w.hv, hq = w.hq, U = w.U, V = w.V, q = w.q;
+    const int nx = w.nx, ny = w.ny, ep = w.ep;
+    L.d2(nx + 2, ny + 2, [=] __host__ __device__(int i, int j) {
+        const T half = T(0.5), quarter = T(0.25);
+        auto h = [&](int a, int b) { return e(a, b) + H(a, b); };
+        if (i <= nx + 1) hu(i, j) = half * (h(i + 1, j) + h(i, j));
+        if (j <= ny + 1) hv(i, j) = half * (h(i, j + 1) + h(i, j));
+        if (i <= nx + 1 && j <= ny + 1) hq(i, j) = quarter * (h(i, j) + h(i + 1, j)) + quarter * (h(i, j + 1) + h(i + 1, j + 1));
+    });
+    L.d2(nx + 2, ny + 2, [=] __host__ __device__(int i, int j) {
+        if (i <= nx + 1) U(i, j) = u(1 + ep + i, 1 + j) * hu(i, j);
+        if (j <= ny + 1) V(i, j) = v(i + 1, j + 1) * hv(i, j);
+        if (i <= nx + 1 && j <= ny + 1) {
+            const T dvdx = v(i + 2, j + 1) - v(i + 1, j + 1);
+            const T dudy = u(i + 1 + ep, j + 2) - u(i + 1 + ep, j + 1);
+            q(i, j) = (f_q(i, j) + dvdx - dudy) / hq(i, j);
+        }
+    });
+    const A2<T> qa = w.qa, qb = w.qb, qc = w.qc, qd = w.qd, p = w.p;
+    const T g = w.g;
+    L.d2(nx + 2, ny + 2, [=] __host__ __device__(int i, int j) {
+        const T o12 = T(1.0 / 12.0), half = T(0.5);
+        const int qend = q.m;
+        if (i <= nx && j <= ny) {
+            qa(i, j) = o12 * (q(i, j) + q(i, j + 1) + q(i + 1, j + 1));
+            qd(i, j) = o12 * (q(i, j) + q(i, j + 1) + q(i + 1, j));
+        }
+        if (i <= nx + 1 && j <= ny) {
+            if (i == 1) {
+                qb(1, j) = o12 * (q(1, j) + q(1, j + 1) + q(qend, j + 1));
+                qc(1, j) = o12 * (q(1, j) + q(1, j + 1) + q(qend, j));
+            } else {
+                qb(i, j) = o12 * (q(i, j) + q(i, j + 1) + q(i - 1, j + 1));
+                qc(i, j) = o12 * (q(i, j) + q(i - 1, j) + q(i, j + 1));
+            }
+        }
+        const int a = i + ep, b = j + 1;   // KEu(a, b) = Ix(u^2), KEv(i+1, j) = Iy(v^2)
+        const T KEu = half * (u(a + 1, b) * u(a + 1, b) + u(a, b) * u(a, b));
+        const T KEv = half * (v(i + 1, j + 1) * v(i + 1, j + 1) + v(i + 1, j) * v(i + 1, j));
+        p(i, j) = half * (KEu + KEv) + g * e(i, j);
+    });
+}
+
+// momentum_u!/v! (src/rhs.jl:218-274), continuity_itself! (src/continuity.jl:52-68)
+// and the RK combination (src/time_integration.jl:64-72): Y1 = Xt + b*d (k < RKo),
+// X0 += a*d.  d is zero on the halo, so halo points keep Xt / X0.
+template <class T>
+void stage_update(Launcher& L, const Work<T>& w, int k, const State<T>& Xt, const State<T>* Y1, const State<T>& X0) {
+    const A2<T> qa = w.qa, qb = w.qb, qc = w.qc, qd = w.qd, p = w.p, U = w.U, V = w.V, Fx = w.Fx, Fy = w.Fy;
+    const int nx = w.nx, ny = w.ny, nux = w.nux, nuy = w.nuy, nvx = w.nvx, nvy = w.nvy, ep = w.ep;
+    const T a = w.RKa[k - 1], b = k < w.rko ? w.RKb[k - 1] : T(0);
+    const bool next = Y1 != nullptr;
+    const State<T> xt = Xt, x0 = X0, y1 = next ? *Y1 : Xt;
+    L.d2(nx + 4, ny + 4, [=] __host__ __device__(int I, int J) {
+        const T zero = T(0);
+        if (I <= xt.u.m && J <= xt.u.n) {
+            T d = zero;
+            if (I >= 3 && I <= nux + 2 && J >= 3 && J <= nuy + 2) {
+                const int i = I - 2, j = J - 2, c = 1 - ep + i;
+                const T qhv = qa(c, j) * V(c + 1, j + 1) + qb(c, j) * V(c, j + 1) + qc(c, j) * V(c, j) + qd(c, j) * V(c + 1, j);
+                const T dpdx = p(i + 2 - ep, j + 1) - p(i + 1 - ep, j + 1);
+                d = (qhv - dpdx) + Fx(i, j);
+            }
+            if (next) y1.u(I, J) = xt.u(I, J) + b * d;
+            x0.u(I, J) += a * d;
+        }
+        if (I <= xt.v.m && J <= xt.v.n) {
+            T d = zero;
+            if (I >= 3 && I <= nvx + 2 && J >= 3 && J <= nvy + 2) {
+                const int i = I - 2, j = J - 2;
+                const T qhu = qa(i, j) * U(i, j + 1) + qb(i + 1, j) * U(i + 1, j + 1) + qc(i + 1, j + 1) * U(i + 1, j + 2) +
+                              qd(i, j + 1) * U(i, j + 2);
+                const T dpdy = p(i + 1, j + 2) - p(i + 1, j + 1);
+                d = -(qhu + dpdy) + Fy(i, j);
+            }
+            if (next) y1.v(I, J) = xt.v(I, J) + b * d;
+            x0.v(I, J) += a * d;
+        }
+        if (I <= xt.e.m && J <= xt.e.n) {
+            T d = zero;
+            if (I >= 2 && I <= nx + 1 && J >= 2 && J <= ny + 1) {
+                const int i = I - 1, j = J - 1;
+                const T dUdx = U(i + 1, j + 1) - U(i, j + 1);
+                const T dVdy = V(i + 1, j + 1) - V(i + 1, j);
+                d = -(dUdx + dVdy);
+            }
+            if (next) y1.e(I, J) = xt.e(I, J) + b * d;
+            x0.e(I, J) += a * d;
+        }
+    });
+}
+
+// ------------------------------------------------------------ RK stage, reverse
+// Given the stage's tendency adjoint  dbar = a*Xb0 + b*Wb  (interior points),
+// adds the adjoint of the stage input Y into Yb.  Transposes, in reverse
+// order, the passes of stage_fwd and stage_update.
+template <class T>
+void stage_rev(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const State<T>& Xb0, const State<T>* Wb,
+               const State<T>& Yb) {
+    const A2<T> u = Y.u, v = Y.v;
+    const A2<T> hu = w.hu, hv = w.hv, hq = w.hq, U = w.U, V = w.V, q = w.q, qa = w.qa, qb = w.qb, qc = w.qc, qd = w.qd;
+    const A2<T> bU = w.bU, bV = w.bV, bp = w.bp, bqa = w.bqa, bqb = w.bqb, bqc = w.bqc, bqd = w.bqd, bq = w.bq,
+                bhu = w.bhu, bhv = w.bhv, bhq = w.bhq, bFx = w.bFx;
+    const int nx = w.nx, ny = w.ny, nux = w.nux, nuy = w.nuy, nvx = w.nvx, nvy = w.nvy, ep = w.ep;
+    const T a = w.RKa[k - 1], b = Wb ? w.RKb[k - 1] : T(0);
+    const State<T> x0 = Xb0, wb = Wb ? *Wb : Xb0, yb = Yb;
+    const bool has_w = Wb != nullptr;
+    L.zero(w.stage_adj, w.stage_adj_elems * sizeof(T));
+    // momentum_u^T, momentum_v^T (with PV_ArakawaHsu^T), continuity^T
+    L.d2(nx, ny, [=] __host__ __device__(int i, int j) {
+        if (i <= nux && j <= nuy) {
+            T g = a * x0.u(i + 2, j + 2);
+            if (has_w) g += b * wb.u(i + 2, j + 2);
+            bFx(i, j) += g;
+            add(bp(i + 2 - ep, j + 1), -g);
+            add(bp(i + 1 - ep, j + 1), g);
+            const int c = 1 - ep + i;      // qhv (src/PV_advection.jl:73)
+            add(bqa(c, j), g * V(c + 1, j + 1)); add(bV(c + 1, j + 1), g * qa(c, j));
+            add(bqb(c, j), g * V(c, j + 1));     add(bV(c, j + 1), g * qb(c, j));
+            add(bqc(c, j), g * V(c, j));         add(bV(c, j), g * qc(c, j));
+            add(bqd(c, j), g * V(c + 1, j));     add(bV(c + 1, j), g * qd(c, j));
+        }
+        if (i <= nvx && j <= nvy) {
+            T g = a * x0.v(i + 2, j + 2);
+            if (has_w) g += b * wb.v(i + 2, j + 2);
+            const T m = -g;                 // dv = -(qhu + dpdy) + Fy
+            add(bp(i + 1, j + 2), m);
+            add(bp(i + 1, j + 1), -m);
+            add(bqa(i, j), m * U(i, j + 1));             add(bU(i, j + 1), m * qa(i, j));
+            add(bqb(i + 1, j), m * U(i + 1, j + 1));     add(bU(i + 1, j + 1), m * qb(i + 1, j));
+            add(bqc(i + 1, j + 1), m * U(i + 1, j + 2)); add(bU(i + 1, j + 2), m * qc(i + 1, j + 1));
+            add(bqd(i, j + 1), m * U(i, j + 2));         add(bU(i, j + 2), m * qd(i, j + 1));
+        }
+        {
+            T g = a * x0.e(i + 1, j + 1);
+            if (has_w) g += b * wb.e(i + 1, j + 1);
+            add(bU(i + 1, j + 1), -g); add(bU(i, j + 1), g);
+            add(bV(i + 1, j + 1), -g); add(bV(i + 1, j), g);
+        }
+    });
+    // bernoulli^T (through KEu = Ix(u^2), KEv = Iy(v^2)) and AHα..δ^T
+    const T g = w.g;
+    L.d2(nx + 2, ny + 2, [=] __host__ __device__(int i, int j) {
+        const T half = T(0.5), o12 = T(1.0 / 12.0);
+        const T wp = bp(i, j);
+        add(yb.e(i, j), g * wp);
+        const T hw = half * wp;
+        const int a2 = i + ep, b2 = j + 1;
+        add(yb.u(a2 + 1, b2), hw * u(a2 + 1, b2));
+        add(yb.u(a2, b2), hw * u(a2, b2));
+        add(yb.v(i + 1, j + 1), hw * v(i + 1, j + 1));
+        add(yb.v(i + 1, j), hw * v(i + 1, j));
+        const int qend = q.m;
+        if (i <= nx && j <= ny) {
+            const T ta = o12 * bqa(i, j), td = o12 * bqd(i, j);
+            add(bq(i, j), ta + td); add(bq(i, j + 1), ta + td);
+            add(bq(i + 1, j + 1), ta); add(bq(i + 1, j), td);
+        }
+        if (i <= nx + 1 && j <= ny) {
+            const T tb = o12 * bqb(i, j), tc = o12 * bqc(i, j);
+            add(bq(i, j), tb + tc); add(bq(i, j + 1), tb + tc);
+            if (i == 1) { add(bq(qend, j + 1), tb); add(bq(qend, j), tc); }
+            else { add(bq(i - 1, j + 1), tb); add(bq(i - 1, j), tc); }
+        }
+    });
+    // PV^T, Uflux^T, Vflux^T
+    L.d2(nx + 2, ny + 2, [=] __host__ __device__(int i, int j) {
+        if (i <= nx + 1 && j <= ny + 1) {
+            const T n = bq(i, j) / hq(i, j);
+            add(yb.v(i + 2, j + 1), n); add(yb.v(i + 1, j + 1), -n);
+            add(yb.u(i + 1 + ep, j + 2), -n); add(yb.u(i + 1 + ep, j + 1), n);
+            bhq(i, j) = -(n * q(i, j));
+        }
+        if (i <= nx + 1) {
+            const T wU = bU(i, j);
+            add(yb.u(1 + ep + i, 1 + j), wU * hu(i, j));
+            bhu(i, j) = wU * u(1 + ep + i, 1 + j);
+        }
+        if (j <= ny + 1) {
+            const T wV = bV(i, j);
+            add(yb.v(i + 1, j + 1), wV * hv(i, j));
+            bhv(i, j) = wV * v(i + 1, j + 1);
+        }
+    });
+    // Ix^T, Iy^T, Ixy^T of h = eta + H
+    L.d2(nx + 2, ny + 2, [=] __host__ __device__(int i, int j) {
+        const T half = T(0.5), quarter = T(0.25);
+        if (i <= nx + 1) { const T t = half * bhu(i, j); add(yb.e(i + 1, j), t); add(yb.e(i, j), t); }
+        if (j <= ny + 1) { const T t = half * bhv(i, j); add(yb.e(i, j + 1), t); add(yb.e(i, j), t); }
+        if (i <= nx + 1 && j <= ny + 1) {
+            const T t = quarter * bhq(i, j);
+            add(yb.e(i, j), t); add(yb.e(i + 1, j), t); add(yb.e(i, j + 1), t); add(yb.e(i + 1, j + 1), t);
+        }
+    });
+}
+
+// ------------------------------------------------------------ tail, forward
+// bottom_drag! (src/bottom_drag.jl:2-119), diffusion! (src/diffusion.jl:2-218)
+// and add_drag_diff_tendencies! (src/diffusion.jl:221-251) on Z; the result
+// goes to X (eta copied), then ghost_points_uv! (src/time_integration.jl:231).
+template <class T>
+void tail_fwd(Launcher& L, const Work<T>& w, const State<T>& Zs, const State<T>& Xs) {
+    const A2<T> u = Zs.u, v = Zs.v, e = Zs.e, H = w.H;
+    const A2<T> thu = w.thu, thv = w.thv, sKE = w.sKE, Lu = w.Lu, Lv = w.Lv, sDT = w.sDT, sDS = w.sDS, DSq = w.DSq;
+    const int nx = w.nx, ny = w.ny, ep = w.ep, drag = w.drag;
+    const bool smag = w.diff == SW_DIFF_SMAGORINSKY;
+    L.d2(nx + 4, ny + 4, [=] __host__ __device__(int i, int j) {
+        const T half = T(0.5);
+        auto h = [&](int a, int b) { return e(a, b) + H(a, b); };
+        if (drag == SW_DRAG_QUADRATIC) {
+            if (i <= nx + 1 && j <= ny + 2) thu(i, j) = half * (h(i + 1, j) + h(i, j));
+            if (i <= nx + 2 && j <= ny + 1) thv(i, j) = half * (h(i, j + 1) + h(i, j));
+            if (i <= nx + 2 && j <= ny + 2) {
+                const int a = i + ep, b = j + 1;
+                const T KEu = half * (u(a + 1, b) * u(a + 1, b) + u(a, b) * u(a, b));
+                const T KEv = half * (v(i + 1, j + 1) * v(i + 1, j + 1) + v(i + 1, j) * v(i + 1, j));
+                sKE(i, j) = sqrt_(KEu + KEv);
+            }
+        }
+        if (i <= Lu.m && j <= Lu.n) {   // ∇² (src/gradients.jl:39)
+            const T c = u(i + 1, j + 1);
+            Lu(i, j) = ((u(i, j + 1) - c) + (u(i + 2, j + 1) - c)) + ((u(i + 1, j) - c) + (u(i + 1, j + 2) - c));
+        }
+        if (i <= Lv.m && j <= Lv.n) {
+            const T c = v(i + 1, j + 1);
+            Lv(i, j) = ((v(i, j + 1) - c) + (v(i + 2, j + 1) - c)) + ((v(i + 1, j) - c) + (v(i + 1, j + 2) - c));
+        }
+        if (smag) {
+            if (i <= nx + 2 && j <= ny + 2) {      // DT (src/diffusion.jl:88-97)
+                const T s = (u(i + ep + 1, j + 1) - u(i + ep, j + 1)) + (v(i + 1, j + 1) - v(i + 1, j));
+                sDT(i, j) = s;
+            }
+            if (i <= nx + 3 && j <= ny + 3) {      // DS_q (src/diffusion.jl:72-80)
+                const T s = (u(i + ep, j + 1) - u(i + ep, j)) + (v(i + 1, j) - v(i, j));
+                sDS(i, j) = s;
+                DSq(i, j) = s * s;
+            }
+        }
+    });
+    const A2<T> dLudx = w.dLudx, dLudy = w.dLudy, dLvdx = w.dLvdx, dLvdy = w.dLvdy, sKEu = w.sKEu, sKEv = w.sKEv,
+                rS = w.rS, nuS = w.nuS;
+    const T cSmag = w.cSmag;
+    L.d2(nx + 4, ny + 4, [=] __host__ __device__(int i, int j) {
+        const T half = T(0.5), quarter = T(0.25);
+        if (i <= dLudx.m && j <= dLudx.n) dLudx(i, j) = Lu(i + 1, j) - Lu(i, j);
+        if (i <= dLudy.m && j <= dLudy.n) dLudy(i, j) = Lu(i, j + 1) - Lu(i, j);
+        if (i <= dLvdx.m && j <= dLvdx.n) dLvdx(i, j) = Lv(i + 1, j) - Lv(i, j);
+        if (i <= dLvdy.m && j <= dLvdy.n) dLvdy(i, j) = Lv(i, j + 1) - Lv(i, j);
+        if (drag == SW_DRAG_QUADRATIC) {
+            if (i <= nx + 1 && j <= ny + 2) sKEu(i, j) = half * (sKE(i + 1, j) + sKE(i, j));
+            if (i <= nx + 2 && j <= ny + 1) sKEv(i, j) = half * (sKE(i, j + 1) + sKE(i, j));
+        }
+        if (smag && i <= nx + 2 && j <= ny + 2) {
+            const T DS = quarter * (DSq(i, j) + DSq(i + 1, j)) + quarter * (DSq(i, j + 1) + DSq(i + 1, j + 1));
+            const T DT = sDT(i, j) * sDT(i, j);
+            const T r = sqrt_(DS + DT);
+            rS(i, j) = r;
+            nuS(i, j) = cSmag * r;
+        }
+    });
+    const A2<T> Bu = w.Bu, Bv = w.Bv, nuSq = w.nuSq, S11 = w.S11, S12 = w.S12, S21 = w.S21, S22 = w.S22;
+    const T cD = w.cD, rD = w.rD, nuB = w.nuB;
+    L.d2(nx + 2, ny + 2, [=] __host__ __device__(int i, int j) {
+        const T quarter = T(0.25);
+        if (i <= nx + 1 && j <= ny + 2) {
+            if (drag == SW_DRAG_QUADRATIC) Bu(i, j) = cD * sKEu(i, j) * u(i + 1 + ep, j + 1) / thu(i, j);
+            else if (drag == SW_DRAG_LINEAR) Bu(i, j) = rD * u(i + 1 + ep, j + 1);
+            else Bu(i, j) = T(0);
+        }
+        if (i <= nx + 2 && j <= ny + 1) {
+            if (drag == SW_DRAG_QUADRATIC) Bv(i, j) = cD * sKEv(i, j) * v(i + 1, j + 1) / thv(i, j);
+            else if (drag == SW_DRAG_LINEAR) Bv(i, j) = rD * v(i + 1, j + 1);
+            else Bv(i, j) = T(0);
+        }
+        if (smag && i <= nx + 1 && j <= ny + 1)
+            nuSq(i, j) = quarter * (nuS(i, j) + nuS(i + 1, j)) + quarter * (nuS(i, j + 1) + nuS(i + 1, j + 1));
+    });
+    L.d2(nx + 2, ny + 2, [=] __host__ __device__(int i, int j) {    // viscous tensor (src/diffusion.jl:126-218)
+        if (i <= S11.m && j <= S11.n) S11(i, j) = smag ? nuS(i + 1 - ep, j) * dLudx(i, j) : nuB * dLudx(i, j);
+        if (i <= S12.m && j <= S12.n) S12(i, j) = smag ? nuSq(i, j) * dLudy(i + ep, j) : nuB * dLudy(i + ep, j);
+        if (i <= S21.m && j <= S21.n) S21(i, j) = smag ? nuSq(i, j) * dLvdx(i, j) : nuB * dLvdx(i, j);
+        if (i <= S22.m && j <= S22.n) S22(i, j) = smag ? nuS(i, j + 1) * dLvdy(i, j) : nuB * dLvdy(i, j);
+    });
+    const int nux = w.nux, nuy = w.nuy, nvx = w.nvx, nvy = w.nvy;
+    const T Dt = w.Dt_diff;
+    const A2<T> xu = Xs.u, xv = Xs.v, xe = Xs.e;
+    L.d2(nx + 4, ny + 4, [=] __host__ __device__(int I, int J) {
+        if (I <= u.m && J <= u.n) {
+            T r = u(I, J);
+            if (I >= 3 && I <= nux + 2 && J >= 3 && J <= nuy + 2) {
+                const int i = I - 2, j = J - 2;
+                const T LLu1 = S11(i + 1, j + 1) - S11(i, j + 1);
+                const T LLu2 = S12(i + 1 - ep, j + 1) - S12(i + 1 - ep, j);
+                r += Dt * (Bu(i + 1 - ep, j + 1) + LLu1 + LLu2);
+            }
+            xu(I, J) = r;
+        }
+        if (I <= v.m && J <= v.n) {
+            T r = v(I, J);
+            if (I >= 3 && I <= nvx + 2 && J >= 3 && J <= nvy + 2) {
+                const int i = I - 2, j = J - 2;
+                const T LLv1 = S21(i + 1, j + 1) - S21(i, j + 1);
+                const T LLv2 = S22(i + 1, j + 1) - S22(i + 1, j);
+                r += Dt * (Bv(i + 1, j + 1) + LLv1 + LLv2);
+            }
+            xv(I, J) = r;
+        }
+        if (I <= e.m && J <= e.n) xe(I, J) = e(I, J);
+    });
+    ghost(L, w, Xs, true);
+}
+
+// ------------------------------------------------------------ tail, reverse
+// On entry Xb holds the adjoint of the tail's output before ghost_points_uv!
+// (already transposed); on return it holds the adjoint of Z.
+template <class T>
+void tail_rev(Launcher& L, const Work<T>& w, const State<T>& Zs, const State<T>& Xb) {
+    const A2<T> u = Zs.u, v = Zs.v;
+    const State<T> zb = Xb;
+    const int nx = w.nx, ny = w.ny, nux = w.nux, nuy = w.nuy, nvx = w.nvx, nvy = w.nvy, ep = w.ep, drag = w.drag;
+    const bool smag = w.diff == SW_DIFF_SMAGORINSKY;
+    const T Dt = w.Dt_diff;
+    const A2<T> bBu = w.bBu, bBv = w.bBv, bS11 = w.bS11, bS12 = w.bS12, bS21 = w.bS21, bS22 = w.bS22;
+    L.zero(w.tail_adj, w.tail_adj_elems * sizeof(T));
+    // add_drag_diff_tendencies^T and dx/dy^T of the stress tensor
+    L.d2(nx, ny, [=] __host__ __device__(int i, int j) {
+        if (i <= nux && j <= nuy) {
+            const T t = Dt * zb.u(i + 2, j + 2);
+            bBu(i + 1 - ep, j + 1) += t;
+            add(bS11(i + 1, j + 1), t); add(bS11(i, j + 1), -t);
+            add(bS12(i + 1 - ep, j + 1), t); add(bS12(i + 1 - ep, j), -t);
+        }
+        if (i <= nvx && j <= nvy) {
+            const T t = Dt * zb.v(i + 2, j + 2);
+            bBv(i + 1, j + 1) += t;
+            add(bS21(i + 1, j + 1), t); add(bS21(i, j + 1), -t);
+            add(bS22(i + 1, j + 1), t); add(bS22(i + 1, j), -t);
+        }
+    });
+    const A2<T> nuS = w.nuS, nuSq = w.nuSq, dLudx = w.dLudx, dLudy = w.dLudy, dLvdx = w.dLvdx, dLvdy = w.dLvdy;
+    const A2<T> bnuS = w.bnuS, bnuSq = w.bnuSq, bdLudx = w.bdLudx, bdLudy = w.bdLudy, bdLvdx = w.bdLvdx,
+                bdLvdy = w.bdLvdy;
+    const A2<T> thu = w.thu, thv = w.thv, sKEu = w.sKEu, sKEv = w.sKEv, Bu = w.Bu, Bv = w.Bv;
+    const A2<T> bsKEu = w.bsKEu, bsKEv = w.bsKEv, bthu = w.bthu, bthv = w.bthv;
+    const T cD = w.cD, rD = w.rD, nuB = w.nuB;
+    // viscous tensor^T, bottom drag^T
+    L.d2(nx + 2, ny + 2, [=] __host__ __device__(int i, int j) {
+        if (i <= bS11.m && j <= bS11.n) {
+            const T s = bS11(i, j);
+            if (smag) { add(bnuS(i + 1 - ep, j), s * dLudx(i, j)); add(bdLudx(i, j), s * nuS(i + 1 - ep, j)); }
+            else add(bdLudx(i, j), s * nuB);
+        }
+        if (i <= bS12.m && j <= bS12.n) {
+            const T s = bS12(i, j);
+            if (smag) { add(bnuSq(i, j), s * dLudy(i + ep, j)); add(bdLudy(i + ep, j), s * nuSq(i, j)); }
+            else add(bdLudy(i + ep, j), s * nuB);
+        }
+        if (i <= bS21.m && j <= bS21.n) {
+            const T s = bS21(i, j);
+            if (smag) { add(bnuSq(i, j), s * dLvdx(i, j)); add(bdLvdx(i, j), s * nuSq(i, j)); }
+            else add(bdLvdx(i, j), s * nuB);
+        }
+        if (i <= bS22.m && j <= bS22.n) {
+            const T s = bS22(i, j);
+            if (smag) { add(bnuS(i, j + 1), s * dLvdy(i, j)); add(bdLvdy(i, j), s * nuS(i, j + 1)); }
+            else add(bdLvdy(i, j), s * nuB);
+        }
+        if (i <= nx + 1 && j <= ny + 2) {
+            const T bb = bBu(i, j);
+            const T uu = u(i + 1 + ep, j + 1);
+            if (drag == SW_DRAG_QUADRATIC) {     // Bu = cD*s*u/h
+                const T hh = thu(i, j);
+                bsKEu(i, j) = bb * (cD * uu / hh);
+                add(zb.u(i + 1 + ep, j + 1), bb * (cD * sKEu(i, j) / hh));
+                bthu(i, j) = -(bb * Bu(i, j) / hh);
+            } else if (drag == SW_DRAG_LINEAR) {
+                add(zb.u(i + 1 + ep, j + 1), bb * rD);
+            }
+        }
+        if (i <= nx + 2 && j <= ny + 1) {
+            const T bb = bBv(i, j);
+            const T vv = v(i + 1, j + 1);
+            if (drag == SW_DRAG_QUADRATIC) {
+                const T hh = thv(i, j);
+                bsKEv(i, j) = bb * (cD * vv / hh);
+                add(zb.v(i + 1, j + 1), bb * (cD * sKEv(i, j) / hh));
+                bthv(i, j) = -(bb * Bv(i, j) / hh);
+            } else if (drag == SW_DRAG_LINEAR) {
+                add(zb.v(i + 1, j + 1), bb * rD);
+            }
+        }
+    });
+    const A2<T> bLu = w.bLu, bLv = w.bLv, bsKE = w.bsKE;
+    // Ixy^T of nuSmag_q, dx/dy^T of the Laplacians, Ix/Iy^T of sqrtKE and of h
+    L.d2(nx + 4, ny + 4, [=] __host__ __device__(int i, int j) {
+        const T half = T(0.5), quarter = T(0.25);
+        if (smag && i <= nx + 1 && j <= ny + 1) {
+            const T t = quarter * bnuSq(i, j);
+            add(bnuS(i, j), t); add(bnuS(i + 1, j), t); add(bnuS(i, j + 1), t); add(bnuS(i + 1, j + 1), t);
+        }
+        if (i <= bdLudx.m && j <= bdLudx.n) { const T t = bdLudx(i, j); add(bLu(i + 1, j), t); add(bLu(i, j), -t); }
+        if (i <= bdLudy.m && j <= bdLudy.n) { const T t = bdLudy(i, j); add(bLu(i, j + 1), t); add(bLu(i, j), -t); }
+        if (i <= bdLvdx.m && j <= bdLvdx.n) { const T t = bdLvdx(i, j); add(bLv(i + 1, j), t); add(bLv(i, j), -t); }
+        if (i <= bdLvdy.m && j <= bdLvdy.n) { const T t = bdLvdy(i, j); add(bLv(i, j + 1), t); add(bLv(i, j), -t); }
+        if (drag == SW_DRAG_QUADRATIC) {
+            if (i <= nx + 1 && j <= ny + 2) {
+                const T t = half * bsKEu(i, j);
+                add(bsKE(i + 1, j), t); add(bsKE(i, j), t);
+                const T th = half * bthu(i, j);
+                add(zb.e(i + 1, j), th); add(zb.e(i, j), th);
+            }
+            if (i <= nx + 2 && j <= ny + 1) {
+                const T t = half * bsKEv(i, j);
+                add(bsKE(i, j + 1), t); add(bsKE(i, j), t);
+                const T th = half * bthv(i, j);
+                add(zb.e(i, j + 1), th); add(zb.e(i, j), th);
+            }
+        }
+    });
+    const A2<T> rS = w.rS, sKE = w.sKE, bDS = w.bDS, bDT = w.bDT;
+    const T cSmag = w.cSmag;
+    const A2<T> Lu = w.Lu, Lv = w.Lv;
+    // sqrt^T (Smagorinsky coefficient and sqrtKE, through KE = Ix(u^2) + Iy(v^2)), ∇²^T
+    L.d2(nx + 4, ny + 4, [=] __host__ __device__(int i, int j) {
+        const T zero = T(0), two = T(2);
+        if (smag && i <= nx + 2 && j <= ny + 2) {
+            const T r = rS(i, j);
+            const T d = r > zero ? bnuS(i, j) * cSmag / (two * r) : zero;
+            bDS(i, j) = d;
+            bDT(i, j) = d;
+        }
+        if (drag == SW_DRAG_QUADRATIC && i <= nx + 2 && j <= ny + 2) {
+            const T r = sKE(i, j);
+            const T k = r > zero ? bsKE(i, j) / (two * r) : zero;
+            const int a = i + ep, b = j + 1;    // d/du of half*(u(a+1)^2 + u(a)^2) is u
+            add(zb.u(a + 1, b), k * u(a + 1, b)); add(zb.u(a, b), k * u(a, b));
+            add(zb.v(i + 1, j + 1), k * v(i + 1, j + 1)); add(zb.v(i + 1, j), k * v(i + 1, j));
+        }
+        if (i <= Lu.m && j <= Lu.n) {
+            const T t = bLu(i, j);
+            add(zb.u(i, j + 1), t); add(zb.u(i + 2, j + 1), t); add(zb.u(i + 1, j), t); add(zb.u(i + 1, j + 2), t);
+            add(zb.u(i + 1, j + 1), -(T(4) * t));
+        }
+        if (i <= Lv.m && j <= Lv.n) {
+            const T t = bLv(i, j);
+            add(zb.v(i, j + 1), t); add(zb.v(i + 2, j + 1), t); add(zb.v(i + 1, j), t); add(zb.v(i + 1, j + 2), t);
+            add(zb.v(i + 1, j + 1), -(T(4) * t));
+        }
+    });
+    if (!smag) return;
+    const A2<T> sDT = w.sDT, sDS = w.sDS, bDSq = w.bDSq;
+    // DT^T (s^2 with s = dudx + dvdy) and Ixy^T of DS
+    L.d2(nx + 2, ny + 2, [=] __host__ __device__(int i, int j) {
+        const T quarter = T(0.25), two = T(2);
+        const T t = two * sDT(i, j) * bDT(i, j);
+        add(zb.u(i + ep + 1, j + 1), t); add(zb.u(i + ep, j + 1), -t);
+        add(zb.v(i + 1, j + 1), t); add(zb.v(i + 1, j), -t);
+        const T s = quarter * bDS(i, j);
+        add(bDSq(i, j), s); add(bDSq(i + 1, j), s); add(bDSq(i, j + 1), s); add(bDSq(i + 1, j + 1), s);
+    });
+    // DS_q^T (s^2 with s = dudy + dvdx)
+    L.d2(nx + 3, ny + 3, [=] __host__ __device__(int i, int j) {
+        const T t = T(2) * sDS(i, j) * bDSq(i, j);
+        add(zb.u(i + ep, j + 1), t); add(zb.u(i + ep, j), -t);
+        add(zb.v(i + 1, j), t); add(zb.v(i, j), -t);
+    });
+}
+
+// ------------------------------------------------------------ whole steps
+template <class T>
+void copy_state(Launcher& L, const State<T>& dst, const State<T>& src) {
+    L.copy(dst.base, src.base, src.elems * sizeof(T));
+}
+
+// one time step X -> X (src/time_integration.jl:45-243, RK branch); leaves the
+// stage inputs in Ys, the tail input in Z and the last stage's intermediates.
+template <class T>
+void fwd_step(Launcher& L, const Work<T>& w) {
+    copy_state(L, w.Ys[0], w.X);
+    ghost(L, w, w.Ys[0], false);
+    copy_state(L, w.Z, w.Ys[0]);
+    for (int k = 1; k <= w.rko; k++) {
+        if (k > 1) ghost(L, w, w.Ys[k - 1], false);
+        stage_fwd(L, w, w.Ys[k - 1]);
+        stage_update(L, w, k, w.Ys[0], k < w.rko ? &w.Ys[k] : nullptr, w.Z);
+    }
+    ghost(L, w, w.Z, false);
+    tail_fwd(L, w, w.Z, w.X);
+}
+
+// adjoint of one step: on entry X holds the step's input state and Xb the
+// adjoint of its output; on return Xb holds the adjoint of the input, and bFx
+// has this step's forcing adjoint added.
+template <class T>
+void adj_step(Launcher& L, const Work<T>& w) {
+    fwd_step(L, w);
+    ghostT(L, w, w.Xb, true);
+    tail_rev(L, w, w.Z, w.Xb);
+    ghostT(L, w, w.Xb, false);     // Xb is now the adjoint of the RK sum X0
+    copy_state(L, w.acc, w.Xb);  // X0 starts as the ghosted input
+    const State<T>* Wb = nullptr;
+    for (int k = w.rko; k >= 1; k--) {
+        const State<T>& Yb = w.Yb[k % 2];
+        L.zero(Yb.base, Yb.elems * sizeof(T));
+        if (k < w.rko) stage_fwd(L, w, w.Ys[k - 1]);   // the last stage's intermediates are still in place
+        stage_rev(L, w, k, w.Ys[k - 1], w.Xb, Wb, Yb);
+        if (k > 1) ghostT(L, w, Yb, false);             // Ys[k-1] = ghost(Y1)
+        const T* src = Yb.base;
+        T* dst = w.acc.base;
+        L.d1((long long)Yb.elems, [=] __host__ __device__(long long i) { dst[i] += src[i]; });
+        Wb = &Yb;
+    }
+    ghostT(L, w, w.acc, false);    // the step starts with ghost_points!
+    copy_state(L, w.Xb, w.acc);
+}
+
+// J = sum (eta - obs)^2 over the interior, the differences and squares in
+// FP64, as row sums (out[j-1]); and the seed eb = dJ/deta = 2 (eta - obs) on
+// the interior, rounded once to T
+template <class T>
+void cost_seed(Launcher& L, const A2<T>& ef, const A2<T>& obs, const A2<T>& eb, double* out) {
+    const A2<T> e = ef, o = obs, b = eb;
+    const int nx = obs.m;
+    L.d1(obs.n, [=] __host__ __device__(long long jj) {
+        const int j = (int)jj + 1;
+        double acc = 0.0;
+        for (int i = 1; i <= nx; i++) {
+            const double d = (double)e(i + 1, j + 1) - (double)o(i, j);
+            acc += d * d;
+            b(i + 1, j + 1) = (T)(2.0 * d);
+        }
+        out[jj] = acc;
+    });
+}
+
+}  // namespace swa
+
+// ================================================================ host side
+namespace {
+
+using namespace swa;
+
+struct AdjCfgError {
+    int code;
+    const char* why;
+};
+
+AdjCfgError adjoint_check(const sw_config& c) {
+    if (c.abi_version != SWB200_ABI_VERSION) return {SW_ERR_ARG, "abi_version"};
+    if (c.halo != 2 || c.haloeta != 1 || c.halosstx != 1 || c.halossty != 0) return {SW_ERR_ARG, "halo sizes"};
+    if (c.nx < 8 || c.ny < 8) return {SW_ERR_ARG, "grid smaller than 8 x 8"};
+    if (c.T != c.Tprog || (c.T != SW_FLOAT32 && c.T != SW_FLOAT64) || c.Tcomm != c.T)
+        return {SW_ERR_UNSUPPORTED, "the adjoint computes in T = Tprog = Tcomm, Float32 or Float64"};
+    if (c.time_scheme != SW_RK || c.RKo < 2 || c.RKo > 4) return {SW_ERR_UNSUPPORTED, "the adjoint follows the RK2/3/4 schemes"};
+    if (c.dynamics != SW_NONLINEAR || c.adv_scheme != SW_ARAKAWA_HSU || c.nstep_advcor != 0)
+        return {SW_ERR_UNSUPPORTED, "the adjoint follows nonlinear dynamics with Arakawa-Hsu and nstep_advcor = 0"};
+    if (c.nstep_diff != 1) return {SW_ERR_UNSUPPORTED, "the adjoint needs nstep_diff = 1"};
+    if (c.surface_relax || c.surface_forcing || c.seasonal_wind_x || c.seasonal_wind_y)
+        return {SW_ERR_UNSUPPORTED, "the adjoint has no time-dependent forcing or relaxation"};
+    if (c.storage != SW_STORE_NATIVE) return {SW_ERR_UNSUPPORTED, "the adjoint keeps the native storage"};
+    return {SW_OK, nullptr};
+}
+
+// The work buffers, the checkpoint slots, the two captured step graphs
+// (forward step, adjoint step) and the checkpoint schedule.  With host = true
+// (the host check build only) the same passes run in host loops on host
+// memory.
+template <class T>
+struct Adjoint {
+    Work<T> w;
+    bool host = false;
+    std::vector<void*> blocks;
+    cudaStream_t s = nullptr;
+    cudaGraphExec_t g_fwd = nullptr, g_adj = nullptr;
+    std::vector<State<T>> slots;
+    long long fwd_steps = 0, adj_steps = 0;
+    int launches_fwd = 0, launches_adj = 0;
+    std::string err;
+
+    ~Adjoint() {
+        if (s) cudaStreamSynchronize(s);
+        if (g_fwd) cudaGraphExecDestroy(g_fwd);
+        if (g_adj) cudaGraphExecDestroy(g_adj);
+        for (void* p : blocks) {
+            if (host) std::free(p); else cudaFree(p);
+        }
+        if (s) cudaStreamDestroy(s);
+    }
+
+    Launcher launcher() { Launcher L{s}; L.host = host; return L; }
+
+    T* alloc(size_t elems) {
+        const size_t bytes = std::max<size_t>(elems, 1) * sizeof(T);
+        void* p = nullptr;
+        if (host) p = std::calloc(1, bytes);
+        else if (cudaMalloc(&p, bytes) != cudaSuccess) p = nullptr;
+        if (!p) return nullptr;
+        blocks.push_back(p);
+        return static_cast<T*>(p);
+    }
+    cudaError_t upload(void* dst, const void* src, size_t bytes) {
+        if (host) { std::memcpy(dst, src, bytes); return cudaSuccess; }
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+    }
+    cudaError_t download(void* dst, const void* src, size_t bytes) {
+        if (host) { std::memcpy(dst, src, bytes); return cudaSuccess; }
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
+    }
+    cudaError_t zero(void* p, size_t bytes) {
+        if (host) { std::memset(p, 0, bytes); return cudaSuccess; }
+        return cudaMemsetAsync(p, 0, bytes, s);
+    }
+    void copy(const State<T>& dst, const State<T>& src) {
+        Launcher L = launcher();
+        copy_state(L, dst, src);
+    }
+
+    // arrays carved from one block, in declaration order (each padded to 32 elements)
+    struct Carver {
+        std::vector<std::pair<A2<T>*, std::pair<int, int>>> list;
+        void add(A2<T>& a, int m, int n) { list.push_back({&a, {m, n}}); }
+        static size_t padded(int m, int n) { return ((size_t)m * (size_t)n + 31) & ~(size_t)31; }
+        size_t total() const {
+            size_t t = 0;
+            for (auto& x : list) t += padded(x.second.first, x.second.second);
+            return t;
+        }
+        void place(T* base) {
+            size_t o = 0;
+            for (auto& x : list) {
+                x.first->d = base + o;
+                x.first->m = x.second.first;
+                x.first->n = x.second.second;
+                o += padded(x.second.first, x.second.second);
+            }
+        }
+    };
+
+    bool carve(Carver& cv, T** base = nullptr, size_t* elems = nullptr) {
+        const size_t n = cv.total();
+        T* b = alloc(n);
+        if (!b) return false;
+        cv.place(b);
+        if (base) *base = b;
+        if (elems) *elems = n;
+        return zero(b, n * sizeof(T)) == cudaSuccess;
+    }
+
+    bool make_state(State<T>& st) {
+        Carver c;
+        c.add(st.u, w.nux + 4, w.nuy + 4);
+        c.add(st.v, w.nvx + 4, w.nvy + 4);
+        c.add(st.e, w.nx + 2, w.ny + 2);
+        return carve(c, &st.base, &st.elems);
+    }
+
+    int setup(const sw_config& c, const sw_static& stt) {
+        if (!host && cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return SW_ERR_CUDA;
+        w.nx = c.nx; w.ny = c.ny; w.ep = c.periodic ? 1 : 0;
+        w.nux = w.ep ? c.nx : c.nx - 1; w.nuy = c.ny; w.nvx = c.nx; w.nvy = c.ny - 1;
+        w.rko = c.RKo;
+        w.g = (T)c.g; w.cD = (T)c.cD; w.rD = (T)c.rD; w.cSmag = (T)c.cSmag; w.nuB = (T)c.nuB;
+        w.Dt_diff = (T)c.Dt_diff; w.oma = (T)c.one_minus_alpha;
+        for (int k = 0; k < 4; k++) w.RKa[k] = (T)c.RKaDt[k];
+        for (int k = 0; k < 3; k++) w.RKb[k] = (T)c.RKbDt[k];
+        w.drag = c.bottom_drag; w.diff = c.diffusion;
+        const int nx = w.nx, ny = w.ny, nux = w.nux, nuy = w.nuy, nvx = w.nvx, nvy = w.nvy;
+        {
+            Carver cv;   // static fields and the forcing adjoint
+            cv.add(w.H, nx + 2, ny + 2); cv.add(w.f_q, nx + 1, ny + 1); cv.add(w.Fx, nux, nuy); cv.add(w.Fy, nvx, nvy);
+            cv.add(w.bFx, nux, nuy);
+            if (!carve(cv)) return SW_ERR_NOMEM;
+            const void* src[4] = {stt.H, stt.f_q, stt.Fx, stt.Fy};
+            A2<T>* dst[4] = {&w.H, &w.f_q, &w.Fx, &w.Fy};
+            for (int k = 0; k < 4; k++) {
+                if (!src[k]) return SW_ERR_ARG;
+                if (upload(dst[k]->d, src[k], dst[k]->size() * sizeof(T)) != cudaSuccess) return SW_ERR_CUDA;
+            }
+        }
+        if (!make_state(w.X) || !make_state(w.Z) || !make_state(w.Xb) || !make_state(w.acc) || !make_state(w.Yb[0]) ||
+            !make_state(w.Yb[1]))
+            return SW_ERR_NOMEM;
+        for (int k = 0; k < w.rko; k++)
+            if (!make_state(w.Ys[k])) return SW_ERR_NOMEM;
+        {
+            Carver cv;   // stage intermediates
+            cv.add(w.hu, nx + 1, ny + 2); cv.add(w.hv, nx + 2, ny + 1); cv.add(w.hq, nx + 1, ny + 1);
+            cv.add(w.U, nx + 1, ny + 2); cv.add(w.V, nx + 2, ny + 1); cv.add(w.q, nx + 1, ny + 1);
+            cv.add(w.qa, nx, ny); cv.add(w.qb, nx + 1, ny); cv.add(w.qc, nx + 1, ny); cv.add(w.qd, nx, ny);
+            cv.add(w.p, nx + 2, ny + 2);
+            // tail intermediates
+            cv.add(w.thu, nx + 1, ny + 2); cv.add(w.thv, nx + 2, ny + 1); cv.add(w.sKE, nx + 2, ny + 2);
+            cv.add(w.sKEu, nx + 1, ny + 2); cv.add(w.sKEv, nx + 2, ny + 1);
+            cv.add(w.Bu, nx + 1, ny + 2); cv.add(w.Bv, nx + 2, ny + 1);
+            cv.add(w.Lu, nux + 2, nuy + 2); cv.add(w.Lv, nvx + 2, nvy + 2);
+            cv.add(w.dLudx, nux + 1, nuy + 2); cv.add(w.dLudy, nux + 2, nuy + 1);
+            cv.add(w.dLvdx, nvx + 1, nvy + 2); cv.add(w.dLvdy, nvx + 2, nvy + 1);
+            cv.add(w.sDT, nx + 2, ny + 2); cv.add(w.sDS, nvx + 3, nvy + 4); cv.add(w.DSq, nvx + 3, nvy + 4);
+            cv.add(w.rS, nx + 2, ny + 2); cv.add(w.nuS, nx + 2, ny + 2); cv.add(w.nuSq, nx + 1, ny + 1);
+            cv.add(w.S11, nux + 1, nuy + 2); cv.add(w.S12, nx + 1, ny + 1); cv.add(w.S21, nx + 1, ny + 1);
+            cv.add(w.S22, nvx + 2, nvy + 1);
+            if (!carve(cv)) return SW_ERR_NOMEM;
+        }
+        {
+            Carver cv;   // stage adjoints (zeroed per stage)
+            cv.add(w.bU, nx + 1, ny + 2); cv.add(w.bV, nx + 2, ny + 1); cv.add(w.bp, nx + 2, ny + 2);
+            cv.add(w.bqa, nx, ny); cv.add(w.bqb, nx + 1, ny); cv.add(w.bqc, nx + 1, ny); cv.add(w.bqd, nx, ny);
+            cv.add(w.bq, nx + 1, ny + 1); cv.add(w.bhu, nx + 1, ny + 2); cv.add(w.bhv, nx + 2, ny + 1);
+            cv.add(w.bhq, nx + 1, ny + 1);
+            if (!carve(cv, &w.stage_adj, &w.stage_adj_elems)) return SW_ERR_NOMEM;
+        }
+        {
+            Carver cv;   // tail adjoints (zeroed per step)
+            cv.add(w.bBu, nx + 1, ny + 2); cv.add(w.bBv, nx + 2, ny + 1);
+            cv.add(w.bS11, nux + 1, nuy + 2); cv.add(w.bS12, nx + 1, ny + 1); cv.add(w.bS21, nx + 1, ny + 1);
+            cv.add(w.bS22, nvx + 2, nvy + 1); cv.add(w.bnuS, nx + 2, ny + 2); cv.add(w.bnuSq, nx + 1, ny + 1);
+            cv.add(w.bdLudx, nux + 1, nuy + 2); cv.add(w.bdLudy, nux + 2, nuy + 1);
+            cv.add(w.bdLvdx, nvx + 1, nvy + 2); cv.add(w.bdLvdy, nvx + 2, nvy + 1);
+            cv.add(w.bLu, nux + 2, nuy + 2); cv.add(w.bLv, nvx + 2, nvy + 2);
+            cv.add(w.bsKE, nx + 2, ny + 2); cv.add(w.bsKEu, nx + 1, ny + 2); cv.add(w.bsKEv, nx + 2, ny + 1);
+            cv.add(w.bthu, nx + 1, ny + 2); cv.add(w.bthv, nx + 2, ny + 1);
+            cv.add(w.bDS, nx + 2, ny + 2); cv.add(w.bDT, nx + 2, ny + 2); cv.add(w.bDSq, nvx + 3, nvy + 4);
+            if (!carve(cv, &w.tail_adj, &w.tail_adj_elems)) return SW_ERR_NOMEM;
+        }
+        return host ? SW_OK : capture();
+    }
+
+    int capture() {
+        for (int k = 0; k < 2; k++) {
+            if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return SW_ERR_CUDA;
+            Launcher L = launcher();
+            if (k == 0) fwd_step(L, w); else adj_step(L, w);
+            cudaError_t e = cudaGetLastError();
+            cudaGraph_t graph = nullptr;
+            const cudaError_t ec = cudaStreamEndCapture(s, &graph);
+            if (e == cudaSuccess) e = ec;
+            if (e == cudaSuccess) e = cudaGraphInstantiate(k == 0 ? &g_fwd : &g_adj, graph, 0);
+            if (graph) cudaGraphDestroy(graph);
+            if (e != cudaSuccess) {
+                err = std::string("adjoint graph: ") + cudaGetErrorString(e);
+                return SW_ERR_CUDA;
+            }
+            (k == 0 ? launches_fwd : launches_adj) = L.launches;
+        }
+        return SW_OK;
+    }
+
+    cudaError_t advance(long long n) {
+        cudaError_t e = cudaSuccess;
+        for (long long k = 0; k < n && e == cudaSuccess; k++) {
+            if (host) { Launcher L = launcher(); fwd_step(L, w); }
+            else e = cudaGraphLaunch(g_fwd, s);
+        }
+        fwd_steps += n;
+        return e;
+    }
+    cudaError_t adjoint_here() {   // Xb <- adjoint of the step that starts at the state in X
+        adj_steps++;
+        if (host) { Launcher L = launcher(); adj_step(L, w); return cudaSuccess; }
+        return cudaGraphLaunch(g_adj, s);
+    }
+    cudaError_t adjoint_of(const State<T>& state) {
+        copy(w.X, state);
+        return adjoint_here();
+    }
+
+    // binomial reversal of steps [a, b): the state of step a is in slot `slot`;
+    // slots above `slot` are free; Xb holds the adjoint of step b's state.
+    cudaError_t reverse(long long a, long long b, int slot) {
+        cudaError_t e = cudaSuccess;
+        while (b > a && e == cudaSuccess) {
+            const long long t = b - a;
+            const int free_slots = (int)slots.size() - 1 - slot;
+            if (t == 1) return adjoint_of(slots[slot]);
+            if (free_slots <= 0) {   // no slot left: recompute the state of step b - 1 from a
+                copy(w.X, slots[slot]);
+                e = advance(t - 1);
+                if (e == cudaSuccess) e = adjoint_here();
+                b--;
+                continue;
+            }
+            // r: fewest repetitions with C(free + r, free) >= t; the left part gets C(free + r - 1, free) steps
+            auto binom = [](long long nn, long long kk) {
+                double x = 1.0;
+                for (long long q = 1; q <= kk; q++) x = x * (double)(nn - kk + q) / (double)q;
+                return x;
+            };
+            long long r = 0;
+            while (binom(free_slots + r, free_slots) < (double)t) r++;
+            long long left = r >= 1 ? (long long)binom(free_slots + r - 1, free_slots) : 1;
+            left = std::max(1LL, std::min(left, t - 1));
+            const long long m = a + left;
+            copy(w.X, slots[slot]);
+            e = advance(m - a);
+            if (e != cudaSuccess) return e;
+            copy(slots[slot + 1], w.X);
+            e = reverse(m, b, slot + 1);
+            b = m;       // then reverse [a, m) with the same slot
+        }
+        return e;
+    }
+};
+
+template <class T>
+int adjoint_run(bool host, const sw_config& c, const sw_static& st, const void* u, const void* v, const void* eta,
+                const void* eta_obs, int64_t nsteps, int32_t ncheckpoints, double* J, void* g_u, void* g_v,
+                void* g_eta, void* g_Fx, void* eta_final, sw_adjoint_stats* stats) {
+    Adjoint<T> A;
+    A.host = host;
+    int rc = A.setup(c, st);
+    if (rc) {
+        if (!A.err.empty()) fprintf(stderr, "swb200: %s\n", A.err.c_str());
+        return rc;
+    }
+    Work<T>& w = A.w;
+    const size_t bytes_u = w.X.u.size() * sizeof(T), bytes_v = w.X.v.size() * sizeof(T), bytes_e = w.X.e.size() * sizeof(T);
+    const int nslots = (int)std::max<long long>(1, std::min<long long>(ncheckpoints, nsteps));
+    A.slots.resize(nslots);
+    for (auto& sl : A.slots)
+        if (!A.make_state(sl)) return SW_ERR_NOMEM;
+    cudaEvent_t ev[3] = {};
+    if (!host)
+        for (auto& x : ev)
+            if (cudaEventCreate(&x) != cudaSuccess) return SW_ERR_CUDA;
+    auto record = [&](int k) { if (!host) cudaEventRecord(ev[k], A.s); };
+    cudaError_t e = A.upload(A.slots[0].u.d, u, bytes_u);
+    if (e == cudaSuccess) e = A.upload(A.slots[0].v.d, v, bytes_v);
+    if (e == cudaSuccess) e = A.upload(A.slots[0].e.d, eta, bytes_e);
+    // eta_obs (nx x ny) is kept in Yb[0]'s eta block until J is formed; the
+    // reverse sweep clears that block before its first use
+    A2<T> obs{w.Yb[0].e.d, w.nx, w.ny};
+    if (e == cudaSuccess) e = A.upload(obs.d, eta_obs, obs.size() * sizeof(T));
+    record(0);
+    // forward sweep: with a slot per step every state is kept, otherwise only the first
+    A.copy(w.X, A.slots[0]);
+    const bool keep_all = nslots >= nsteps;
+    for (long long k = 1; k <= nsteps && e == cudaSuccess; k++) {
+        e = A.advance(1);
+        if (keep_all && k < nsteps) A.copy(A.slots[k], w.X);
+    }
+    record(1);
+    // J (FP64 row sums, added on the host in a fixed order) and the seed Xb = dJ/d(state at nsteps)
+    double* rowsum = host ? static_cast<double*>(std::calloc(w.ny, sizeof(double))) : nullptr;
+    std::vector<double> rows(w.ny);
+    if (e == cudaSuccess && !host) e = cudaMalloc(&rowsum, w.ny * sizeof(double));
+    if (e == cudaSuccess) e = A.zero(w.Xb.base, w.Xb.elems * sizeof(T));
+    if (e == cudaSuccess) {
+        Launcher L = A.launcher();
+        cost_seed(L, w.X.e, obs, w.Xb.e, rowsum);
+        if (!host) e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && eta_final) e = A.download(eta_final, w.X.e.d, bytes_e);
+    if (e == cudaSuccess) e = A.download(rows.data(), rowsum, w.ny * sizeof(double));
+    if (e == cudaSuccess) e = A.zero(w.bFx.d, w.bFx.size() * sizeof(T));
+    // reverse sweep
+    if (e == cudaSuccess) {
+        if (keep_all) {
+            for (long long k = nsteps - 1; k >= 0 && e == cudaSuccess; k--) e = A.adjoint_of(A.slots[k]);
+        } else {
+            e = A.reverse(0, nsteps, 0);
+        }
+    }
+    record(2);
+    if (e == cudaSuccess && g_u) e = A.download(g_u, w.Xb.u.d, bytes_u);
+    if (e == cudaSuccess && g_v) e = A.download(g_v, w.Xb.v.d, bytes_v);
+    if (e == cudaSuccess && g_eta) e = A.download(g_eta, w.Xb.e.d, bytes_e);
+    if (e == cudaSuccess && g_Fx) e = A.download(g_Fx, w.bFx.d, w.bFx.size() * sizeof(T));
+    if (e == cudaSuccess && !host) e = cudaStreamSynchronize(A.s);
+    if (host) std::free(rowsum); else if (rowsum) cudaFree(rowsum);
+    float ms_f = 0.f, ms_r = 0.f;
+    if (!host && e == cudaSuccess) {
+        cudaEventElapsedTime(&ms_f, ev[0], ev[1]);
+        cudaEventElapsedTime(&ms_r, ev[1], ev[2]);
+    }
+    for (auto& x : ev)
+        if (x) cudaEventDestroy(x);
+    if (e != cudaSuccess) {
+        fprintf(stderr, "swb200: adjoint: %s\n", cudaGetErrorString(e));
+        return SW_ERR_CUDA;
+    }
+    double Jv = 0.0;
+    for (double r : rows) Jv += r;
+    if (J) *J = Jv;
+    if (stats) {
+        stats->forward_ms = ms_f;
+        stats->reverse_ms = ms_r;
+        stats->forward_steps = A.fwd_steps;
+        stats->adjoint_steps = A.adj_steps;
+        stats->checkpoints = nslots;
+        stats->launches_per_forward_step = A.launches_fwd;
+        stats->launches_per_adjoint_step = A.launches_adj;
+        stats->reserved = 0;
+    }
+    return SW_OK;
+}
+
+int adjoint_entry(bool host, const sw_config* cfg, const sw_static* st, const void* u, const void* v,
+                  const void* eta, const void* eta_obs, int64_t nsteps, int32_t ncheckpoints, double* J, void* g_u,
+                  void* g_v, void* g_eta, void* g_Fx, void* eta_final, sw_adjoint_stats* stats) {
+    if (!cfg || !st || !u || !v || !eta || !eta_obs || nsteps < 1 || ncheckpoints < 1) return SW_ERR_ARG;
+    const AdjCfgError ce = adjoint_check(*cfg);
+    if (ce.code) {
+        fprintf(stderr, "swb200: adjoint: %s\n", ce.why);
+        return ce.code;
+    }
+    if (!host) {
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return SW_ERR_NODEVICE;
+    }
+    if (cfg->T == SW_FLOAT64)
+        return adjoint_run<double>(host, *cfg, *st, u, v, eta, eta_obs, nsteps, ncheckpoints, J, g_u, g_v, g_eta,
+                                   g_Fx, eta_final, stats);
+    return adjoint_run<float>(host, *cfg, *st, u, v, eta, eta_obs, nsteps, ncheckpoints, J, g_u, g_v, g_eta, g_Fx,
+                              eta_final, stats);
+}
+
+}  // namespace
+
+extern "C" int sw_adjoint_run(const sw_config* cfg, const sw_static* st, const void* u, const void* v,
+                              const void* eta, const void* eta_obs, int64_t nsteps, int32_t ncheckpoints,
+                              double* J, void* g_u, void* g_v, void* g_eta, void* g_Fx, void* eta_final,
+                              sw_adjoint_stats* stats) {
+    return adjoint_entry(false, cfg, st, u, v, eta, eta_obs, nsteps, ncheckpoints, J, g_u, g_v, g_eta, g_Fx,
+                         eta_final, stats);
+}
+
+#ifdef SWA_HOST_CHECK
+// Host check build (tests only, never part of libswb200.so): the same passes,
+// checkpoint schedule and reductions executed in host loops with every array
+// access checked against its reference shape.  Returns the number of accesses
+// that fell outside in *bounds_failures.
+namespace swa { long long swa_bounds_failures = 0; }
+extern "C" int swa_host_check_run(const sw_config* cfg, const sw_static* st, const void* u, const void* v,
+                                  const void* eta, const void* eta_obs, int64_t nsteps, int32_t ncheckpoints,
+                                  double* J, void* g_u, void* g_v, void* g_eta, void* g_Fx, void* eta_final,
+                                  long long* bounds_failures) {
+    swa::swa_bounds_failures = 0;
+    const int rc = adjoint_entry(true, cfg, st, u, v, eta, eta_obs, nsteps, ncheckpoints, J, g_u, g_v, g_eta, g_Fx,
+                                 eta_final, nullptr);
+    if (bounds_failures) *bounds_failures = swa::swa_bounds_failures;
+    return rc;
+}
+#endif

@@ -78,6 +78,12 @@ class SwStatus(C.Structure):
                 ("code", C.c_int32), ("reserved", C.c_int32)]
 
 
+class SwAdjointStats(C.Structure):
+    _fields_ = [("forward_ms", C.c_double), ("reverse_ms", C.c_double), ("forward_steps", C.c_int64),
+                ("adjoint_steps", C.c_int64), ("checkpoints", C.c_int32), ("launches_per_forward_step", C.c_int32),
+                ("launches_per_adjoint_step", C.c_int32), ("reserved", C.c_int32)]
+
+
 class SwDiag(C.Structure):
     _fields_ = [("mass", C.c_double), ("energy", C.c_double), ("max_speed", C.c_double),
                 ("nan_count", C.c_int64)]
@@ -192,6 +198,9 @@ EXPORTS = {
     "sw_batch_launches": (C.c_int64, [C.c_void_p]),
     "sw_batch_member": (C.c_void_p, [C.c_void_p, C.c_int32]),
     "sw_batch_destroy": (None, [C.c_void_p]),
+    "sw_adjoint_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.c_int64, C.c_int32, C.POINTER(C.c_double), C.c_void_p, C.c_void_p,
+                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "sw_kernel_launches": (C.c_int64, [C.c_void_p]),
     "sw_destroy": (None, [C.c_void_p]),
     "sw_strerror": (C.c_char_p, [C.c_int]),

@@ -40,7 +40,8 @@ def test_python_mirror_covers_exports():
 
 @pytest.mark.parametrize("struct,cname", [(abi.SwConfig, "sw_config"), (abi.SwStatic, "sw_static"),
                                           (abi.SwStatus, "sw_status"), (abi.SwDiag, "sw_diag"),
-                                          (abi.SwProfile, "sw_profile")])
+                                          (abi.SwProfile, "sw_profile"),
+                                          (abi.SwAdjointStats, "sw_adjoint_stats")])
 def test_ctypes_layout_matches_c(struct, cname):
     """sizeof and every field offset of the ctypes mirror equal the C compiler's."""
     fields = [f[0] for f in struct._fields_]
