@@ -170,7 +170,8 @@ def bench_ensemble(args, rank, world, barrier, allmax):
     run_local(warm, threads=2)
     run_batched(warm)
     barrier()
-    table, secs = run_ensemble(members, threads=args.threads, costs=costs, batched=True)
+    binfo = {}
+    table, secs = run_ensemble(members, threads=args.threads, costs=costs, batched=True, info=binfo)
     barrier()
     t = allmax(secs)
     value = sum(costs) / t
@@ -188,8 +189,11 @@ def bench_ensemble(args, rank, world, barrier, allmax):
             "higher_is_better": True, "scaling": "strong", "dtype": "f32", "data": "synthetic (seeded members)",
             "config": {"workload": f"{len(members)} members, nx in {{64..256}}, L_ratio 1-2, periodic/nonperiodic, "
                                    f"{args.days} days each", "mode": "batched: one launch per sub-step for all members",
-                       "cell_updates": int(sum(costs)), "parallelism": f"members sharded over {world} GPU(s)"},
-            "seconds": t, "threaded_value": threaded, "threads": args.threads, "sequential_value": seq,
+                       "cell_updates": int(sum(costs)), "parallelism": f"members sharded over {world} GPU(s)",
+                       "tile_rows": binfo.get("tile_rows")},
+            "seconds": t, "batch_run_seconds": binfo.get("run_seconds"),
+            "batch_run_value": (sum(costs) / binfo["run_seconds"]) if world == 1 and binfo.get("run_seconds") else None,
+            "threaded_value": threaded, "threads": args.threads, "sequential_value": seq,
             "nan_members": int((table[:, COLUMNS.index("nan_count")] > 0).sum())}))
     return 0
 

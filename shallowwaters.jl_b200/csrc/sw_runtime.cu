@@ -1187,19 +1187,25 @@ int run_steps(sw_ctx* ctx, long long nsteps, sw_status* status) {
 // CUDA graphs (by the parity of the step): each group's launches run on a
 // stream of its own, forked from and joined back to the batch stream, and a
 // last one-thread kernel moves the device-side step counter on.
+// Rows per warp strip of the batched stage and tail kernels: the candidates
+// the batch's autotuner times on the first steps of a run.  Every candidate
+// computes the same values (only the assignment of rows to warps differs).
+constexpr int BATCH_NTY = 3;
+constexpr int BATCH_TYS[BATCH_NTY] = {8, 16, 32};
+
 struct BatchGroup {
     int per = 1, rko = 4, drag = 0;
     bool smag = false, um_is_u = true, cons = false, tracer_any = false;
     std::vector<int> idx;                      // member indices
-    StageArgs<float, float>* stage[2][4] = {};  // per parity of X, per stage
-    TailArgs<float, float>* tail[2] = {};
+    StageArgs<float, float>* stage[BATCH_NTY][2][4] = {};  // per tile height, parity of X, stage
+    TailArgs<float, float>* tail[BATCH_NTY][2] = {};
     TracerArgs<float, float>* tracer[2] = {};   // 2n entries: k odd, then k even
     BatchCopy* copy[2] = {};
     BatchNan* nan[2] = {};                      // 2n entries: even, then odd tracer count
     BatchMember* memb = nullptr;
-    int *b_stage = nullptr, *b_tail = nullptr, *b_tracer = nullptr, *nbx_tracer = nullptr, *b_copy = nullptr,
-        *b_nan = nullptr;
-    int n_stage = 0, n_tail = 0, n_tracer = 0, n_copy = 0, n_nan = 0;
+    int *b_stage[BATCH_NTY] = {}, *b_tail[BATCH_NTY] = {}, *b_tracer = nullptr, *nbx_tracer = nullptr,
+        *b_copy = nullptr, *b_nan = nullptr;
+    int n_stage[BATCH_NTY] = {}, n_tail[BATCH_NTY] = {}, n_tracer = 0, n_copy = 0, n_nan = 0;
 };
 
 struct sw_batch {
@@ -1210,9 +1216,11 @@ struct sw_batch {
     std::vector<cudaStream_t> gstreams;        // one per group
     std::vector<cudaEvent_t> events;           // fork, then one join per group
     long long* d_step = nullptr;               // the global step the next replay runs
-    cudaGraphExec_t graph[2] = {};             // global steps i with (i - 1) % 2 == 0, 1
+    cudaGraphExec_t graph[BATCH_NTY][2] = {};  // per tile height; global steps i with (i - 1) % 2 == 0, 1
+    int ty = -1;                               // chosen tile height (index into BATCH_TYS), -1 until tuned
+    std::string shape_key;                     // member shapes and options, the autotuner's cache key
     long long step = 0, max_nt = 0;
-    long long launches = 0, launches_per_step[2] = {};
+    long long launches = 0, launches_per_step[BATCH_NTY][2] = {};
     std::string err;
 };
 
@@ -1269,7 +1277,7 @@ int batch_build(sw_batch* b) {
     }
     for (BatchGroup& gr : b->groups) {
         const int n = (int)gr.idx.size();
-        std::vector<int> cs, ct, ctr, nbx, cc, cn;
+        std::vector<int> cs[BATCH_NTY], ct[BATCH_NTY], ctr, nbx, cc, cn;
         std::vector<BatchMember> mems;
         for (int m : gr.idx) {
             sw_ctx* ctx = b->mem[m];
@@ -1278,8 +1286,12 @@ int batch_build(sw_batch* b) {
             E* e = dynamic_cast<E*>(ctx->eng.get());
             const StageArgs<float, float> s1 = e->stage_args(ctx, 1, 0, true, 1.f, 1.f);
             const TailArgs<float, float> t0 = e->tail_args(ctx, 0);
-            cs.push_back((s1.nsx * s1.nsy + 3) / 4 + s1.nring_blocks);
-            ct.push_back((t0.nsx * t0.nsy + 3) / 4 + t0.nring_blocks);
+            for (int ti = 0; ti < BATCH_NTY; ti++) {
+                const int nsy = (g.M + BATCH_TYS[ti] - 1) / BATCH_TYS[ti];
+                cs[ti].push_back((s1.nsx * nsy + 3) / 4 + s1.nring_blocks);
+                ct[ti].push_back((t0.nsx * nsy + 3) / 4 + t0.nring_blocks);
+            }
+            b->shape_key += std::to_string(g.N) + "x" + std::to_string(g.M) + (c.periodic ? "p" : "n") + ",";
             const int bx = (g.N + 127) / 128, gy = std::min(g.M, 256);
             nbx.push_back(bx);
             ctr.push_back(bx * gy);
@@ -1293,21 +1305,31 @@ int batch_build(sw_batch* b) {
             b->max_nt = std::max(b->max_nt, (long long)c.nt);
         }
         int rc;
+        b->shape_key += "|" + std::to_string(gr.per) + std::to_string(gr.um_is_u) + std::to_string(gr.rko) +
+                        std::to_string(gr.drag) + std::to_string(gr.smag) + std::to_string(gr.cons) + ";";
         for (int p = 0; p < 2; p++) {
-            for (int k = 1; k <= gr.rko; k++) {
-                std::vector<StageArgs<float, float>> v;
-                for (int m : gr.idx)
-                    v.push_back(dynamic_cast<E*>(b->mem[m]->eng.get())->stage_args(b->mem[m], k, p, true, 1.f, 1.f));
-                if ((rc = upload_table(b, v, &gr.stage[p][k - 1]))) return rc;
+            for (int ti = 0; ti < BATCH_NTY; ti++) {
+                for (int k = 1; k <= gr.rko; k++) {
+                    std::vector<StageArgs<float, float>> v;
+                    for (int m : gr.idx) {
+                        v.push_back(dynamic_cast<E*>(b->mem[m]->eng.get())->stage_args(b->mem[m], k, p, true, 1.f, 1.f));
+                        v.back().nsy = (b->mem[m]->g.M + BATCH_TYS[ti] - 1) / BATCH_TYS[ti];
+                    }
+                    if ((rc = upload_table(b, v, &gr.stage[ti][p][k - 1]))) return rc;
+                }
+                std::vector<TailArgs<float, float>> vt;
+                for (int m : gr.idx) {
+                    vt.push_back(dynamic_cast<E*>(b->mem[m]->eng.get())->tail_args(b->mem[m], p));
+                    vt.back().nsy = (b->mem[m]->g.M + BATCH_TYS[ti] - 1) / BATCH_TYS[ti];
+                }
+                if ((rc = upload_table(b, vt, &gr.tail[ti][p]))) return rc;
             }
-            std::vector<TailArgs<float, float>> vt;
             std::vector<TracerArgs<float, float>> vr(2 * n);
             std::vector<BatchCopy> vc;
             std::vector<BatchNan> vn(2 * n);
             for (int q = 0; q < n; q++) {
                 sw_ctx* ctx = b->mem[gr.idx[q]];
                 E* e = dynamic_cast<E*>(ctx->eng.get());
-                vt.push_back(e->tail_args(ctx, p));
                 vr[q] = e->tracer_args(ctx, p, 0);          // k odd: sst[0] -> sst[1]
                 vr[n + q] = e->tracer_args(ctx, p, 1);      // k even: sst[1] -> sst[0]
                 const Fields3& X = ctx->S[p];
@@ -1318,15 +1340,19 @@ int batch_build(sw_batch* b) {
                     vn[par * n + q] = BatchNan{ctx->g, (const float*)X.u, (const float*)X.v, (const float*)X.e,
                                                (const float*)ctx->sst[par], ctx->dst};
             }
-            if ((rc = upload_table(b, vt, &gr.tail[p]))) return rc;
             if ((rc = upload_table(b, vr, &gr.tracer[p]))) return rc;
             if ((rc = upload_table(b, vc, &gr.copy[p]))) return rc;
             if ((rc = upload_table(b, vn, &gr.nan[p]))) return rc;
         }
-        const std::vector<int> ps = prefix(cs), pt = prefix(ct), ptr = prefix(ctr), pc = prefix(cc), pn = prefix(cn);
-        gr.n_stage = ps.back(); gr.n_tail = pt.back(); gr.n_tracer = ptr.back(); gr.n_copy = pc.back(); gr.n_nan = pn.back();
-        if ((rc = upload_table(b, ps, &gr.b_stage)) || (rc = upload_table(b, pt, &gr.b_tail)) ||
-            (rc = upload_table(b, ptr, &gr.b_tracer)) || (rc = upload_table(b, nbx, &gr.nbx_tracer)) ||
+        for (int ti = 0; ti < BATCH_NTY; ti++) {
+            const std::vector<int> ps = prefix(cs[ti]), pt = prefix(ct[ti]);
+            gr.n_stage[ti] = ps.back();
+            gr.n_tail[ti] = pt.back();
+            if ((rc = upload_table(b, ps, &gr.b_stage[ti])) || (rc = upload_table(b, pt, &gr.b_tail[ti]))) return rc;
+        }
+        const std::vector<int> ptr = prefix(ctr), pc = prefix(cc), pn = prefix(cn);
+        gr.n_tracer = ptr.back(); gr.n_copy = pc.back(); gr.n_nan = pn.back();
+        if ((rc = upload_table(b, ptr, &gr.b_tracer)) || (rc = upload_table(b, nbx, &gr.nbx_tracer)) ||
             (rc = upload_table(b, pc, &gr.b_copy)) || (rc = upload_table(b, pn, &gr.b_nan)) ||
             (rc = upload_table(b, mems, &gr.memb)))
             return rc;
@@ -1346,26 +1372,28 @@ int batch_build(sw_batch* b) {
 
 // the launches of group gr for a global step of parity p (the step read from
 // b->d_step), on stream s; returns how many
-template <bool PER>
-int batch_group_step(sw_batch* b, const BatchGroup& gr, int p, cudaStream_t s) {
+template <bool PER, int TY>
+int batch_group_step(sw_batch* b, const BatchGroup& gr, int p, cudaStream_t s, int ti) {
     const int n = (int)gr.idx.size();
     const long long* i = b->d_step;
     int launches = 0;
+    const int nst = gr.n_stage[ti], ntl = gr.n_tail[ti];
+    const int* bst = gr.b_stage[ti];
     for (int k = 1; k <= gr.rko; k++) {
-        const StageArgs<float, float>* a = gr.stage[p][k - 1];
-        if (k == 1) rk_stage_batch<float, float, PER, true, false, STAGE_TY><<<gr.n_stage, 128, 0, s>>>(a, gr.b_stage, n, gr.memb, i);
-        else if (k == gr.rko) rk_stage_batch<float, float, PER, false, true, STAGE_TY><<<gr.n_stage, 128, 0, s>>>(a, gr.b_stage, n, gr.memb, i);
-        else rk_stage_batch<float, float, PER, false, false, STAGE_TY><<<gr.n_stage, 128, 0, s>>>(a, gr.b_stage, n, gr.memb, i);
+        const StageArgs<float, float>* a = gr.stage[ti][p][k - 1];
+        if (k == 1) rk_stage_batch<float, float, PER, true, false, TY><<<nst, 128, 0, s>>>(a, bst, n, gr.memb, i);
+        else if (k == gr.rko) rk_stage_batch<float, float, PER, false, true, TY><<<nst, 128, 0, s>>>(a, bst, n, gr.memb, i);
+        else rk_stage_batch<float, float, PER, false, false, TY><<<nst, 128, 0, s>>>(a, bst, n, gr.memb, i);
     }
-    auto tail = [&](auto kern) { kern<<<gr.n_tail, 128, 0, s>>>(gr.tail[p], gr.b_tail, n, gr.memb, i); };
+    auto tail = [&](auto kern) { kern<<<ntl, 128, 0, s>>>(gr.tail[ti][p], gr.b_tail[ti], n, gr.memb, i); };
     if (gr.smag) {
-        if (gr.drag == SW_DRAG_QUADRATIC) tail(tail_batch<float, float, PER, SW_DRAG_QUADRATIC, true, TAIL_TY>);
-        else if (gr.drag == SW_DRAG_LINEAR) tail(tail_batch<float, float, PER, SW_DRAG_LINEAR, true, TAIL_TY>);
-        else tail(tail_batch<float, float, PER, SW_DRAG_NONE, true, TAIL_TY>);
+        if (gr.drag == SW_DRAG_QUADRATIC) tail(tail_batch<float, float, PER, SW_DRAG_QUADRATIC, true, TY>);
+        else if (gr.drag == SW_DRAG_LINEAR) tail(tail_batch<float, float, PER, SW_DRAG_LINEAR, true, TY>);
+        else tail(tail_batch<float, float, PER, SW_DRAG_NONE, true, TY>);
     } else {
-        if (gr.drag == SW_DRAG_QUADRATIC) tail(tail_batch<float, float, PER, SW_DRAG_QUADRATIC, false, TAIL_TY>);
-        else if (gr.drag == SW_DRAG_LINEAR) tail(tail_batch<float, float, PER, SW_DRAG_LINEAR, false, TAIL_TY>);
-        else tail(tail_batch<float, float, PER, SW_DRAG_NONE, false, TAIL_TY>);
+        if (gr.drag == SW_DRAG_QUADRATIC) tail(tail_batch<float, float, PER, SW_DRAG_QUADRATIC, false, TY>);
+        else if (gr.drag == SW_DRAG_LINEAR) tail(tail_batch<float, float, PER, SW_DRAG_LINEAR, false, TY>);
+        else tail(tail_batch<float, float, PER, SW_DRAG_NONE, false, TY>);
     }
     launches += gr.rko + 1;
     if (gr.tracer_any) {
@@ -1382,9 +1410,18 @@ int batch_group_step(sw_batch* b, const BatchGroup& gr, int p, cudaStream_t s) {
     return launches + 1;
 }
 
-// captures the graph of a global step of parity p: fork to the group streams,
-// each group's launches, join, then batch_advance
-int batch_graph(sw_batch* b, int p) {
+template <bool PER>
+int batch_group_step_ty(sw_batch* b, const BatchGroup& gr, int p, cudaStream_t s, int ti) {
+    switch (BATCH_TYS[ti]) {
+        case 8: return batch_group_step<PER, 8>(b, gr, p, s, ti);
+        case 16: return batch_group_step<PER, 16>(b, gr, p, s, ti);
+        default: return batch_group_step<PER, 32>(b, gr, p, s, ti);
+    }
+}
+
+// captures the graph of a global step of parity p with tile height index ti:
+// fork to the group streams, each group's launches, join, then batch_advance
+int batch_graph(sw_batch* b, int p, int ti) {
     cudaStream_t s = b->stream;
     if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return SW_ERR_CUDA;
     int launches = 0;
@@ -1393,7 +1430,7 @@ int batch_graph(sw_batch* b, int p) {
         const BatchGroup& gr = b->groups[g];
         cudaStream_t gs = b->gstreams[g];
         if ((e = cudaStreamWaitEvent(gs, b->events[0], 0)) != cudaSuccess) break;
-        launches += gr.per ? batch_group_step<true>(b, gr, p, gs) : batch_group_step<false>(b, gr, p, gs);
+        launches += gr.per ? batch_group_step_ty<true>(b, gr, p, gs, ti) : batch_group_step_ty<false>(b, gr, p, gs, ti);
         if ((e = cudaEventRecord(b->events[g + 1], gs)) != cudaSuccess) break;
         e = cudaStreamWaitEvent(s, b->events[g + 1], 0);
     }
@@ -1405,15 +1442,26 @@ int batch_graph(sw_batch* b, int p) {
     cudaGraph_t graph = nullptr;
     const cudaError_t ec = cudaStreamEndCapture(s, &graph);
     if (e == cudaSuccess) e = ec;
-    if (e == cudaSuccess) e = cudaGraphInstantiate(&b->graph[p], graph, 0);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&b->graph[ti][p], graph, 0);
     if (graph) cudaGraphDestroy(graph);
     if (e != cudaSuccess) {
         b->err = std::string("batch graph: ") + cudaGetErrorString(e);
         return SW_ERR_CUDA;
     }
-    b->launches_per_step[p] = launches;
+    b->launches_per_step[ti][p] = launches;
     return SW_OK;
 }
+
+int batch_graphs(sw_batch* b, int ti) {
+    for (int p = 0; p < 2; p++)
+        if (!b->graph[ti][p])
+            if (const int rc = batch_graph(b, p, ti)) return rc;
+    return SW_OK;
+}
+
+// tile heights chosen earlier in this process, by batch shape
+std::mutex g_tune_mu;
+std::map<std::string, int> g_tune_cache;
 
 }  // namespace
 
@@ -1470,18 +1518,84 @@ int sw_batch_run(sw_batch* b, int64_t nsteps, sw_status* statuses) {
     if (!b || nsteps < 0) return SW_ERR_ARG;
     for (sw_ctx* ctx : b->mem)          // states uploaded on the members' own streams
         if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return SW_ERR_CUDA;
-    for (int p = 0; p < 2; p++)
-        if (!b->graph[p])
-            if (const int rc = batch_graph(b, p)) return rc;
     const long long until = std::min(b->max_nt, b->step + (long long)nsteps);
     const long long next = b->step + 1;
     cudaError_t e = cudaMemcpyAsync(b->d_step, &next, sizeof(next), cudaMemcpyHostToDevice, b->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
-    for (long long i = next; i <= until && e == cudaSuccess; i++) {
+    long long i = next;
+    auto launch_step = [&](int ti) {
         const int p = (int)((i - 1) % 2);
-        e = cudaGraphLaunch(b->graph[p], b->stream);
-        b->launches += b->launches_per_step[p];
+        e = cudaGraphLaunch(b->graph[ti][p], b->stream);
+        b->launches += b->launches_per_step[ti][p];
+        i++;
+    };
+    if (b->ty < 0) {   // the tile height: forced, remembered for this shape, or timed now
+        const char* env = getenv("SWB200_BATCH_TY");
+        const int want = env ? atoi(env) : 0;
+        for (int ti = 0; ti < BATCH_NTY; ti++)
+            if (BATCH_TYS[ti] == want) b->ty = ti;
+        if (b->ty < 0) {
+            std::lock_guard<std::mutex> lock(g_tune_mu);
+            auto it = g_tune_cache.find(b->shape_key);
+            if (it != g_tune_cache.end()) b->ty = it->second;
+        }
     }
+    // Autotuner: with no choice yet and enough steps in this call, every
+    // candidate first advances two untimed global steps (both parities: the
+    // graphs' first launches), then TUNE_ROUNDS interleaved rounds time
+    // TUNE_STEPS steps of each candidate; the best round of each decides.
+    // These are real steps of the run (every candidate computes the same
+    // values).  The choice is kept for the batch and for later batches of the
+    // same shape in this process.  SWB200_TUNE_LOG=1 prints the timings.
+    constexpr int TUNE_STEPS = 3, TUNE_ROUNDS = 3;
+    constexpr long long TUNE_TOTAL = (long long)BATCH_NTY * (2 + TUNE_ROUNDS * TUNE_STEPS);
+    if (b->ty < 0 && until - next + 1 > TUNE_TOTAL) {
+        cudaEvent_t ev[TUNE_ROUNDS][BATCH_NTY][2] = {};
+        for (int ti = 0; ti < BATCH_NTY && e == cudaSuccess; ti++) {
+            if (const int rc = batch_graphs(b, ti)) return rc;
+            launch_step(ti);
+            if (e == cudaSuccess) launch_step(ti);
+        }
+        for (int r = 0; r < TUNE_ROUNDS && e == cudaSuccess; r++)
+            for (int ti = 0; ti < BATCH_NTY && e == cudaSuccess; ti++) {
+                e = cudaEventCreate(&ev[r][ti][0]);
+                if (e == cudaSuccess) e = cudaEventCreate(&ev[r][ti][1]);
+                if (e == cudaSuccess) e = cudaEventRecord(ev[r][ti][0], b->stream);
+                for (int k = 0; k < TUNE_STEPS && e == cudaSuccess; k++) launch_step(ti);
+                if (e == cudaSuccess) e = cudaEventRecord(ev[r][ti][1], b->stream);
+            }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+        float best_ms[BATCH_NTY];
+        for (float& x : best_ms) x = 1e30f;
+        for (int r = 0; r < TUNE_ROUNDS && e == cudaSuccess; r++)
+            for (int ti = 0; ti < BATCH_NTY && e == cudaSuccess; ti++) {
+                float ms = 0.f;
+                e = cudaEventElapsedTime(&ms, ev[r][ti][0], ev[r][ti][1]);
+                best_ms[ti] = std::min(best_ms[ti], ms);
+            }
+        for (auto& rr : ev)
+            for (auto& pr : rr)
+                for (cudaEvent_t x : pr)
+                    if (x) cudaEventDestroy(x);
+        if (e == cudaSuccess) {
+            int best = BATCH_NTY - 1;
+            for (int ti = 0; ti < BATCH_NTY; ti++)
+                if (best_ms[ti] < best_ms[best]) best = ti;
+            const char* lg = getenv("SWB200_TUNE_LOG");
+            if (lg && lg[0] == '1') {
+                fprintf(stderr, "swb200: batch tile rows:");
+                for (int ti = 0; ti < BATCH_NTY; ti++) fprintf(stderr, " %d: %.3f ms", BATCH_TYS[ti], best_ms[ti]);
+                fprintf(stderr, " -> %d\n", BATCH_TYS[best]);
+            }
+            b->ty = best;
+            std::lock_guard<std::mutex> lock(g_tune_mu);
+            g_tune_cache[b->shape_key] = best;
+        }
+    }
+    const int ti = b->ty >= 0 ? b->ty : BATCH_NTY - 1;   // short calls before any tuning: the tallest tile
+    if (e == cudaSuccess)
+        if (const int rc = batch_graphs(b, ti)) return rc;
+    while (i <= until && e == cudaSuccess) launch_step(ti);
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
     if (e != cudaSuccess) {
@@ -1526,6 +1640,8 @@ int sw_batch_get_state(sw_batch* b, int32_t member, void* u, void* v, void* eta,
 
 int64_t sw_batch_launches(const sw_batch* b) { return b ? b->launches : 0; }
 
+int32_t sw_batch_tile_rows(const sw_batch* b) { return (b && b->ty >= 0) ? BATCH_TYS[b->ty] : 0; }
+
 sw_ctx* sw_batch_member(sw_batch* b, int32_t member) {
     return (b && member >= 0 && member < (int)b->mem.size()) ? b->mem[member] : nullptr;
 }
@@ -1533,8 +1649,9 @@ sw_ctx* sw_batch_member(sw_batch* b, int32_t member) {
 void sw_batch_destroy(sw_batch* b) {
     if (!b) return;
     if (b->stream) cudaStreamSynchronize(b->stream);
-    for (cudaGraphExec_t g : b->graph)
-        if (g) cudaGraphExecDestroy(g);
+    for (auto& gp : b->graph)
+        for (cudaGraphExec_t g : gp)
+            if (g) cudaGraphExecDestroy(g);
     for (cudaEvent_t ev : b->events) cudaEventDestroy(ev);
     for (cudaStream_t st : b->gstreams) cudaStreamDestroy(st);
     for (auto& t : b->tables) cached_free(t.first, t.second);

@@ -196,6 +196,7 @@ EXPORTS = {
     "sw_batch_run": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p]),
     "sw_batch_get_state": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "sw_batch_launches": (C.c_int64, [C.c_void_p]),
+    "sw_batch_tile_rows": (C.c_int32, [C.c_void_p]),
     "sw_batch_member": (C.c_void_p, [C.c_void_p, C.c_int32]),
     "sw_batch_destroy": (None, [C.c_void_p]),
     "sw_adjoint_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

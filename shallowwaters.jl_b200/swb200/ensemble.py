@@ -95,10 +95,13 @@ def run_member(m: Member) -> np.ndarray:
                     dtype=np.float64)
 
 
-def run_batched(members: List[Member], lib=None, return_states: bool = False):
+def run_batched(members: List[Member], lib=None, return_states: bool = False, info: Optional[dict] = None):
     """Run members as one batch (sw_batch_*): one launch per sub-step for all
     members sharing the boundary type and options.  Returns {index: row of
-    COLUMNS} (and the final states without halo when ``return_states``)."""
+    COLUMNS} (and the final states without halo when ``return_states``).
+    ``info``, if given, receives the batch's tile height ("tile_rows"), its
+    kernel launches ("launches") and the seconds of the sw_batch_run call
+    ("run_seconds": the steps only, without member set-up and uploads)."""
     import ctypes as C
     from . import abi
     from .initial_conditions import remove_halo
@@ -116,9 +119,15 @@ def run_batched(members: List[Member], lib=None, return_states: bool = False):
             states.append(arrs)
             abi.check(lib, lib.sw_batch_set_state(b, k, *abi.state_ptrs(*arrs)))
         status = (abi.SwStatus * len(members))()
+        t0 = time.perf_counter()
         rc = lib.sw_batch_run(b, 1 << 62, status)
+        run_seconds = time.perf_counter() - t0
         if rc not in (abi.SW_OK, abi.SW_NAN_DETECTED):
             abi.check(lib, rc)
+        if info is not None:
+            info["tile_rows"] = int(lib.sw_batch_tile_rows(b))
+            info["launches"] = int(lib.sw_batch_launches(b))
+            info["run_seconds"] = run_seconds
         out, fin = {}, {}
         for k, (m, (P, S, _)) in enumerate(zip(members, setups)):
             d = abi.SwDiag()
@@ -145,7 +154,8 @@ def run_local(members: List[Member], threads: int = 8,
 
 
 def run_ensemble(members: List[Member], *, threads: int = 8, costs: Optional[List[int]] = None,
-                 runner: Callable[[Member], np.ndarray] = run_member, batched: bool = False):
+                 runner: Callable[[Member], np.ndarray] = run_member, batched: bool = False,
+                 info: Optional[dict] = None):
     """Run an ensemble over all ranks of the default process group (or alone).
 
     Returns ``(table, seconds)``: the (len(members), len(COLUMNS)) FP64 table of
@@ -159,7 +169,7 @@ def run_ensemble(members: List[Member], *, threads: int = 8, costs: Optional[Lis
         costs = [member_cost(m) for m in members]
     mine = [members[i] for i in partition(costs, world)[rank]]
     t0 = time.perf_counter()
-    local = run_batched(mine) if batched and mine else run_local(mine, threads, runner)
+    local = run_batched(mine, info=info) if batched and mine else run_local(mine, threads, runner)
     seconds = time.perf_counter() - t0
     table = np.zeros((len(members), len(COLUMNS)), dtype=np.float64)
     pos = {m.index: k for k, m in enumerate(members)}

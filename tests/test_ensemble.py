@@ -74,6 +74,55 @@ def test_concurrent_members_equal_lone_runs():
         assert together[k][COLUMNS.index("nan_count")] == 0
 
 
+def _batch_members():
+    return [
+        Member(0, dict(nx=24, Ndays=0.3, Uadv=1000), seed=1),
+        Member(1, dict(nx=40, L_ratio=1, Ndays=0.2, bc="nonperiodic", α=0.0, topography="seamount"), seed=2),
+        Member(2, dict(nx=64, Ndays=0.25, Uadv=1000, diffusion="Smagorinsky"), seed=3),
+        Member(3, dict(nx=30, Ndays=0.4, Uadv=1000, bc="nonperiodic", α=0.5), seed=4),
+        Member(4, dict(nx=32, Ndays=0.5, Uadv=2.0), seed=5),                      # tracer every few steps
+        Member(5, dict(nx=36, Ndays=0.5, Uadv=2.5, tracer_consumption=True), seed=6),
+        Member(6, dict(nx=28, Ndays=0.3, Uadv=1000, adv_scheme="Sadourny", surface_relax=True), seed=7),
+    ]
+
+
+def _lone_states(members):
+    from swb200.ensemble import member_setup
+    from swb200 import Model
+    from swb200.initial_conditions import remove_halo
+    out = {}
+    for m in members:
+        P, S, Prog = member_setup(m)
+        with Model(S) as model:
+            model.set_state(Prog)
+            st = model.run(S.grid.nt)
+            out[m.index] = (remove_halo(*model.get_state(), S), st.steps_done, S.grid.nt)
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rows", ["8", "16", "32", "tuned"])
+def test_every_batch_tile_height_equals_lone_runs(rows, monkeypatch):
+    """The autotuner's candidates (forced with SWB200_BATCH_TY) and its own
+    choice all give the lone runs' results bit for bit."""
+    from swb200.ensemble import run_batched
+    if rows != "tuned":
+        monkeypatch.setenv("SWB200_BATCH_TY", rows)
+    else:
+        monkeypatch.delenv("SWB200_BATCH_TY", raising=False)
+    members = _batch_members()[:4]
+    info = {}
+    table, states = run_batched(members, return_states=True, info=info)
+    if rows == "tuned":
+        assert info["tile_rows"] in (8, 16, 32)
+    else:
+        assert info["tile_rows"] == int(rows)
+    for k, (ref, done, nt) in _lone_states(members).items():
+        assert table[k][COLUMNS.index("steps")] == done == nt
+        for x, y in zip(states[k], ref):
+            assert np.array_equal(x.view(np.uint32), y.view(np.uint32))
+
+
 @pytest.mark.gpu
 def test_batched_members_equal_lone_runs():
     """sw_batch_*: members of different sizes, boundaries and tracer schedules,
