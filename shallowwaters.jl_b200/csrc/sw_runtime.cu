@@ -194,6 +194,7 @@ struct sw_ctx {
     struct StepGraph { cudaGraphExec_t exec = nullptr; long long launches = 0; bool flips_sp = false; };
     std::map<unsigned, StepGraph> graphs;
     int nsm = 148;
+    int tail_ty = TAIL_TY;        // rows per warp strip of the streaming tail (see pick_tail_ty)
     DevStatus* dst = nullptr;     // device status
     DiagPartial* diag = nullptr;  // DIAG_BLOCKS partials + the result (allocated on first use)
     DevStatus* hst = nullptr;     // pinned host mirror
@@ -223,6 +224,25 @@ cudaEvent_t sw_ctx::evget() {
 }
 
 namespace {
+
+// Strip height of the streaming tail for Float32 / Float64 contexts: the
+// tallest of 32, 16, 8 rows whose strips still give four blocks (the
+// resident limit at the tail's register count) per SM, else 8.
+// SWB200_TAIL_TY=8|16|32 forces one.  Other number types keep 32.
+int pick_tail_ty(const sw_config& c, const Geom& g, int nsm) {
+    if (c.T != c.Tprog || (c.T != SW_FLOAT32 && c.T != SW_FLOAT64)) return TAIL_TY;
+    const char* env = getenv("SWB200_TAIL_TY");
+    if (env) {
+        const int want = atoi(env);
+        if (want == 8 || want == 16 || want == 32) return want;
+    }
+    const int nsx = (g.N + STRIP - 1) / STRIP;
+    for (int ty : {32, 16, 8}) {
+        const long long blocks = ((long long)nsx * ((g.M + ty - 1) / ty) + 3) / 4;
+        if (blocks >= 4LL * nsm) return ty;
+    }
+    return 8;
+}
 
 int fail(sw_ctx* c, int code, const std::string& msg) {
     if (c) c->err = msg;
@@ -490,8 +510,15 @@ struct Engine : EngineBase {
         return stage2_launch<false, false, false>(ctx, a, mp);
     }
 
+    // Shorter strips for Float32 / Float64 grids too small to fill the GPU
+    // with 32-row strips (the values do not depend on the strip height).
     template <bool PER, int DRAG, bool SMAG>
-    static void tail_launch(const TailArgs<T, Tp>& a, int nblk, cudaStream_t s) {
+    static void tail_launch(const TailArgs<T, Tp>& a, int nblk, cudaStream_t s, int ty) {
+        constexpr bool SAME = std::is_same<T, Tp>::value && (std::is_same<T, float>::value || std::is_same<T, double>::value);
+        if constexpr (SAME) {
+            if (ty == 8) { tail_kernel<T, Tp, PER, DRAG, SMAG, 8><<<nblk, 128, 0, s>>>(a); return; }
+            if (ty == 16) { tail_kernel<T, Tp, PER, DRAG, SMAG, 16><<<nblk, 128, 0, s>>>(a); return; }
+        }
         tail_kernel<T, Tp, PER, DRAG, SMAG, TAIL_TY><<<nblk, 128, 0, s>>>(a);
     }
     // TMA-fed tail (Float32): returns -1 if it cannot be configured
@@ -532,15 +559,15 @@ struct Engine : EngineBase {
         return tail_tma_launch<PER, SW_DRAG_NONE, false, true>(ctx, a, mp);
     }
     template <bool PER>
-    static void tail_dispatch2(const TailArgs<T, Tp>& a, int drag, bool smag, int nblk, cudaStream_t s) {
+    static void tail_dispatch2(const TailArgs<T, Tp>& a, int drag, bool smag, int nblk, cudaStream_t s, int ty) {
         if (smag) {
-            if (drag == SW_DRAG_QUADRATIC) tail_launch<PER, SW_DRAG_QUADRATIC, true>(a, nblk, s);
-            else if (drag == SW_DRAG_LINEAR) tail_launch<PER, SW_DRAG_LINEAR, true>(a, nblk, s);
-            else tail_launch<PER, SW_DRAG_NONE, true>(a, nblk, s);
+            if (drag == SW_DRAG_QUADRATIC) tail_launch<PER, SW_DRAG_QUADRATIC, true>(a, nblk, s, ty);
+            else if (drag == SW_DRAG_LINEAR) tail_launch<PER, SW_DRAG_LINEAR, true>(a, nblk, s, ty);
+            else tail_launch<PER, SW_DRAG_NONE, true>(a, nblk, s, ty);
         } else {
-            if (drag == SW_DRAG_QUADRATIC) tail_launch<PER, SW_DRAG_QUADRATIC, false>(a, nblk, s);
-            else if (drag == SW_DRAG_LINEAR) tail_launch<PER, SW_DRAG_LINEAR, false>(a, nblk, s);
-            else tail_launch<PER, SW_DRAG_NONE, false>(a, nblk, s);
+            if (drag == SW_DRAG_QUADRATIC) tail_launch<PER, SW_DRAG_QUADRATIC, false>(a, nblk, s, ty);
+            else if (drag == SW_DRAG_LINEAR) tail_launch<PER, SW_DRAG_LINEAR, false>(a, nblk, s, ty);
+            else tail_launch<PER, SW_DRAG_NONE, false>(a, nblk, s, ty);
         }
     }
     template <bool PER>
@@ -748,7 +775,7 @@ struct Engine : EngineBase {
         const Fields3& Y = ctx->S[1 - p];
         TailArgs<T, Tp> a;
         a.g = g;
-        a.nsx = (g.N + STRIP - 1) / STRIP; a.nsy = (g.M + TAIL_TY - 1) / TAIL_TY;
+        a.nsx = (g.N + STRIP - 1) / STRIP; a.nsy = (g.M + ctx->tail_ty - 1) / ctx->tail_ty;
         a.nring_blocks = ring_blocks(g, 128);
         a.u0 = (const Tp*)ctx->Acc.u; a.v0 = (const Tp*)ctx->Acc.v; a.e0 = (const Tp*)Y.e;
         a.uo = (Tp*)Y.u; a.vo = (Tp*)Y.v;
@@ -854,8 +881,8 @@ struct Engine : EngineBase {
                 if (!rc && lr) rc = fail(ctx, SW_ERR_CUDA, "TMA tail kernel could not be configured");
             } else {
                 rc = launch(ctx, 1, [&] {
-                    if (g.ep) tail_dispatch2<true>(a, c.bottom_drag, smag, nb, ctx->stream);
-                    else tail_dispatch2<false>(a, c.bottom_drag, smag, nb, ctx->stream);
+                    if (g.ep) tail_dispatch2<true>(a, c.bottom_drag, smag, nb, ctx->stream, ctx->tail_ty);
+                    else tail_dispatch2<false>(a, c.bottom_drag, smag, nb, ctx->stream, ctx->tail_ty);
                 });
             }
             if (rc) return rc;
@@ -1790,6 +1817,7 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
         ctx->tail_tma = (envt && envt[0] == '1');
         const char* envg = getenv("SWB200_GRAPHS");
         ctx->use_graphs = !(envg && envg[0] == '0');
+        ctx->tail_ty = pick_tail_ty(*cfg, g, ctx->nsm);
     }
     if (cfg->T == SW_FLOAT32 && cfg->Tprog == SW_FLOAT32) {
         auto* e = new Engine<float, float>(); ctx->eng.reset(e); if ((rc = e->init(ctx))) return rc;

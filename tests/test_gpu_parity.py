@@ -192,6 +192,17 @@ def test_kernel_launch_count():
     assert m.kernel_launches - n0 >= 60
 
 
+@pytest.mark.parametrize("rows", ["8", "16", "32"])
+@pytest.mark.parametrize("kw", [dict(diffusion="Smagorinsky"), dict(bc="nonperiodic", α=0.5, T=np.float64)])
+def test_every_tail_strip_height_is_bit_exact(rows, kw, monkeypatch):
+    """The streaming tail's strip height (chosen by grid size, forced here with
+    SWB200_TAIL_TY) does not change a bit of the result."""
+    monkeypatch.setenv("SWB200_TAIL_TY", rows)
+    k = dict(BASE)
+    k.update(kw)
+    both(k, 0, checkpoints=[1, 5])
+
+
 def test_graph_replay_equals_direct_launches(monkeypatch):
     """Steps replayed from CUDA graphs equal steps launched one kernel at a
     time, over enough steps to use every graph key (parities, tracer and
