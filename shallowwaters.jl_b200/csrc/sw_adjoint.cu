@@ -176,31 +176,32 @@ struct Work {
 
 // ------------------------------------------------------------ ghost points
 // ghost_points! (src/ghost_points.jl:182-199) on u, v (and eta); with uv_only
-// only ghost_points_uv! (:202-216).  Two launches: eta's y-halo rows copy the
-// x-halo columns written by the first (src/ghost_points.jl:119-133).
+// only ghost_points_uv! (:202-216).  One thread per halo copy (row or column
+// t, copy q of four).  Two launches: eta's y-halo rows copy the x-halo columns
+// written by the first (src/ghost_points.jl:119-133).
 template <class T>
 void ghost(Launcher& L, const Work<T>& w, const State<T>& s, bool uv_only) {
     const A2<T> u = s.u, v = s.v, e = s.e;
     const int ep = w.ep;
     const T c = w.oma;
     const int nmax = std::max(std::max(u.m, u.n), std::max(std::max(v.m, v.n), std::max(e.m, e.n)));
-    L.d1(nmax, [=] __host__ __device__(long long k) {
-        const int t = (int)k + 1;
-        if (ep) {
-            if (t <= u.n) { const int m = u.m; u(1, t) = u(m - 3, t); u(2, t) = u(m - 2, t); u(m - 1, t) = u(3, t); u(m, t) = u(4, t); }
-            if (t <= v.n) { const int m = v.m; v(1, t) = v(m - 3, t); v(2, t) = v(m - 2, t); v(m - 1, t) = v(3, t); v(m, t) = v(4, t); }
-            if (!uv_only && t <= e.n) { const int m = e.m; e(1, t) = e(m - 1, t); e(m, t) = e(2, t); }
-        } else {
-            if (t <= u.m) { const int n = u.n; u(t, 1) = c * u(t, 4); u(t, 2) = c * u(t, 3); u(t, n - 1) = c * u(t, n - 2); u(t, n) = c * u(t, n - 3); }
-            if (t <= v.n) { const int m = v.m; v(1, t) = c * v(4, t); v(2, t) = c * v(3, t); v(m - 1, t) = c * v(m - 2, t); v(m, t) = c * v(m - 3, t); }
-            if (!uv_only && t <= e.n) { const int m = e.m; e(1, t) = e(2, t); e(m, t) = e(m - 1, t); }
+    L.d1(4LL * nmax, [=] __host__ __device__(long long k) {
+        const int t = (int)(k >> 2) + 1, q = (int)(k & 3);
+        if (ep) {   // x-halo columns 1, 2, m-1, m from m-3, m-2, 3, 4
+            if (t <= u.n) { const int m = u.m, d[4] = {1, 2, m - 1, m}, sx[4] = {m - 3, m - 2, 3, 4}; u(d[q], t) = u(sx[q], t); }
+            if (t <= v.n) { const int m = v.m, d[4] = {1, 2, m - 1, m}, sx[4] = {m - 3, m - 2, 3, 4}; v(d[q], t) = v(sx[q], t); }
+            if (!uv_only && q < 2 && t <= e.n) { const int m = e.m; if (q == 0) e(1, t) = e(m - 1, t); else e(m, t) = e(2, t); }
+        } else {    // u: y-halo rows 1, 2, n-1, n from 4, 3, n-2, n-3; v: x-halo columns likewise
+            if (t <= u.m) { const int n = u.n, d[4] = {1, 2, n - 1, n}, sy[4] = {4, 3, n - 2, n - 3}; u(t, d[q]) = c * u(t, sy[q]); }
+            if (t <= v.n) { const int m = v.m, d[4] = {1, 2, m - 1, m}, sx[4] = {4, 3, m - 2, m - 3}; v(d[q], t) = c * v(sx[q], t); }
+            if (!uv_only && q < 2 && t <= e.n) { const int m = e.m; if (q == 0) e(1, t) = e(2, t); else e(m, t) = e(m - 1, t); }
         }
     });
     if (uv_only) return;
-    L.d1(e.m, [=] __host__ __device__(long long k) {
-        const int i = (int)k + 1, n = e.n;
-        e(i, 1) = e(i, 2);
-        e(i, n) = e(i, n - 1);
+    L.d1(2LL * e.m, [=] __host__ __device__(long long k) {
+        const int i = (int)(k >> 1) + 1, n = e.n;
+        if (k & 1) e(i, n) = e(i, n - 1);
+        else e(i, 1) = e(i, 2);
     });
 }
 
@@ -212,43 +213,41 @@ void ghostT(Launcher& L, const Work<T>& w, const State<T>& s, bool uv_only) {
     const T c = w.oma;
     const T zero = T(0);
     if (!uv_only)
-        L.d1(e.m, [=] __host__ __device__(long long k) {
-            const int i = (int)k + 1, n = e.n;
-            e(i, 2) += e(i, 1); e(i, 1) = zero;
-            e(i, n - 1) += e(i, n); e(i, n) = zero;
+        L.d1(2LL * e.m, [=] __host__ __device__(long long k) {
+            const int i = (int)(k >> 1) + 1, n = e.n;
+            if (k & 1) { e(i, n - 1) += e(i, n); e(i, n) = zero; }
+            else { e(i, 2) += e(i, 1); e(i, 1) = zero; }
         });
     const int nmax = std::max(std::max(u.m, u.n), std::max(std::max(v.m, v.n), std::max(e.m, e.n)));
-    L.d1(nmax, [=] __host__ __device__(long long k) {
-        const int t = (int)k + 1;
+    L.d1(4LL * nmax, [=] __host__ __device__(long long k) {
+        const int t = (int)(k >> 2) + 1, q = (int)(k & 3);
         if (ep) {
             if (t <= u.n) {
-                const int m = u.m;
-                u(m - 3, t) += u(1, t); u(m - 2, t) += u(2, t); u(3, t) += u(m - 1, t); u(4, t) += u(m, t);
-                u(1, t) = zero; u(2, t) = zero; u(m - 1, t) = zero; u(m, t) = zero;
+                const int m = u.m, d[4] = {1, 2, m - 1, m}, sx[4] = {m - 3, m - 2, 3, 4};
+                u(sx[q], t) += u(d[q], t); u(d[q], t) = zero;
             }
             if (t <= v.n) {
-                const int m = v.m;
-                v(m - 3, t) += v(1, t); v(m - 2, t) += v(2, t); v(3, t) += v(m - 1, t); v(4, t) += v(m, t);
-                v(1, t) = zero; v(2, t) = zero; v(m - 1, t) = zero; v(m, t) = zero;
+                const int m = v.m, d[4] = {1, 2, m - 1, m}, sx[4] = {m - 3, m - 2, 3, 4};
+                v(sx[q], t) += v(d[q], t); v(d[q], t) = zero;
             }
-            if (!uv_only && t <= e.n) {
+            if (!uv_only && q < 2 && t <= e.n) {
                 const int m = e.m;
-                e(m - 1, t) += e(1, t); e(2, t) += e(m, t); e(1, t) = zero; e(m, t) = zero;
+                if (q == 0) { e(m - 1, t) += e(1, t); e(1, t) = zero; }
+                else { e(2, t) += e(m, t); e(m, t) = zero; }
             }
         } else {
             if (t <= u.m) {
-                const int n = u.n;
-                u(t, 4) += c * u(t, 1); u(t, 3) += c * u(t, 2); u(t, n - 2) += c * u(t, n - 1); u(t, n - 3) += c * u(t, n);
-                u(t, 1) = zero; u(t, 2) = zero; u(t, n - 1) = zero; u(t, n) = zero;
+                const int n = u.n, d[4] = {1, 2, n - 1, n}, sy[4] = {4, 3, n - 2, n - 3};
+                u(t, sy[q]) += c * u(t, d[q]); u(t, d[q]) = zero;
             }
             if (t <= v.n) {
-                const int m = v.m;
-                v(4, t) += c * v(1, t); v(3, t) += c * v(2, t); v(m - 2, t) += c * v(m - 1, t); v(m - 3, t) += c * v(m, t);
-                v(1, t) = zero; v(2, t) = zero; v(m - 1, t) = zero; v(m, t) = zero;
+                const int m = v.m, d[4] = {1, 2, m - 1, m}, sx[4] = {4, 3, m - 2, m - 3};
+                v(sx[q], t) += c * v(d[q], t); v(d[q], t) = zero;
             }
-            if (!uv_only && t <= e.n) {
+            if (!uv_only && q < 2 && t <= e.n) {
                 const int m = e.m;
-                e(2, t) += e(1, t); e(m - 1, t) += e(m, t); e(1, t) = zero; e(m, t) = zero;
+                if (q == 0) { e(2, t) += e(1, t); e(1, t) = zero; }
+                else { e(m - 1, t) += e(m, t); e(m, t) = zero; }
             }
         }
     });
