@@ -282,8 +282,10 @@ void sw_batch_destroy(sw_batch* b);
  * Inputs and outputs are HOST buffers in T: u, v, eta the initial state,
  * eta_obs nx x ny; g_u, g_v, g_eta (state shapes), g_Fx and eta_final (the eta
  * after nsteps, with halo) may be NULL.  ncheckpoints >= nsteps keeps every
- * step state on the device; fewer slots recompute states with the binomial
- * checkpoint schedule.  The derivative of sqrt at 0 (drag and Smagorinsky at
+ * step state on the device and, memory permitting (off with
+ * SWB200_ADJ_STORE=0), every step's RK stage inputs and tail input as well, so
+ * the reverse sweep recomputes only each pass's intermediates; fewer slots
+ * recompute states with the binomial checkpoint schedule.  The derivative of sqrt at 0 (drag and Smagorinsky at
  * rest) is taken as 0.  Gradients are summed with atomics, so repeated calls
  * agree to rounding, not bit for bit.  stats may be NULL. */
 typedef struct sw_adjoint_stats {
@@ -294,7 +296,7 @@ typedef struct sw_adjoint_stats {
     int32_t checkpoints;               /* state slots used                            */
     int32_t launches_per_forward_step;
     int32_t launches_per_adjoint_step;
-    int32_t reserved;
+    int32_t stored_stage_states;       /* 1: every step's stage inputs were kept (no forward recomputation) */
 } sw_adjoint_stats;
 int sw_adjoint_run(const sw_config* cfg, const sw_static* st,
                    const void* u, const void* v, const void* eta, const void* eta_obs,

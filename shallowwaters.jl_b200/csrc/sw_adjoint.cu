@@ -159,6 +159,8 @@ struct Work {
     State<T> X;                 // the state being advanced (in / out of a step)
     State<T> Ys[4];             // stage inputs after their ghost points; Ys[0] = ghosted start state
     State<T> Z;                 // RK result after ghost points = the tail's input
+    T* stage_block = nullptr;   // Ys[0..rko-1] and Z, contiguous in this order
+    size_t stage_block_elems = 0;
     State<T> Xb, acc, Yb[2];    // adjoints: of the step output / input, of the stage inputs
     // stage intermediates (src/preallocate.jl:70-152, 227-254)
     A2<T> hu, hv, hq, U, V, q, qa, qb, qc, qd, p;
@@ -459,9 +461,10 @@ void stage_rev(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const St
 // ------------------------------------------------------------ tail, forward
 // bottom_drag! (src/bottom_drag.jl:2-119), diffusion! (src/diffusion.jl:2-218)
 // and add_drag_diff_tendencies! (src/diffusion.jl:221-251) on Z; the result
-// goes to X (eta copied), then ghost_points_uv! (src/time_integration.jl:231).
+// goes to *Xs (eta copied), then ghost_points_uv! (src/time_integration.jl:231).
+// With Xs null only the intermediates the reverse tail reads are formed.
 template <class T>
-void tail_fwd(Launcher& L, const Work<T>& w, const State<T>& Zs, const State<T>& Xs) {
+void tail_fwd(Launcher& L, const Work<T>& w, const State<T>& Zs, const State<T>* Xs) {
     const A2<T> u = Zs.u, v = Zs.v, e = Zs.e, H = w.H;
     const A2<T> thu = w.thu, thv = w.thv, sKE = w.sKE, Lu = w.Lu, Lv = w.Lv, sDT = w.sDT, sDS = w.sDS, DSq = w.DSq;
     const int nx = w.nx, ny = w.ny, ep = w.ep, drag = w.drag;
@@ -543,9 +546,10 @@ void tail_fwd(Launcher& L, const Work<T>& w, const State<T>& Zs, const State<T>&
         if (i <= S21.m && j <= S21.n) S21(i, j) = smag ? nuSq(i, j) * dLvdx(i, j) : nuB * dLvdx(i, j);
         if (i <= S22.m && j <= S22.n) S22(i, j) = smag ? nuS(i, j + 1) * dLvdy(i, j) : nuB * dLvdy(i, j);
     });
+    if (!Xs) return;
     const int nux = w.nux, nuy = w.nuy, nvx = w.nvx, nvy = w.nvy;
     const T Dt = w.Dt_diff;
-    const A2<T> xu = Xs.u, xv = Xs.v, xe = Xs.e;
+    const A2<T> xu = Xs->u, xv = Xs->v, xe = Xs->e;
     L.d2(nx + 4, ny + 4, [=] __host__ __device__(int I, int J) {
         if (I <= u.m && J <= u.n) {
             T r = u(I, J);
@@ -569,7 +573,7 @@ void tail_fwd(Launcher& L, const Work<T>& w, const State<T>& Zs, const State<T>&
         }
         if (I <= e.m && J <= e.n) xe(I, J) = e(I, J);
     });
-    ghost(L, w, Xs, true);
+    ghost(L, w, *Xs, true);
 }
 
 // ------------------------------------------------------------ tail, reverse
@@ -747,15 +751,18 @@ void fwd_step(Launcher& L, const Work<T>& w) {
         stage_update(L, w, k, w.Ys[0], k < w.rko ? &w.Ys[k] : nullptr, w.Z);
     }
     ghost(L, w, w.Z, false);
-    tail_fwd(L, w, w.Z, w.X);
+    tail_fwd(L, w, w.Z, &w.X);
 }
 
-// adjoint of one step: on entry X holds the step's input state and Xb the
-// adjoint of its output; on return Xb holds the adjoint of the input, and bFx
-// has this step's forcing adjoint added.
+// adjoint of one step: on entry Xb holds the adjoint of the step's output and
+// either X its input state (stored = false: the step is recomputed) or Ys and
+// Z its stage inputs and tail input as the forward sweep kept them (stored =
+// true: only the passes' intermediates are recomputed).  On return Xb holds
+// the adjoint of the input, and bFx has this step's forcing adjoint added.
 template <class T>
-void adj_step(Launcher& L, const Work<T>& w) {
-    fwd_step(L, w);
+void adj_step(Launcher& L, const Work<T>& w, bool stored) {
+    if (stored) tail_fwd(L, w, w.Z, (const State<T>*)nullptr);
+    else fwd_step(L, w);
     ghostT(L, w, w.Xb, true);
     tail_rev(L, w, w.Z, w.Xb);
     ghostT(L, w, w.Xb, false);     // Xb is now the adjoint of the RK sum X0
@@ -764,7 +771,7 @@ void adj_step(Launcher& L, const Work<T>& w) {
     for (int k = w.rko; k >= 1; k--) {
         const State<T>& Yb = w.Yb[k % 2];
         L.zero(Yb.base, Yb.elems * sizeof(T));
-        if (k < w.rko) stage_fwd(L, w, w.Ys[k - 1]);   // the last stage's intermediates are still in place
+        if (stored || k < w.rko) stage_fwd(L, w, w.Ys[k - 1]);   // after fwd_step the last stage's are in place
         stage_rev(L, w, k, w.Ys[k - 1], w.Xb, Wb, Yb);
         if (k > 1) ghostT(L, w, Yb, false);             // Ys[k-1] = ghost(Y1)
         const T* src = Yb.base;
@@ -833,7 +840,9 @@ struct Adjoint {
     bool host = false;
     std::vector<void*> blocks;
     cudaStream_t s = nullptr;
-    cudaGraphExec_t g_fwd = nullptr, g_adj = nullptr;
+    cudaGraphExec_t g_fwd = nullptr, g_adj = nullptr, g_adj_st = nullptr;
+    T* records = nullptr;       // per step: Ys[0..rko-1] and Z as the forward sweep left them
+    bool stored = false;
     std::vector<State<T>> slots;
     long long fwd_steps = 0, adj_steps = 0;
     int launches_fwd = 0, launches_adj = 0;
@@ -843,6 +852,7 @@ struct Adjoint {
         if (s) cudaStreamSynchronize(s);
         if (g_fwd) cudaGraphExecDestroy(g_fwd);
         if (g_adj) cudaGraphExecDestroy(g_adj);
+        if (g_adj_st) cudaGraphExecDestroy(g_adj_st);
         for (void* p : blocks) {
             if (host) std::free(p); else cudaFree(p);
         }
@@ -916,7 +926,7 @@ struct Adjoint {
         return carve(c, &st.base, &st.elems);
     }
 
-    int setup(const sw_config& c, const sw_static& stt) {
+    int setup(const sw_config& c, const sw_static& stt, bool want_store, long long nsteps) {
         if (!host && cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return SW_ERR_CUDA;
         w.nx = c.nx; w.ny = c.ny; w.ep = c.periodic ? 1 : 0;
         w.nux = w.ep ? c.nx : c.nx - 1; w.nuy = c.ny; w.nvx = c.nx; w.nvy = c.ny - 1;
@@ -939,11 +949,24 @@ struct Adjoint {
                 if (upload(dst[k]->d, src[k], dst[k]->size() * sizeof(T)) != cudaSuccess) return SW_ERR_CUDA;
             }
         }
-        if (!make_state(w.X) || !make_state(w.Z) || !make_state(w.Xb) || !make_state(w.acc) || !make_state(w.Yb[0]) ||
-            !make_state(w.Yb[1]))
+        if (!make_state(w.X) || !make_state(w.Xb) || !make_state(w.acc) || !make_state(w.Yb[0]) || !make_state(w.Yb[1]))
             return SW_ERR_NOMEM;
-        for (int k = 0; k < w.rko; k++)
-            if (!make_state(w.Ys[k])) return SW_ERR_NOMEM;
+        {
+            Carver cv;   // the stage inputs Ys[0..rko-1] and the tail input Z, contiguous (one copy saves them)
+            std::vector<State<T>*> st;
+            for (int k = 0; k < w.rko; k++) st.push_back(&w.Ys[k]);
+            st.push_back(&w.Z);
+            for (State<T>* x : st) {
+                cv.add(x->u, w.nux + 4, w.nuy + 4);
+                cv.add(x->v, w.nvx + 4, w.nvy + 4);
+                cv.add(x->e, w.nx + 2, w.ny + 2);
+            }
+            if (!carve(cv, &w.stage_block, &w.stage_block_elems)) return SW_ERR_NOMEM;
+            for (State<T>* x : st) {
+                x->base = x->u.d;
+                x->elems = Carver::padded(x->u.m, x->u.n) + Carver::padded(x->v.m, x->v.n) + Carver::padded(x->e.m, x->e.n);
+            }
+        }
         {
             Carver cv;   // stage intermediates
             cv.add(w.hu, nx + 1, ny + 2); cv.add(w.hv, nx + 2, ny + 1); cv.add(w.hq, nx + 1, ny + 1);
@@ -984,25 +1007,38 @@ struct Adjoint {
             cv.add(w.bDS, nx + 2, ny + 2); cv.add(w.bDT, nx + 2, ny + 2); cv.add(w.bDSq, nvx + 3, nvy + 4);
             if (!carve(cv, &w.tail_adj, &w.tail_adj_elems)) return SW_ERR_NOMEM;
         }
+        if (want_store) {   // one record per step; without the memory the steps are recomputed instead
+            const size_t n = (size_t)nsteps * w.stage_block_elems;
+            void* p = nullptr;
+            if (host) p = std::calloc(n, sizeof(T));
+            else if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) { p = nullptr; cudaGetLastError(); }
+            if (p) {
+                blocks.push_back(p);
+                records = static_cast<T*>(p);
+                stored = true;
+            }
+        }
         return host ? SW_OK : capture();
     }
 
     int capture() {
-        for (int k = 0; k < 2; k++) {
+        for (int k = 0; k < 3; k++) {
             if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return SW_ERR_CUDA;
             Launcher L = launcher();
-            if (k == 0) fwd_step(L, w); else adj_step(L, w);
+            if (k == 0) fwd_step(L, w);
+            else adj_step(L, w, k == 2);
             cudaError_t e = cudaGetLastError();
             cudaGraph_t graph = nullptr;
             const cudaError_t ec = cudaStreamEndCapture(s, &graph);
             if (e == cudaSuccess) e = ec;
-            if (e == cudaSuccess) e = cudaGraphInstantiate(k == 0 ? &g_fwd : &g_adj, graph, 0);
+            if (e == cudaSuccess) e = cudaGraphInstantiate(k == 0 ? &g_fwd : (k == 1 ? &g_adj : &g_adj_st), graph, 0);
             if (graph) cudaGraphDestroy(graph);
             if (e != cudaSuccess) {
                 err = std::string("adjoint graph: ") + cudaGetErrorString(e);
                 return SW_ERR_CUDA;
             }
-            (k == 0 ? launches_fwd : launches_adj) = L.launches;
+            if (k == 0) launches_fwd = L.launches;
+            else if (k == (stored ? 2 : 1)) launches_adj = L.launches;
         }
         return SW_OK;
     }
@@ -1018,8 +1054,15 @@ struct Adjoint {
     }
     cudaError_t adjoint_here() {   // Xb <- adjoint of the step that starts at the state in X
         adj_steps++;
-        if (host) { Launcher L = launcher(); adj_step(L, w); return cudaSuccess; }
+        if (host) { Launcher L = launcher(); adj_step(L, w, false); return cudaSuccess; }
         return cudaGraphLaunch(g_adj, s);
+    }
+    cudaError_t adjoint_stored(long long k) {   // Xb <- adjoint of step k from its kept stage states
+        Launcher L = launcher();
+        L.copy(w.stage_block, records + (size_t)k * w.stage_block_elems, w.stage_block_elems * sizeof(T));
+        adj_steps++;
+        if (host) { adj_step(L, w, true); return cudaSuccess; }
+        return cudaGraphLaunch(g_adj_st, s);
     }
     cudaError_t adjoint_of(const State<T>& state) {
         copy(w.X, state);
@@ -1069,14 +1112,19 @@ int adjoint_run(bool host, const sw_config& c, const sw_static& st, const void* 
                 void* g_eta, void* g_Fx, void* eta_final, sw_adjoint_stats* stats) {
     Adjoint<T> A;
     A.host = host;
-    int rc = A.setup(c, st);
+    // Keeping every step's stage inputs (rko + 1 states a step) spares the
+    // reverse sweep the recomputation of the forward step; it needs a slot per
+    // step and is off with SWB200_ADJ_STORE=0.
+    const char* env = getenv("SWB200_ADJ_STORE");
+    const bool want_store = ncheckpoints >= nsteps && !(env && env[0] == '0');
+    int rc = A.setup(c, st, want_store, nsteps);
     if (rc) {
         if (!A.err.empty()) fprintf(stderr, "swb200: %s\n", A.err.c_str());
         return rc;
     }
     Work<T>& w = A.w;
     const size_t bytes_u = w.X.u.size() * sizeof(T), bytes_v = w.X.v.size() * sizeof(T), bytes_e = w.X.e.size() * sizeof(T);
-    const int nslots = (int)std::max<long long>(1, std::min<long long>(ncheckpoints, nsteps));
+    const int nslots = A.stored ? 1 : (int)std::max<long long>(1, std::min<long long>(ncheckpoints, nsteps));
     A.slots.resize(nslots);
     for (auto& sl : A.slots)
         if (!A.make_state(sl)) return SW_ERR_NOMEM;
@@ -1095,10 +1143,14 @@ int adjoint_run(bool host, const sw_config& c, const sw_static& st, const void* 
     record(0);
     // forward sweep: with a slot per step every state is kept, otherwise only the first
     A.copy(w.X, A.slots[0]);
-    const bool keep_all = nslots >= nsteps;
+    const bool keep_all = !A.stored && nslots >= nsteps;
     for (long long k = 1; k <= nsteps && e == cudaSuccess; k++) {
         e = A.advance(1);
         if (keep_all && k < nsteps) A.copy(A.slots[k], w.X);
+        if (A.stored) {
+            Launcher L = A.launcher();
+            L.copy(A.records + (size_t)(k - 1) * w.stage_block_elems, w.stage_block, w.stage_block_elems * sizeof(T));
+        }
     }
     record(1);
     // J (FP64 row sums, added on the host in a fixed order) and the seed Xb = dJ/d(state at nsteps)
@@ -1116,7 +1168,9 @@ int adjoint_run(bool host, const sw_config& c, const sw_static& st, const void* 
     if (e == cudaSuccess) e = A.zero(w.bFx.d, w.bFx.size() * sizeof(T));
     // reverse sweep
     if (e == cudaSuccess) {
-        if (keep_all) {
+        if (A.stored) {
+            for (long long k = nsteps - 1; k >= 0 && e == cudaSuccess; k--) e = A.adjoint_stored(k);
+        } else if (keep_all) {
             for (long long k = nsteps - 1; k >= 0 && e == cudaSuccess; k--) e = A.adjoint_of(A.slots[k]);
         } else {
             e = A.reverse(0, nsteps, 0);
@@ -1151,7 +1205,7 @@ int adjoint_run(bool host, const sw_config& c, const sw_static& st, const void* 
         stats->checkpoints = nslots;
         stats->launches_per_forward_step = A.launches_fwd;
         stats->launches_per_adjoint_step = A.launches_adj;
-        stats->reserved = 0;
+        stats->stored_stage_states = A.stored ? 1 : 0;
     }
     return SW_OK;
 }

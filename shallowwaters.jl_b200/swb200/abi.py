@@ -81,7 +81,7 @@ class SwStatus(C.Structure):
 class SwAdjointStats(C.Structure):
     _fields_ = [("forward_ms", C.c_double), ("reverse_ms", C.c_double), ("forward_steps", C.c_int64),
                 ("adjoint_steps", C.c_int64), ("checkpoints", C.c_int32), ("launches_per_forward_step", C.c_int32),
-                ("launches_per_adjoint_step", C.c_int32), ("reserved", C.c_int32)]
+                ("launches_per_adjoint_step", C.c_int32), ("stored_stage_states", C.c_int32)]
 
 
 class SwDiag(C.Structure):

@@ -144,6 +144,14 @@ def test_host_check_of_the_adjoint_passes(host_check_lib, opts):
     assert bad3 == 0 and J3 == J
     for a, b in zip(g3, g):
         assert np.array_equal(a, b)
+    os.environ["SWB200_ADJ_STORE"] = "0"       # every state kept, steps recomputed instead of stored
+    try:
+        J0, g0, _, bad0 = host_check_gradient(host_check_lib, S, Prog, obs, n, n)
+    finally:
+        del os.environ["SWB200_ADJ_STORE"]
+    assert bad0 == 0 and J0 == J
+    for a, b in zip(g0, g):
+        assert np.array_equal(a, b)
 
 
 @pytest.mark.gpu
@@ -179,11 +187,17 @@ def test_gradient_matches_dual_directional_derivative(opts):
 
 
 @pytest.mark.gpu
-def test_checkpoint_schedule_does_not_change_the_gradient():
+def test_checkpoint_schedule_does_not_change_the_gradient(monkeypatch):
     S, Prog, obs, _ = setup(nx=64, seed=5)
     n = 37
     full = gradient(S, Prog, obs, n)
-    assert full.stats.forward_steps == n
+    assert full.stats.forward_steps == n and full.stats.stored_stage_states == 1
+    monkeypatch.setenv("SWB200_ADJ_STORE", "0")
+    rec = gradient(S, Prog, obs, n)
+    monkeypatch.delenv("SWB200_ADJ_STORE")
+    assert rec.stats.stored_stage_states == 0 and rec.J == full.J
+    for a, b in ((rec.u, full.u), (rec.v, full.v), (rec.eta, full.eta), (rec.Fx, full.Fx)):
+        np.testing.assert_allclose(a, b, rtol=1e-9, atol=1e-12 * np.abs(b).max())
     for nc in (6, 2, 1):
         r = gradient(S, Prog, obs, n, ncheckpoints=nc)
         assert r.J == full.J
