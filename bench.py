@@ -171,12 +171,16 @@ def bench_ensemble(args, rank, world, barrier, allmax):
     run_batched(warm)
     barrier()
     binfo = {}
-    table, secs = run_ensemble(members, threads=args.threads, costs=costs, batched=True, info=binfo)
+    table, secs = run_ensemble(members, threads=args.threads, costs=costs, batched=True, info=binfo,
+                               chunks=args.chunks)
     barrier()
     t = allmax(secs)
     value = sum(costs) / t
     threaded = seq = None
     if world == 1:
+        one = {}                                    # a single batch, for the time of its steps alone
+        run_ensemble(members, costs=costs, batched=True, info=one, chunks=1)
+        binfo["run_seconds"] = one["run_seconds"]
         t0 = time.perf_counter()
         run_local(members, threads=args.threads)
         threaded = sum(costs) / (time.perf_counter() - t0)
@@ -190,7 +194,8 @@ def bench_ensemble(args, rank, world, barrier, allmax):
             "config": {"workload": f"{len(members)} members, nx in {{64..256}}, L_ratio 1-2, periodic/nonperiodic, "
                                    f"{args.days} days each", "mode": "batched: one launch per sub-step for all members",
                        "cell_updates": int(sum(costs)), "parallelism": f"members sharded over {world} GPU(s)",
-                       "tile_rows": binfo.get("tile_rows")},
+                       "tile_rows": binfo.get("chunk_tile_rows"), "batches": args.chunks,
+                       "pipelining": "each batch runs on a worker thread while the next is set up"},
             "seconds": t, "batch_run_seconds": binfo.get("run_seconds"),
             "batch_run_value": (sum(costs) / binfo["run_seconds"]) if world == 1 and binfo.get("run_seconds") else None,
             "threaded_value": threaded, "threads": args.threads, "sequential_value": seq,
@@ -256,6 +261,7 @@ def main():
     ap.add_argument("--members", type=int, default=256)
     ap.add_argument("--days", type=float, default=1.0, help="model days per ensemble member")
     ap.add_argument("--threads", type=int, default=8, help="members run at once per GPU")
+    ap.add_argument("--chunks", type=int, default=2, help="ensemble batches per GPU, pipelined with their set-up")
     ap.add_argument("--form", default="fp32", choices=["fp32", "bf16", "f16"],
                     help="state storage between steps: plain FP32 or compensated 16-bit pairs (u, v scaled by 2^10)")
     args = ap.parse_args()

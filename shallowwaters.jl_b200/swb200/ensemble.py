@@ -95,17 +95,10 @@ def run_member(m: Member) -> np.ndarray:
                     dtype=np.float64)
 
 
-def run_batched(members: List[Member], lib=None, return_states: bool = False, info: Optional[dict] = None):
-    """Run members as one batch (sw_batch_*): one launch per sub-step for all
-    members sharing the boundary type and options.  Returns {index: row of
-    COLUMNS} (and the final states without halo when ``return_states``).
-    ``info``, if given, receives the batch's tile height ("tile_rows"), its
-    kernel launches ("launches") and the seconds of the sw_batch_run call
-    ("run_seconds": the steps only, without member set-up and uploads)."""
+def _batch_create(members: List[Member], lib):
+    """Host set-up of the members and the batch (sw_batch_create + states)."""
     import ctypes as C
     from . import abi
-    from .initial_conditions import remove_halo
-    lib = lib or abi.load_library()
     setups = [member_setup(m) for m in members]
     cfgs = (abi.SwConfig * len(members))(*[abi.make_config(S) for _, S, _ in setups])
     statics = [abi.StaticFields(S) for _, S, _ in setups]
@@ -118,16 +111,27 @@ def run_batched(members: List[Member], lib=None, return_states: bool = False, in
             arrs = [np.ascontiguousarray(a, dtype=P.Tprog) for a in Prog]
             states.append(arrs)
             abi.check(lib, lib.sw_batch_set_state(b, k, *abi.state_ptrs(*arrs)))
+    except Exception:
+        lib.sw_batch_destroy(b)
+        raise
+    return b, setups, states
+
+
+def _batch_run(lib, b, members, setups, states, return_states):
+    """Runs a created batch to its end, collects each member's row (and state)
+    and destroys it.  Returns (rows, states, info)."""
+    import ctypes as C
+    from . import abi
+    from .initial_conditions import remove_halo
+    try:
         status = (abi.SwStatus * len(members))()
         t0 = time.perf_counter()
         rc = lib.sw_batch_run(b, 1 << 62, status)
         run_seconds = time.perf_counter() - t0
         if rc not in (abi.SW_OK, abi.SW_NAN_DETECTED):
             abi.check(lib, rc)
-        if info is not None:
-            info["tile_rows"] = int(lib.sw_batch_tile_rows(b))
-            info["launches"] = int(lib.sw_batch_launches(b))
-            info["run_seconds"] = run_seconds
+        info = {"tile_rows": int(lib.sw_batch_tile_rows(b)), "launches": int(lib.sw_batch_launches(b)),
+                "run_seconds": run_seconds}
         out, fin = {}, {}
         for k, (m, (P, S, _)) in enumerate(zip(members, setups)):
             d = abi.SwDiag()
@@ -140,6 +144,52 @@ def run_batched(members: List[Member], lib=None, return_states: bool = False, in
                 fin[m.index] = remove_halo(*arrs, S)
     finally:
         lib.sw_batch_destroy(b)
+    return out, fin, info
+
+
+def run_batched(members: List[Member], lib=None, return_states: bool = False, info: Optional[dict] = None,
+                chunks: int = 1):
+    """Run members as batches (sw_batch_*): one launch per sub-step for all
+    members of a batch sharing the boundary type and options.  Returns
+    {index: row of COLUMNS} (and the final states without halo when
+    ``return_states``).
+
+    ``chunks`` > 1 splits the members (round robin by decreasing cost) into
+    that many batches and pipelines them: while a batch runs on a worker
+    thread (the library call releases the GIL), the next one is set up on the
+    host, and the batches' steps overlap on the GPU.  ``info``, if given,
+    receives the tile heights ("tile_rows", "chunk_tile_rows"), kernel
+    launches ("launches") and, for one batch, the seconds of the sw_batch_run
+    call ("run_seconds": the steps only, without member set-up and uploads)."""
+    from . import abi
+    lib = lib or abi.load_library()
+    if chunks <= 1 or len(members) < 2 * chunks:
+        b, setups, states = _batch_create(members, lib)
+        out, fin, inf = _batch_run(lib, b, members, setups, states, return_states)
+        if info is not None:
+            info.update(inf)
+            info["chunk_tile_rows"] = [inf["tile_rows"]]
+        return (out, fin) if return_states else out
+    order = sorted(members, key=lambda m: -(m.kwargs.get("nx", 0) ** 2))
+    groups = [order[k::chunks] for k in range(chunks)]
+    futs = []
+    with cf.ThreadPoolExecutor(max_workers=chunks) as ex:
+        try:
+            for grp in groups:
+                b, setups, states = _batch_create(grp, lib)
+                futs.append(ex.submit(_batch_run, lib, b, grp, setups, states, return_states))
+        finally:
+            results = [f.result() for f in futs]
+    out, fin = {}, {}
+    for o, f, _ in results:
+        out.update(o)
+        fin.update(f)
+    if info is not None:
+        infos = [r[2] for r in results]
+        info["tile_rows"] = infos[0]["tile_rows"]
+        info["chunk_tile_rows"] = [x["tile_rows"] for x in infos]
+        info["launches"] = sum(x["launches"] for x in infos)
+        info["run_seconds"] = None
     return (out, fin) if return_states else out
 
 
@@ -155,7 +205,7 @@ def run_local(members: List[Member], threads: int = 8,
 
 def run_ensemble(members: List[Member], *, threads: int = 8, costs: Optional[List[int]] = None,
                  runner: Callable[[Member], np.ndarray] = run_member, batched: bool = False,
-                 info: Optional[dict] = None):
+                 info: Optional[dict] = None, chunks: int = 1):
     """Run an ensemble over all ranks of the default process group (or alone).
 
     Returns ``(table, seconds)``: the (len(members), len(COLUMNS)) FP64 table of
@@ -169,7 +219,7 @@ def run_ensemble(members: List[Member], *, threads: int = 8, costs: Optional[Lis
         costs = [member_cost(m) for m in members]
     mine = [members[i] for i in partition(costs, world)[rank]]
     t0 = time.perf_counter()
-    local = run_batched(mine, info=info) if batched and mine else run_local(mine, threads, runner)
+    local = run_batched(mine, info=info, chunks=chunks) if batched and mine else run_local(mine, threads, runner)
     seconds = time.perf_counter() - t0
     table = np.zeros((len(members), len(COLUMNS)), dtype=np.float64)
     pos = {m.index: k for k, m in enumerate(members)}

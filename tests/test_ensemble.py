@@ -101,6 +101,21 @@ def _lone_states(members):
 
 
 @pytest.mark.gpu
+def test_pipelined_batches_equal_lone_runs():
+    """Members split into two batches that run on worker threads while the
+    next is set up end where each member ends alone, bit for bit."""
+    from swb200.ensemble import run_batched
+    members = _batch_members()
+    info = {}
+    table, states = run_batched(members, return_states=True, info=info, chunks=2)
+    assert len(info["chunk_tile_rows"]) == 2
+    for k, (ref, done, nt) in _lone_states(members).items():
+        assert table[k][COLUMNS.index("steps")] == done == nt
+        for x, y in zip(states[k], ref):
+            assert np.array_equal(x.view(np.uint32), y.view(np.uint32))
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("rows", ["8", "16", "32", "tuned"])
 def test_every_batch_tile_height_equals_lone_runs(rows, monkeypatch):
     """The autotuner's candidates (forced with SWB200_BATCH_TY) and its own
