@@ -119,8 +119,8 @@ def test_bitwise_parity(name):
 
 
 def test_reference_config_c1_one_day():
-    """configs[0]'s physics (periodic channel, Smagorinsky, quadratic drag,
-    tracer every step) at 100x50 for one day: identical to the oracle."""
+    """The periodic wind-driven channel at 100x50 (Smagorinsky, quadratic drag,
+    tracer every step) for one day: identical to the oracle."""
     kw = dict(nx=100, L_ratio=2, bc="periodic", wind_forcing_x="channel", Fx0=0.12, topography="flat",
               H=500, g=10, cfl=1, adv_scheme="ArakawaHsu", diffusion="Smagorinsky",
               bottom_drag="quadratic", tracer_advection=True, Uadv=1000, Ndays=1)
