@@ -178,9 +178,18 @@ struct Work {
 
 // ------------------------------------------------------------ ghost points
 // ghost_points! (src/ghost_points.jl:182-199) on u, v (and eta); with uv_only
-// only ghost_points_uv! (:202-216).  One thread per halo copy (row or column
-// t, copy q of four).  Two launches: eta's y-halo rows copy the x-halo columns
-// written by the first (src/ghost_points.jl:119-133).
+// only ghost_points_uv! (:202-216).  One launch, one thread per halo copy
+// (row or column t, copy q of four).  eta's y-halo rows copy row 2 and row
+// n-1 after its x-halo columns were set (src/ghost_points.jl:119-133), so the
+// corner of row 1 (or n) takes the x-halo source of row 2 (or n-1) directly:
+// etasrc(i) is that column.
+template <class T>
+__host__ __device__ __forceinline__ int etasrc(int i, int m, int ep) {
+    if (i == 1) return ep ? m - 1 : 2;
+    if (i == m) return ep ? 2 : m - 1;
+    return i;
+}
+
 template <class T>
 void ghost(Launcher& L, const Work<T>& w, const State<T>& s, bool uv_only) {
     const A2<T> u = s.u, v = s.v, e = s.e;
@@ -192,18 +201,21 @@ void ghost(Launcher& L, const Work<T>& w, const State<T>& s, bool uv_only) {
         if (ep) {   // x-halo columns 1, 2, m-1, m from m-3, m-2, 3, 4
             if (t <= u.n) { const int m = u.m, d[4] = {1, 2, m - 1, m}, sx[4] = {m - 3, m - 2, 3, 4}; u(d[q], t) = u(sx[q], t); }
             if (t <= v.n) { const int m = v.m, d[4] = {1, 2, m - 1, m}, sx[4] = {m - 3, m - 2, 3, 4}; v(d[q], t) = v(sx[q], t); }
-            if (!uv_only && q < 2 && t <= e.n) { const int m = e.m; if (q == 0) e(1, t) = e(m - 1, t); else e(m, t) = e(2, t); }
         } else {    // u: y-halo rows 1, 2, n-1, n from 4, 3, n-2, n-3; v: x-halo columns likewise
             if (t <= u.m) { const int n = u.n, d[4] = {1, 2, n - 1, n}, sy[4] = {4, 3, n - 2, n - 3}; u(t, d[q]) = c * u(t, sy[q]); }
             if (t <= v.n) { const int m = v.m, d[4] = {1, 2, m - 1, m}, sx[4] = {4, 3, m - 2, m - 3}; v(d[q], t) = c * v(sx[q], t); }
-            if (!uv_only && q < 2 && t <= e.n) { const int m = e.m; if (q == 0) e(1, t) = e(2, t); else e(m, t) = e(m - 1, t); }
         }
-    });
-    if (uv_only) return;
-    L.d1(2LL * e.m, [=] __host__ __device__(long long k) {
-        const int i = (int)(k >> 1) + 1, n = e.n;
-        if (k & 1) e(i, n) = e(i, n - 1);
-        else e(i, 1) = e(i, 2);
+        if (uv_only) return;
+        const int m = e.m, n = e.n;
+        if (q < 2) {   // x-halo columns of rows 2..n-1
+            if (t >= 2 && t <= n - 1) {
+                if (q == 0) e(1, t) = e(etasrc<T>(1, m, ep), t);
+                else e(m, t) = e(etasrc<T>(m, m, ep), t);
+            }
+        } else if (t <= m) {   // y-halo rows 1 and n, corners included
+            if (q == 2) e(t, 1) = e(etasrc<T>(t, m, ep), 2);
+            else e(t, n) = e(etasrc<T>(t, m, ep), n - 1);
+        }
     });
 }
 
@@ -214,12 +226,6 @@ void ghostT(Launcher& L, const Work<T>& w, const State<T>& s, bool uv_only) {
     const int ep = w.ep;
     const T c = w.oma;
     const T zero = T(0);
-    if (!uv_only)
-        L.d1(2LL * e.m, [=] __host__ __device__(long long k) {
-            const int i = (int)(k >> 1) + 1, n = e.n;
-            if (k & 1) { e(i, n - 1) += e(i, n); e(i, n) = zero; }
-            else { e(i, 2) += e(i, 1); e(i, 1) = zero; }
-        });
     const int nmax = std::max(std::max(u.m, u.n), std::max(std::max(v.m, v.n), std::max(e.m, e.n)));
     L.d1(4LL * nmax, [=] __host__ __device__(long long k) {
         const int t = (int)(k >> 2) + 1, q = (int)(k & 3);
@@ -232,11 +238,6 @@ void ghostT(Launcher& L, const Work<T>& w, const State<T>& s, bool uv_only) {
                 const int m = v.m, d[4] = {1, 2, m - 1, m}, sx[4] = {m - 3, m - 2, 3, 4};
                 v(sx[q], t) += v(d[q], t); v(d[q], t) = zero;
             }
-            if (!uv_only && q < 2 && t <= e.n) {
-                const int m = e.m;
-                if (q == 0) { e(m - 1, t) += e(1, t); e(1, t) = zero; }
-                else { e(2, t) += e(m, t); e(m, t) = zero; }
-            }
         } else {
             if (t <= u.m) {
                 const int n = u.n, d[4] = {1, 2, n - 1, n}, sy[4] = {4, 3, n - 2, n - 3};
@@ -246,11 +247,22 @@ void ghostT(Launcher& L, const Work<T>& w, const State<T>& s, bool uv_only) {
                 const int m = v.m, d[4] = {1, 2, m - 1, m}, sx[4] = {4, 3, m - 2, m - 3};
                 v(sx[q], t) += c * v(d[q], t); v(d[q], t) = zero;
             }
-            if (!uv_only && q < 2 && t <= e.n) {
-                const int m = e.m;
-                if (q == 0) { e(2, t) += e(1, t); e(1, t) = zero; }
-                else { e(m - 1, t) += e(m, t); e(m, t) = zero; }
+        }
+        if (uv_only) return;
+        // eta: sources of rows 2 and n-1 are shared by the x-halo and y-halo
+        // copies, so those sums are atomic; every halo cell is read and
+        // cleared by one thread only
+        const int m = e.m, n = e.n;
+        if (q < 2) {
+            if (t >= 2 && t <= n - 1) {
+                const int d = q == 0 ? 1 : m;
+                add(e(etasrc<T>(d, m, ep), t), e(d, t));
+                e(d, t) = zero;
             }
+        } else if (t <= m) {
+            const int r = q == 2 ? 1 : n, rs = q == 2 ? 2 : n - 1;
+            add(e(etasrc<T>(t, m, ep), rs), e(t, r));
+            e(t, r) = zero;
         }
     });
 }
@@ -267,17 +279,22 @@ void stage_fwd(Launcher& L, const Work<T>& w, const State<T>& Y) {
     L.d2(nx + 2, ny + 2, [=] __host__ __device__(int i, int j) {
         const T half = T(0.5), quarter = T(0.25);
         auto h = [&](int a, int b) { return e(a, b) + H(a, b); };
-        if (i <= nx + 1) hu(i, j) = half * (h(i + 1, j) + h(i, j));
-        if (j <= ny + 1) hv(i, j) = half * (h(i, j + 1) + h(i, j));
-        if (i <= nx + 1 && j <= ny + 1) hq(i, j) = quarter * (h(i, j) + h(i + 1, j)) + quarter * (h(i, j + 1) + h(i + 1, j + 1));
-    });
-    L.d2(nx + 2, ny + 2, [=] __host__ __device__(int i, int j) {
-        if (i <= nx + 1) U(i, j) = u(1 + ep + i, 1 + j) * hu(i, j);
-        if (j <= ny + 1) V(i, j) = v(i + 1, j + 1) * hv(i, j);
+        if (i <= nx + 1) {
+            const T hu_ = half * (h(i + 1, j) + h(i, j));
+            hu(i, j) = hu_;
+            U(i, j) = u(1 + ep + i, 1 + j) * hu_;
+        }
+        if (j <= ny + 1) {
+            const T hv_ = half * (h(i, j + 1) + h(i, j));
+            hv(i, j) = hv_;
+            V(i, j) = v(i + 1, j + 1) * hv_;
+        }
         if (i <= nx + 1 && j <= ny + 1) {
+            const T hq_ = quarter * (h(i, j) + h(i + 1, j)) + quarter * (h(i, j + 1) + h(i + 1, j + 1));
+            hq(i, j) = hq_;
             const T dvdx = v(i + 2, j + 1) - v(i + 1, j + 1);
             const T dudy = u(i + 1 + ep, j + 2) - u(i + 1 + ep, j + 1);
-            q(i, j) = (f_q(i, j) + dvdx - dudy) / hq(i, j);
+            q(i, j) = (f_q(i, j) + dvdx - dudy) / hq_;
         }
     });
     const A2<T> qa = w.qa, qb = w.qb, qc = w.qc, qd = w.qd, p = w.p;
