@@ -165,14 +165,13 @@ struct Work {
     // stage intermediates (src/preallocate.jl:70-152, 227-254)
     A2<T> hu, hv, hq, U, V, q, qa, qb, qc, qd, p;
     // their adjoints
-    A2<T> bU, bV, bp, bqa, bqb, bqc, bqd, bq, bhu, bhv, bhq;
+    A2<T> bU, bV, bp, bqa, bqb, bqc, bqd, bq;
     // tail intermediates (src/preallocate.jl:193-222, 259-338)
     A2<T> thu, thv, sKE, sKEu, sKEv, Bu, Bv, Lu, Lv, dLudx, dLudy, dLvdx, dLvdy, sDT, sDS, DSq, rS, nuS, nuSq, S11,
         S12, S21, S22;
-    A2<T> bBu, bBv, bS11, bS12, bS21, bS22, bnuS, bnuSq, bdLudx, bdLudy, bdLvdx, bdLvdy, bLu, bLv, bsKE, bsKEu,
-        bsKEv, bthu, bthv, bDS, bDT, bDSq;
+    A2<T> bBu, bBv, bS11, bS12, bS21, bS22, bnuS, bLu, bLv, bsKE, bDSq;
     A2<T> bFx;                  // gradient with respect to Fx
-    T* stage_adj = nullptr; size_t stage_adj_elems = 0;   // bU..bhq, one block (zeroed per stage)
+    T* stage_adj = nullptr; size_t stage_adj_elems = 0;   // bU..bq, one block (zeroed per stage)
     T* tail_adj = nullptr; size_t tail_adj_elems = 0;     // bBu..bDSq, one block (zeroed per step)
 };
 
@@ -381,7 +380,7 @@ void stage_rev(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const St
     const A2<T> u = Y.u, v = Y.v;
     const A2<T> hu = w.hu, hv = w.hv, hq = w.hq, U = w.U, V = w.V, q = w.q, qa = w.qa, qb = w.qb, qc = w.qc, qd = w.qd;
     const A2<T> bU = w.bU, bV = w.bV, bp = w.bp, bqa = w.bqa, bqb = w.bqb, bqc = w.bqc, bqd = w.bqd, bq = w.bq,
-                bhu = w.bhu, bhv = w.bhv, bhq = w.bhq, bFx = w.bFx;
+                bFx = w.bFx;
     const int nx = w.nx, ny = w.ny, nux = w.nux, nuy = w.nuy, nvx = w.nvx, nvy = w.nvy, ep = w.ep;
     const T a = w.RKa[k - 1], b = Wb ? w.RKb[k - 1] : T(0);
     const State<T> x0 = Xb0, wb = Wb ? *Wb : Xb0, yb = Yb;
@@ -444,33 +443,28 @@ void stage_rev(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const St
             else { add(bq(i - 1, j + 1), tb); add(bq(i - 1, j), tc); }
         }
     });
-    // PV^T, Uflux^T, Vflux^T
+    // PV^T, Uflux^T, Vflux^T, each followed at once by the Ixy^T, Ix^T, Iy^T of
+    // h = eta + H that its h_q, h_u, h_v adjoint (formed here alone) feeds
     L.d2(nx + 2, ny + 2, [=] __host__ __device__(int i, int j) {
+        const T half = T(0.5), quarter = T(0.25);
         if (i <= nx + 1 && j <= ny + 1) {
             const T n = bq(i, j) / hq(i, j);
             add(yb.v(i + 2, j + 1), n); add(yb.v(i + 1, j + 1), -n);
             add(yb.u(i + 1 + ep, j + 2), -n); add(yb.u(i + 1 + ep, j + 1), n);
-            bhq(i, j) = -(n * q(i, j));
+            const T t = quarter * -(n * q(i, j));
+            add(yb.e(i, j), t); add(yb.e(i + 1, j), t); add(yb.e(i, j + 1), t); add(yb.e(i + 1, j + 1), t);
         }
         if (i <= nx + 1) {
             const T wU = bU(i, j);
             add(yb.u(1 + ep + i, 1 + j), wU * hu(i, j));
-            bhu(i, j) = wU * u(1 + ep + i, 1 + j);
+            const T t = half * (wU * u(1 + ep + i, 1 + j));
+            add(yb.e(i + 1, j), t); add(yb.e(i, j), t);
         }
         if (j <= ny + 1) {
             const T wV = bV(i, j);
             add(yb.v(i + 1, j + 1), wV * hv(i, j));
-            bhv(i, j) = wV * v(i + 1, j + 1);
-        }
-    });
-    // Ix^T, Iy^T, Ixy^T of h = eta + H
-    L.d2(nx + 2, ny + 2, [=] __host__ __device__(int i, int j) {
-        const T half = T(0.5), quarter = T(0.25);
-        if (i <= nx + 1) { const T t = half * bhu(i, j); add(yb.e(i + 1, j), t); add(yb.e(i, j), t); }
-        if (j <= ny + 1) { const T t = half * bhv(i, j); add(yb.e(i, j + 1), t); add(yb.e(i, j), t); }
-        if (i <= nx + 1 && j <= ny + 1) {
-            const T t = quarter * bhq(i, j);
-            add(yb.e(i, j), t); add(yb.e(i + 1, j), t); add(yb.e(i, j + 1), t); add(yb.e(i + 1, j + 1), t);
+            const T t = half * (wV * v(i + 1, j + 1));
+            add(yb.e(i, j + 1), t); add(yb.e(i, j), t);
         }
     });
 }
@@ -554,13 +548,15 @@ void tail_fwd(Launcher& L, const Work<T>& w, const State<T>& Zs, const State<T>*
             else if (drag == SW_DRAG_LINEAR) Bv(i, j) = rD * v(i + 1, j + 1);
             else Bv(i, j) = T(0);
         }
-        if (smag && i <= nx + 1 && j <= ny + 1)
-            nuSq(i, j) = quarter * (nuS(i, j) + nuS(i + 1, j)) + quarter * (nuS(i, j + 1) + nuS(i + 1, j + 1));
-    });
-    L.d2(nx + 2, ny + 2, [=] __host__ __device__(int i, int j) {    // viscous tensor (src/diffusion.jl:126-218)
+        T nq = T(0);   // nuSmag_q at (i, j), used by S12 and S21 at the same point
+        if (smag && i <= nx + 1 && j <= ny + 1) {
+            nq = quarter * (nuS(i, j) + nuS(i + 1, j)) + quarter * (nuS(i, j + 1) + nuS(i + 1, j + 1));
+            nuSq(i, j) = nq;
+        }
+        // viscous tensor (src/diffusion.jl:126-218)
         if (i <= S11.m && j <= S11.n) S11(i, j) = smag ? nuS(i + 1 - ep, j) * dLudx(i, j) : nuB * dLudx(i, j);
-        if (i <= S12.m && j <= S12.n) S12(i, j) = smag ? nuSq(i, j) * dLudy(i + ep, j) : nuB * dLudy(i + ep, j);
-        if (i <= S21.m && j <= S21.n) S21(i, j) = smag ? nuSq(i, j) * dLvdx(i, j) : nuB * dLvdx(i, j);
+        if (i <= S12.m && j <= S12.n) S12(i, j) = smag ? nq * dLudy(i + ep, j) : nuB * dLudy(i + ep, j);
+        if (i <= S21.m && j <= S21.n) S21(i, j) = smag ? nq * dLvdx(i, j) : nuB * dLvdx(i, j);
         if (i <= S22.m && j <= S22.n) S22(i, j) = smag ? nuS(i, j + 1) * dLvdy(i, j) : nuB * dLvdy(i, j);
     });
     if (!Xs) return;
@@ -621,41 +617,57 @@ void tail_rev(Launcher& L, const Work<T>& w, const State<T>& Zs, const State<T>&
         }
     });
     const A2<T> nuS = w.nuS, nuSq = w.nuSq, dLudx = w.dLudx, dLudy = w.dLudy, dLvdx = w.dLvdx, dLvdy = w.dLvdy;
-    const A2<T> bnuS = w.bnuS, bnuSq = w.bnuSq, bdLudx = w.bdLudx, bdLudy = w.bdLudy, bdLvdx = w.bdLvdx,
-                bdLvdy = w.bdLvdy;
     const A2<T> thu = w.thu, thv = w.thv, sKEu = w.sKEu, sKEv = w.sKEv, Bu = w.Bu, Bv = w.Bv;
-    const A2<T> bsKEu = w.bsKEu, bsKEv = w.bsKEv, bthu = w.bthu, bthv = w.bthv;
+    const A2<T> bnuS = w.bnuS, bLu = w.bLu, bLv = w.bLv, bsKE = w.bsKE;
     const T cD = w.cD, rD = w.rD, nuB = w.nuB;
-    // viscous tensor^T, bottom drag^T
+    // viscous tensor^T and bottom drag^T; the adjoints these form alone (of the
+    // Laplacians' gradients, nuSmag_q, sqrtKE_u/v and h_u/h_v at this point) go
+    // straight through their dx/dy^T, Ixy^T, Ix/Iy^T
     L.d2(nx + 2, ny + 2, [=] __host__ __device__(int i, int j) {
+        const T half = T(0.5), quarter = T(0.25);
+        T nq = T(0);   // adjoint of nuSmag_q(i, j)
         if (i <= bS11.m && j <= bS11.n) {
             const T s = bS11(i, j);
-            if (smag) { add(bnuS(i + 1 - ep, j), s * dLudx(i, j)); add(bdLudx(i, j), s * nuS(i + 1 - ep, j)); }
-            else add(bdLudx(i, j), s * nuB);
+            T t;
+            if (smag) { add(bnuS(i + 1 - ep, j), s * dLudx(i, j)); t = s * nuS(i + 1 - ep, j); }
+            else t = s * nuB;
+            add(bLu(i + 1, j), t); add(bLu(i, j), -t);            // dLudx = dx(Lu)
         }
         if (i <= bS12.m && j <= bS12.n) {
             const T s = bS12(i, j);
-            if (smag) { add(bnuSq(i, j), s * dLudy(i + ep, j)); add(bdLudy(i + ep, j), s * nuSq(i, j)); }
-            else add(bdLudy(i + ep, j), s * nuB);
+            T t;
+            if (smag) { nq += s * dLudy(i + ep, j); t = s * nuSq(i, j); }
+            else t = s * nuB;
+            add(bLu(i + ep, j + 1), t); add(bLu(i + ep, j), -t);  // dLudy = dy(Lu)
         }
         if (i <= bS21.m && j <= bS21.n) {
             const T s = bS21(i, j);
-            if (smag) { add(bnuSq(i, j), s * dLvdx(i, j)); add(bdLvdx(i, j), s * nuSq(i, j)); }
-            else add(bdLvdx(i, j), s * nuB);
+            T t;
+            if (smag) { nq += s * dLvdx(i, j); t = s * nuSq(i, j); }
+            else t = s * nuB;
+            add(bLv(i + 1, j), t); add(bLv(i, j), -t);            // dLvdx = dx(Lv)
         }
         if (i <= bS22.m && j <= bS22.n) {
             const T s = bS22(i, j);
-            if (smag) { add(bnuS(i, j + 1), s * dLvdy(i, j)); add(bdLvdy(i, j), s * nuS(i, j + 1)); }
-            else add(bdLvdy(i, j), s * nuB);
+            T t;
+            if (smag) { add(bnuS(i, j + 1), s * dLvdy(i, j)); t = s * nuS(i, j + 1); }
+            else t = s * nuB;
+            add(bLv(i, j + 1), t); add(bLv(i, j), -t);            // dLvdy = dy(Lv)
+        }
+        if (smag && i <= nx + 1 && j <= ny + 1) {                // nuSmag_q = Ixy(nuSmag)
+            const T t = quarter * nq;
+            add(bnuS(i, j), t); add(bnuS(i + 1, j), t); add(bnuS(i, j + 1), t); add(bnuS(i + 1, j + 1), t);
         }
         if (i <= nx + 1 && j <= ny + 2) {
             const T bb = bBu(i, j);
             const T uu = u(i + 1 + ep, j + 1);
             if (drag == SW_DRAG_QUADRATIC) {     // Bu = cD*s*u/h
                 const T hh = thu(i, j);
-                bsKEu(i, j) = bb * (cD * uu / hh);
+                const T ts = half * (bb * (cD * uu / hh));        // sqrtKE_u = Ix(sqrtKE)
+                add(bsKE(i + 1, j), ts); add(bsKE(i, j), ts);
                 add(zb.u(i + 1 + ep, j + 1), bb * (cD * sKEu(i, j) / hh));
-                bthu(i, j) = -(bb * Bu(i, j) / hh);
+                const T th = half * -(bb * Bu(i, j) / hh);        // h_u = Ix(eta + H)
+                add(zb.e(i + 1, j), th); add(zb.e(i, j), th);
             } else if (drag == SW_DRAG_LINEAR) {
                 add(zb.u(i + 1 + ep, j + 1), bb * rD);
             }
@@ -665,52 +677,31 @@ void tail_rev(Launcher& L, const Work<T>& w, const State<T>& Zs, const State<T>&
             const T vv = v(i + 1, j + 1);
             if (drag == SW_DRAG_QUADRATIC) {
                 const T hh = thv(i, j);
-                bsKEv(i, j) = bb * (cD * vv / hh);
+                const T ts = half * (bb * (cD * vv / hh));        // sqrtKE_v = Iy(sqrtKE)
+                add(bsKE(i, j + 1), ts); add(bsKE(i, j), ts);
                 add(zb.v(i + 1, j + 1), bb * (cD * sKEv(i, j) / hh));
-                bthv(i, j) = -(bb * Bv(i, j) / hh);
+                const T th = half * -(bb * Bv(i, j) / hh);        // h_v = Iy(eta + H)
+                add(zb.e(i, j + 1), th); add(zb.e(i, j), th);
             } else if (drag == SW_DRAG_LINEAR) {
                 add(zb.v(i + 1, j + 1), bb * rD);
             }
         }
     });
-    const A2<T> bLu = w.bLu, bLv = w.bLv, bsKE = w.bsKE;
-    // Ixy^T of nuSmag_q, dx/dy^T of the Laplacians, Ix/Iy^T of sqrtKE and of h
-    L.d2(nx + 4, ny + 4, [=] __host__ __device__(int i, int j) {
-        const T half = T(0.5), quarter = T(0.25);
-        if (smag && i <= nx + 1 && j <= ny + 1) {
-            const T t = quarter * bnuSq(i, j);
-            add(bnuS(i, j), t); add(bnuS(i + 1, j), t); add(bnuS(i, j + 1), t); add(bnuS(i + 1, j + 1), t);
-        }
-        if (i <= bdLudx.m && j <= bdLudx.n) { const T t = bdLudx(i, j); add(bLu(i + 1, j), t); add(bLu(i, j), -t); }
-        if (i <= bdLudy.m && j <= bdLudy.n) { const T t = bdLudy(i, j); add(bLu(i, j + 1), t); add(bLu(i, j), -t); }
-        if (i <= bdLvdx.m && j <= bdLvdx.n) { const T t = bdLvdx(i, j); add(bLv(i + 1, j), t); add(bLv(i, j), -t); }
-        if (i <= bdLvdy.m && j <= bdLvdy.n) { const T t = bdLvdy(i, j); add(bLv(i, j + 1), t); add(bLv(i, j), -t); }
-        if (drag == SW_DRAG_QUADRATIC) {
-            if (i <= nx + 1 && j <= ny + 2) {
-                const T t = half * bsKEu(i, j);
-                add(bsKE(i + 1, j), t); add(bsKE(i, j), t);
-                const T th = half * bthu(i, j);
-                add(zb.e(i + 1, j), th); add(zb.e(i, j), th);
-            }
-            if (i <= nx + 2 && j <= ny + 1) {
-                const T t = half * bsKEv(i, j);
-                add(bsKE(i, j + 1), t); add(bsKE(i, j), t);
-                const T th = half * bthv(i, j);
-                add(zb.e(i, j + 1), th); add(zb.e(i, j), th);
-            }
-        }
-    });
-    const A2<T> rS = w.rS, sKE = w.sKE, bDS = w.bDS, bDT = w.bDT;
+    const A2<T> rS = w.rS, sKE = w.sKE, sDT = w.sDT, sDS = w.sDS, bDSq = w.bDSq;
     const T cSmag = w.cSmag;
     const A2<T> Lu = w.Lu, Lv = w.Lv;
-    // sqrt^T (Smagorinsky coefficient and sqrtKE, through KE = Ix(u^2) + Iy(v^2)), ∇²^T
+    // sqrt^T (Smagorinsky coefficient, then DT^T and Ixy^T of DS at the same
+    // point; sqrtKE through KE = Ix(u^2) + Iy(v^2)) and ∇²^T
     L.d2(nx + 4, ny + 4, [=] __host__ __device__(int i, int j) {
-        const T zero = T(0), two = T(2);
+        const T zero = T(0), two = T(2), quarter = T(0.25);
         if (smag && i <= nx + 2 && j <= ny + 2) {
             const T r = rS(i, j);
-            const T d = r > zero ? bnuS(i, j) * cSmag / (two * r) : zero;
-            bDS(i, j) = d;
-            bDT(i, j) = d;
+            const T d = r > zero ? bnuS(i, j) * cSmag / (two * r) : zero;   // adjoint of DS and of DT
+            const T t = two * sDT(i, j) * d;                                 // DT = s^2, s = dudx + dvdy
+            add(zb.u(i + ep + 1, j + 1), t); add(zb.u(i + ep, j + 1), -t);
+            add(zb.v(i + 1, j + 1), t); add(zb.v(i + 1, j), -t);
+            const T q4 = quarter * d;                                        // DS = Ixy(DS_q)
+            add(bDSq(i, j), q4); add(bDSq(i + 1, j), q4); add(bDSq(i, j + 1), q4); add(bDSq(i + 1, j + 1), q4);
         }
         if (drag == SW_DRAG_QUADRATIC && i <= nx + 2 && j <= ny + 2) {
             const T r = sKE(i, j);
@@ -731,16 +722,6 @@ void tail_rev(Launcher& L, const Work<T>& w, const State<T>& Zs, const State<T>&
         }
     });
     if (!smag) return;
-    const A2<T> sDT = w.sDT, sDS = w.sDS, bDSq = w.bDSq;
-    // DT^T (s^2 with s = dudx + dvdy) and Ixy^T of DS
-    L.d2(nx + 2, ny + 2, [=] __host__ __device__(int i, int j) {
-        const T quarter = T(0.25), two = T(2);
-        const T t = two * sDT(i, j) * bDT(i, j);
-        add(zb.u(i + ep + 1, j + 1), t); add(zb.u(i + ep, j + 1), -t);
-        add(zb.v(i + 1, j + 1), t); add(zb.v(i + 1, j), -t);
-        const T s = quarter * bDS(i, j);
-        add(bDSq(i, j), s); add(bDSq(i + 1, j), s); add(bDSq(i, j + 1), s); add(bDSq(i + 1, j + 1), s);
-    });
     // DS_q^T (s^2 with s = dudy + dvdx)
     L.d2(nx + 3, ny + 3, [=] __host__ __device__(int i, int j) {
         const T t = T(2) * sDS(i, j) * bDSq(i, j);
@@ -1007,21 +988,16 @@ struct Adjoint {
             Carver cv;   // stage adjoints (zeroed per stage)
             cv.add(w.bU, nx + 1, ny + 2); cv.add(w.bV, nx + 2, ny + 1); cv.add(w.bp, nx + 2, ny + 2);
             cv.add(w.bqa, nx, ny); cv.add(w.bqb, nx + 1, ny); cv.add(w.bqc, nx + 1, ny); cv.add(w.bqd, nx, ny);
-            cv.add(w.bq, nx + 1, ny + 1); cv.add(w.bhu, nx + 1, ny + 2); cv.add(w.bhv, nx + 2, ny + 1);
-            cv.add(w.bhq, nx + 1, ny + 1);
+            cv.add(w.bq, nx + 1, ny + 1);
             if (!carve(cv, &w.stage_adj, &w.stage_adj_elems)) return SW_ERR_NOMEM;
         }
         {
             Carver cv;   // tail adjoints (zeroed per step)
             cv.add(w.bBu, nx + 1, ny + 2); cv.add(w.bBv, nx + 2, ny + 1);
             cv.add(w.bS11, nux + 1, nuy + 2); cv.add(w.bS12, nx + 1, ny + 1); cv.add(w.bS21, nx + 1, ny + 1);
-            cv.add(w.bS22, nvx + 2, nvy + 1); cv.add(w.bnuS, nx + 2, ny + 2); cv.add(w.bnuSq, nx + 1, ny + 1);
-            cv.add(w.bdLudx, nux + 1, nuy + 2); cv.add(w.bdLudy, nux + 2, nuy + 1);
-            cv.add(w.bdLvdx, nvx + 1, nvy + 2); cv.add(w.bdLvdy, nvx + 2, nvy + 1);
+            cv.add(w.bS22, nvx + 2, nvy + 1); cv.add(w.bnuS, nx + 2, ny + 2);
             cv.add(w.bLu, nux + 2, nuy + 2); cv.add(w.bLv, nvx + 2, nvy + 2);
-            cv.add(w.bsKE, nx + 2, ny + 2); cv.add(w.bsKEu, nx + 1, ny + 2); cv.add(w.bsKEv, nx + 2, ny + 1);
-            cv.add(w.bthu, nx + 1, ny + 2); cv.add(w.bthv, nx + 2, ny + 1);
-            cv.add(w.bDS, nx + 2, ny + 2); cv.add(w.bDT, nx + 2, ny + 2); cv.add(w.bDSq, nvx + 3, nvy + 4);
+            cv.add(w.bsKE, nx + 2, ny + 2); cv.add(w.bDSq, nvx + 3, nvy + 4);
             if (!carve(cv, &w.tail_adj, &w.tail_adj_elems)) return SW_ERR_NOMEM;
         }
         if (want_store) {   // one record per step; without the memory the steps are recomputed instead
