@@ -187,6 +187,21 @@ def test_gradient_matches_dual_directional_derivative(opts):
 
 
 @pytest.mark.gpu
+def test_float32_gradient_agrees_with_float64():
+    """The Float32 adjoint of the same problem gives the Float64 directional
+    derivative to about the precision of the Float32 forward run."""
+    n = 40
+    r64, r32 = [gradient(*setup(T=T, nx=64, seed=13)[:3], n) for T in (np.float64, np.float32)]
+    rng = np.random.default_rng(2)
+    S, Prog, _, _ = setup(nx=64, seed=13)
+    du, dv, de, dF = direction(S, Prog, rng)
+    d64 = directional((r64.u, r64.v, r64.eta, r64.Fx), (du, dv, de, dF))
+    d32 = directional(tuple(np.asarray(x, np.float64) for x in (r32.u, r32.v, r32.eta, r32.Fx)), (du, dv, de, dF))
+    assert d32 == pytest.approx(d64, rel=1e-3)
+    assert r32.J == pytest.approx(r64.J, rel=1e-3)
+
+
+@pytest.mark.gpu
 def test_checkpoint_schedule_does_not_change_the_gradient(monkeypatch):
     S, Prog, obs, _ = setup(nx=64, seed=5)
     n = 37
