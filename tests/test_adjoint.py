@@ -76,6 +76,28 @@ def test_dual_oracle_matches_central_differences(bc):
     assert fd == pytest.approx(dJ, rel=1e-7)
 
 
+def test_adjoint_entry_rejects_bad_arguments_and_unbuilt_options():
+    """sw_adjoint_run's checks: bad arguments give SW_ERR_ARG and option
+    combinations outside the differentiated loop SW_ERR_UNSUPPORTED, before any
+    device work; on a machine without a GPU a valid call gives SW_ERR_NODEVICE."""
+    import torch
+    from swb200.adjoint import gradient as grad
+    S, Prog, obs, _ = setup()
+    with pytest.raises(abi.SwError) as e:
+        grad(S, Prog, obs, 0)
+    assert e.value.code == abi.SW_ERR_ARG
+    for kw in (dict(time_scheme="SSPRK2"), dict(dynamics="linear"), dict(adv_scheme="Sadourny"),
+               dict(nstep_diff=2), dict(T=np.float32, Tprog=np.float64)):
+        S2, P2, o2, _ = setup(**kw)
+        with pytest.raises(abi.SwError) as e:
+            grad(S2, P2, o2, 3)
+        assert e.value.code == abi.SW_ERR_UNSUPPORTED, kw
+    if not torch.cuda.is_available():
+        with pytest.raises(abi.SwError) as e:
+            grad(S, Prog, obs, 3)
+        assert e.value.code == abi.SW_ERR_NODEVICE
+
+
 def _production_eta(S, Prog, n):
     from swb200 import Model
     with Model(S) as m:
