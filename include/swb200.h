@@ -285,7 +285,9 @@ void sw_batch_destroy(sw_batch* b);
  * step state on the device and, memory permitting (off with
  * SWB200_ADJ_STORE=0), every step's RK stage inputs and tail input as well, so
  * the reverse sweep recomputes only each pass's intermediates; fewer slots
- * recompute states with the binomial checkpoint schedule.  The derivative of sqrt at 0 (drag and Smagorinsky at
+ * recompute states with the binomial checkpoint schedule.  ncheckpoints is an
+ * upper bound: when that many state slots do not fit in device memory, half
+ * as many are tried (down to one); stats->checkpoints reports the number used.  The derivative of sqrt at 0 (drag and Smagorinsky at
  * rest) is taken as 0.  Gradients are summed with atomics, so repeated calls
  * agree to rounding, not bit for bit.  stats may be NULL. */
 typedef struct sw_adjoint_stats {

@@ -916,6 +916,33 @@ struct Adjoint {
         return zero(b, n * sizeof(T)) == cudaSuccess;
     }
 
+    // n state slots in one block; on allocation failure n is halved (to 1)
+    bool make_slots(int n) {
+        for (; n >= 1; n /= 2) {
+            std::vector<State<T>> sl(n);
+            Carver cv;
+            for (auto& x : sl) {
+                cv.add(x.u, w.nux + 4, w.nuy + 4);
+                cv.add(x.v, w.nvx + 4, w.nvy + 4);
+                cv.add(x.e, w.nx + 2, w.ny + 2);
+            }
+            const size_t total = cv.total();
+            void* p = nullptr;
+            if (host) p = std::calloc(total, sizeof(T));
+            else if (cudaMalloc(&p, total * sizeof(T)) != cudaSuccess) { p = nullptr; cudaGetLastError(); }
+            if (!p) continue;
+            blocks.push_back(p);
+            cv.place(static_cast<T*>(p));
+            for (auto& x : sl) {
+                x.base = x.u.d;
+                x.elems = Carver::padded(x.u.m, x.u.n) + Carver::padded(x.v.m, x.v.n) + Carver::padded(x.e.m, x.e.n);
+            }
+            slots = std::move(sl);
+            return true;
+        }
+        return false;
+    }
+
     bool make_state(State<T>& st) {
         Carver c;
         c.add(st.u, w.nux + 4, w.nuy + 4);
@@ -1117,10 +1144,12 @@ int adjoint_run(bool host, const sw_config& c, const sw_static& st, const void* 
     }
     Work<T>& w = A.w;
     const size_t bytes_u = w.X.u.size() * sizeof(T), bytes_v = w.X.v.size() * sizeof(T), bytes_e = w.X.e.size() * sizeof(T);
-    const int nslots = A.stored ? 1 : (int)std::max<long long>(1, std::min<long long>(ncheckpoints, nsteps));
-    A.slots.resize(nslots);
-    for (auto& sl : A.slots)
-        if (!A.make_state(sl)) return SW_ERR_NOMEM;
+    // ncheckpoints is an upper bound: when that many state slots do not fit in
+    // device memory, half as many are tried (down to one), and the binomial
+    // schedule recomputes what the missing slots would have kept
+    int nslots = A.stored ? 1 : (int)std::max<long long>(1, std::min<long long>(ncheckpoints, nsteps));
+    if (!A.make_slots(nslots)) return SW_ERR_NOMEM;
+    nslots = (int)A.slots.size();
     cudaEvent_t ev[3] = {};
     if (!host)
         for (auto& x : ev)
