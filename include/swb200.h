@@ -275,8 +275,9 @@ void sw_batch_destroy(sw_batch* b);
  * ForwardDiff/ChainRules route of the Julia ecosystem, which the reference
  * cannot take (its number types are restricted to AbstractFloat), so it has no
  * counterpart in the reference; the forward model it differentiates is
- * src/time_integration.jl:45-78,204-233.  Supported: T = Tprog = Tcomm in
- * Float32 or Float64, RK2/3/4, nonlinear dynamics, Arakawa-Hsu, nstep_advcor =
+ * src/time_integration.jl:45-104,204-233.  Supported: T = Tprog = Tcomm in
+ * Float32 or Float64, RK2/3/4 or SSPRK2 (2-4 sub-stages, with its
+ * semi-implicit continuity), nonlinear dynamics, Arakawa-Hsu, nstep_advcor =
  * 0, nstep_diff = 1, any drag and diffusion, either boundary, no time-dependent
  * forcing (else SW_ERR_UNSUPPORTED).  The tracer is passive and plays no part.
  * Inputs and outputs are HOST buffers in T: u, v, eta the initial state,

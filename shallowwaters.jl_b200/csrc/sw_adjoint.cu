@@ -3,8 +3,9 @@
 //   J = sum over the interior of (eta after nsteps - eta_obs)^2
 //
 // differentiated with respect to the initial state (u, v, eta with their
-// halos) and the wind forcing Fx.  The forward model is the RK branch of
-// time_integration (src/time_integration.jl:45-78 and the tail :204-233) with
+// halos) and the wind forcing Fx.  The forward model is the RK or the SSPRK2
+// branch of time_integration (src/time_integration.jl:45-104, the SSPRK2 one
+// with its semi-implicit continuity, and the tail :204-233) with
 // nonlinear dynamics, Arakawa-Hsu PV advection, quadratic / linear / no bottom
 // drag and Smagorinsky / constant biharmonic diffusion, periodic or
 // nonperiodic boundaries.  The tracer is passive (it never feeds back into
@@ -150,6 +151,9 @@ struct State {
 template <class T>
 struct Work {
     int nx, ny, nux, nuy, nvx, nvy, ep, rko;
+    bool ssp = false;           // SSPRK2 (src/time_integration.jl:80-104) instead of RK
+    int rks = 0, nst = 0;       // SSPRK2 sub-stages; stage states kept per step
+    T cssp, ssp_a, ssp_b;       // Δt_Δs, 1/RKs, (RKs-1)/RKs (Tprog)
     T g, cD, rD, cSmag, nuB, Dt_diff, oma;   // oma = 1 - alpha (Tprog = T)
     T RKa[4], RKb[3];
     int drag, diff;
@@ -157,9 +161,14 @@ struct Work {
     A2<T> H, f_q, Fx, Fy;
     // states
     State<T> X;                 // the state being advanced (in / out of a step)
-    State<T> Ys[4];             // stage inputs after their ghost points; Ys[0] = ghosted start state
+    // stage states.  RK: Ys[k-1] = input of stage k after its ghost points
+    // (Ys[0] = ghosted start state).  SSPRK2: Ys[0] = ghosted start state,
+    // Ys[2k-1] = sub-stage k's input after ghost_points_eta!, Ys[2k] = its
+    // state after the momentum update and ghost_points_uv!, Ys[2 RKs + 1] =
+    // the state after the last sub-stage.
+    State<T> Ys[10];
     State<T> Z;                 // RK result after ghost points = the tail's input
-    T* stage_block = nullptr;   // Ys[0..rko-1] and Z, contiguous in this order
+    T* stage_block = nullptr;   // Ys[0..nst-1] and Z, contiguous in this order
     size_t stage_block_elems = 0;
     State<T> Xb, acc, Yb[2];    // adjoints: of the step output / input, of the stage inputs
     // stage intermediates (src/preallocate.jl:70-152, 227-254)
@@ -189,15 +198,21 @@ __host__ __device__ __forceinline__ int etasrc(int i, int m, int ep) {
     return i;
 }
 
+// ghost() / ghostT() modes: all fields, u and v only (ghost_points_uv!), eta
+// only (ghost_points_eta!, src/ghost_points.jl:219-229)
+constexpr int GH_ALL = 0, GH_UV = 1, GH_ETA = 2;
+
 template <class T>
-void ghost(Launcher& L, const Work<T>& w, const State<T>& s, bool uv_only) {
+void ghost(Launcher& L, const Work<T>& w, const State<T>& s, int mode) {
+    const bool uv_only = mode == GH_UV, eta_only = mode == GH_ETA;
     const A2<T> u = s.u, v = s.v, e = s.e;
     const int ep = w.ep;
     const T c = w.oma;
     const int nmax = std::max(std::max(u.m, u.n), std::max(std::max(v.m, v.n), std::max(e.m, e.n)));
     L.d1(4LL * nmax, [=] __host__ __device__(long long k) {
         const int t = (int)(k >> 2) + 1, q = (int)(k & 3);
-        if (ep) {   // x-halo columns 1, 2, m-1, m from m-3, m-2, 3, 4
+        if (eta_only) {
+        } else if (ep) {   // x-halo columns 1, 2, m-1, m from m-3, m-2, 3, 4
             if (t <= u.n) { const int m = u.m, d[4] = {1, 2, m - 1, m}, sx[4] = {m - 3, m - 2, 3, 4}; u(d[q], t) = u(sx[q], t); }
             if (t <= v.n) { const int m = v.m, d[4] = {1, 2, m - 1, m}, sx[4] = {m - 3, m - 2, 3, 4}; v(d[q], t) = v(sx[q], t); }
         } else {    // u: y-halo rows 1, 2, n-1, n from 4, 3, n-2, n-3; v: x-halo columns likewise
@@ -220,7 +235,8 @@ void ghost(Launcher& L, const Work<T>& w, const State<T>& s, bool uv_only) {
 
 // transpose of ghost(): each halo adjoint is added onto its source and cleared
 template <class T>
-void ghostT(Launcher& L, const Work<T>& w, const State<T>& s, bool uv_only) {
+void ghostT(Launcher& L, const Work<T>& w, const State<T>& s, int mode) {
+    const bool uv_only = mode == GH_UV, eta_only = mode == GH_ETA;
     const A2<T> u = s.u, v = s.v, e = s.e;
     const int ep = w.ep;
     const T c = w.oma;
@@ -228,7 +244,8 @@ void ghostT(Launcher& L, const Work<T>& w, const State<T>& s, bool uv_only) {
     const int nmax = std::max(std::max(u.m, u.n), std::max(std::max(v.m, v.n), std::max(e.m, e.n)));
     L.d1(4LL * nmax, [=] __host__ __device__(long long k) {
         const int t = (int)(k >> 2) + 1, q = (int)(k & 3);
-        if (ep) {
+        if (eta_only) {
+        } else if (ep) {
             if (t <= u.n) {
                 const int m = u.m, d[4] = {1, 2, m - 1, m}, sx[4] = {m - 3, m - 2, 3, 4};
                 u(sx[q], t) += u(d[q], t); u(d[q], t) = zero;
@@ -376,15 +393,18 @@ void stage_update(Launcher& L, const Work<T>& w, int k, const State<T>& Xt, cons
 // order, the passes of stage_fwd and stage_update.
 template <class T>
 void stage_rev(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const State<T>& Xb0, const State<T>* Wb,
-               const State<T>& Yb) {
+               const State<T>& Yb, bool mom_only = false, T coef = T(0)) {
     const A2<T> u = Y.u, v = Y.v;
     const A2<T> hu = w.hu, hv = w.hv, hq = w.hq, U = w.U, V = w.V, q = w.q, qa = w.qa, qb = w.qb, qc = w.qc, qd = w.qd;
     const A2<T> bU = w.bU, bV = w.bV, bp = w.bp, bqa = w.bqa, bqb = w.bqb, bqc = w.bqc, bqd = w.bqd, bq = w.bq,
                 bFx = w.bFx;
     const int nx = w.nx, ny = w.ny, nux = w.nux, nuy = w.nuy, nvx = w.nvx, nvy = w.nvy, ep = w.ep;
-    const T a = w.RKa[k - 1], b = Wb ? w.RKb[k - 1] : T(0);
+    // RK: dbar = RKa*Xb0 + RKb*Wb.  Momentum only (SSPRK2): dbar = coef*Xb0 for
+    // u and v, no continuity part (Yb may then be Xb0 itself: this first pass
+    // reads Xb0 and writes no state adjoint)
+    const T a = mom_only ? coef : w.RKa[k - 1], b = (Wb && !mom_only) ? w.RKb[k - 1] : T(0);
     const State<T> x0 = Xb0, wb = Wb ? *Wb : Xb0, yb = Yb;
-    const bool has_w = Wb != nullptr;
+    const bool has_w = Wb != nullptr && !mom_only;
     L.zero(w.stage_adj, w.stage_adj_elems * sizeof(T));
     // momentum_u^T, momentum_v^T (with PV_ArakawaHsu^T), continuity^T
     L.d2(nx, ny, [=] __host__ __device__(int i, int j) {
@@ -411,7 +431,7 @@ void stage_rev(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const St
             add(bqc(i + 1, j + 1), m * U(i + 1, j + 2)); add(bU(i + 1, j + 2), m * qc(i + 1, j + 1));
             add(bqd(i, j + 1), m * U(i, j + 2));         add(bU(i, j + 2), m * qd(i, j + 1));
         }
-        {
+        if (!mom_only) {
             T g = a * x0.e(i + 1, j + 1);
             if (has_w) g += b * wb.e(i + 1, j + 1);
             add(bU(i + 1, j + 1), -g); add(bU(i, j + 1), g);
@@ -467,6 +487,112 @@ void stage_rev(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const St
             add(yb.e(i, j + 1), t); add(yb.e(i, j), t);
         }
     });
+}
+
+// ------------------------------------------------------------ SSPRK2 sub-stage
+// src/time_integration.jl:80-104: u1 += Δt_Δs*du, v1 += Δt_Δs*dv (axb!, whole
+// arrays, du zero on the halo) after rhs! at the sub-stage input Yp (whose
+// stage_fwd intermediates are current); eta is carried over.
+template <class T>
+void ssp_mom(Launcher& L, const Work<T>& w, const State<T>& Yp, const State<T>& Ym) {
+    const A2<T> qa = w.qa, qb = w.qb, qc = w.qc, qd = w.qd, p = w.p, U = w.U, V = w.V, Fx = w.Fx, Fy = w.Fy;
+    const int nx = w.nx, ny = w.ny, nux = w.nux, nuy = w.nuy, nvx = w.nvx, nvy = w.nvy, ep = w.ep;
+    const T c = w.cssp;
+    const State<T> yp = Yp, ym = Ym;
+    L.d2(nx + 4, ny + 4, [=] __host__ __device__(int I, int J) {
+        const T zero = T(0);
+        if (I <= yp.u.m && J <= yp.u.n) {
+            T d = zero;
+            if (I >= 3 && I <= nux + 2 && J >= 3 && J <= nuy + 2) {
+                const int i = I - 2, j = J - 2, cc = 1 - ep + i;
+                const T qhv = qa(cc, j) * V(cc + 1, j + 1) + qb(cc, j) * V(cc, j + 1) + qc(cc, j) * V(cc, j) + qd(cc, j) * V(cc + 1, j);
+                const T dpdx = p(i + 2 - ep, j + 1) - p(i + 1 - ep, j + 1);
+                d = (qhv - dpdx) + Fx(i, j);
+            }
+            ym.u(I, J) = yp.u(I, J) + c * d;
+        }
+        if (I <= yp.v.m && J <= yp.v.n) {
+            T d = zero;
+            if (I >= 3 && I <= nvx + 2 && J >= 3 && J <= nvy + 2) {
+                const int i = I - 2, j = J - 2;
+                const T qhu = qa(i, j) * U(i, j + 1) + qb(i + 1, j) * U(i + 1, j + 1) + qc(i + 1, j + 1) * U(i + 1, j + 2) +
+                              qd(i, j + 1) * U(i, j + 2);
+                const T dpdy = p(i + 1, j + 2) - p(i + 1, j + 1);
+                d = -(qhu + dpdy) + Fy(i, j);
+            }
+            ym.v(I, J) = yp.v(I, J) + c * d;
+        }
+        if (I <= yp.e.m && J <= yp.e.n) ym.e(I, J) = yp.e(I, J);
+    });
+}
+
+// the semi-implicit continuity (src/continuity.jl:72-97 with UVfluxes! of the
+// updated u1, v1 and the sub-stage's eta1, whose h_u, h_v stage_fwd formed)
+// and eta1 += Δt_Δs*deta; u1, v1 carried over into Yn
+template <class T>
+void ssp_cont(Launcher& L, const Work<T>& w, const State<T>& Ym, const State<T>& Yn) {
+    const A2<T> hu = w.hu, hv = w.hv;
+    const int nx = w.nx, ny = w.ny, ep = w.ep;
+    const T c = w.cssp;
+    const State<T> ym = Ym, yn = Yn;
+    L.d2(nx + 4, ny + 4, [=] __host__ __device__(int I, int J) {
+        if (I <= ym.u.m && J <= ym.u.n) yn.u(I, J) = ym.u(I, J);
+        if (I <= ym.v.m && J <= ym.v.n) yn.v(I, J) = ym.v(I, J);
+        if (I <= ym.e.m && J <= ym.e.n) {
+            T d = T(0);
+            if (I >= 2 && I <= nx + 1 && J >= 2 && J <= ny + 1) {
+                const int i = I - 1, j = J - 1;
+                auto Uf = [&](int a, int b) { return ym.u(1 + ep + a, 1 + b) * hu(a, b); };
+                auto Vf = [&](int a, int b) { return ym.v(a + 1, b + 1) * hv(a, b); };
+                const T dUdx = Uf(i + 1, j + 1) - Uf(i, j + 1);
+                const T dVdy = Vf(i + 1, j + 1) - Vf(i + 1, j);
+                d = -(dUdx + dVdy);
+            }
+            yn.e(I, J) = ym.e(I, J) + c * d;
+        }
+    });
+}
+
+// transpose of ssp_cont on the adjoint Yb of Yn (in place: Yb becomes the
+// adjoint of Ym).  Two passes: the flux adjoints in gather form (they read
+// Yb's eta), then their scatter onto u, v and, through h_u, h_v, eta.
+template <class T>
+void ssp_cont_rev(Launcher& L, const Work<T>& w, const State<T>& Ym, const State<T>& Yb) {
+    const A2<T> hu = w.hu, hv = w.hv, bU = w.bU, bV = w.bV;
+    const int nx = w.nx, ny = w.ny, ep = w.ep;
+    const T c = w.cssp;
+    const State<T> ym = Ym, yb = Yb;
+    L.d2(nx + 2, ny + 2, [=] __host__ __device__(int I, int J) {
+        auto g = [&](int i, int j) {   // deta adjoint at T-point (i, j), zero off the interior
+            return (i >= 1 && i <= nx && j >= 1 && j <= ny) ? c * yb.e(i + 1, j + 1) : T(0);
+        };
+        if (I <= nx + 1) bU(I, J) = g(I, J - 1) - g(I - 1, J - 1);        // dUdx(i, j+1) = U(i+1, j+1) - U(i, j+1)
+        if (J <= ny + 1) bV(I, J) = g(I - 1, J) - g(I - 1, J - 1);        // dVdy(i+1, j) = V(i+1, j+1) - V(i+1, j)
+    });
+    L.d2(nx + 2, ny + 2, [=] __host__ __device__(int I, int J) {
+        const T half = T(0.5);
+        if (I <= nx + 1) {   // U = u1(1+ep+I, 1+J) * h_u(I, J), h_u = Ix(eta + H)
+            const T b = bU(I, J);
+            add(yb.u(1 + ep + I, 1 + J), b * hu(I, J));
+            const T t = half * (b * ym.u(1 + ep + I, 1 + J));
+            add(yb.e(I + 1, J), t); add(yb.e(I, J), t);
+        }
+        if (J <= ny + 1) {   // V = v1(I+1, J+1) * h_v(I, J), h_v = Iy(eta + H)
+            const T b = bV(I, J);
+            add(yb.v(I + 1, J + 1), b * hv(I, J));
+            const T t = half * (b * ym.v(I + 1, J + 1));
+            add(yb.e(I, J + 1), t); add(yb.e(I, J), t);
+        }
+    });
+}
+
+// d = x*a + y*b over whole states (cxayb!, src/time_integration.jl:293-305)
+template <class T>
+void combine(Launcher& L, const State<T>& d, T x, const State<T>& a, T y, const State<T>& b) {
+    T* dp = d.base;
+    const T* ap = a.base;
+    const T* bp = b.base;
+    L.d1((long long)d.elems, [=] __host__ __device__(long long i) { dp[i] = x * ap[i] + y * bp[i]; });
 }
 
 // ------------------------------------------------------------ tail, forward
@@ -739,7 +865,11 @@ void copy_state(Launcher& L, const State<T>& dst, const State<T>& src) {
 // one time step X -> X (src/time_integration.jl:45-243, RK branch); leaves the
 // stage inputs in Ys, the tail input in Z and the last stage's intermediates.
 template <class T>
+void fwd_step_ssp(Launcher& L, const Work<T>& w);
+
+template <class T>
 void fwd_step(Launcher& L, const Work<T>& w) {
+    if (w.ssp) { fwd_step_ssp(L, w); return; }
     copy_state(L, w.Ys[0], w.X);
     ghost(L, w, w.Ys[0], false);
     copy_state(L, w.Z, w.Ys[0]);
@@ -757,8 +887,53 @@ void fwd_step(Launcher& L, const Work<T>& w) {
 // Z its stage inputs and tail input as the forward sweep kept them (stored =
 // true: only the passes' intermediates are recomputed).  On return Xb holds
 // the adjoint of the input, and bFx has this step's forcing adjoint added.
+// one SSPRK2 time step X -> X (src/time_integration.jl:80-104, 204-243)
+template <class T>
+void fwd_step_ssp(Launcher& L, const Work<T>& w) {
+    copy_state(L, w.Ys[0], w.X);
+    ghost(L, w, w.Ys[0], GH_ALL);
+    copy_state(L, w.Ys[1], w.Ys[0]);
+    for (int k = 1; k <= w.rks; k++) {
+        const State<T>&yp = w.Ys[2 * k - 1], &ym = w.Ys[2 * k], &yn = w.Ys[2 * k + 1];
+        if (k > 1) ghost(L, w, yp, GH_ETA);
+        stage_fwd(L, w, yp);
+        ssp_mom(L, w, yp, ym);
+        ghost(L, w, ym, GH_UV);
+        ssp_cont(L, w, ym, yn);
+    }
+    combine(L, w.Z, w.ssp_a, w.Ys[0], w.ssp_b, w.Ys[2 * w.rks + 1]);
+    ghost(L, w, w.Z, GH_ALL);
+    tail_fwd(L, w, w.Z, &w.X);
+}
+
+template <class T>
+void adj_step_ssp(Launcher& L, const Work<T>& w, bool stored) {
+    if (stored) tail_fwd(L, w, w.Z, (const State<T>*)nullptr);
+    else fwd_step_ssp(L, w);
+    ghostT(L, w, w.Xb, GH_UV);
+    tail_rev(L, w, w.Z, w.Xb);
+    ghostT(L, w, w.Xb, GH_ALL);    // Xb: adjoint of X0 = a*Ys[0] + b*Ys[2 RKs + 1]
+    const State<T>& Yb = w.Yb[0];
+    combine(L, w.acc, w.ssp_a, w.Xb, T(0), w.Xb);
+    combine(L, Yb, w.ssp_b, w.Xb, T(0), w.Xb);
+    for (int k = w.rks; k >= 1; k--) {
+        const State<T>&yp = w.Ys[2 * k - 1], &ym = w.Ys[2 * k];
+        stage_fwd(L, w, yp);                              // h_u, h_v and the rhs intermediates of sub-stage k
+        ssp_cont_rev(L, w, ym, Yb);                       // Yb: adjoint of Ym
+        ghostT(L, w, Yb, GH_UV);
+        stage_rev(L, w, 1, yp, Yb, (const State<T>*)nullptr, Yb, true, w.cssp);   // adjoint of Yp
+        if (k > 1) ghostT(L, w, Yb, GH_ETA);
+    }
+    const T* src = Yb.base;
+    T* dst = w.acc.base;
+    L.d1((long long)Yb.elems, [=] __host__ __device__(long long i) { dst[i] += src[i]; });
+    ghostT(L, w, w.acc, GH_ALL);
+    copy_state(L, w.Xb, w.acc);
+}
+
 template <class T>
 void adj_step(Launcher& L, const Work<T>& w, bool stored) {
+    if (w.ssp) { adj_step_ssp(L, w, stored); return; }
     if (stored) tail_fwd(L, w, w.Z, (const State<T>*)nullptr);
     else fwd_step(L, w);
     ghostT(L, w, w.Xb, true);
@@ -818,7 +993,8 @@ AdjCfgError adjoint_check(const sw_config& c) {
     if (c.nx < 8 || c.ny < 8) return {SW_ERR_ARG, "grid smaller than 8 x 8"};
     if (c.T != c.Tprog || (c.T != SW_FLOAT32 && c.T != SW_FLOAT64) || c.Tcomm != c.T)
         return {SW_ERR_UNSUPPORTED, "the adjoint computes in T = Tprog = Tcomm, Float32 or Float64"};
-    if (c.time_scheme != SW_RK || c.RKo < 2 || c.RKo > 4) return {SW_ERR_UNSUPPORTED, "the adjoint follows the RK2/3/4 schemes"};
+    if (!((c.time_scheme == SW_RK && c.RKo >= 2 && c.RKo <= 4) || (c.time_scheme == SW_SSPRK2 && c.RKs >= 2 && c.RKs <= 4)))
+        return {SW_ERR_UNSUPPORTED, "the adjoint follows RK2/3/4 and SSPRK2 with 2-4 sub-stages"};
     if (c.dynamics != SW_NONLINEAR || c.adv_scheme != SW_ARAKAWA_HSU || c.nstep_advcor != 0)
         return {SW_ERR_UNSUPPORTED, "the adjoint follows nonlinear dynamics with Arakawa-Hsu and nstep_advcor = 0"};
     if (c.nstep_diff != 1) return {SW_ERR_UNSUPPORTED, "the adjoint needs nstep_diff = 1"};
@@ -839,7 +1015,7 @@ struct Adjoint {
     std::vector<void*> blocks;
     cudaStream_t s = nullptr;
     cudaGraphExec_t g_fwd = nullptr, g_adj = nullptr, g_adj_st = nullptr;
-    T* records = nullptr;       // per step: Ys[0..rko-1] and Z as the forward sweep left them
+    T* records = nullptr;       // per step: Ys[0..nst-1] and Z as the forward sweep left them
     bool stored = false;
     std::vector<State<T>> slots;
     long long fwd_steps = 0, adj_steps = 0;
@@ -956,6 +1132,12 @@ struct Adjoint {
         w.nx = c.nx; w.ny = c.ny; w.ep = c.periodic ? 1 : 0;
         w.nux = w.ep ? c.nx : c.nx - 1; w.nuy = c.ny; w.nvx = c.nx; w.nvy = c.ny - 1;
         w.rko = c.RKo;
+        w.ssp = c.time_scheme == SW_SSPRK2;
+        w.rks = c.RKs;
+        w.cssp = (T)c.Dt_Ds;
+        w.ssp_a = (T)(1.0 / c.RKs);
+        w.ssp_b = (T)((double)(c.RKs - 1) / c.RKs);
+        w.nst = w.ssp ? 2 * w.rks + 2 : w.rko;
         w.g = (T)c.g; w.cD = (T)c.cD; w.rD = (T)c.rD; w.cSmag = (T)c.cSmag; w.nuB = (T)c.nuB;
         w.Dt_diff = (T)c.Dt_diff; w.oma = (T)c.one_minus_alpha;
         for (int k = 0; k < 4; k++) w.RKa[k] = (T)c.RKaDt[k];
@@ -977,9 +1159,9 @@ struct Adjoint {
         if (!make_state(w.X) || !make_state(w.Xb) || !make_state(w.acc) || !make_state(w.Yb[0]) || !make_state(w.Yb[1]))
             return SW_ERR_NOMEM;
         {
-            Carver cv;   // the stage inputs Ys[0..rko-1] and the tail input Z, contiguous (one copy saves them)
+            Carver cv;   // the stage states Ys[0..nst-1] and the tail input Z, contiguous (one copy saves them)
             std::vector<State<T>*> st;
-            for (int k = 0; k < w.rko; k++) st.push_back(&w.Ys[k]);
+            for (int k = 0; k < w.nst; k++) st.push_back(&w.Ys[k]);
             st.push_back(&w.Z);
             for (State<T>* x : st) {
                 cv.add(x->u, w.nux + 4, w.nuy + 4);

@@ -32,7 +32,9 @@ DUAL_RTOL = 1e-4       # adjoint vs Dual directional derivative (Float64)
 # option sets covered (stable at their cfl)
 OPTIONS = [dict(), dict(bc="nonperiodic", α=0.5), dict(diffusion="constant"),
            dict(bottom_drag="linear", bc="nonperiodic", α=0.0), dict(RKo=3, bottom_drag="none", cfl=0.5),
-           dict(RKo=2, bc="nonperiodic", α=2.0, cfl=0.3)]
+           dict(RKo=2, bc="nonperiodic", α=2.0, cfl=0.3),
+           dict(time_scheme="SSPRK2", RKs=3, cfl=1.0),
+           dict(time_scheme="SSPRK2", RKs=2, cfl=0.6, bc="nonperiodic", α=0.5, diffusion="constant")]
 
 
 def setup(T=np.float64, seed=3, **kw):
@@ -86,7 +88,7 @@ def test_adjoint_entry_rejects_bad_arguments_and_unbuilt_options():
     with pytest.raises(abi.SwError) as e:
         grad(S, Prog, obs, 0)
     assert e.value.code == abi.SW_ERR_ARG
-    for kw in (dict(time_scheme="SSPRK2"), dict(dynamics="linear"), dict(adv_scheme="Sadourny"),
+    for kw in (dict(time_scheme="SSPRK3"), dict(dynamics="linear"), dict(adv_scheme="Sadourny"),
                dict(nstep_diff=2), dict(T=np.float32, Tprog=np.float64)):
         S2, P2, o2, _ = setup(**kw)
         with pytest.raises(abi.SwError) as e:
