@@ -140,6 +140,25 @@ struct Launcher {
     }
 };
 
+// qhv at u-point (i, j) and qhu at v-point (i, j) of the PV advection, from
+// the Arakawa-Hsu coefficients (src/PV_advection.jl:63-84) or the Sadourny
+// averages (src/PV_advection.jl:31-59)
+template <class T>
+struct PVterms {
+    A2<T> qa, qb, qc, qd, qu, qv, Vu, Uv, U, V;
+    bool sad;
+    int ep;
+    __host__ __device__ __forceinline__ T qhv(int i, int j) const {
+        const int c = 1 - ep + i;
+        if (sad) return qu(c, j) * Vu(c, j);
+        return qa(c, j) * V(c + 1, j + 1) + qb(c, j) * V(c, j + 1) + qc(c, j) * V(c, j) + qd(c, j) * V(c + 1, j);
+    }
+    __host__ __device__ __forceinline__ T qhu(int i, int j) const {
+        if (sad) return qv(i, j + 1) * Uv(i, j + 1);
+        return qa(i, j) * U(i, j + 1) + qb(i + 1, j) * U(i + 1, j + 1) + qc(i + 1, j + 1) * U(i + 1, j + 2) + qd(i, j + 1) * U(i, j + 2);
+    }
+};
+
 // the three prognostic fields of one state, contiguous in one block
 template <class T>
 struct State {
@@ -157,6 +176,7 @@ struct Work {
     T g, cD, rD, cSmag, nuB, Dt_diff, oma;   // oma = 1 - alpha (Tprog = T)
     T RKa[4], RKb[3];
     int drag, diff;
+    bool sadourny = false;      // PV_Sadourny! (src/PV_advection.jl:31-59) instead of Arakawa-Hsu
     // static fields
     A2<T> H, f_q, Fx, Fy;
     // states
@@ -173,8 +193,9 @@ struct Work {
     State<T> Xb, acc, Yb[2];    // adjoints: of the step output / input, of the stage inputs
     // stage intermediates (src/preallocate.jl:70-152, 227-254)
     A2<T> hu, hv, hq, U, V, q, qa, qb, qc, qd, p;
+    A2<T> qu, qv, Vu, Uv;       // Sadourny: Iy(q), Ix(q), Ixy(V), Ixy(U)
     // their adjoints
-    A2<T> bU, bV, bp, bqa, bqb, bqc, bqd, bq;
+    A2<T> bU, bV, bp, bqa, bqb, bqc, bqd, bq, bqu, bqv, bVu, bUv;
     // tail intermediates (src/preallocate.jl:193-222, 259-338)
     A2<T> thu, thv, sKE, sKEu, sKEv, Bu, Bv, Lu, Lv, dLudx, dLudy, dLvdx, dLvdy, sDT, sDS, DSq, rS, nuS, nuSq, S11,
         S12, S21, S22;
@@ -183,6 +204,11 @@ struct Work {
     T* stage_adj = nullptr; size_t stage_adj_elems = 0;   // bU..bq, one block (zeroed per stage)
     T* tail_adj = nullptr; size_t tail_adj_elems = 0;     // bBu..bDSq, one block (zeroed per step)
 };
+
+template <class T>
+PVterms<T> pvterms(const Work<T>& w) {
+    return PVterms<T>{w.qa, w.qb, w.qc, w.qd, w.qu, w.qv, w.Vu, w.Uv, w.U, w.V, w.sadourny, w.ep};
+}
 
 // ------------------------------------------------------------ ghost points
 // ghost_points! (src/ghost_points.jl:182-199) on u, v (and eta); with uv_only
@@ -314,15 +340,26 @@ void stage_fwd(Launcher& L, const Work<T>& w, const State<T>& Y) {
         }
     });
     const A2<T> qa = w.qa, qb = w.qb, qc = w.qc, qd = w.qd, p = w.p;
+    const A2<T> qu = w.qu, qv = w.qv, Vu = w.Vu, Uv = w.Uv;
+    const bool sad = w.sadourny;
     const T g = w.g;
     L.d2(nx + 2, ny + 2, [=] __host__ __device__(int i, int j) {
-        const T o12 = T(1.0 / 12.0), half = T(0.5);
+        const T o12 = T(1.0 / 12.0), half = T(0.5), quarter = T(0.25);
         const int qend = q.m;
-        if (i <= nx && j <= ny) {
+        if (sad) {   // Iy!(q_u, q), Ix!(q_v, q), Ixy!(V_u, V), Ixy!(U_v, U)
+            if (i <= nx + 1 && j <= ny) {
+                qu(i, j) = half * (q(i, j + 1) + q(i, j));
+                Vu(i, j) = quarter * (V(i, j) + V(i + 1, j)) + quarter * (V(i, j + 1) + V(i + 1, j + 1));
+            }
+            if (i <= nx && j <= ny + 1) {
+                qv(i, j) = half * (q(i + 1, j) + q(i, j));
+                Uv(i, j) = quarter * (U(i, j) + U(i + 1, j)) + quarter * (U(i, j + 1) + U(i + 1, j + 1));
+            }
+        } else if (i <= nx && j <= ny) {
             qa(i, j) = o12 * (q(i, j) + q(i, j + 1) + q(i + 1, j + 1));
             qd(i, j) = o12 * (q(i, j) + q(i, j + 1) + q(i + 1, j));
         }
-        if (i <= nx + 1 && j <= ny) {
+        if (!sad && i <= nx + 1 && j <= ny) {
             if (i == 1) {
                 qb(1, j) = o12 * (q(1, j) + q(1, j + 1) + q(qend, j + 1));
                 qc(1, j) = o12 * (q(1, j) + q(1, j + 1) + q(qend, j));
@@ -343,7 +380,8 @@ void stage_fwd(Launcher& L, const Work<T>& w, const State<T>& Y) {
 // X0 += a*d.  d is zero on the halo, so halo points keep Xt / X0.
 template <class T>
 void stage_update(Launcher& L, const Work<T>& w, int k, const State<T>& Xt, const State<T>* Y1, const State<T>& X0) {
-    const A2<T> qa = w.qa, qb = w.qb, qc = w.qc, qd = w.qd, p = w.p, U = w.U, V = w.V, Fx = w.Fx, Fy = w.Fy;
+    const A2<T> p = w.p, Fx = w.Fx, Fy = w.Fy, U = w.U, V = w.V;
+    const PVterms<T> pv = pvterms(w);
     const int nx = w.nx, ny = w.ny, nux = w.nux, nuy = w.nuy, nvx = w.nvx, nvy = w.nvy, ep = w.ep;
     const T a = w.RKa[k - 1], b = k < w.rko ? w.RKb[k - 1] : T(0);
     const bool next = Y1 != nullptr;
@@ -353,8 +391,8 @@ void stage_update(Launcher& L, const Work<T>& w, int k, const State<T>& Xt, cons
         if (I <= xt.u.m && J <= xt.u.n) {
             T d = zero;
             if (I >= 3 && I <= nux + 2 && J >= 3 && J <= nuy + 2) {
-                const int i = I - 2, j = J - 2, c = 1 - ep + i;
-                const T qhv = qa(c, j) * V(c + 1, j + 1) + qb(c, j) * V(c, j + 1) + qc(c, j) * V(c, j) + qd(c, j) * V(c + 1, j);
+                const int i = I - 2, j = J - 2;
+                const T qhv = pv.qhv(i, j);
                 const T dpdx = p(i + 2 - ep, j + 1) - p(i + 1 - ep, j + 1);
                 d = (qhv - dpdx) + Fx(i, j);
             }
@@ -365,8 +403,7 @@ void stage_update(Launcher& L, const Work<T>& w, int k, const State<T>& Xt, cons
             T d = zero;
             if (I >= 3 && I <= nvx + 2 && J >= 3 && J <= nvy + 2) {
                 const int i = I - 2, j = J - 2;
-                const T qhu = qa(i, j) * U(i, j + 1) + qb(i + 1, j) * U(i + 1, j + 1) + qc(i + 1, j + 1) * U(i + 1, j + 2) +
-                              qd(i, j + 1) * U(i, j + 2);
+                const T qhu = pv.qhu(i, j);
                 const T dpdy = p(i + 1, j + 2) - p(i + 1, j + 1);
                 d = -(qhu + dpdy) + Fy(i, j);
             }
@@ -398,6 +435,8 @@ void stage_rev(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const St
     const A2<T> hu = w.hu, hv = w.hv, hq = w.hq, U = w.U, V = w.V, q = w.q, qa = w.qa, qb = w.qb, qc = w.qc, qd = w.qd;
     const A2<T> bU = w.bU, bV = w.bV, bp = w.bp, bqa = w.bqa, bqb = w.bqb, bqc = w.bqc, bqd = w.bqd, bq = w.bq,
                 bFx = w.bFx;
+    const A2<T> qu = w.qu, qv = w.qv, Vu = w.Vu, Uv = w.Uv, bqu = w.bqu, bqv = w.bqv, bVu = w.bVu, bUv = w.bUv;
+    const bool sad = w.sadourny;
     const int nx = w.nx, ny = w.ny, nux = w.nux, nuy = w.nuy, nvx = w.nvx, nvy = w.nvy, ep = w.ep;
     // RK: dbar = RKa*Xb0 + RKb*Wb.  Momentum only (SSPRK2): dbar = coef*Xb0 for
     // u and v, no continuity part (Yb may then be Xb0 itself: this first pass
@@ -414,11 +453,15 @@ void stage_rev(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const St
             bFx(i, j) += g;
             add(bp(i + 2 - ep, j + 1), -g);
             add(bp(i + 1 - ep, j + 1), g);
-            const int c = 1 - ep + i;      // qhv (src/PV_advection.jl:73)
-            add(bqa(c, j), g * V(c + 1, j + 1)); add(bV(c + 1, j + 1), g * qa(c, j));
-            add(bqb(c, j), g * V(c, j + 1));     add(bV(c, j + 1), g * qb(c, j));
-            add(bqc(c, j), g * V(c, j));         add(bV(c, j), g * qc(c, j));
-            add(bqd(c, j), g * V(c + 1, j));     add(bV(c + 1, j), g * qd(c, j));
+            const int c = 1 - ep + i;      // qhv (src/PV_advection.jl:73, Sadourny :49)
+            if (sad) {
+                add(bqu(c, j), g * Vu(c, j)); add(bVu(c, j), g * qu(c, j));
+            } else {
+                add(bqa(c, j), g * V(c + 1, j + 1)); add(bV(c + 1, j + 1), g * qa(c, j));
+                add(bqb(c, j), g * V(c, j + 1));     add(bV(c, j + 1), g * qb(c, j));
+                add(bqc(c, j), g * V(c, j));         add(bV(c, j), g * qc(c, j));
+                add(bqd(c, j), g * V(c + 1, j));     add(bV(c + 1, j), g * qd(c, j));
+            }
         }
         if (i <= nvx && j <= nvy) {
             T g = a * x0.v(i + 2, j + 2);
@@ -426,10 +469,14 @@ void stage_rev(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const St
             const T m = -g;                 // dv = -(qhu + dpdy) + Fy
             add(bp(i + 1, j + 2), m);
             add(bp(i + 1, j + 1), -m);
-            add(bqa(i, j), m * U(i, j + 1));             add(bU(i, j + 1), m * qa(i, j));
-            add(bqb(i + 1, j), m * U(i + 1, j + 1));     add(bU(i + 1, j + 1), m * qb(i + 1, j));
-            add(bqc(i + 1, j + 1), m * U(i + 1, j + 2)); add(bU(i + 1, j + 2), m * qc(i + 1, j + 1));
-            add(bqd(i, j + 1), m * U(i, j + 2));         add(bU(i, j + 2), m * qd(i, j + 1));
+            if (sad) {                      // qhu = q_v(i, j+1) * U_v(i, j+1)
+                add(bqv(i, j + 1), m * Uv(i, j + 1)); add(bUv(i, j + 1), m * qv(i, j + 1));
+            } else {
+                add(bqa(i, j), m * U(i, j + 1));             add(bU(i, j + 1), m * qa(i, j));
+                add(bqb(i + 1, j), m * U(i + 1, j + 1));     add(bU(i + 1, j + 1), m * qb(i + 1, j));
+                add(bqc(i + 1, j + 1), m * U(i + 1, j + 2)); add(bU(i + 1, j + 2), m * qc(i + 1, j + 1));
+                add(bqd(i, j + 1), m * U(i, j + 2));         add(bU(i, j + 2), m * qd(i, j + 1));
+            }
         }
         if (!mom_only) {
             T g = a * x0.e(i + 1, j + 1);
@@ -451,12 +498,26 @@ void stage_rev(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const St
         add(yb.v(i + 1, j + 1), hw * v(i + 1, j + 1));
         add(yb.v(i + 1, j), hw * v(i + 1, j));
         const int qend = q.m;
-        if (i <= nx && j <= ny) {
+        if (sad) {   // Iy^T, Ix^T of q; Ixy^T of V and U (their U, V adjoints are read in the next pass)
+            const T quarter = T(0.25);
+            if (i <= nx + 1 && j <= ny) {
+                const T t = half * bqu(i, j);
+                add(bq(i, j + 1), t); add(bq(i, j), t);
+                const T s = quarter * bVu(i, j);
+                add(bV(i, j), s); add(bV(i + 1, j), s); add(bV(i, j + 1), s); add(bV(i + 1, j + 1), s);
+            }
+            if (i <= nx && j <= ny + 1) {
+                const T t = half * bqv(i, j);
+                add(bq(i + 1, j), t); add(bq(i, j), t);
+                const T s = quarter * bUv(i, j);
+                add(bU(i, j), s); add(bU(i + 1, j), s); add(bU(i, j + 1), s); add(bU(i + 1, j + 1), s);
+            }
+        } else if (i <= nx && j <= ny) {
             const T ta = o12 * bqa(i, j), td = o12 * bqd(i, j);
             add(bq(i, j), ta + td); add(bq(i, j + 1), ta + td);
             add(bq(i + 1, j + 1), ta); add(bq(i + 1, j), td);
         }
-        if (i <= nx + 1 && j <= ny) {
+        if (!sad && i <= nx + 1 && j <= ny) {
             const T tb = o12 * bqb(i, j), tc = o12 * bqc(i, j);
             add(bq(i, j), tb + tc); add(bq(i, j + 1), tb + tc);
             if (i == 1) { add(bq(qend, j + 1), tb); add(bq(qend, j), tc); }
@@ -495,7 +556,8 @@ void stage_rev(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const St
 // stage_fwd intermediates are current); eta is carried over.
 template <class T>
 void ssp_mom(Launcher& L, const Work<T>& w, const State<T>& Yp, const State<T>& Ym) {
-    const A2<T> qa = w.qa, qb = w.qb, qc = w.qc, qd = w.qd, p = w.p, U = w.U, V = w.V, Fx = w.Fx, Fy = w.Fy;
+    const A2<T> p = w.p, Fx = w.Fx, Fy = w.Fy;
+    const PVterms<T> pv = pvterms(w);
     const int nx = w.nx, ny = w.ny, nux = w.nux, nuy = w.nuy, nvx = w.nvx, nvy = w.nvy, ep = w.ep;
     const T c = w.cssp;
     const State<T> yp = Yp, ym = Ym;
@@ -504,8 +566,8 @@ void ssp_mom(Launcher& L, const Work<T>& w, const State<T>& Yp, const State<T>& 
         if (I <= yp.u.m && J <= yp.u.n) {
             T d = zero;
             if (I >= 3 && I <= nux + 2 && J >= 3 && J <= nuy + 2) {
-                const int i = I - 2, j = J - 2, cc = 1 - ep + i;
-                const T qhv = qa(cc, j) * V(cc + 1, j + 1) + qb(cc, j) * V(cc, j + 1) + qc(cc, j) * V(cc, j) + qd(cc, j) * V(cc + 1, j);
+                const int i = I - 2, j = J - 2;
+                const T qhv = pv.qhv(i, j);
                 const T dpdx = p(i + 2 - ep, j + 1) - p(i + 1 - ep, j + 1);
                 d = (qhv - dpdx) + Fx(i, j);
             }
@@ -515,8 +577,7 @@ void ssp_mom(Launcher& L, const Work<T>& w, const State<T>& Yp, const State<T>& 
             T d = zero;
             if (I >= 3 && I <= nvx + 2 && J >= 3 && J <= nvy + 2) {
                 const int i = I - 2, j = J - 2;
-                const T qhu = qa(i, j) * U(i, j + 1) + qb(i + 1, j) * U(i + 1, j + 1) + qc(i + 1, j + 1) * U(i + 1, j + 2) +
-                              qd(i, j + 1) * U(i, j + 2);
+                const T qhu = pv.qhu(i, j);
                 const T dpdy = p(i + 1, j + 2) - p(i + 1, j + 1);
                 d = -(qhu + dpdy) + Fy(i, j);
             }
@@ -995,8 +1056,8 @@ AdjCfgError adjoint_check(const sw_config& c) {
         return {SW_ERR_UNSUPPORTED, "the adjoint computes in T = Tprog = Tcomm, Float32 or Float64"};
     if (!((c.time_scheme == SW_RK && c.RKo >= 2 && c.RKo <= 4) || (c.time_scheme == SW_SSPRK2 && c.RKs >= 2 && c.RKs <= 4)))
         return {SW_ERR_UNSUPPORTED, "the adjoint follows RK2/3/4 and SSPRK2 with 2-4 sub-stages"};
-    if (c.dynamics != SW_NONLINEAR || c.adv_scheme != SW_ARAKAWA_HSU || c.nstep_advcor != 0)
-        return {SW_ERR_UNSUPPORTED, "the adjoint follows nonlinear dynamics with Arakawa-Hsu and nstep_advcor = 0"};
+    if (c.dynamics != SW_NONLINEAR || c.nstep_advcor != 0)
+        return {SW_ERR_UNSUPPORTED, "the adjoint follows nonlinear dynamics with nstep_advcor = 0"};
     if (c.nstep_diff != 1) return {SW_ERR_UNSUPPORTED, "the adjoint needs nstep_diff = 1"};
     if (c.surface_relax || c.surface_forcing || c.seasonal_wind_x || c.seasonal_wind_y)
         return {SW_ERR_UNSUPPORTED, "the adjoint has no time-dependent forcing or relaxation"};
@@ -1143,6 +1204,7 @@ struct Adjoint {
         for (int k = 0; k < 4; k++) w.RKa[k] = (T)c.RKaDt[k];
         for (int k = 0; k < 3; k++) w.RKb[k] = (T)c.RKbDt[k];
         w.drag = c.bottom_drag; w.diff = c.diffusion;
+        w.sadourny = c.adv_scheme == SW_SADOURNY;
         const int nx = w.nx, ny = w.ny, nux = w.nux, nuy = w.nuy, nvx = w.nvx, nvy = w.nvy;
         {
             Carver cv;   // static fields and the forcing adjoint
@@ -1180,6 +1242,7 @@ struct Adjoint {
             cv.add(w.U, nx + 1, ny + 2); cv.add(w.V, nx + 2, ny + 1); cv.add(w.q, nx + 1, ny + 1);
             cv.add(w.qa, nx, ny); cv.add(w.qb, nx + 1, ny); cv.add(w.qc, nx + 1, ny); cv.add(w.qd, nx, ny);
             cv.add(w.p, nx + 2, ny + 2);
+            cv.add(w.qu, nx + 1, ny); cv.add(w.qv, nx, ny + 1); cv.add(w.Vu, nx + 1, ny); cv.add(w.Uv, nx, ny + 1);
             // tail intermediates
             cv.add(w.thu, nx + 1, ny + 2); cv.add(w.thv, nx + 2, ny + 1); cv.add(w.sKE, nx + 2, ny + 2);
             cv.add(w.sKEu, nx + 1, ny + 2); cv.add(w.sKEv, nx + 2, ny + 1);
@@ -1198,6 +1261,7 @@ struct Adjoint {
             cv.add(w.bU, nx + 1, ny + 2); cv.add(w.bV, nx + 2, ny + 1); cv.add(w.bp, nx + 2, ny + 2);
             cv.add(w.bqa, nx, ny); cv.add(w.bqb, nx + 1, ny); cv.add(w.bqc, nx + 1, ny); cv.add(w.bqd, nx, ny);
             cv.add(w.bq, nx + 1, ny + 1);
+            cv.add(w.bqu, nx + 1, ny); cv.add(w.bqv, nx, ny + 1); cv.add(w.bVu, nx + 1, ny); cv.add(w.bUv, nx, ny + 1);
             if (!carve(cv, &w.stage_adj, &w.stage_adj_elems)) return SW_ERR_NOMEM;
         }
         {
