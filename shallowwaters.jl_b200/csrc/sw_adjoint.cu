@@ -178,7 +178,9 @@ struct Work {
     int drag, diff;
     bool sadourny = false;      // PV_Sadourny! (src/PV_advection.jl:31-59) instead of Arakawa-Hsu
     // static fields
-    A2<T> H, f_q, Fx, Fy;
+    A2<T> H, f_q, Fx, Fy, eta_ref;
+    bool relax = false;         // continuity_surf_relax! (src/continuity.jl:3-24)
+    T gamma = T(0);
     // states
     State<T> X;                 // the state being advanced (in / out of a step)
     // stage states.  RK: Ys[k-1] = input of stage k after its ghost points
@@ -379,13 +381,17 @@ void stage_fwd(Launcher& L, const Work<T>& w, const State<T>& Y) {
 // and the RK combination (src/time_integration.jl:64-72): Y1 = Xt + b*d (k < RKo),
 // X0 += a*d.  d is zero on the halo, so halo points keep Xt / X0.
 template <class T>
-void stage_update(Launcher& L, const Work<T>& w, int k, const State<T>& Xt, const State<T>* Y1, const State<T>& X0) {
+void stage_update(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const State<T>& Xt, const State<T>* Y1,
+                  const State<T>& X0) {
     const A2<T> p = w.p, Fx = w.Fx, Fy = w.Fy, U = w.U, V = w.V;
     const PVterms<T> pv = pvterms(w);
     const int nx = w.nx, ny = w.ny, nux = w.nux, nuy = w.nuy, nvx = w.nvx, nvy = w.nvy, ep = w.ep;
     const T a = w.RKa[k - 1], b = k < w.rko ? w.RKb[k - 1] : T(0);
     const bool next = Y1 != nullptr;
     const State<T> xt = Xt, x0 = X0, y1 = next ? *Y1 : Xt;
+    const A2<T> eta_ref = w.eta_ref, ye = Y.e;
+    const bool relax = w.relax;
+    const T gamma = w.gamma;
     L.d2(nx + 4, ny + 4, [=] __host__ __device__(int I, int J) {
         const T zero = T(0);
         if (I <= xt.u.m && J <= xt.u.n) {
@@ -417,6 +423,7 @@ void stage_update(Launcher& L, const Work<T>& w, int k, const State<T>& Xt, cons
                 const T dUdx = U(i + 1, j + 1) - U(i, j + 1);
                 const T dVdy = V(i + 1, j + 1) - V(i + 1, j);
                 d = -(dUdx + dVdy);
+                if (relax) d = d + gamma * (eta_ref(i, j) - ye(i + 1, j + 1));
             }
             if (next) y1.e(I, J) = xt.e(I, J) + b * d;
             x0.e(I, J) += a * d;
@@ -436,7 +443,8 @@ void stage_rev(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const St
     const A2<T> bU = w.bU, bV = w.bV, bp = w.bp, bqa = w.bqa, bqb = w.bqb, bqc = w.bqc, bqd = w.bqd, bq = w.bq,
                 bFx = w.bFx;
     const A2<T> qu = w.qu, qv = w.qv, Vu = w.Vu, Uv = w.Uv, bqu = w.bqu, bqv = w.bqv, bVu = w.bVu, bUv = w.bUv;
-    const bool sad = w.sadourny;
+    const bool sad = w.sadourny, relax = w.relax;
+    const T gamma = w.gamma;
     const int nx = w.nx, ny = w.ny, nux = w.nux, nuy = w.nuy, nvx = w.nvx, nvy = w.nvy, ep = w.ep;
     // RK: dbar = RKa*Xb0 + RKb*Wb.  Momentum only (SSPRK2): dbar = coef*Xb0 for
     // u and v, no continuity part (Yb may then be Xb0 itself: this first pass
@@ -483,6 +491,7 @@ void stage_rev(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const St
             if (has_w) g += b * wb.e(i + 1, j + 1);
             add(bU(i + 1, j + 1), -g); add(bU(i, j + 1), g);
             add(bV(i + 1, j + 1), -g); add(bV(i + 1, j), g);
+            if (relax) add(yb.e(i + 1, j + 1), -(gamma * g));   // gamma*(eta_ref - eta); yb is not x0 here
         }
     });
     // bernoulli^T (through KEu = Ix(u^2), KEv = Iy(v^2)) and AHα..δ^T
@@ -596,6 +605,9 @@ void ssp_cont(Launcher& L, const Work<T>& w, const State<T>& Ym, const State<T>&
     const int nx = w.nx, ny = w.ny, ep = w.ep;
     const T c = w.cssp;
     const State<T> ym = Ym, yn = Yn;
+    const A2<T> eta_ref = w.eta_ref;
+    const bool relax = w.relax;
+    const T gamma = w.gamma;
     L.d2(nx + 4, ny + 4, [=] __host__ __device__(int I, int J) {
         if (I <= ym.u.m && J <= ym.u.n) yn.u(I, J) = ym.u(I, J);
         if (I <= ym.v.m && J <= ym.v.n) yn.v(I, J) = ym.v(I, J);
@@ -608,6 +620,7 @@ void ssp_cont(Launcher& L, const Work<T>& w, const State<T>& Ym, const State<T>&
                 const T dUdx = Uf(i + 1, j + 1) - Uf(i, j + 1);
                 const T dVdy = Vf(i + 1, j + 1) - Vf(i + 1, j);
                 d = -(dUdx + dVdy);
+                if (relax) d = d + gamma * (eta_ref(i, j) - ym.e(i + 1, j + 1));
             }
             yn.e(I, J) = ym.e(I, J) + c * d;
         }
@@ -619,7 +632,9 @@ void ssp_cont(Launcher& L, const Work<T>& w, const State<T>& Ym, const State<T>&
 // Yb's eta), then their scatter onto u, v and, through h_u, h_v, eta.
 template <class T>
 void ssp_cont_rev(Launcher& L, const Work<T>& w, const State<T>& Ym, const State<T>& Yb) {
-    const A2<T> hu = w.hu, hv = w.hv, bU = w.bU, bV = w.bV;
+    const A2<T> hu = w.hu, hv = w.hv, bU = w.bU, bV = w.bV, bp = w.bp;
+    const bool relax = w.relax;
+    const T gamma = w.gamma;
     const int nx = w.nx, ny = w.ny, ep = w.ep;
     const T c = w.cssp;
     const State<T> ym = Ym, yb = Yb;
@@ -629,9 +644,11 @@ void ssp_cont_rev(Launcher& L, const Work<T>& w, const State<T>& Ym, const State
         };
         if (I <= nx + 1) bU(I, J) = g(I, J - 1) - g(I - 1, J - 1);        // dUdx(i, j+1) = U(i+1, j+1) - U(i, j+1)
         if (J <= ny + 1) bV(I, J) = g(I - 1, J) - g(I - 1, J - 1);        // dVdy(i+1, j) = V(i+1, j+1) - V(i+1, j)
+        if (relax && I <= nx && J <= ny) bp(I, J) = g(I, J);              // for the relaxation term, next pass
     });
     L.d2(nx + 2, ny + 2, [=] __host__ __device__(int I, int J) {
         const T half = T(0.5);
+        if (relax && I <= nx && J <= ny) add(yb.e(I + 1, J + 1), -(gamma * bp(I, J)));   // gamma*(eta_ref - eta)
         if (I <= nx + 1) {   // U = u1(1+ep+I, 1+J) * h_u(I, J), h_u = Ix(eta + H)
             const T b = bU(I, J);
             add(yb.u(1 + ep + I, 1 + J), b * hu(I, J));
@@ -937,7 +954,7 @@ void fwd_step(Launcher& L, const Work<T>& w) {
     for (int k = 1; k <= w.rko; k++) {
         if (k > 1) ghost(L, w, w.Ys[k - 1], false);
         stage_fwd(L, w, w.Ys[k - 1]);
-        stage_update(L, w, k, w.Ys[0], k < w.rko ? &w.Ys[k] : nullptr, w.Z);
+        stage_update(L, w, k, w.Ys[k - 1], w.Ys[0], k < w.rko ? &w.Ys[k] : nullptr, w.Z);
     }
     ghost(L, w, w.Z, false);
     tail_fwd(L, w, w.Z, &w.X);
@@ -1059,8 +1076,8 @@ AdjCfgError adjoint_check(const sw_config& c) {
     if (c.dynamics != SW_NONLINEAR || c.nstep_advcor != 0)
         return {SW_ERR_UNSUPPORTED, "the adjoint follows nonlinear dynamics with nstep_advcor = 0"};
     if (c.nstep_diff != 1) return {SW_ERR_UNSUPPORTED, "the adjoint needs nstep_diff = 1"};
-    if (c.surface_relax || c.surface_forcing || c.seasonal_wind_x || c.seasonal_wind_y)
-        return {SW_ERR_UNSUPPORTED, "the adjoint has no time-dependent forcing or relaxation"};
+    if (c.surface_forcing || c.seasonal_wind_x || c.seasonal_wind_y)
+        return {SW_ERR_UNSUPPORTED, "the adjoint has no time-dependent forcing"};
     if (c.storage != SW_STORE_NATIVE) return {SW_ERR_UNSUPPORTED, "the adjoint keeps the native storage"};
     return {SW_OK, nullptr};
 }
@@ -1205,15 +1222,18 @@ struct Adjoint {
         for (int k = 0; k < 3; k++) w.RKb[k] = (T)c.RKbDt[k];
         w.drag = c.bottom_drag; w.diff = c.diffusion;
         w.sadourny = c.adv_scheme == SW_SADOURNY;
+        w.relax = c.surface_relax != 0;
+        w.gamma = (T)c.gamma;
         const int nx = w.nx, ny = w.ny, nux = w.nux, nuy = w.nuy, nvx = w.nvx, nvy = w.nvy;
         {
             Carver cv;   // static fields and the forcing adjoint
             cv.add(w.H, nx + 2, ny + 2); cv.add(w.f_q, nx + 1, ny + 1); cv.add(w.Fx, nux, nuy); cv.add(w.Fy, nvx, nvy);
+            cv.add(w.eta_ref, nx, ny);
             cv.add(w.bFx, nux, nuy);
             if (!carve(cv)) return SW_ERR_NOMEM;
-            const void* src[4] = {stt.H, stt.f_q, stt.Fx, stt.Fy};
-            A2<T>* dst[4] = {&w.H, &w.f_q, &w.Fx, &w.Fy};
-            for (int k = 0; k < 4; k++) {
+            const void* src[5] = {stt.H, stt.f_q, stt.Fx, stt.Fy, stt.eta_ref};
+            A2<T>* dst[5] = {&w.H, &w.f_q, &w.Fx, &w.Fy, &w.eta_ref};
+            for (int k = 0; k < (w.relax ? 5 : 4); k++) {
                 if (!src[k]) return SW_ERR_ARG;
                 if (upload(dst[k]->d, src[k], dst[k]->size() * sizeof(T)) != cudaSuccess) return SW_ERR_CUDA;
             }

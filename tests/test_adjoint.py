@@ -36,7 +36,8 @@ OPTIONS = [dict(), dict(bc="nonperiodic", α=0.5), dict(diffusion="constant"),
            dict(time_scheme="SSPRK2", RKs=3, cfl=1.0),
            dict(time_scheme="SSPRK2", RKs=2, cfl=0.6, bc="nonperiodic", α=0.5, diffusion="constant"),
            dict(adv_scheme="Sadourny"), dict(adv_scheme="Sadourny", bc="nonperiodic", α=1.0, time_scheme="SSPRK2",
-                                             RKs=3, cfl=1.0)]
+                                             RKs=3, cfl=1.0),
+           dict(surface_relax=True), dict(surface_relax=True, time_scheme="SSPRK2", RKs=3, cfl=1.0)]
 
 
 def setup(T=np.float64, seed=3, **kw):
