@@ -943,11 +943,21 @@ void copy_state(Launcher& L, const State<T>& dst, const State<T>& src) {
 // one time step X -> X (src/time_integration.jl:45-243, RK branch); leaves the
 // stage inputs in Ys, the tail input in Z and the last stage's intermediates.
 template <class T>
-void fwd_step_ssp(Launcher& L, const Work<T>& w);
+void fwd_step_ssp(Launcher& L, const Work<T>& w, bool tail);
+
+// the end of a step (src/time_integration.jl:204-233): after ghost_points! of
+// the RK sum, drag and diffusion on steps i with i % nstep_diff == 0 (tail),
+// else the ghosted sum is the new state
+template <class T>
+void step_end(Launcher& L, const Work<T>& w, bool tail) {
+    ghost(L, w, w.Z, GH_ALL);
+    if (tail) tail_fwd(L, w, w.Z, &w.X);
+    else copy_state(L, w.X, w.Z);
+}
 
 template <class T>
-void fwd_step(Launcher& L, const Work<T>& w) {
-    if (w.ssp) { fwd_step_ssp(L, w); return; }
+void fwd_step(Launcher& L, const Work<T>& w, bool tail = true) {
+    if (w.ssp) { fwd_step_ssp(L, w, tail); return; }
     copy_state(L, w.Ys[0], w.X);
     ghost(L, w, w.Ys[0], false);
     copy_state(L, w.Z, w.Ys[0]);
@@ -956,8 +966,7 @@ void fwd_step(Launcher& L, const Work<T>& w) {
         stage_fwd(L, w, w.Ys[k - 1]);
         stage_update(L, w, k, w.Ys[k - 1], w.Ys[0], k < w.rko ? &w.Ys[k] : nullptr, w.Z);
     }
-    ghost(L, w, w.Z, false);
-    tail_fwd(L, w, w.Z, &w.X);
+    step_end(L, w, tail);
 }
 
 // adjoint of one step: on entry Xb holds the adjoint of the step's output and
@@ -967,7 +976,7 @@ void fwd_step(Launcher& L, const Work<T>& w) {
 // the adjoint of the input, and bFx has this step's forcing adjoint added.
 // one SSPRK2 time step X -> X (src/time_integration.jl:80-104, 204-243)
 template <class T>
-void fwd_step_ssp(Launcher& L, const Work<T>& w) {
+void fwd_step_ssp(Launcher& L, const Work<T>& w, bool tail) {
     copy_state(L, w.Ys[0], w.X);
     ghost(L, w, w.Ys[0], GH_ALL);
     copy_state(L, w.Ys[1], w.Ys[0]);
@@ -980,16 +989,17 @@ void fwd_step_ssp(Launcher& L, const Work<T>& w) {
         ssp_cont(L, w, ym, yn);
     }
     combine(L, w.Z, w.ssp_a, w.Ys[0], w.ssp_b, w.Ys[2 * w.rks + 1]);
-    ghost(L, w, w.Z, GH_ALL);
-    tail_fwd(L, w, w.Z, &w.X);
+    step_end(L, w, tail);
 }
 
 template <class T>
-void adj_step_ssp(Launcher& L, const Work<T>& w, bool stored) {
-    if (stored) tail_fwd(L, w, w.Z, (const State<T>*)nullptr);
-    else fwd_step_ssp(L, w);
-    ghostT(L, w, w.Xb, GH_UV);
-    tail_rev(L, w, w.Z, w.Xb);
+void adj_step_ssp(Launcher& L, const Work<T>& w, bool stored, bool tail) {
+    if (!stored) fwd_step_ssp(L, w, tail);
+    else if (tail) tail_fwd(L, w, w.Z, (const State<T>*)nullptr);
+    if (tail) {
+        ghostT(L, w, w.Xb, GH_UV);
+        tail_rev(L, w, w.Z, w.Xb);
+    }
     ghostT(L, w, w.Xb, GH_ALL);    // Xb: adjoint of X0 = a*Ys[0] + b*Ys[2 RKs + 1]
     const State<T>& Yb = w.Yb[0];
     combine(L, w.acc, w.ssp_a, w.Xb, T(0), w.Xb);
@@ -1010,12 +1020,14 @@ void adj_step_ssp(Launcher& L, const Work<T>& w, bool stored) {
 }
 
 template <class T>
-void adj_step(Launcher& L, const Work<T>& w, bool stored) {
-    if (w.ssp) { adj_step_ssp(L, w, stored); return; }
-    if (stored) tail_fwd(L, w, w.Z, (const State<T>*)nullptr);
-    else fwd_step(L, w);
-    ghostT(L, w, w.Xb, true);
-    tail_rev(L, w, w.Z, w.Xb);
+void adj_step(Launcher& L, const Work<T>& w, bool stored, bool tail = true) {
+    if (w.ssp) { adj_step_ssp(L, w, stored, tail); return; }
+    if (!stored) fwd_step(L, w, tail);
+    else if (tail) tail_fwd(L, w, w.Z, (const State<T>*)nullptr);
+    if (tail) {
+        ghostT(L, w, w.Xb, GH_UV);
+        tail_rev(L, w, w.Z, w.Xb);
+    }
     ghostT(L, w, w.Xb, false);     // Xb is now the adjoint of the RK sum X0
     copy_state(L, w.acc, w.Xb);  // X0 starts as the ghosted input
     const State<T>* Wb = nullptr;
@@ -1075,7 +1087,7 @@ AdjCfgError adjoint_check(const sw_config& c) {
         return {SW_ERR_UNSUPPORTED, "the adjoint follows RK2/3/4 and SSPRK2 with 2-4 sub-stages"};
     if (c.dynamics != SW_NONLINEAR || c.nstep_advcor != 0)
         return {SW_ERR_UNSUPPORTED, "the adjoint follows nonlinear dynamics with nstep_advcor = 0"};
-    if (c.nstep_diff != 1) return {SW_ERR_UNSUPPORTED, "the adjoint needs nstep_diff = 1"};
+    if (c.nstep_diff < 1) return {SW_ERR_ARG, "nstep_diff"};
     if (c.surface_forcing || c.seasonal_wind_x || c.seasonal_wind_y)
         return {SW_ERR_UNSUPPORTED, "the adjoint has no time-dependent forcing"};
     if (c.storage != SW_STORE_NATIVE) return {SW_ERR_UNSUPPORTED, "the adjoint keeps the native storage"};
@@ -1092,7 +1104,9 @@ struct Adjoint {
     bool host = false;
     std::vector<void*> blocks;
     cudaStream_t s = nullptr;
-    cudaGraphExec_t g_fwd = nullptr, g_adj = nullptr, g_adj_st = nullptr;
+    // step graphs, by whether the step ends with drag and diffusion ([1]) or not ([0])
+    cudaGraphExec_t g_fwd[2] = {}, g_adj[2] = {}, g_adj_st[2] = {};
+    int nstep_diff = 1;
     T* records = nullptr;       // per step: Ys[0..nst-1] and Z as the forward sweep left them
     bool stored = false;
     std::vector<State<T>> slots;
@@ -1102,9 +1116,9 @@ struct Adjoint {
 
     ~Adjoint() {
         if (s) cudaStreamSynchronize(s);
-        if (g_fwd) cudaGraphExecDestroy(g_fwd);
-        if (g_adj) cudaGraphExecDestroy(g_adj);
-        if (g_adj_st) cudaGraphExecDestroy(g_adj_st);
+        for (int t = 0; t < 2; t++)
+            for (cudaGraphExec_t g : {g_fwd[t], g_adj[t], g_adj_st[t]})
+                if (g) cudaGraphExecDestroy(g);
         for (void* p : blocks) {
             if (host) std::free(p); else cudaFree(p);
         }
@@ -1222,6 +1236,7 @@ struct Adjoint {
         for (int k = 0; k < 3; k++) w.RKb[k] = (T)c.RKbDt[k];
         w.drag = c.bottom_drag; w.diff = c.diffusion;
         w.sadourny = c.adv_scheme == SW_SADOURNY;
+        nstep_diff = c.nstep_diff;
         w.relax = c.surface_relax != 0;
         w.gamma = (T)c.gamma;
         const int nx = w.nx, ny = w.ny, nux = w.nux, nuy = w.nuy, nvx = w.nvx, nvy = w.nvy;
@@ -1308,51 +1323,59 @@ struct Adjoint {
     }
 
     int capture() {
-        for (int k = 0; k < 3; k++) {
-            if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return SW_ERR_CUDA;
-            Launcher L = launcher();
-            if (k == 0) fwd_step(L, w);
-            else adj_step(L, w, k == 2);
-            cudaError_t e = cudaGetLastError();
-            cudaGraph_t graph = nullptr;
-            const cudaError_t ec = cudaStreamEndCapture(s, &graph);
-            if (e == cudaSuccess) e = ec;
-            if (e == cudaSuccess) e = cudaGraphInstantiate(k == 0 ? &g_fwd : (k == 1 ? &g_adj : &g_adj_st), graph, 0);
-            if (graph) cudaGraphDestroy(graph);
-            if (e != cudaSuccess) {
-                err = std::string("adjoint graph: ") + cudaGetErrorString(e);
-                return SW_ERR_CUDA;
+        for (int t = (nstep_diff > 1 ? 0 : 1); t < 2; t++)
+            for (int k = 0; k < 3; k++) {
+                if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return SW_ERR_CUDA;
+                Launcher L = launcher();
+                if (k == 0) fwd_step(L, w, t == 1);
+                else adj_step(L, w, k == 2, t == 1);
+                cudaError_t e = cudaGetLastError();
+                cudaGraph_t graph = nullptr;
+                const cudaError_t ec = cudaStreamEndCapture(s, &graph);
+                if (e == cudaSuccess) e = ec;
+                if (e == cudaSuccess) e = cudaGraphInstantiate(k == 0 ? &g_fwd[t] : (k == 1 ? &g_adj[t] : &g_adj_st[t]), graph, 0);
+                if (graph) cudaGraphDestroy(graph);
+                if (e != cudaSuccess) {
+                    err = std::string("adjoint graph: ") + cudaGetErrorString(e);
+                    return SW_ERR_CUDA;
+                }
+                if (t == 1 && k == 0) launches_fwd = L.launches;
+                else if (t == 1 && k == (stored ? 2 : 1)) launches_adj = L.launches;
             }
-            if (k == 0) launches_fwd = L.launches;
-            else if (k == (stored ? 2 : 1)) launches_adj = L.launches;
-        }
         return SW_OK;
     }
 
-    cudaError_t advance(long long n) {
+    // the step i = k + 1 that starts at state k ends with drag and diffusion?
+    bool tail_of(long long k) const { return ((k + 1) % nstep_diff) == 0; }
+
+    // X: state `from` -> state `from + n`
+    cudaError_t advance(long long from, long long n) {
         cudaError_t e = cudaSuccess;
-        for (long long k = 0; k < n && e == cudaSuccess; k++) {
-            if (host) { Launcher L = launcher(); fwd_step(L, w); }
-            else e = cudaGraphLaunch(g_fwd, s);
+        for (long long k = from; k < from + n && e == cudaSuccess; k++) {
+            const int t = tail_of(k) ? 1 : 0;
+            if (host) { Launcher L = launcher(); fwd_step(L, w, t == 1); }
+            else e = cudaGraphLaunch(g_fwd[t], s);
         }
         fwd_steps += n;
         return e;
     }
-    cudaError_t adjoint_here() {   // Xb <- adjoint of the step that starts at the state in X
+    cudaError_t adjoint_here(long long k) {   // Xb <- adjoint of the step that starts at state k (in X)
         adj_steps++;
-        if (host) { Launcher L = launcher(); adj_step(L, w, false); return cudaSuccess; }
-        return cudaGraphLaunch(g_adj, s);
+        const int t = tail_of(k) ? 1 : 0;
+        if (host) { Launcher L = launcher(); adj_step(L, w, false, t == 1); return cudaSuccess; }
+        return cudaGraphLaunch(g_adj[t], s);
     }
-    cudaError_t adjoint_stored(long long k) {   // Xb <- adjoint of step k from its kept stage states
+    cudaError_t adjoint_stored(long long k) {   // Xb <- adjoint of the step from state k, from its kept stage states
         Launcher L = launcher();
         L.copy(w.stage_block, records + (size_t)k * w.stage_block_elems, w.stage_block_elems * sizeof(T));
         adj_steps++;
-        if (host) { adj_step(L, w, true); return cudaSuccess; }
-        return cudaGraphLaunch(g_adj_st, s);
+        const int t = tail_of(k) ? 1 : 0;
+        if (host) { adj_step(L, w, true, t == 1); return cudaSuccess; }
+        return cudaGraphLaunch(g_adj_st[t], s);
     }
-    cudaError_t adjoint_of(const State<T>& state) {
+    cudaError_t adjoint_of(const State<T>& state, long long k) {
         copy(w.X, state);
-        return adjoint_here();
+        return adjoint_here(k);
     }
 
     // binomial reversal of steps [a, b): the state of step a is in slot `slot`;
@@ -1362,11 +1385,11 @@ struct Adjoint {
         while (b > a && e == cudaSuccess) {
             const long long t = b - a;
             const int free_slots = (int)slots.size() - 1 - slot;
-            if (t == 1) return adjoint_of(slots[slot]);
+            if (t == 1) return adjoint_of(slots[slot], a);
             if (free_slots <= 0) {   // no slot left: recompute the state of step b - 1 from a
                 copy(w.X, slots[slot]);
-                e = advance(t - 1);
-                if (e == cudaSuccess) e = adjoint_here();
+                e = advance(a, t - 1);
+                if (e == cudaSuccess) e = adjoint_here(b - 1);
                 b--;
                 continue;
             }
@@ -1382,7 +1405,7 @@ struct Adjoint {
             left = std::max(1LL, std::min(left, t - 1));
             const long long m = a + left;
             copy(w.X, slots[slot]);
-            e = advance(m - a);
+            e = advance(a, m - a);
             if (e != cudaSuccess) return e;
             copy(slots[slot + 1], w.X);
             e = reverse(m, b, slot + 1);
@@ -1433,7 +1456,7 @@ int adjoint_run(bool host, const sw_config& c, const sw_static& st, const void* 
     A.copy(w.X, A.slots[0]);
     const bool keep_all = !A.stored && nslots >= nsteps;
     for (long long k = 1; k <= nsteps && e == cudaSuccess; k++) {
-        e = A.advance(1);
+        e = A.advance(k - 1, 1);
         if (keep_all && k < nsteps) A.copy(A.slots[k], w.X);
         if (A.stored) {
             Launcher L = A.launcher();
@@ -1459,7 +1482,7 @@ int adjoint_run(bool host, const sw_config& c, const sw_static& st, const void* 
         if (A.stored) {
             for (long long k = nsteps - 1; k >= 0 && e == cudaSuccess; k--) e = A.adjoint_stored(k);
         } else if (keep_all) {
-            for (long long k = nsteps - 1; k >= 0 && e == cudaSuccess; k--) e = A.adjoint_of(A.slots[k]);
+            for (long long k = nsteps - 1; k >= 0 && e == cudaSuccess; k--) e = A.adjoint_of(A.slots[k], k);
         } else {
             e = A.reverse(0, nsteps, 0);
         }
