@@ -279,7 +279,7 @@ void sw_batch_destroy(sw_batch* b);
  * Float32 or Float64, RK2/3/4 or SSPRK2 (2-4 sub-stages, with its
  * semi-implicit continuity), nonlinear dynamics, Arakawa-Hsu or Sadourny, nstep_advcor =
  * 0, any nstep_diff, any drag and diffusion, either boundary, surface
- * relaxation, no time-dependent forcing (else SW_ERR_UNSUPPORTED).  The tracer is passive and plays no part.
+ * relaxation or forcing, seasonal wind (else SW_ERR_UNSUPPORTED).  The tracer is passive and plays no part.
  * Inputs and outputs are HOST buffers in T: u, v, eta the initial state,
  * eta_obs nx x ny; g_u, g_v, g_eta (state shapes), g_Fx and eta_final (the eta
  * after nsteps, with halo) may be NULL.  ncheckpoints >= nsteps keeps every

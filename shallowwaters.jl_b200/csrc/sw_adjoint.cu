@@ -178,7 +178,12 @@ struct Work {
     int drag, diff;
     bool sadourny = false;      // PV_Sadourny! (src/PV_advection.jl:31-59) instead of Arakawa-Hsu
     // static fields
-    A2<T> H, f_q, Fx, Fy, eta_ref;
+    A2<T> H, f_q, Fx, Fy, eta_ref, Feta;
+    // time-dependent forcing: the step's Fxt, Fyt (seasonal wind, src/rhs.jl:233-238,
+    // 262-267) and Fetat (continuity_forcing!, src/continuity.jl:27-49) are read
+    // from force[0..2], which the host sets before each step's replay
+    bool timedep = false, forcing = false;
+    T* force = nullptr;
     bool relax = false;         // continuity_surf_relax! (src/continuity.jl:3-24)
     T gamma = T(0);
     // states
@@ -389,9 +394,10 @@ void stage_update(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const
     const T a = w.RKa[k - 1], b = k < w.rko ? w.RKb[k - 1] : T(0);
     const bool next = Y1 != nullptr;
     const State<T> xt = Xt, x0 = X0, y1 = next ? *Y1 : Xt;
-    const A2<T> eta_ref = w.eta_ref, ye = Y.e;
-    const bool relax = w.relax;
+    const A2<T> eta_ref = w.eta_ref, ye = Y.e, Feta = w.Feta;
+    const bool relax = w.relax, timedep = w.timedep, forcing = w.forcing;
     const T gamma = w.gamma;
+    const T* force = w.force;
     L.d2(nx + 4, ny + 4, [=] __host__ __device__(int I, int J) {
         const T zero = T(0);
         if (I <= xt.u.m && J <= xt.u.n) {
@@ -400,7 +406,7 @@ void stage_update(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const
                 const int i = I - 2, j = J - 2;
                 const T qhv = pv.qhv(i, j);
                 const T dpdx = p(i + 2 - ep, j + 1) - p(i + 1 - ep, j + 1);
-                d = (qhv - dpdx) + Fx(i, j);
+                d = timedep ? (qhv - dpdx) + force[0] * Fx(i, j) : (qhv - dpdx) + Fx(i, j);
             }
             if (next) y1.u(I, J) = xt.u(I, J) + b * d;
             x0.u(I, J) += a * d;
@@ -411,7 +417,7 @@ void stage_update(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const
                 const int i = I - 2, j = J - 2;
                 const T qhu = pv.qhu(i, j);
                 const T dpdy = p(i + 1, j + 2) - p(i + 1, j + 1);
-                d = -(qhu + dpdy) + Fy(i, j);
+                d = timedep ? -(qhu + dpdy) + force[1] * Fy(i, j) : -(qhu + dpdy) + Fy(i, j);
             }
             if (next) y1.v(I, J) = xt.v(I, J) + b * d;
             x0.v(I, J) += a * d;
@@ -424,6 +430,7 @@ void stage_update(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const
                 const T dVdy = V(i + 1, j + 1) - V(i + 1, j);
                 d = -(dUdx + dVdy);
                 if (relax) d = d + gamma * (eta_ref(i, j) - ye(i + 1, j + 1));
+                else if (forcing) d = d + force[2] * Feta(i, j);
             }
             if (next) y1.e(I, J) = xt.e(I, J) + b * d;
             x0.e(I, J) += a * d;
@@ -443,8 +450,9 @@ void stage_rev(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const St
     const A2<T> bU = w.bU, bV = w.bV, bp = w.bp, bqa = w.bqa, bqb = w.bqb, bqc = w.bqc, bqd = w.bqd, bq = w.bq,
                 bFx = w.bFx;
     const A2<T> qu = w.qu, qv = w.qv, Vu = w.Vu, Uv = w.Uv, bqu = w.bqu, bqv = w.bqv, bVu = w.bVu, bUv = w.bUv;
-    const bool sad = w.sadourny, relax = w.relax;
+    const bool sad = w.sadourny, relax = w.relax, timedep = w.timedep;
     const T gamma = w.gamma;
+    const T* force = w.force;
     const int nx = w.nx, ny = w.ny, nux = w.nux, nuy = w.nuy, nvx = w.nvx, nvy = w.nvy, ep = w.ep;
     // RK: dbar = RKa*Xb0 + RKb*Wb.  Momentum only (SSPRK2): dbar = coef*Xb0 for
     // u and v, no continuity part (Yb may then be Xb0 itself: this first pass
@@ -458,7 +466,7 @@ void stage_rev(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const St
         if (i <= nux && j <= nuy) {
             T g = a * x0.u(i + 2, j + 2);
             if (has_w) g += b * wb.u(i + 2, j + 2);
-            bFx(i, j) += g;
+            bFx(i, j) += timedep ? force[0] * g : g;
             add(bp(i + 2 - ep, j + 1), -g);
             add(bp(i + 1 - ep, j + 1), g);
             const int c = 1 - ep + i;      // qhv (src/PV_advection.jl:73, Sadourny :49)
@@ -569,6 +577,8 @@ void ssp_mom(Launcher& L, const Work<T>& w, const State<T>& Yp, const State<T>& 
     const PVterms<T> pv = pvterms(w);
     const int nx = w.nx, ny = w.ny, nux = w.nux, nuy = w.nuy, nvx = w.nvx, nvy = w.nvy, ep = w.ep;
     const T c = w.cssp;
+    const bool timedep = w.timedep;
+    const T* force = w.force;
     const State<T> yp = Yp, ym = Ym;
     L.d2(nx + 4, ny + 4, [=] __host__ __device__(int I, int J) {
         const T zero = T(0);
@@ -578,7 +588,7 @@ void ssp_mom(Launcher& L, const Work<T>& w, const State<T>& Yp, const State<T>& 
                 const int i = I - 2, j = J - 2;
                 const T qhv = pv.qhv(i, j);
                 const T dpdx = p(i + 2 - ep, j + 1) - p(i + 1 - ep, j + 1);
-                d = (qhv - dpdx) + Fx(i, j);
+                d = timedep ? (qhv - dpdx) + force[0] * Fx(i, j) : (qhv - dpdx) + Fx(i, j);
             }
             ym.u(I, J) = yp.u(I, J) + c * d;
         }
@@ -588,7 +598,7 @@ void ssp_mom(Launcher& L, const Work<T>& w, const State<T>& Yp, const State<T>& 
                 const int i = I - 2, j = J - 2;
                 const T qhu = pv.qhu(i, j);
                 const T dpdy = p(i + 1, j + 2) - p(i + 1, j + 1);
-                d = -(qhu + dpdy) + Fy(i, j);
+                d = timedep ? -(qhu + dpdy) + force[1] * Fy(i, j) : -(qhu + dpdy) + Fy(i, j);
             }
             ym.v(I, J) = yp.v(I, J) + c * d;
         }
@@ -605,9 +615,10 @@ void ssp_cont(Launcher& L, const Work<T>& w, const State<T>& Ym, const State<T>&
     const int nx = w.nx, ny = w.ny, ep = w.ep;
     const T c = w.cssp;
     const State<T> ym = Ym, yn = Yn;
-    const A2<T> eta_ref = w.eta_ref;
-    const bool relax = w.relax;
+    const A2<T> eta_ref = w.eta_ref, Feta = w.Feta;
+    const bool relax = w.relax, forcing = w.forcing;
     const T gamma = w.gamma;
+    const T* force = w.force;
     L.d2(nx + 4, ny + 4, [=] __host__ __device__(int I, int J) {
         if (I <= ym.u.m && J <= ym.u.n) yn.u(I, J) = ym.u(I, J);
         if (I <= ym.v.m && J <= ym.v.n) yn.v(I, J) = ym.v(I, J);
@@ -621,6 +632,7 @@ void ssp_cont(Launcher& L, const Work<T>& w, const State<T>& Ym, const State<T>&
                 const T dVdy = Vf(i + 1, j + 1) - Vf(i + 1, j);
                 d = -(dUdx + dVdy);
                 if (relax) d = d + gamma * (eta_ref(i, j) - ym.e(i + 1, j + 1));
+                else if (forcing) d = d + force[2] * Feta(i, j);
             }
             yn.e(I, J) = ym.e(I, J) + c * d;
         }
@@ -1088,8 +1100,7 @@ AdjCfgError adjoint_check(const sw_config& c) {
     if (c.dynamics != SW_NONLINEAR || c.nstep_advcor != 0)
         return {SW_ERR_UNSUPPORTED, "the adjoint follows nonlinear dynamics with nstep_advcor = 0"};
     if (c.nstep_diff < 1) return {SW_ERR_ARG, "nstep_diff"};
-    if (c.surface_forcing || c.seasonal_wind_x || c.seasonal_wind_y)
-        return {SW_ERR_UNSUPPORTED, "the adjoint has no time-dependent forcing"};
+    if (c.surface_forcing && c.surface_relax) return {SW_ERR_ARG, "surface relaxation and forcing together"};
     if (c.storage != SW_STORE_NATIVE) return {SW_ERR_UNSUPPORTED, "the adjoint keeps the native storage"};
     return {SW_OK, nullptr};
 }
@@ -1107,6 +1118,7 @@ struct Adjoint {
     // step graphs, by whether the step ends with drag and diffusion ([1]) or not ([0])
     cudaGraphExec_t g_fwd[2] = {}, g_adj[2] = {}, g_adj_st[2] = {};
     int nstep_diff = 1;
+    T* step_force = nullptr;    // per step k: Fxt, Fyt, Fetat at t = k*dtint (pinned host memory)
     T* records = nullptr;       // per step: Ys[0..nst-1] and Z as the forward sweep left them
     bool stored = false;
     std::vector<State<T>> slots;
@@ -1116,6 +1128,7 @@ struct Adjoint {
 
     ~Adjoint() {
         if (s) cudaStreamSynchronize(s);
+        if (step_force) { if (host) std::free(step_force); else cudaFreeHost(step_force); }
         for (int t = 0; t < 2; t++)
             for (cudaGraphExec_t g : {g_fwd[t], g_adj[t], g_adj_st[t]})
                 if (g) cudaGraphExecDestroy(g);
@@ -1239,16 +1252,22 @@ struct Adjoint {
         nstep_diff = c.nstep_diff;
         w.relax = c.surface_relax != 0;
         w.gamma = (T)c.gamma;
+        w.forcing = c.surface_forcing != 0;
+        w.timedep = c.seasonal_wind_x || c.seasonal_wind_y || w.forcing;
         const int nx = w.nx, ny = w.ny, nux = w.nux, nuy = w.nuy, nvx = w.nvx, nvy = w.nvy;
         {
             Carver cv;   // static fields and the forcing adjoint
             cv.add(w.H, nx + 2, ny + 2); cv.add(w.f_q, nx + 1, ny + 1); cv.add(w.Fx, nux, nuy); cv.add(w.Fy, nvx, nvy);
-            cv.add(w.eta_ref, nx, ny);
+            cv.add(w.eta_ref, nx, ny); cv.add(w.Feta, nx, ny);
             cv.add(w.bFx, nux, nuy);
+            A2<T> fv;
+            cv.add(fv, 4, 1);
             if (!carve(cv)) return SW_ERR_NOMEM;
-            const void* src[5] = {stt.H, stt.f_q, stt.Fx, stt.Fy, stt.eta_ref};
-            A2<T>* dst[5] = {&w.H, &w.f_q, &w.Fx, &w.Fy, &w.eta_ref};
-            for (int k = 0; k < (w.relax ? 5 : 4); k++) {
+            w.force = fv.d;
+            const void* src[6] = {stt.H, stt.f_q, stt.Fx, stt.Fy, stt.eta_ref, stt.Feta};
+            A2<T>* dst[6] = {&w.H, &w.f_q, &w.Fx, &w.Fy, &w.eta_ref, &w.Feta};
+            for (int k = 0; k < 6; k++) {
+                if ((k == 4 && !w.relax) || (k == 5 && !w.forcing)) continue;
                 if (!src[k]) return SW_ERR_ARG;
                 if (upload(dst[k]->d, src[k], dst[k]->size() * sizeof(T)) != cudaSuccess) return SW_ERR_CUDA;
             }
@@ -1345,6 +1364,28 @@ struct Adjoint {
         return SW_OK;
     }
 
+    // the time-dependent multipliers of every step (src/rhs.jl:233-238, 262-267,
+    // src/continuity.jl:27-49 with t = k*dtint, the model time at step k's start)
+    int make_forcing(const sw_config& c, long long nsteps) {
+        if (!w.timedep) return SW_OK;
+        const size_t bytes = (size_t)nsteps * 3 * sizeof(T);
+        if (host) step_force = static_cast<T*>(std::malloc(bytes));
+        else if (cudaMallocHost(&step_force, bytes) != cudaSuccess) step_force = nullptr;
+        if (!step_force) return SW_ERR_NOMEM;
+        for (long long k = 0; k < nsteps; k++) {
+            const double t = (double)(k * (long long)c.dtint);
+            step_force[3 * k] = c.seasonal_wind_x ? (T)std::sin(c.omegaFx * t) : T(1);
+            step_force[3 * k + 1] = c.seasonal_wind_y ? (T)std::sin(c.omegaFy * t) : T(1);
+            step_force[3 * k + 2] = c.surface_forcing ? (T)std::sin(c.omegaFeta * t) : T(0);
+        }
+        return SW_OK;
+    }
+    void set_force(long long k) {   // before the replay of the step that starts at state k
+        if (!w.timedep) return;
+        if (host) std::memcpy(w.force, step_force + 3 * k, 3 * sizeof(T));
+        else cudaMemcpyAsync(w.force, step_force + 3 * k, 3 * sizeof(T), cudaMemcpyHostToDevice, s);
+    }
+
     // the step i = k + 1 that starts at state k ends with drag and diffusion?
     bool tail_of(long long k) const { return ((k + 1) % nstep_diff) == 0; }
 
@@ -1353,6 +1394,7 @@ struct Adjoint {
         cudaError_t e = cudaSuccess;
         for (long long k = from; k < from + n && e == cudaSuccess; k++) {
             const int t = tail_of(k) ? 1 : 0;
+            set_force(k);
             if (host) { Launcher L = launcher(); fwd_step(L, w, t == 1); }
             else e = cudaGraphLaunch(g_fwd[t], s);
         }
@@ -1362,6 +1404,7 @@ struct Adjoint {
     cudaError_t adjoint_here(long long k) {   // Xb <- adjoint of the step that starts at state k (in X)
         adj_steps++;
         const int t = tail_of(k) ? 1 : 0;
+        set_force(k);
         if (host) { Launcher L = launcher(); adj_step(L, w, false, t == 1); return cudaSuccess; }
         return cudaGraphLaunch(g_adj[t], s);
     }
@@ -1370,6 +1413,7 @@ struct Adjoint {
         L.copy(w.stage_block, records + (size_t)k * w.stage_block_elems, w.stage_block_elems * sizeof(T));
         adj_steps++;
         const int t = tail_of(k) ? 1 : 0;
+        set_force(k);
         if (host) { adj_step(L, w, true, t == 1); return cudaSuccess; }
         return cudaGraphLaunch(g_adj_st[t], s);
     }
@@ -1427,6 +1471,7 @@ int adjoint_run(bool host, const sw_config& c, const sw_static& st, const void* 
     const char* env = getenv("SWB200_ADJ_STORE");
     const bool want_store = ncheckpoints >= nsteps && !(env && env[0] == '0');
     int rc = A.setup(c, st, want_store, nsteps);
+    if (!rc) rc = A.make_forcing(c, nsteps);
     if (rc) {
         if (!A.err.empty()) fprintf(stderr, "swb200: %s\n", A.err.c_str());
         return rc;

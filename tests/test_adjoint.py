@@ -38,7 +38,9 @@ OPTIONS = [dict(), dict(bc="nonperiodic", α=0.5), dict(diffusion="constant"),
            dict(adv_scheme="Sadourny"), dict(adv_scheme="Sadourny", bc="nonperiodic", α=1.0, time_scheme="SSPRK2",
                                              RKs=3, cfl=1.0),
            dict(surface_relax=True), dict(surface_relax=True, time_scheme="SSPRK2", RKs=3, cfl=1.0),
-           dict(nstep_diff=3), dict(nstep_diff=2, time_scheme="SSPRK2", RKs=2, cfl=0.6)]
+           dict(nstep_diff=3), dict(nstep_diff=2, time_scheme="SSPRK2", RKs=2, cfl=0.6),
+           dict(seasonal_wind_x=True, ωFx=40.0), dict(surface_forcing=True, ωFη=40.0, seasonal_wind_y=True, ωFy=30.0,
+                                                     time_scheme="SSPRK2", RKs=3, cfl=1.0)]
 
 
 def setup(T=np.float64, seed=3, **kw):
@@ -93,7 +95,7 @@ def test_adjoint_entry_rejects_bad_arguments_and_unbuilt_options():
         grad(S, Prog, obs, 0)
     assert e.value.code == abi.SW_ERR_ARG
     for kw in (dict(time_scheme="SSPRK3"), dict(dynamics="linear"), dict(nstep_advcor=2),
-               dict(surface_forcing=True), dict(T=np.float32, Tprog=np.float64)):
+               dict(T=np.float32, Tprog=np.float64)):
         S2, P2, o2, _ = setup(**kw)
         with pytest.raises(abi.SwError) as e:
             grad(S2, P2, o2, 3)
