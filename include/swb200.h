@@ -277,7 +277,8 @@ void sw_batch_destroy(sw_batch* b);
  * counterpart in the reference; the forward model it differentiates is
  * src/time_integration.jl:45-104,204-233.  Supported: T = Tprog = Tcomm in
  * Float32 or Float64, RK2/3/4 or SSPRK2 (2-4 sub-stages, with its
- * semi-implicit continuity), nonlinear dynamics, Arakawa-Hsu or Sadourny, nstep_advcor =
+ * semi-implicit continuity), linear dynamics or nonlinear with Arakawa-Hsu or
+ * Sadourny and nstep_advcor =
  * 0, any nstep_diff, any drag and diffusion, either boundary, surface
  * relaxation or forcing, seasonal wind (else SW_ERR_UNSUPPORTED).  The tracer is passive and plays no part.
  * Inputs and outputs are HOST buffers in T: u, v, eta the initial state,

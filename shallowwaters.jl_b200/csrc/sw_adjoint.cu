@@ -177,8 +177,9 @@ struct Work {
     T RKa[4], RKb[3];
     int drag, diff;
     bool sadourny = false;      // PV_Sadourny! (src/PV_advection.jl:31-59) instead of Arakawa-Hsu
+    bool linear = false;        // rhs_linear! (src/rhs.jl:59-86)
     // static fields
-    A2<T> H, f_q, Fx, Fy, eta_ref, Feta;
+    A2<T> H, f_q, Fx, Fy, eta_ref, Feta, f_u, f_v;
     // time-dependent forcing: the step's Fxt, Fyt (seasonal wind, src/rhs.jl:233-238,
     // 262-267) and Fetat (continuity_forcing!, src/continuity.jl:27-49) are read
     // from force[0..2], which the host sets before each step's replay
@@ -210,6 +211,32 @@ struct Work {
     A2<T> bFx;                  // gradient with respect to Fx
     T* stage_adj = nullptr; size_t stage_adj_elems = 0;   // bU..bq, one block (zeroed per stage)
     T* tail_adj = nullptr; size_t tail_adj_elems = 0;     // bBu..bDSq, one block (zeroed per step)
+};
+
+// rhs_linear! tendencies at u-point (i, j) and v-point (i, j) of state y
+// (src/rhs.jl:59-86, fv! :183-198, fu! :201-215): Coriolis on Ixy! of the other
+// velocity and the gradient of g*eta, before the forcing term
+template <class T>
+struct LinTerms {
+    A2<T> f_u, f_v;
+    T g;
+    int ep;
+    __host__ __device__ __forceinline__ T du(const A2<T>& u, const A2<T>& v, const A2<T>& e, int i, int j) const {
+        const T quarter = T(0.25);
+        const int I = i + 2 - ep, J = j + 1;   // v_u(i+2-ep, j+1) = Ixy(v)
+        const T vu = quarter * (v(I, J) + v(I + 1, J)) + quarter * (v(I, J + 1) + v(I + 1, J + 1));
+        const T qhv = f_u(i, j) * vu;
+        const T dpdx = g * e(i + 2 - ep, j + 1) - g * e(i + 1 - ep, j + 1);
+        (void)u;
+        return qhv - dpdx;
+    }
+    __host__ __device__ __forceinline__ T dv_part(const A2<T>& u, const A2<T>& e, int i, int j, T& dpdy) const {
+        const T quarter = T(0.25);
+        const int I = i + 1 + ep, J = j + 2;   // u_v(i+1+ep, j+2) = Ixy(u)
+        const T uv = quarter * (u(I, J) + u(I + 1, J)) + quarter * (u(I, J + 1) + u(I + 1, J + 1));
+        dpdy = g * e(i + 1, j + 2) - g * e(i + 1, j + 1);
+        return f_v(i, j) * uv;   // qhu
+    }
 };
 
 template <class T>
@@ -346,6 +373,7 @@ void stage_fwd(Launcher& L, const Work<T>& w, const State<T>& Y) {
             q(i, j) = (f_q(i, j) + dvdx - dudy) / hq_;
         }
     });
+    if (w.linear) return;   // rhs_linear! needs none of the PV and Bernoulli terms
     const A2<T> qa = w.qa, qb = w.qb, qc = w.qc, qd = w.qd, p = w.p;
     const A2<T> qu = w.qu, qv = w.qv, Vu = w.Vu, Uv = w.Uv;
     const bool sad = w.sadourny;
@@ -394,19 +422,26 @@ void stage_update(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const
     const T a = w.RKa[k - 1], b = k < w.rko ? w.RKb[k - 1] : T(0);
     const bool next = Y1 != nullptr;
     const State<T> xt = Xt, x0 = X0, y1 = next ? *Y1 : Xt;
-    const A2<T> eta_ref = w.eta_ref, ye = Y.e, Feta = w.Feta;
-    const bool relax = w.relax, timedep = w.timedep, forcing = w.forcing;
+    const A2<T> eta_ref = w.eta_ref, ye = Y.e, Feta = w.Feta, yu = Y.u, yv = Y.v;
+    const bool relax = w.relax, timedep = w.timedep, forcing = w.forcing, linear = w.linear;
     const T gamma = w.gamma;
     const T* force = w.force;
+    const LinTerms<T> lt{w.f_u, w.f_v, w.g, w.ep};
     L.d2(nx + 4, ny + 4, [=] __host__ __device__(int I, int J) {
         const T zero = T(0);
         if (I <= xt.u.m && J <= xt.u.n) {
             T d = zero;
             if (I >= 3 && I <= nux + 2 && J >= 3 && J <= nuy + 2) {
                 const int i = I - 2, j = J - 2;
-                const T qhv = pv.qhv(i, j);
-                const T dpdx = p(i + 2 - ep, j + 1) - p(i + 1 - ep, j + 1);
-                d = timedep ? (qhv - dpdx) + force[0] * Fx(i, j) : (qhv - dpdx) + Fx(i, j);
+                T m;
+                if (linear) {
+                    m = lt.du(yu, yv, ye, i, j);
+                } else {
+                    const T qhv = pv.qhv(i, j);
+                    const T dpdx = p(i + 2 - ep, j + 1) - p(i + 1 - ep, j + 1);
+                    m = qhv - dpdx;
+                }
+                d = timedep ? m + force[0] * Fx(i, j) : m + Fx(i, j);
             }
             if (next) y1.u(I, J) = xt.u(I, J) + b * d;
             x0.u(I, J) += a * d;
@@ -415,8 +450,13 @@ void stage_update(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const
             T d = zero;
             if (I >= 3 && I <= nvx + 2 && J >= 3 && J <= nvy + 2) {
                 const int i = I - 2, j = J - 2;
-                const T qhu = pv.qhu(i, j);
-                const T dpdy = p(i + 1, j + 2) - p(i + 1, j + 1);
+                T qhu, dpdy;
+                if (linear) {
+                    qhu = lt.dv_part(yu, ye, i, j, dpdy);
+                } else {
+                    qhu = pv.qhu(i, j);
+                    dpdy = p(i + 1, j + 2) - p(i + 1, j + 1);
+                }
                 d = timedep ? -(qhu + dpdy) + force[1] * Fy(i, j) : -(qhu + dpdy) + Fy(i, j);
             }
             if (next) y1.v(I, J) = xt.v(I, J) + b * d;
@@ -426,8 +466,10 @@ void stage_update(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const
             T d = zero;
             if (I >= 2 && I <= nx + 1 && J >= 2 && J <= ny + 1) {
                 const int i = I - 1, j = J - 1;
-                const T dUdx = U(i + 1, j + 1) - U(i, j + 1);
-                const T dVdy = V(i + 1, j + 1) - V(i + 1, j);
+                // with linear dynamics the RK continuity reads U, V that rhs_linear!
+                // never forms, i.e. zeros (src/time_integration.jl:71, src/continuity.jl:72-97)
+                const T dUdx = linear ? zero - zero : U(i + 1, j + 1) - U(i, j + 1);
+                const T dVdy = linear ? zero - zero : V(i + 1, j + 1) - V(i + 1, j);
                 d = -(dUdx + dVdy);
                 if (relax) d = d + gamma * (eta_ref(i, j) - ye(i + 1, j + 1));
                 else if (forcing) d = d + force[2] * Feta(i, j);
@@ -442,9 +484,62 @@ void stage_update(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const
 // Given the stage's tendency adjoint  dbar = a*Xb0 + b*Wb  (interior points),
 // adds the adjoint of the stage input Y into Yb.  Transposes, in reverse
 // order, the passes of stage_fwd and stage_update.
+// transpose of a linear-dynamics stage (rhs_linear!, src/rhs.jl:59-86, and
+// the RK continuity, whose only state dependence is the relaxation term).
+// Two passes: the tendency adjoints into scratch (bqa at u-points, bqd at
+// v-points, with the sign of dv), then their scatter onto the state adjoint,
+// so Yb may be Xb0 itself.
+template <class T>
+void stage_rev_linear(Launcher& L, const Work<T>& w, int k, const State<T>& Xb0, const State<T>* Wb, const State<T>& Yb,
+                      bool mom_only, T coef) {
+    const A2<T> gu = w.bqa, gv = w.bqd, bFx = w.bFx, f_u = w.f_u, f_v = w.f_v;
+    const int nx = w.nx, ny = w.ny, nux = w.nux, nuy = w.nuy, nvx = w.nvx, nvy = w.nvy, ep = w.ep;
+    const T a = mom_only ? coef : w.RKa[k - 1], b = (Wb && !mom_only) ? w.RKb[k - 1] : T(0);
+    const State<T> x0 = Xb0, wb = Wb ? *Wb : Xb0, yb = Yb;
+    const bool has_w = Wb != nullptr && !mom_only, relax = w.relax, timedep = w.timedep;
+    const T gamma = w.gamma, g = w.g;
+    const T* force = w.force;
+    L.d2(nx, ny, [=] __host__ __device__(int i, int j) {
+        if (i <= nux && j <= nuy) {
+            T t = a * x0.u(i + 2, j + 2);
+            if (has_w) t += b * wb.u(i + 2, j + 2);
+            gu(i, j) = t;
+            bFx(i, j) += timedep ? force[0] * t : t;
+        }
+        if (i <= nvx && j <= nvy) {
+            T t = a * x0.v(i + 2, j + 2);
+            if (has_w) t += b * wb.v(i + 2, j + 2);
+            gv(i, j) = -t;
+        }
+        if (!mom_only && relax) {
+            T t = a * x0.e(i + 1, j + 1);
+            if (has_w) t += b * wb.e(i + 1, j + 1);
+            add(yb.e(i + 1, j + 1), -(gamma * t));
+        }
+    });
+    L.d2(nx, ny, [=] __host__ __device__(int i, int j) {
+        const T quarter = T(0.25);
+        if (i <= nux && j <= nuy) {   // du = (f_u*Ixy(v) - (g*eta(i+2-ep) - g*eta(i+1-ep))) + ...
+            const T t = gu(i, j);
+            const int I = i + 2 - ep, J = j + 1;
+            const T s = quarter * (f_u(i, j) * t);
+            add(yb.v(I, J), s); add(yb.v(I + 1, J), s); add(yb.v(I, J + 1), s); add(yb.v(I + 1, J + 1), s);
+            add(yb.e(i + 2 - ep, j + 1), -(g * t)); add(yb.e(i + 1 - ep, j + 1), g * t);
+        }
+        if (i <= nvx && j <= nvy) {   // dv = -(f_v*Ixy(u) + (g*eta(j+2) - g*eta(j+1))) + ...
+            const T m = gv(i, j);
+            const int I = i + 1 + ep, J = j + 2;
+            const T s = quarter * (f_v(i, j) * m);
+            add(yb.u(I, J), s); add(yb.u(I + 1, J), s); add(yb.u(I, J + 1), s); add(yb.u(I + 1, J + 1), s);
+            add(yb.e(i + 1, j + 2), g * m); add(yb.e(i + 1, j + 1), -(g * m));
+        }
+    });
+}
+
 template <class T>
 void stage_rev(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const State<T>& Xb0, const State<T>* Wb,
                const State<T>& Yb, bool mom_only = false, T coef = T(0)) {
+    if (w.linear) { stage_rev_linear(L, w, k, Xb0, Wb, Yb, mom_only, coef); return; }
     const A2<T> u = Y.u, v = Y.v;
     const A2<T> hu = w.hu, hv = w.hv, hq = w.hq, U = w.U, V = w.V, q = w.q, qa = w.qa, qb = w.qb, qc = w.qc, qd = w.qd;
     const A2<T> bU = w.bU, bV = w.bV, bp = w.bp, bqa = w.bqa, bqb = w.bqb, bqc = w.bqc, bqd = w.bqd, bq = w.bq,
@@ -575,6 +670,8 @@ template <class T>
 void ssp_mom(Launcher& L, const Work<T>& w, const State<T>& Yp, const State<T>& Ym) {
     const A2<T> p = w.p, Fx = w.Fx, Fy = w.Fy;
     const PVterms<T> pv = pvterms(w);
+    const LinTerms<T> lt{w.f_u, w.f_v, w.g, w.ep};
+    const bool linear = w.linear;
     const int nx = w.nx, ny = w.ny, nux = w.nux, nuy = w.nuy, nvx = w.nvx, nvy = w.nvy, ep = w.ep;
     const T c = w.cssp;
     const bool timedep = w.timedep;
@@ -586,9 +683,15 @@ void ssp_mom(Launcher& L, const Work<T>& w, const State<T>& Yp, const State<T>& 
             T d = zero;
             if (I >= 3 && I <= nux + 2 && J >= 3 && J <= nuy + 2) {
                 const int i = I - 2, j = J - 2;
-                const T qhv = pv.qhv(i, j);
-                const T dpdx = p(i + 2 - ep, j + 1) - p(i + 1 - ep, j + 1);
-                d = timedep ? (qhv - dpdx) + force[0] * Fx(i, j) : (qhv - dpdx) + Fx(i, j);
+                T m;
+                if (linear) {
+                    m = lt.du(yp.u, yp.v, yp.e, i, j);
+                } else {
+                    const T qhv = pv.qhv(i, j);
+                    const T dpdx = p(i + 2 - ep, j + 1) - p(i + 1 - ep, j + 1);
+                    m = qhv - dpdx;
+                }
+                d = timedep ? m + force[0] * Fx(i, j) : m + Fx(i, j);
             }
             ym.u(I, J) = yp.u(I, J) + c * d;
         }
@@ -596,8 +699,13 @@ void ssp_mom(Launcher& L, const Work<T>& w, const State<T>& Yp, const State<T>& 
             T d = zero;
             if (I >= 3 && I <= nvx + 2 && J >= 3 && J <= nvy + 2) {
                 const int i = I - 2, j = J - 2;
-                const T qhu = pv.qhu(i, j);
-                const T dpdy = p(i + 1, j + 2) - p(i + 1, j + 1);
+                T qhu, dpdy;
+                if (linear) {
+                    qhu = lt.dv_part(yp.u, yp.e, i, j, dpdy);
+                } else {
+                    qhu = pv.qhu(i, j);
+                    dpdy = p(i + 1, j + 2) - p(i + 1, j + 1);
+                }
                 d = timedep ? -(qhu + dpdy) + force[1] * Fy(i, j) : -(qhu + dpdy) + Fy(i, j);
             }
             ym.v(I, J) = yp.v(I, J) + c * d;
@@ -1097,7 +1205,7 @@ AdjCfgError adjoint_check(const sw_config& c) {
         return {SW_ERR_UNSUPPORTED, "the adjoint computes in T = Tprog = Tcomm, Float32 or Float64"};
     if (!((c.time_scheme == SW_RK && c.RKo >= 2 && c.RKo <= 4) || (c.time_scheme == SW_SSPRK2 && c.RKs >= 2 && c.RKs <= 4)))
         return {SW_ERR_UNSUPPORTED, "the adjoint follows RK2/3/4 and SSPRK2 with 2-4 sub-stages"};
-    if (c.dynamics != SW_NONLINEAR || c.nstep_advcor != 0)
+    if (c.dynamics == SW_NONLINEAR && c.nstep_advcor != 0)
         return {SW_ERR_UNSUPPORTED, "the adjoint follows nonlinear dynamics with nstep_advcor = 0"};
     if (c.nstep_diff < 1) return {SW_ERR_ARG, "nstep_diff"};
     if (c.surface_forcing && c.surface_relax) return {SW_ERR_ARG, "surface relaxation and forcing together"};
@@ -1249,6 +1357,7 @@ struct Adjoint {
         for (int k = 0; k < 3; k++) w.RKb[k] = (T)c.RKbDt[k];
         w.drag = c.bottom_drag; w.diff = c.diffusion;
         w.sadourny = c.adv_scheme == SW_SADOURNY;
+        w.linear = c.dynamics == SW_LINEAR;
         nstep_diff = c.nstep_diff;
         w.relax = c.surface_relax != 0;
         w.gamma = (T)c.gamma;
@@ -1258,16 +1367,16 @@ struct Adjoint {
         {
             Carver cv;   // static fields and the forcing adjoint
             cv.add(w.H, nx + 2, ny + 2); cv.add(w.f_q, nx + 1, ny + 1); cv.add(w.Fx, nux, nuy); cv.add(w.Fy, nvx, nvy);
-            cv.add(w.eta_ref, nx, ny); cv.add(w.Feta, nx, ny);
+            cv.add(w.eta_ref, nx, ny); cv.add(w.Feta, nx, ny); cv.add(w.f_u, nux, nuy); cv.add(w.f_v, nvx, nvy);
             cv.add(w.bFx, nux, nuy);
             A2<T> fv;
             cv.add(fv, 4, 1);
             if (!carve(cv)) return SW_ERR_NOMEM;
             w.force = fv.d;
-            const void* src[6] = {stt.H, stt.f_q, stt.Fx, stt.Fy, stt.eta_ref, stt.Feta};
-            A2<T>* dst[6] = {&w.H, &w.f_q, &w.Fx, &w.Fy, &w.eta_ref, &w.Feta};
-            for (int k = 0; k < 6; k++) {
-                if ((k == 4 && !w.relax) || (k == 5 && !w.forcing)) continue;
+            const void* src[8] = {stt.H, stt.f_q, stt.Fx, stt.Fy, stt.eta_ref, stt.Feta, stt.f_u, stt.f_v};
+            A2<T>* dst[8] = {&w.H, &w.f_q, &w.Fx, &w.Fy, &w.eta_ref, &w.Feta, &w.f_u, &w.f_v};
+            for (int k = 0; k < 8; k++) {
+                if ((k == 4 && !w.relax) || (k == 5 && !w.forcing) || (k >= 6 && !w.linear)) continue;
                 if (!src[k]) return SW_ERR_ARG;
                 if (upload(dst[k]->d, src[k], dst[k]->size() * sizeof(T)) != cudaSuccess) return SW_ERR_CUDA;
             }
