@@ -276,11 +276,11 @@ void sw_batch_destroy(sw_batch* b);
  * cannot take (its number types are restricted to AbstractFloat), so it has no
  * counterpart in the reference; the forward model it differentiates is
  * src/time_integration.jl:45-104,204-233.  Supported: T = Tprog = Tcomm in
- * Float32 or Float64, RK2/3/4 or SSPRK2 (2-4 sub-stages, with its
- * semi-implicit continuity), linear dynamics or nonlinear with Arakawa-Hsu or
- * Sadourny and nstep_advcor =
- * 0, any nstep_diff, any drag and diffusion, either boundary, surface
- * relaxation or forcing, seasonal wind (else SW_ERR_UNSUPPORTED).  The tracer is passive and plays no part.
+ * Float32 or Float64; RK2/3/4 or SSPRK2 (2-4 sub-stages, with its
+ * semi-implicit continuity); linear dynamics, or nonlinear with Arakawa-Hsu
+ * or Sadourny and nstep_advcor = 0; any nstep_diff, drag and diffusion;
+ * either boundary; surface relaxation or forcing; seasonal wind.  Other
+ * options give SW_ERR_UNSUPPORTED.  The tracer is passive and plays no part.
  * Inputs and outputs are HOST buffers in T: u, v, eta the initial state,
  * eta_obs nx x ny; g_u, g_v, g_eta (state shapes), g_Fx and eta_final (the eta
  * after nsteps, with halo) may be NULL.  ncheckpoints >= nsteps keeps every
