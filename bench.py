@@ -214,7 +214,8 @@ def bench_adjoint(args):
     from swb200.adjoint import gradient, twin
     T = {"f64": np.float64, "f32": np.float32}[args.adj_dtype]
     n = args.adj_steps
-    S, Prog, obs, dFx = twin(nx=args.adj_nx, nsteps=n, T=T)
+    scheme = dict(time_scheme="SSPRK2", RKs=3, cfl=1.0) if args.adj_scheme == "ssprk2" else {}
+    S, Prog, obs, dFx = twin(nx=args.adj_nx, nsteps=n, T=T, **scheme)
     nc = args.checkpoints or n
     gradient(S, Prog, obs, 4, ncheckpoints=4)                              # warm-up
     with Model(S) as m:
@@ -231,7 +232,8 @@ def bench_adjoint(args):
     print(json.dumps({
         "metric": "adjoint cost / forward cost", "value": adj_ms / fwd_ms, "unit": "x", "n_gpus": 1,
         "higher_is_better": False, "dtype": args.adj_dtype, "data": "synthetic (seeded twin experiment)",
-        "config": {"workload": f"twin experiment {G.nx}x{G.ny} periodic channel, RK4, Arakawa-Hsu, Smagorinsky, "
+        "config": {"workload": f"twin experiment {G.nx}x{G.ny} periodic channel, "
+                               f"{'SSPRK2 (3 sub-stages)' if args.adj_scheme == 'ssprk2' else 'RK4'}, Arakawa-Hsu, Smagorinsky, "
                                f"quadratic drag, {n} steps, J = sum (eta_T - eta_obs)^2, gradient w.r.t. u0, v0, "
                                f"eta0 and Fx", "checkpoints": st_.checkpoints},
         "forward_ms": fwd_ms, "adjoint_forward_sweep_ms": st_.forward_ms, "adjoint_reverse_sweep_ms": st_.reverse_ms,
@@ -257,6 +259,7 @@ def main():
     ap.add_argument("--adj-steps", type=int, default=2000)
     ap.add_argument("--adj-nx", type=int, default=512)
     ap.add_argument("--adj-dtype", default="f64", choices=["f64", "f32"])
+    ap.add_argument("--adj-scheme", default="rk4", choices=["rk4", "ssprk2"])
     ap.add_argument("--checkpoints", type=int, default=0, help="adjoint checkpoint slots (0: one per step)")
     ap.add_argument("--members", type=int, default=256)
     ap.add_argument("--days", type=float, default=1.0, help="model days per ensemble member")
