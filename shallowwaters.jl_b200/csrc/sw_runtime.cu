@@ -194,7 +194,8 @@ struct sw_ctx {
     struct StepGraph { cudaGraphExec_t exec = nullptr; long long launches = 0; bool flips_sp = false; };
     std::map<unsigned, StepGraph> graphs;
     int nsm = 148;
-    int tail_ty = TAIL_TY;        // rows per warp strip of the streaming tail (see pick_tail_ty)
+    int tail_ty = TAIL_TY;        // rows per warp strip of the streaming tail (see pick_strip_ty)
+    int stage_ty = STAGE_TY;      // rows per warp strip of the streaming stage and SSP momentum kernels
     DevStatus* dst = nullptr;     // device status
     DiagPartial* diag = nullptr;  // DIAG_BLOCKS partials + the result (allocated on first use)
     DevStatus* hst = nullptr;     // pinned host mirror
@@ -225,13 +226,14 @@ cudaEvent_t sw_ctx::evget() {
 
 namespace {
 
-// Strip height of the streaming tail for Float32 / Float64 contexts: the
-// tallest of 32, 16, 8 rows whose strips still give four blocks (the
-// resident limit at the tail's register count) per SM, else 8.
-// SWB200_TAIL_TY=8|16|32 forces one.  Other number types keep 32.
-int pick_tail_ty(const sw_config& c, const Geom& g, int nsm) {
-    if (c.T != c.Tprog || (c.T != SW_FLOAT32 && c.T != SW_FLOAT64)) return TAIL_TY;
-    const char* env = getenv("SWB200_TAIL_TY");
+// Strip height of the streaming tail and stage kernels for Float32 / Float64
+// contexts: the tallest of 32, 16, 8 rows whose strips still give four
+// blocks per SM, else 8 (the values do not depend on it).  The environment
+// variable `env` (SWB200_TAIL_TY, SWB200_STAGE_TY) = 8|16|32 forces one.
+// Other number types keep 32.
+int pick_strip_ty(const sw_config& c, const Geom& g, int nsm, const char* envname) {
+    if (c.T != c.Tprog || (c.T != SW_FLOAT32 && c.T != SW_FLOAT64)) return 32;
+    const char* env = getenv(envname);
     if (env) {
         const int want = atoi(env);
         if (want == 8 || want == 16 || want == 32) return want;
@@ -411,19 +413,26 @@ struct Engine : EngineBase {
         return std::min(RING_BLOCKS_MAX, (n + nt - 1) / nt);
     }
 
+    static constexpr bool SAME_TY = std::is_same<T, Tp>::value &&
+                                    (std::is_same<T, float>::value || std::is_same<T, double>::value);
     template <bool PER, bool FIRST, bool LAST>
-    static void stage_launch(const StageArgs<T, Tp>& a, int nblk, cudaStream_t s) {
+    static void stage_launch(const StageArgs<T, Tp>& a, int nblk, cudaStream_t s, int ty) {
+        if constexpr (SAME_TY) {
+            if (ty == 8) { rk_stage_kernel<T, Tp, PER, FIRST, LAST, 8><<<nblk, 128, 0, s>>>(a); return; }
+            if (ty == 16) { rk_stage_kernel<T, Tp, PER, FIRST, LAST, 16><<<nblk, 128, 0, s>>>(a); return; }
+        }
         rk_stage_kernel<T, Tp, PER, FIRST, LAST, STAGE_TY><<<nblk, 128, 0, s>>>(a);
     }
-    static void stage_dispatch(const StageArgs<T, Tp>& a, bool per, bool first, bool last, int nblk, cudaStream_t s) {
+    static void stage_dispatch(const StageArgs<T, Tp>& a, bool per, bool first, bool last, int nblk, cudaStream_t s,
+                               int ty) {
         if (per) {
-            if (first) stage_launch<true, true, false>(a, nblk, s);
-            else if (last) stage_launch<true, false, true>(a, nblk, s);
-            else stage_launch<true, false, false>(a, nblk, s);
+            if (first) stage_launch<true, true, false>(a, nblk, s, ty);
+            else if (last) stage_launch<true, false, true>(a, nblk, s, ty);
+            else stage_launch<true, false, false>(a, nblk, s, ty);
         } else {
-            if (first) stage_launch<false, true, false>(a, nblk, s);
-            else if (last) stage_launch<false, false, true>(a, nblk, s);
-            else stage_launch<false, false, false>(a, nblk, s);
+            if (first) stage_launch<false, true, false>(a, nblk, s, ty);
+            else if (last) stage_launch<false, false, true>(a, nblk, s, ty);
+            else stage_launch<false, false, false>(a, nblk, s, ty);
         }
     }
     // the TMA stage kernel serves Float32/Float64 compute; Float16 compute runs streaming
@@ -601,6 +610,10 @@ struct Engine : EngineBase {
             return;
         }
         const int nb = (a.nsx * a.nsy + 3) / 4 + a.nring_blocks;
+        if constexpr (SAME_TY) {
+            if (ctx->stage_ty == 8) { ssp_momentum_kernel<T, Tp, PER, MODE, FINAL, 8><<<nb, 128, 0, ctx->stream>>>(a); return; }
+            if (ctx->stage_ty == 16) { ssp_momentum_kernel<T, Tp, PER, MODE, FINAL, 16><<<nb, 128, 0, ctx->stream>>>(a); return; }
+        }
         ssp_momentum_kernel<T, Tp, PER, MODE, FINAL, STAGE_TY><<<nb, 128, 0, ctx->stream>>>(a);
     }
     // the point-wise linear kernels run their ring with 256 threads per block
@@ -667,7 +680,7 @@ struct Engine : EngineBase {
 
         SspArgs<T, Tp> a;
         a.g = g;
-        a.nsx = (g.N + STRIP - 1) / STRIP; a.nsy = (g.M + STAGE_TY - 1) / STAGE_TY;
+        a.nsx = (g.N + STRIP - 1) / STRIP; a.nsy = (g.M + ctx->stage_ty - 1) / ctx->stage_ty;
         a.nring_blocks = ring_blocks(g, 128);
         a.uS = (const Tp*)X.u; a.vS = (const Tp*)X.v; a.eS = (const Tp*)X.e;
         a.ufo = a.vfo = a.efo = nullptr;
@@ -739,7 +752,7 @@ struct Engine : EngineBase {
         const Fields3& Y = ctx->S[1 - p];
         StageArgs<T, Tp> a;
         a.g = g;
-        a.nsx = (g.N + STRIP - 1) / STRIP; a.nsy = (g.M + STAGE_TY - 1) / STAGE_TY;
+        a.nsx = (g.N + STRIP - 1) / STRIP; a.nsy = (g.M + ctx->stage_ty - 1) / ctx->stage_ty;
         a.nring_blocks = ring_blocks(g, 128);
         const Fields3& in = (k == 1) ? X : ((k % 2 == 0) ? ctx->A : ctx->B);
         const Fields3& out1 = (k % 2 == 1) ? ctx->A : ctx->B;
@@ -815,7 +828,7 @@ struct Engine : EngineBase {
         T Fyt = c.seasonal_wind_y ? (T)std::sin(c.omegaFy * (double)ctx->t) : one;
 
         // ------------------------------------------------ RK stages (:55-78)
-        const int nsx = (g.N + STRIP - 1) / STRIP, nsy = (g.M + STAGE_TY - 1) / STAGE_TY;
+        const int nsx = (g.N + STRIP - 1) / STRIP, nsy = (g.M + ctx->stage_ty - 1) / ctx->stage_ty;
         const int nring = ring_blocks(g, 128);
         const int nblk = (nsx * nsy + 3) / 4 + nring;
         if (c.time_scheme != SW_RK) {
@@ -846,7 +859,7 @@ struct Engine : EngineBase {
                 rc = launch(ctx, 0, [&] { lr = stage_tma_dispatch(ctx, a, mp, g.ep != 0, first, last); });
                 if (!rc && lr) rc = fail(ctx, SW_ERR_CUDA, "TMA stage kernel could not be configured");
             } else {
-                rc = launch(ctx, 0, [&] { stage_dispatch(a, g.ep != 0, first, last, nblk, ctx->stream); });
+                rc = launch(ctx, 0, [&] { stage_dispatch(a, g.ep != 0, first, last, nblk, ctx->stream, ctx->stage_ty); });
             }
             if (rc) return rc;
         }
@@ -1817,7 +1830,8 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
         ctx->tail_tma = (envt && envt[0] == '1');
         const char* envg = getenv("SWB200_GRAPHS");
         ctx->use_graphs = !(envg && envg[0] == '0');
-        ctx->tail_ty = pick_tail_ty(*cfg, g, ctx->nsm);
+        ctx->tail_ty = pick_strip_ty(*cfg, g, ctx->nsm, "SWB200_TAIL_TY");
+        ctx->stage_ty = pick_strip_ty(*cfg, g, ctx->nsm, "SWB200_STAGE_TY");
     }
     if (cfg->T == SW_FLOAT32 && cfg->Tprog == SW_FLOAT32) {
         auto* e = new Engine<float, float>(); ctx->eng.reset(e); if ((rc = e->init(ctx))) return rc;

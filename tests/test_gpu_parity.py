@@ -203,6 +203,18 @@ def test_every_tail_strip_height_is_bit_exact(rows, kw, monkeypatch):
     both(k, 0, checkpoints=[1, 5])
 
 
+@pytest.mark.parametrize("rows", ["8", "16", "32"])
+@pytest.mark.parametrize("kw", [dict(adv_scheme="Sadourny", diffusion="Smagorinsky"),
+                                dict(time_scheme="SSPRK2", RKs=3, cfl=1.0, bc="nonperiodic", α=0.5, T=np.float64)])
+def test_every_stage_strip_height_is_bit_exact(rows, kw, monkeypatch):
+    """The streaming stage and SSP momentum kernels' strip height (chosen by
+    grid size, forced here with SWB200_STAGE_TY) does not change a bit."""
+    monkeypatch.setenv("SWB200_STAGE_TY", rows)
+    k = dict(BASE)
+    k.update(kw)
+    both(k, 0, checkpoints=[1, 5])
+
+
 def test_graph_replay_equals_direct_launches(monkeypatch):
     """Steps replayed from CUDA graphs equal steps launched one kernel at a
     time, over enough steps to use every graph key (parities, tracer and
