@@ -276,8 +276,8 @@ void sw_batch_destroy(sw_batch* b);
  * cannot take (its number types are restricted to AbstractFloat), so it has no
  * counterpart in the reference; the forward model it differentiates is
  * src/time_integration.jl:45-104,204-233.  Supported: T = Tprog = Tcomm in
- * Float32 or Float64; RK2/3/4 or SSPRK2 (2-4 sub-stages, with its
- * semi-implicit continuity); linear dynamics, or nonlinear with Arakawa-Hsu
+ * Float32 or Float64; RK2/3/4, SSPRK2 (2-4 sub-stages) or 4SSPRK3 (the SSP
+ * schemes with their semi-implicit continuity); linear dynamics, or nonlinear with Arakawa-Hsu
  * or Sadourny and nstep_advcor = 0; any nstep_diff, drag and diffusion;
  * either boundary; surface relaxation or forcing; seasonal wind.  Other
  * options give SW_ERR_UNSUPPORTED.  The tracer is passive and plays no part.

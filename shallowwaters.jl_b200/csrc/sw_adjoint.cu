@@ -170,7 +170,8 @@ struct State {
 template <class T>
 struct Work {
     int nx, ny, nux, nuy, nvx, nvy, ep, rko;
-    bool ssp = false;           // SSPRK2 (src/time_integration.jl:80-104) instead of RK
+    bool ssp = false;           // SSPRK2 (src/time_integration.jl:80-104) or 4SSPRK3 (:150-196) instead of RK
+    bool four = false;          // 4SSPRK3: averaged updates, full ghost points, the third sub-stage's mix
     int rks = 0, nst = 0;       // SSPRK2 sub-stages; stage states kept per step
     T cssp, ssp_a, ssp_b;       // Δt_Δs, 1/RKs, (RKs-1)/RKs (Tprog)
     T g, cD, rD, cSmag, nuB, Dt_diff, oma;   // oma = 1 - alpha (Tprog = T)
@@ -671,7 +672,7 @@ void ssp_mom(Launcher& L, const Work<T>& w, const State<T>& Yp, const State<T>& 
     const A2<T> p = w.p, Fx = w.Fx, Fy = w.Fy;
     const PVterms<T> pv = pvterms(w);
     const LinTerms<T> lt{w.f_u, w.f_v, w.g, w.ep};
-    const bool linear = w.linear;
+    const bool linear = w.linear, four = w.four;
     const int nx = w.nx, ny = w.ny, nux = w.nux, nuy = w.nuy, nvx = w.nvx, nvy = w.nvy, ep = w.ep;
     const T c = w.cssp;
     const bool timedep = w.timedep;
@@ -693,7 +694,12 @@ void ssp_mom(Launcher& L, const Work<T>& w, const State<T>& Yp, const State<T>& 
                 }
                 d = timedep ? m + force[0] * Fx(i, j) : m + Fx(i, j);
             }
-            ym.u(I, J) = yp.u(I, J) + c * d;
+            if (four) {   // u0 = u1 + Δt_Δ*du; u1 = 0.5*(u1 + u0) (caxb!, cxab!)
+                const T t = yp.u(I, J) + c * d;
+                ym.u(I, J) = T(0.5) * (yp.u(I, J) + t);
+            } else {
+                ym.u(I, J) = yp.u(I, J) + c * d;
+            }
         }
         if (I <= yp.v.m && J <= yp.v.n) {
             T d = zero;
@@ -708,7 +714,12 @@ void ssp_mom(Launcher& L, const Work<T>& w, const State<T>& Yp, const State<T>& 
                 }
                 d = timedep ? -(qhu + dpdy) + force[1] * Fy(i, j) : -(qhu + dpdy) + Fy(i, j);
             }
-            ym.v(I, J) = yp.v(I, J) + c * d;
+            if (four) {
+                const T t = yp.v(I, J) + c * d;
+                ym.v(I, J) = T(0.5) * (yp.v(I, J) + t);
+            } else {
+                ym.v(I, J) = yp.v(I, J) + c * d;
+            }
         }
         if (I <= yp.e.m && J <= yp.e.n) ym.e(I, J) = yp.e(I, J);
     });
@@ -724,7 +735,7 @@ void ssp_cont(Launcher& L, const Work<T>& w, const State<T>& Ym, const State<T>&
     const T c = w.cssp;
     const State<T> ym = Ym, yn = Yn;
     const A2<T> eta_ref = w.eta_ref, Feta = w.Feta;
-    const bool relax = w.relax, forcing = w.forcing;
+    const bool relax = w.relax, forcing = w.forcing, four = w.four;
     const T gamma = w.gamma;
     const T* force = w.force;
     L.d2(nx + 4, ny + 4, [=] __host__ __device__(int I, int J) {
@@ -742,7 +753,12 @@ void ssp_cont(Launcher& L, const Work<T>& w, const State<T>& Ym, const State<T>&
                 if (relax) d = d + gamma * (eta_ref(i, j) - ym.e(i + 1, j + 1));
                 else if (forcing) d = d + force[2] * Feta(i, j);
             }
-            yn.e(I, J) = ym.e(I, J) + c * d;
+            if (four) {   // eta0 = eta1 + Δt_Δ*deta; eta1 = 0.5*(eta1 + eta0)
+                const T t = ym.e(I, J) + c * d;
+                yn.e(I, J) = T(0.5) * (ym.e(I, J) + t);
+            } else {
+                yn.e(I, J) = ym.e(I, J) + c * d;
+            }
         }
     });
 }
@@ -751,12 +767,12 @@ void ssp_cont(Launcher& L, const Work<T>& w, const State<T>& Ym, const State<T>&
 // adjoint of Ym).  Two passes: the flux adjoints in gather form (they read
 // Yb's eta), then their scatter onto u, v and, through h_u, h_v, eta.
 template <class T>
-void ssp_cont_rev(Launcher& L, const Work<T>& w, const State<T>& Ym, const State<T>& Yb) {
+void ssp_cont_rev(Launcher& L, const Work<T>& w, const State<T>& Ym, const State<T>& Yb, T coef) {
     const A2<T> hu = w.hu, hv = w.hv, bU = w.bU, bV = w.bV, bp = w.bp;
     const bool relax = w.relax;
     const T gamma = w.gamma;
     const int nx = w.nx, ny = w.ny, ep = w.ep;
-    const T c = w.cssp;
+    const T c = coef;   // d(new eta)/d(deta): Δt_Δs (SSPRK2) or Δt_Δ/2 (4SSPRK3)
     const State<T> ym = Ym, yb = Yb;
     L.d2(nx + 2, ny + 2, [=] __host__ __device__(int I, int J) {
         auto g = [&](int i, int j) {   // deta adjoint at T-point (i, j), zero off the interior
@@ -1102,13 +1118,15 @@ void fwd_step_ssp(Launcher& L, const Work<T>& w, bool tail) {
     copy_state(L, w.Ys[1], w.Ys[0]);
     for (int k = 1; k <= w.rks; k++) {
         const State<T>&yp = w.Ys[2 * k - 1], &ym = w.Ys[2 * k], &yn = w.Ys[2 * k + 1];
-        if (k > 1) ghost(L, w, yp, GH_ETA);
+        if (k > 1) ghost(L, w, yp, w.four ? GH_ALL : GH_ETA);
         stage_fwd(L, w, yp);
         ssp_mom(L, w, yp, ym);
         ghost(L, w, ym, GH_UV);
         ssp_cont(L, w, ym, yn);
+        if (w.four && k == 3) combine(L, yn, w.ssp_a, w.Ys[0], w.ssp_b, yn);   // 2/3 X + 1/3 X1 (cxayb!)
     }
-    combine(L, w.Z, w.ssp_a, w.Ys[0], w.ssp_b, w.Ys[2 * w.rks + 1]);
+    if (w.four) copy_state(L, w.Z, w.Ys[2 * w.rks + 1]);
+    else combine(L, w.Z, w.ssp_a, w.Ys[0], w.ssp_b, w.Ys[2 * w.rks + 1]);
     step_end(L, w, tail);
 }
 
@@ -1122,15 +1140,26 @@ void adj_step_ssp(Launcher& L, const Work<T>& w, bool stored, bool tail) {
     }
     ghostT(L, w, w.Xb, GH_ALL);    // Xb: adjoint of X0 = a*Ys[0] + b*Ys[2 RKs + 1]
     const State<T>& Yb = w.Yb[0];
-    combine(L, w.acc, w.ssp_a, w.Xb, T(0), w.Xb);
-    combine(L, Yb, w.ssp_b, w.Xb, T(0), w.Xb);
+    if (w.four) {   // X0 is the last sub-stage's result
+        copy_state(L, Yb, w.Xb);
+        L.zero(w.acc.base, w.acc.elems * sizeof(T));
+    } else {        // X0 = a*Ys[0] + b*Ys[2 RKs + 1]
+        combine(L, w.acc, w.ssp_a, w.Xb, T(0), w.Xb);
+        combine(L, Yb, w.ssp_b, w.Xb, T(0), w.Xb);
+    }
+    // d(new state)/d(tendency): Δt_Δs, or Δt_Δ/2 for the averaged 4SSPRK3 update
+    const T coef = w.four ? T(0.5) * w.cssp : w.cssp;
     for (int k = w.rks; k >= 1; k--) {
         const State<T>&yp = w.Ys[2 * k - 1], &ym = w.Ys[2 * k];
+        if (w.four && k == 3) {   // Yn = 2/3 X + 1/3 Yn
+            combine(L, w.acc, T(1), w.acc, w.ssp_a, Yb);
+            combine(L, Yb, w.ssp_b, Yb, T(0), Yb);
+        }
         stage_fwd(L, w, yp);                              // h_u, h_v and the rhs intermediates of sub-stage k
-        ssp_cont_rev(L, w, ym, Yb);                       // Yb: adjoint of Ym
+        ssp_cont_rev(L, w, ym, Yb, coef);                 // Yb: adjoint of Ym
         ghostT(L, w, Yb, GH_UV);
-        stage_rev(L, w, 1, yp, Yb, (const State<T>*)nullptr, Yb, true, w.cssp);   // adjoint of Yp
-        if (k > 1) ghostT(L, w, Yb, GH_ETA);
+        stage_rev(L, w, 1, yp, Yb, (const State<T>*)nullptr, Yb, true, coef);   // adjoint of Yp
+        if (k > 1) ghostT(L, w, Yb, w.four ? GH_ALL : GH_ETA);
     }
     const T* src = Yb.base;
     T* dst = w.acc.base;
@@ -1203,8 +1232,9 @@ AdjCfgError adjoint_check(const sw_config& c) {
     if (c.nx < 8 || c.ny < 8) return {SW_ERR_ARG, "grid smaller than 8 x 8"};
     if (c.T != c.Tprog || (c.T != SW_FLOAT32 && c.T != SW_FLOAT64) || c.Tcomm != c.T)
         return {SW_ERR_UNSUPPORTED, "the adjoint computes in T = Tprog = Tcomm, Float32 or Float64"};
-    if (!((c.time_scheme == SW_RK && c.RKo >= 2 && c.RKo <= 4) || (c.time_scheme == SW_SSPRK2 && c.RKs >= 2 && c.RKs <= 4)))
-        return {SW_ERR_UNSUPPORTED, "the adjoint follows RK2/3/4 and SSPRK2 with 2-4 sub-stages"};
+    if (!((c.time_scheme == SW_RK && c.RKo >= 2 && c.RKo <= 4) || (c.time_scheme == SW_SSPRK2 && c.RKs >= 2 && c.RKs <= 4) ||
+          c.time_scheme == SW_4SSPRK3))
+        return {SW_ERR_UNSUPPORTED, "the adjoint follows RK2/3/4, SSPRK2 with 2-4 sub-stages and 4SSPRK3"};
     if (c.dynamics == SW_NONLINEAR && c.nstep_advcor != 0)
         return {SW_ERR_UNSUPPORTED, "the adjoint follows nonlinear dynamics with nstep_advcor = 0"};
     if (c.nstep_diff < 1) return {SW_ERR_ARG, "nstep_diff"};
@@ -1345,11 +1375,12 @@ struct Adjoint {
         w.nx = c.nx; w.ny = c.ny; w.ep = c.periodic ? 1 : 0;
         w.nux = w.ep ? c.nx : c.nx - 1; w.nuy = c.ny; w.nvx = c.nx; w.nvy = c.ny - 1;
         w.rko = c.RKo;
-        w.ssp = c.time_scheme == SW_SSPRK2;
-        w.rks = c.RKs;
-        w.cssp = (T)c.Dt_Ds;
-        w.ssp_a = (T)(1.0 / c.RKs);
-        w.ssp_b = (T)((double)(c.RKs - 1) / c.RKs);
+        w.four = c.time_scheme == SW_4SSPRK3;
+        w.ssp = c.time_scheme == SW_SSPRK2 || w.four;
+        w.rks = w.four ? 4 : c.RKs;
+        w.cssp = (T)(w.four ? c.Dt_D : c.Dt_Ds);
+        w.ssp_a = (T)(w.four ? 2.0 / 3.0 : 1.0 / c.RKs);
+        w.ssp_b = (T)(w.four ? 1.0 / 3.0 : (double)(c.RKs - 1) / c.RKs);
         w.nst = w.ssp ? 2 * w.rks + 2 : w.rko;
         w.g = (T)c.g; w.cD = (T)c.cD; w.rD = (T)c.rD; w.cSmag = (T)c.cSmag; w.nuB = (T)c.nuB;
         w.Dt_diff = (T)c.Dt_diff; w.oma = (T)c.one_minus_alpha;

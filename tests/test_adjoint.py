@@ -42,7 +42,9 @@ OPTIONS = [dict(), dict(bc="nonperiodic", α=0.5), dict(diffusion="constant"),
            dict(seasonal_wind_x=True, ωFx=40.0), dict(surface_forcing=True, ωFη=40.0, seasonal_wind_y=True, ωFy=30.0,
                                                      time_scheme="SSPRK2", RKs=3, cfl=1.0),
            dict(dynamics="linear", surface_relax=True), dict(dynamics="linear", time_scheme="SSPRK2", RKs=3, cfl=1.0,
-                                                             bc="nonperiodic", α=0.5)]
+                                                             bc="nonperiodic", α=0.5),
+           dict(time_scheme="4SSPRK3", cfl=1.0), dict(time_scheme="4SSPRK3", cfl=1.0, bc="nonperiodic", α=0.5,
+                                                      adv_scheme="Sadourny")]
 
 
 def setup(T=np.float64, seed=3, **kw):
@@ -96,7 +98,7 @@ def test_adjoint_entry_rejects_bad_arguments_and_unbuilt_options():
     with pytest.raises(abi.SwError) as e:
         grad(S, Prog, obs, 0)
     assert e.value.code == abi.SW_ERR_ARG
-    for kw in (dict(time_scheme="SSPRK3"), dict(time_scheme="4SSPRK3"), dict(nstep_advcor=2),
+    for kw in (dict(time_scheme="SSPRK3"), dict(nstep_advcor=2),
                dict(T=np.float32, Tprog=np.float64)):
         S2, P2, o2, _ = setup(**kw)
         with pytest.raises(abi.SwError) as e:
