@@ -83,6 +83,12 @@ class ClockSampler:
             if len(f) >= 9 and (self.uuid is None or f[0] == self.uuid):
                 self.rows.append(f)
 
+    def wait_first(self, timeout):
+        """Wait (up to timeout seconds) for the first sample."""
+        t0 = time.time()
+        while self.proc and not self.rows and time.time() - t0 < timeout:
+            time.sleep(0.02)
+
     def stop(self):
         if self.proc:
             self.proc.terminate()
@@ -214,7 +220,8 @@ def bench_adjoint(args):
     from swb200.adjoint import gradient, twin
     T = {"f64": np.float64, "f32": np.float32}[args.adj_dtype]
     n = args.adj_steps
-    scheme = dict(time_scheme="SSPRK2", RKs=3, cfl=1.0) if args.adj_scheme == "ssprk2" else {}
+    scheme = {"rk4": {}, "ssprk2": dict(time_scheme="SSPRK2", RKs=3, cfl=1.0),
+              "4ssprk3": dict(time_scheme="4SSPRK3", cfl=1.0)}[args.adj_scheme]
     S, Prog, obs, dFx = twin(nx=args.adj_nx, nsteps=n, T=T, **scheme)
     nc = args.checkpoints or n
     gradient(S, Prog, obs, 4, ncheckpoints=4)                              # warm-up
@@ -233,7 +240,8 @@ def bench_adjoint(args):
         "metric": "adjoint cost / forward cost", "value": adj_ms / fwd_ms, "unit": "x", "n_gpus": 1,
         "higher_is_better": False, "dtype": args.adj_dtype, "data": "synthetic (seeded twin experiment)",
         "config": {"workload": f"twin experiment {G.nx}x{G.ny} periodic channel, "
-                               f"{'SSPRK2 (3 sub-stages)' if args.adj_scheme == 'ssprk2' else 'RK4'}, Arakawa-Hsu, Smagorinsky, "
+                               f"{ {'rk4': 'RK4', 'ssprk2': 'SSPRK2 (3 sub-stages)', '4ssprk3': '4SSPRK3'}[args.adj_scheme] }, "
+                               f"Arakawa-Hsu, Smagorinsky, "
                                f"quadratic drag, {n} steps, J = sum (eta_T - eta_obs)^2, gradient w.r.t. u0, v0, "
                                f"eta0 and Fx", "checkpoints": st_.checkpoints},
         "forward_ms": fwd_ms, "adjoint_forward_sweep_ms": st_.forward_ms, "adjoint_reverse_sweep_ms": st_.reverse_ms,
@@ -259,12 +267,15 @@ def main():
     ap.add_argument("--adj-steps", type=int, default=2000)
     ap.add_argument("--adj-nx", type=int, default=512)
     ap.add_argument("--adj-dtype", default="f64", choices=["f64", "f32"])
-    ap.add_argument("--adj-scheme", default="rk4", choices=["rk4", "ssprk2"])
+    ap.add_argument("--adj-scheme", default="rk4", choices=["rk4", "ssprk2", "4ssprk3"])
     ap.add_argument("--checkpoints", type=int, default=0, help="adjoint checkpoint slots (0: one per step)")
     ap.add_argument("--members", type=int, default=256)
     ap.add_argument("--days", type=float, default=1.0, help="model days per ensemble member")
     ap.add_argument("--threads", type=int, default=8, help="members run at once per GPU")
     ap.add_argument("--chunks", type=int, default=2, help="ensemble batches per GPU, pipelined with their set-up")
+    ap.add_argument("--build", default="parity", choices=["parity", "fast"],
+                    help="parity: libswb200.so (no FMA contraction, bit-exact with the oracle); "
+                         "fast: libswb200_fast.so (FMA contraction, equal to the oracle to rounding)")
     ap.add_argument("--form", default="fp32", choices=["fp32", "bf16", "f16"],
                     help="state storage between steps: plain FP32 or compensated 16-bit pairs (u, v scaled by 2^10)")
     args = ap.parse_args()
@@ -282,7 +293,7 @@ def main():
     cells = G.nx * G.ny
     config = {"workload": f"periodic wind-driven channel {G.nx}x{G.ny}, RK4, Arakawa-Hsu, Smagorinsky, "
                           f"quadratic drag, tracer every step",
-              "nx": G.nx, "ny": G.ny, "dtint_s": G.dtint, "form": args.form,
+              "nx": G.nx, "ny": G.ny, "dtint_s": G.dtint, "form": args.form, "build": args.build,
               "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{args.gpus}",
               "step_launch": "one CUDA graph per time step"}
     base = {"metric": METRIC, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -341,18 +352,20 @@ def main():
 
     Prog = make_state(S, rng)
     storage = {"fp32": "native", "bf16": "bf16", "f16": "f16"}[args.form]
-    m = Model(S, storage=storage)
+    # clocks are sampled from before the warm-up to after the end-to-end calls,
+    # so that the record covers the timed steps whatever their length
+    clk = ClockSampler(dev_uuid)
+    clk.start()
+    clk.wait_first(10.0)
+    m = Model(S, storage=storage, build=args.build)
     m.set_state(Prog)
     m.run(args.warmup)
 
-    clk = ClockSampler(dev_uuid)
     barrier()
-    clk.start()
     n0 = m.kernel_launches
     step_ms, st = m.run_timed(args.steps, L2_FLUSH)
     launches = m.kernel_launches - n0
     barrier()
-    clk.stop()
     if st.code != 0:
         raise SystemExit(f"run failed with code {st.code}")
     t_dev = allmax(step_ms) / 1e3
@@ -379,7 +392,7 @@ def main():
     for dst, src in zip(pinned, Prog):
         dst[...] = src
     import ctypes as C
-    lib = abi.load_library()
+    lib = abi.load_library(build=args.build)
     cfg = abi.make_config(S, nt=args.steps, storage=storage)
     static = abi.StaticFields(S)
     status = abi.SwStatus()
@@ -400,6 +413,7 @@ def main():
     # median of three timed calls of K steps
     e2e_call(abi.make_config(S, nt=max(args.warmup, 1), storage=storage))
     t_e2e = allmax(statistics.median(e2e_call(cfg) for _ in range(3)))
+    clk.stop()
     state_bytes = sum(a.nbytes for a in pinned)
     static_bytes = sum(a.nbytes for a in static.arrays.values())
     e2e = {"value": args.gpus * cells * args.steps / t_e2e, "unit": UNIT,
@@ -422,7 +436,7 @@ def main():
             "e2e": e2e,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": ncu_traffic(cells),
-                         "kernel": "rk_stage_kernel", "bytes_per_cell": STAGE_BYTES_PER_CELL,
+                         "kernel": "rk_stage_tma", "bytes_per_cell": STAGE_BYTES_PER_CELL,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                          else "fallback 6.65 TB/s"},
             "step_roofline": {"bytes_per_cell_step": STEP_BYTES_PER_CELL,

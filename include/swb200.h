@@ -207,8 +207,10 @@ int sw_diagnostics(sw_ctx* ctx, sw_diag* out);
  * H in T); only cfg->nx, ny, periodic, T, Tprog and g are read.  Reduction
  * scratch is a fixed array inside the library, so it allocates nothing and
  * accepts at most 16,777,216 cells (nx*ny), returning SW_ERR_ARG beyond that.
- * The first call on a device looks up that array (make it before any stream
- * capture); calls whose kernels overlap on one device share the array and
+ * The first call on a device, and the first after the device's CUDA context
+ * was created again (cudaDeviceReset), looks up that array (make it before any
+ * stream capture); a CUDA error already pending at entry is returned as
+ * SW_ERR_CUDA and left pending; calls whose kernels overlap on one device share the array and
  * race.  Runs on `stream` (a cudaStream_t, NULL for the default stream) and
  * returns after the result has reached *out. */
 int sw_diagnostics_noalloc(const sw_config* cfg, const void* u, const void* v,
@@ -307,6 +309,14 @@ int sw_adjoint_run(const sw_config* cfg, const sw_static* st,
                    int64_t nsteps, int32_t ncheckpoints, double* J,
                    void* g_u, void* g_v, void* g_eta, void* g_Fx, void* eta_final,
                    sw_adjoint_stats* stats);
+
+/* Which build of the library this is.  SW_BUILD_PARITY (libswb200.so) is
+ * compiled without FMA contraction and reproduces the reference's Float32 and
+ * Float64 arithmetic bit for bit; SW_BUILD_FAST (libswb200_fast.so) contracts
+ * a*b+c into fused multiply-adds and agrees with the reference to rounding.
+ * No reference counterpart (the reference has one build). */
+enum sw_build { SW_BUILD_PARITY = 0, SW_BUILD_FAST = 1 };
+int sw_build_kind(void);
 
 const char* sw_strerror(int code);
 const char* sw_last_error(const sw_ctx* ctx);

@@ -1621,13 +1621,37 @@ int adjoint_run(bool host, const sw_config& c, const sw_static& st, const void* 
     // ncheckpoints is an upper bound: when that many state slots do not fit in
     // device memory, half as many are tried (down to one), and the binomial
     // schedule recomputes what the missing slots would have kept
+    // the J row sums are allocated before the checkpoint slots, which take the
+    // largest block that fits and would otherwise leave no room for them
+    double* rowsum = host ? static_cast<double*>(std::calloc(w.ny, sizeof(double))) : nullptr;
+    if (!host && cudaMalloc(&rowsum, w.ny * sizeof(double)) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return SW_ERR_NOMEM;
+    }
+    auto free_rowsum = [&] {
+        if (host) std::free(rowsum);
+        else if (rowsum) cudaFree(rowsum);
+        rowsum = nullptr;
+    };
     int nslots = A.stored ? 1 : (int)std::max<long long>(1, std::min<long long>(ncheckpoints, nsteps));
-    if (!A.make_slots(nslots)) return SW_ERR_NOMEM;
+    if (!A.make_slots(nslots)) {
+        free_rowsum();
+        return SW_ERR_NOMEM;
+    }
     nslots = (int)A.slots.size();
     cudaEvent_t ev[3] = {};
+    auto destroy_events = [&] {
+        for (auto& x : ev)
+            if (x) cudaEventDestroy(x);
+    };
     if (!host)
         for (auto& x : ev)
-            if (cudaEventCreate(&x) != cudaSuccess) return SW_ERR_CUDA;
+            if (cudaEventCreate(&x) != cudaSuccess) {
+                x = nullptr;
+                destroy_events();
+                free_rowsum();
+                return SW_ERR_CUDA;
+            }
     auto record = [&](int k) { if (!host) cudaEventRecord(ev[k], A.s); };
     cudaError_t e = A.upload(A.slots[0].u.d, u, bytes_u);
     if (e == cudaSuccess) e = A.upload(A.slots[0].v.d, v, bytes_v);
@@ -1650,9 +1674,7 @@ int adjoint_run(bool host, const sw_config& c, const sw_static& st, const void* 
     }
     record(1);
     // J (FP64 row sums, added on the host in a fixed order) and the seed Xb = dJ/d(state at nsteps)
-    double* rowsum = host ? static_cast<double*>(std::calloc(w.ny, sizeof(double))) : nullptr;
     std::vector<double> rows(w.ny);
-    if (e == cudaSuccess && !host) e = cudaMalloc(&rowsum, w.ny * sizeof(double));
     if (e == cudaSuccess) e = A.zero(w.Xb.base, w.Xb.elems * sizeof(T));
     if (e == cudaSuccess) {
         Launcher L = A.launcher();
@@ -1678,14 +1700,13 @@ int adjoint_run(bool host, const sw_config& c, const sw_static& st, const void* 
     if (e == cudaSuccess && g_eta) e = A.download(g_eta, w.Xb.e.d, bytes_e);
     if (e == cudaSuccess && g_Fx) e = A.download(g_Fx, w.bFx.d, w.bFx.size() * sizeof(T));
     if (e == cudaSuccess && !host) e = cudaStreamSynchronize(A.s);
-    if (host) std::free(rowsum); else if (rowsum) cudaFree(rowsum);
+    free_rowsum();
     float ms_f = 0.f, ms_r = 0.f;
     if (!host && e == cudaSuccess) {
         cudaEventElapsedTime(&ms_f, ev[0], ev[1]);
         cudaEventElapsedTime(&ms_r, ev[1], ev[2]);
     }
-    for (auto& x : ev)
-        if (x) cudaEventDestroy(x);
+    destroy_events();
     if (e != cudaSuccess) {
         fprintf(stderr, "swb200: adjoint: %s\n", cudaGetErrorString(e));
         return SW_ERR_CUDA;

@@ -15,6 +15,7 @@
 // [0, N-1], b in [0, M-1].  Buffers are zero-initialised; padding is never
 // written.
 #pragma once
+#include <cuda.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -106,6 +107,32 @@ __device__ inline T via_comm(int Tcomm, T x) {
     if (Tcomm == SW_FLOAT16) return cvt<T>(__half2float(__double2half((double)cvt<double>(x))));
     if (Tcomm == SW_FLOAT32) return cvt<T>((float)cvt<double>(x));
     return x;
+}
+
+// Identifier of the calling thread's current CUDA context (cuCtxGetId), or 0
+// if there is none or it cannot be read.  Host-side caches of device
+// addresses are keyed by it, so a context that is destroyed and created again
+// (cudaDeviceReset, or the primary context released and retained) never
+// receives addresses that belonged to the old one.
+inline unsigned long long current_context_id() {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static const GetCurrent get_current = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        return (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+                q == cudaDriverEntryPointSuccess) ? reinterpret_cast<GetCurrent>(p) : (GetCurrent) nullptr;
+    }();
+    static const GetId get_id = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        return (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+                q == cudaDriverEntryPointSuccess) ? reinterpret_cast<GetId>(p) : (GetId) nullptr;
+    }();
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+    return id;
 }
 
 // Device status shared by all kernels of a context.

@@ -27,7 +27,10 @@
 // The first call on a device looks up the array's device address with
 // cudaGetSymbolAddress (with that device current), which also loads the
 // library's device code there if nothing has yet; make that first call before
-// any stream capture.  Nothing else is allocated: no cudaMalloc, no cudaFree,
+// any stream capture.  The address is remembered per device and per CUDA
+// context, so after cudaDeviceReset the next call looks it up again.  A CUDA
+// error that is already pending when the call starts (from the caller's own
+// work) is reported as such, returned as SW_ERR_CUDA and left pending.  Nothing else is allocated: no cudaMalloc, no cudaFree,
 // no pinned buffers (the 32-byte result is copied into the caller's sw_diag
 // through an ordinary stream copy).
 #include <cuda_runtime.h>
@@ -35,6 +38,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <mutex>
+#include <vector>
 
 #include "swb200.h"
 #include "sw_common.cuh"
@@ -59,9 +63,16 @@ constexpr int NOALLOC_MAX_DEVICES = 64;
 // the scratch: partials [0, NOALLOC_MAX_PARTIALS) and the result slot after them
 static __device__ __align__(256) NaPartial g_noalloc_scratch[NOALLOC_MAX_PARTIALS + 1];
 
-// device address of g_noalloc_scratch per device (host code may not use the
-// array's name as an address: that is a host-side stand-in)
-NaPartial* g_scratch_addr[NOALLOC_MAX_DEVICES] = {};
+// device address of g_noalloc_scratch per device and CUDA context (host code
+// may not use the array's name as an address: that is a host-side stand-in).
+// A context destroyed and created again (cudaDeviceReset) may load the
+// module at another address, so the lookup is keyed by the context's id.
+struct ScratchAddr {
+    int device;
+    unsigned long long context;
+    NaPartial* addr;
+};
+std::vector<ScratchAddr> g_scratch_addr;
 std::mutex g_scratch_mu;
 
 // Index of a point in the host-ABI arrays (x fastest, with halo; the shapes
@@ -202,6 +213,14 @@ extern "C" int sw_diagnostics_noalloc(const sw_config* cfg, const void* u, const
         (void)cudaGetLastError();
         return SW_ERR_NODEVICE;
     }
+    // an error left by the caller's own earlier work is reported as such and
+    // left pending for the caller, not taken for one of this call's launches
+    const cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess) {
+        fprintf(stderr, "swb200: sw_diagnostics_noalloc: a CUDA error was pending before the call: %s\n",
+                cudaGetErrorString(pending));
+        return SW_ERR_CUDA;
+    }
     if (cudaGetDevice(&dev) != cudaSuccess) return SW_ERR_CUDA;
     if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return reject("device index beyond the supported range");
 
@@ -210,19 +229,22 @@ extern "C" int sw_diagnostics_noalloc(const sw_config* cfg, const void* u, const
         !device_ptr_ok(sst, tp, dev) || !device_ptr_ok(H, ts, dev))
         return reject("u, v, eta, sst and H must be aligned device memory of the current device");
 
-    NaPartial* scratch;
+    NaPartial* scratch = nullptr;
     {
+        const unsigned long long cid = current_context_id();
         std::lock_guard<std::mutex> lock(g_scratch_mu);
-        if (!g_scratch_addr[dev]) {
+        for (const ScratchAddr& a : g_scratch_addr)
+            if (cid && a.device == dev && a.context == cid) scratch = a.addr;
+        if (!scratch) {
             void* p = nullptr;
             const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
             if (e != cudaSuccess || !p) {
                 fprintf(stderr, "swb200: sw_diagnostics_noalloc: cudaGetSymbolAddress: %s\n", cudaGetErrorString(e));
                 return SW_ERR_CUDA;
             }
-            g_scratch_addr[dev] = static_cast<NaPartial*>(p);
+            scratch = static_cast<NaPartial*>(p);
+            if (cid) g_scratch_addr.push_back({dev, cid, scratch});
         }
-        scratch = g_scratch_addr[dev];
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (f32) return run<float, float>(cfg, u, v, eta, sst, H, s, scratch, out);

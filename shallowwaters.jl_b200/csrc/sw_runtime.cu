@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <map>
 #include <cmath>
 #include <cstdio>
@@ -25,13 +26,13 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "swb200.h"
 #include "sw_common.cuh"
 #include "sw_ghost.cuh"
 #include "sw_stage.cuh"
-#include "sw_stage2.cuh"
 #include "sw_ssp.cuh"
 #include "sw_linear.cuh"
 #include "sw_advcor.cuh"
@@ -53,13 +54,6 @@ namespace {
 #endif
 constexpr int STAGE_TY = SWB_STAGE_TY;  // rows per warp strip of the stage kernel
 constexpr int TAIL_TY = SWB_TAIL_TY;
-#ifndef SWB_TAIL_TMA_TY
-#define SWB_TAIL_TMA_TY 24
-#endif
-#ifndef SWB_TAIL_TMA_S
-#define SWB_TAIL_TMA_S 4
-#endif
-constexpr int TAIL_TMA_TY = SWB_TAIL_TMA_TY, TAIL_TMA_S = SWB_TAIL_TMA_S;    // rows per warp strip of the tail kernel
 constexpr int PADX = 72, PADY = 44;     // column/row padding: strips read up to TY+3 rows and 30 columns past the edge
 constexpr int RING_BLOCKS_MAX = 32;
 
@@ -88,11 +82,23 @@ struct Fields3 { void* u = nullptr; void* v = nullptr; void* e = nullptr; };
 // contexts of the same sizes: a drop-in call (create, run, destroy) then costs
 // no cudaMalloc/cudaFree after the first, which are slow and, for cudaFree,
 // erratic (milliseconds to a second).  At most CACHE_LIMIT bytes of device
-// memory are held; sw_trim_memory returns them all.
+// memory are held; sw_trim_memory returns them all.  Device blocks are keyed
+// by the CUDA context that allocated them (current_context_id), so a block of
+// a context that was destroyed meanwhile is never handed out again.
 namespace {
+struct DevKey {
+    int device;
+    unsigned long long context;
+    size_t bytes;
+    bool operator<(const DevKey& o) const {
+        if (device != o.device) return device < o.device;
+        if (context != o.context) return context < o.context;
+        return bytes < o.bytes;
+    }
+};
 struct BlockCache {
     std::mutex mu;
-    std::multimap<std::pair<int, size_t>, void*> dev;   // (device, bytes) -> block
+    std::multimap<DevKey, void*> dev;
     std::multimap<size_t, void*> pinned;
     size_t cached = 0;
 };
@@ -105,10 +111,11 @@ constexpr size_t CACHE_LIMIT = size_t(16) << 30;
 cudaError_t cached_malloc(void** p, size_t bytes) {
     int d = 0;
     cudaGetDevice(&d);
-    {
+    const unsigned long long cid = current_context_id();
+    if (cid) {
         BlockCache& c = block_cache();
         std::lock_guard<std::mutex> lock(c.mu);
-        auto it = c.dev.find({d, bytes});
+        auto it = c.dev.find({d, cid, bytes});
         if (it != c.dev.end()) {
             *p = it->second;
             c.dev.erase(it);
@@ -121,11 +128,12 @@ cudaError_t cached_malloc(void** p, size_t bytes) {
 void cached_free(void* p, size_t bytes) {
     int d = 0;
     cudaGetDevice(&d);
-    {
+    const unsigned long long cid = current_context_id();
+    if (cid) {
         BlockCache& c = block_cache();
         std::lock_guard<std::mutex> lock(c.mu);
         if (c.cached + bytes <= CACHE_LIMIT) {
-            c.dev.insert({{d, bytes}, p});
+            c.dev.insert({{d, cid, bytes}, p});
             c.cached += bytes;
             return;
         }
@@ -171,6 +179,9 @@ struct sw_ctx {
     cudaStream_t stream = nullptr;
     int device = 0;
     std::vector<std::pair<void*, size_t>> allocs;   // device blocks and their sizes (cached_malloc)
+    std::vector<std::pair<void*, size_t>> zeroed;   // the blocks that start at zero (state, stage, status)
+    unsigned long long context_id = 0;              // CUDA context the blocks belong to
+    std::string env;                                // the SWB200_* settings read at creation
     Fields3 S[2], A, B, Acc;
     Fields3 C;                 // third stage buffer of the SSP schemes
     void* qS = nullptr;        // nstep_advcor > 0: stored q, KEu, KEv (type T, sw_advcor.cuh)
@@ -180,14 +191,16 @@ struct sw_ctx {
     void* um = nullptr; void* vm = nullptr;
     void* flush = nullptr; size_t flush_bytes = 0;
     // static fields (type T) and their strides
-    struct SF { void* p = nullptr; int sx = 0, sy = 0; } H, fq, Fx, Fy, fu, fv, eref, Feta;
+    struct SF { void* p = nullptr; int sx = 0, sy = 0; size_t bytes = 0; } H, fq, Fx, Fy, fu, fv, eref, Feta;
+    std::vector<std::vector<unsigned char>> staging;   // host sources of uploads in flight
     // TMA descriptors per state buffer: input box (BOXW_IN x K) and point-wise box (BOXW_X x K)
-    struct Maps { CUtensorMap in, x, in2, x2; };
+    struct Maps { CUtensorMap in, x; };
     TileSched* sched = nullptr;   // device tile counter of the TMA stage kernel
     std::map<const void*, Maps> tmaps;
     bool use_tma = false;
-    bool packed = false;          // FP32x2 stage kernel for Float32 (opt-in: SWB200_PACKED=1)
-    bool tail_tma = false;        // TMA-fed tail for Float32 (opt-in: SWB200_TAIL_TMA=1; measured slower)
+    int stage_blocks_cap = 0;     // > 0: at most this many persistent blocks in rk_stage_tma
+    uint32_t spin_limit = MBAR_SPIN_LIMIT;   // polls per bounded wait of rk_stage_tma
+    int test_skip_chunk = -1;     // test only: a chunk rk_stage_tma's producer leaves out
     // CUDA graphs of one time step, keyed by the buffer parities and the
     // sub-steps that are due (see step_key); off with SWB200_GRAPHS=0
     bool use_graphs = true;
@@ -269,16 +282,6 @@ int fail(sw_ctx* c, int code, const std::string& msg) {
 #define SWB_TMA_S 2
 #endif
 constexpr int STAGE_TMA_TY = SWB_TMA_TY, STAGE_TMA_K = SWB_TMA_K, STAGE_TMA_S = SWB_TMA_S;
-#ifndef SWB_S2_TY
-#define SWB_S2_TY 16
-#endif
-#ifndef SWB_S2_K
-#define SWB_S2_K 4
-#endif
-#ifndef SWB_S2_S
-#define SWB_S2_S 2
-#endif
-constexpr int STAGE2_TY = SWB_S2_TY, STAGE2_K = SWB_S2_K, STAGE2_S = SWB_S2_S;
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     // looked up once, thread-safely (contexts may be created from several threads)
@@ -456,7 +459,8 @@ struct Engine : EngineBase {
         if (occ < 1) return -1;
         const Geom& g = a.g;
         const int ntiles = ((g.N + BAND - 1) / BAND) * ((g.M + TY - 1) / TY);
-        const int npersist = std::min(ntiles, ctx->nsm * occ);
+        int npersist = std::min(ntiles, ctx->nsm * occ);
+        if (ctx->stage_blocks_cap > 0) npersist = std::min(npersist, ctx->stage_blocks_cap);
         const int nring = std::min(RING_BLOCKS_MAX, (Ring::u_count(g.ep, g.N, g.M) + Ring::v_count(g.N) + 159) / 160);
         kern<<<npersist + nring, 160, smem, ctx->stream>>>(a, mp, npersist, ctx->sched);
         return 0;
@@ -483,42 +487,6 @@ struct Engine : EngineBase {
         return stage_tma_launch<false, false, false, ROWF>(ctx, a, mp);
     }
 
-    template <bool PER, bool FIRST, bool LAST>
-    static int stage2_launch(sw_ctx* ctx, const StageArgs<T, Tp>& a, const StageMaps2& mp) {
-        if constexpr (std::is_same<T, float>::value && std::is_same<Tp, float>::value) {
-            constexpr int TY = STAGE2_TY, K = STAGE2_K, S = STAGE2_S;
-            auto kern = rk_stage_f2<PER, FIRST, LAST, TY, K, S>;
-            constexpr int smem = stage2_smem<FIRST, LAST, K, S>();
-            static const int occ = [&] {
-                int o = -1;
-                if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
-                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, 160, smem) != cudaSuccess)
-                    o = -1;
-                return o;
-            }();
-            if (occ < 1) return -1;
-            const Geom& g = a.g;
-            const int ntiles = ((g.N + BAND2 - 1) / BAND2) * ((g.M + TY - 1) / TY);
-            const int npersist = std::min(ntiles, ctx->nsm * occ);
-            const int nring = std::min(RING_BLOCKS_MAX, (Ring::u_count(g.ep, g.N, g.M) + Ring::v_count(g.N) + 159) / 160);
-            kern<<<npersist + nring, 160, smem, ctx->stream>>>(a, mp, npersist, ctx->sched);
-            return 0;
-        } else {
-            return -1;
-        }
-    }
-    static int stage2_dispatch(sw_ctx* ctx, const StageArgs<T, Tp>& a, const StageMaps2& mp, bool per, bool first,
-                               bool last) {
-        if (per) {
-            if (first) return stage2_launch<true, true, false>(ctx, a, mp);
-            if (last) return stage2_launch<true, false, true>(ctx, a, mp);
-            return stage2_launch<true, false, false>(ctx, a, mp);
-        }
-        if (first) return stage2_launch<false, true, false>(ctx, a, mp);
-        if (last) return stage2_launch<false, false, true>(ctx, a, mp);
-        return stage2_launch<false, false, false>(ctx, a, mp);
-    }
-
     // Shorter strips for Float32 / Float64 grids too small to fill the GPU
     // with 32-row strips (the values do not depend on the strip height).
     template <bool PER, int DRAG, bool SMAG>
@@ -529,43 +497,6 @@ struct Engine : EngineBase {
             if (ty == 16) { tail_kernel<T, Tp, PER, DRAG, SMAG, 16><<<nblk, 128, 0, s>>>(a); return; }
         }
         tail_kernel<T, Tp, PER, DRAG, SMAG, TAIL_TY><<<nblk, 128, 0, s>>>(a);
-    }
-    // TMA-fed tail (Float32): returns -1 if it cannot be configured
-    template <bool PER, int DRAG, bool SMAG, bool ROWH>
-    static int tail_tma_launch(sw_ctx* ctx, const TailArgs<T, Tp>& a, const TailMaps& mp) {
-        if constexpr (std::is_same<T, float>::value && std::is_same<Tp, float>::value) {
-            constexpr int TY = TAIL_TMA_TY, K = STAGE_TMA_K, S = TAIL_TMA_S;
-            constexpr bool QUAD = DRAG == SW_DRAG_QUADRATIC;
-            auto kern = tail_tma<PER, DRAG, SMAG, TY, K, S, ROWH>;
-            constexpr int smem = tail_tma_smem<K, S, QUAD>();
-            static const int occ = [&] {
-                int o = -1;
-                if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
-                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, 160, smem) != cudaSuccess)
-                    o = -1;
-                return o;
-            }();
-            if (occ < 1) return -1;
-            const Geom& g = a.g;
-            const int ntiles = ((g.N + BAND - 1) / BAND) * ((g.M + TY - 1) / TY);
-            const int npersist = std::min(ntiles, ctx->nsm * occ);
-            const int nring = std::min(RING_BLOCKS_MAX, (Ring::u_count(g.ep, g.N, g.M) + Ring::v_count(g.N) + 159) / 160);
-            kern<<<npersist + nring, 160, smem, ctx->stream>>>(a, mp, npersist, ctx->sched);
-            return 0;
-        } else {
-            return -1;
-        }
-    }
-    template <bool PER, bool ROWH>
-    static int tail_tma_dispatch(sw_ctx* ctx, const TailArgs<T, Tp>& a, const TailMaps& mp, int drag, bool smag) {
-        if (smag) {
-            if (drag == SW_DRAG_QUADRATIC) return tail_tma_launch<PER, SW_DRAG_QUADRATIC, true, ROWH>(ctx, a, mp);
-            if (drag == SW_DRAG_LINEAR) return tail_tma_launch<PER, SW_DRAG_LINEAR, true, true>(ctx, a, mp);
-            return tail_tma_launch<PER, SW_DRAG_NONE, true, true>(ctx, a, mp);
-        }
-        if (drag == SW_DRAG_QUADRATIC) return tail_tma_launch<PER, SW_DRAG_QUADRATIC, false, ROWH>(ctx, a, mp);
-        if (drag == SW_DRAG_LINEAR) return tail_tma_launch<PER, SW_DRAG_LINEAR, false, true>(ctx, a, mp);
-        return tail_tma_launch<PER, SW_DRAG_NONE, false, true>(ctx, a, mp);
     }
     template <bool PER>
     static void tail_dispatch2(const TailArgs<T, Tp>& a, int drag, bool smag, int nblk, cudaStream_t s, int ty) {
@@ -779,6 +710,8 @@ struct Engine : EngineBase {
         set_cont(ctx, a);
         a.gr = rule(ctx);
         a.st = ctx->dst;
+        a.spin_limit = ctx->spin_limit;
+        a.skip_chunk = ctx->test_skip_chunk;
         return a;
     }
     // The tail's arguments for a step from S[p]: u0, v0 in Acc, eta0 in S[1-p]
@@ -839,17 +772,8 @@ struct Engine : EngineBase {
             const Fields3& in = (k == 1) ? X : ((k % 2 == 0) ? ctx->A : ctx->B);
             const bool first = (k == 1), last = (k == c.RKo);
             int rc;
-            constexpr bool F32 = std::is_same<T, float>::value && std::is_same<Tp, float>::value;
             if (c.dynamics == SW_LINEAR) {
                 rc = launch(ctx, 0, [&] { lin_rk_dispatch(ctx, a, g.ep != 0, first, last); });
-            } else if (ctx->use_tma && F32 && ctx->packed && a.cont == 0 && !a.sadourny && !a.qS) {
-                StageMaps2 mp;
-                mp.in_u = ctx->tmaps[in.u].in2; mp.in_v = ctx->tmaps[in.v].in2; mp.in_e = ctx->tmaps[in.e].in2;
-                mp.x_u = ctx->tmaps[X.u].x2; mp.x_v = ctx->tmaps[X.v].x2; mp.x_e = ctx->tmaps[X.e].x2;
-                mp.a_u = ctx->tmaps[ctx->Acc.u].x2; mp.a_v = ctx->tmaps[ctx->Acc.v].x2; mp.a_e = ctx->tmaps[ctx->Acc.e].x2;
-                int lr = 0;
-                rc = launch(ctx, 0, [&] { lr = stage2_dispatch(ctx, a, mp, g.ep != 0, first, last); });
-                if (!rc && lr) rc = fail(ctx, SW_ERR_CUDA, "packed stage kernel could not be configured");
             } else if (TMA_TYPES && ctx->use_tma && a.cont == 0 && !a.sadourny && !a.qS) {
                 StageMaps mp;
                 mp.in_u = ctx->tmaps[in.u].in; mp.in_v = ctx->tmaps[in.v].in; mp.in_e = ctx->tmaps[in.e].in;
@@ -878,30 +802,14 @@ struct Engine : EngineBase {
             TailArgs<T, Tp> a = tail_args(ctx, ctx->p);
             const int nb = (a.nsx * a.nsy + 3) / 4 + a.nring_blocks;
             const bool smag = (c.diffusion == SW_DIFF_SMAGORINSKY);
-            constexpr bool F32 = std::is_same<T, float>::value && std::is_same<Tp, float>::value;
-            int rc;
-            if (F32 && ctx->use_tma && ctx->tail_tma) {
-                TailMaps mp;
-                mp.u = ctx->tmaps[ctx->Acc.u].in; mp.v = ctx->tmaps[ctx->Acc.v].in; mp.e = ctx->tmaps[Y.e].in;
-                const bool rowh = ctx->H.sx == 0;
-                int lr = 0;
-                rc = launch(ctx, 1, [&] {
-                    if (g.ep) lr = rowh ? tail_tma_dispatch<true, true>(ctx, a, mp, c.bottom_drag, smag)
-                                        : tail_tma_dispatch<true, false>(ctx, a, mp, c.bottom_drag, smag);
-                    else lr = rowh ? tail_tma_dispatch<false, true>(ctx, a, mp, c.bottom_drag, smag)
-                                   : tail_tma_dispatch<false, false>(ctx, a, mp, c.bottom_drag, smag);
-                });
-                if (!rc && lr) rc = fail(ctx, SW_ERR_CUDA, "TMA tail kernel could not be configured");
-            } else {
-                rc = launch(ctx, 1, [&] {
-                    if (g.ep) tail_dispatch2<true>(a, c.bottom_drag, smag, nb, ctx->stream, ctx->tail_ty);
-                    else tail_dispatch2<false>(a, c.bottom_drag, smag, nb, ctx->stream, ctx->tail_ty);
-                });
-            }
+            const int rc = launch(ctx, 1, [&] {
+                if (g.ep) tail_dispatch2<true>(a, c.bottom_drag, smag, nb, ctx->stream, ctx->tail_ty);
+                else tail_dispatch2<false>(a, c.bottom_drag, smag, nb, ctx->stream, ctx->tail_ty);
+            });
             if (rc) return rc;
             // bottom_drag_quadratic! leaves its KEu, KEv (of u0) for the next stages
             if (ctx->qS && c.bottom_drag == SW_DRAG_QUADRATIC)
-                if ((rc = advcor_refresh(ctx, ctx->Acc.u, ctx->Acc.v, Y.e, true))) return rc;
+                if (int rq = advcor_refresh(ctx, ctx->Acc.u, ctx->Acc.v, Y.e, true)) return rq;
         }
         ctx->t += c.dtint;
 
@@ -1063,21 +971,61 @@ int check_config(const sw_config* c, std::string& why) {
     return SW_OK;
 }
 
-// Upload a host field (T, x fastest, host column 0 at physical x = hx0, row 0 at
-// y = hy0, size w x h) as a strided SField: constant fields and fields that vary
-// along one axis only are stored as broadcast vectors.
-int upload_static(sw_ctx* ctx, sw_ctx::SF& out, const void* host, int w, int h, int hx0, int hy0) {
+// Runs f(j0, j1) over row ranges covering [0, h), on up to 8 host threads
+// when the field is large (work = bytes to scan); true if every call was.
+template <class F>
+bool all_row_ranges(int h, size_t work, F&& f) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int nt = (int)std::min<size_t>(std::min(8u, hw), std::max<size_t>(1, work >> 22));
+    if (nt <= 1 || h < 2 * nt) return f(0, h);
+    std::atomic<bool> ok{true};
+    std::vector<std::thread> th;
+    for (int k = 0; k < nt; k++) {
+        const int j0 = (int)((long long)h * k / nt), j1 = (int)((long long)h * (k + 1) / nt);
+        th.emplace_back([&, j0, j1] { if (!f(j0, j1)) ok = false; });
+    }
+    for (auto& t : th) t.join();
+    return ok;
+}
+
+// Rows [j0, j1) of a w-wide host field with W-sized elements: is every row
+// constant along x (bitwise)?
+template <class W>
+bool rows_const_x(const unsigned char* src, int w, int j0, int j1) {
+    for (int j = j0; j < j1; j++) {
+        const unsigned char* r = src + (size_t)j * w * sizeof(W);
+        W a, b;
+        std::memcpy(&a, r, sizeof(W));
+        for (int i = 1; i < w; i++) {
+            std::memcpy(&b, r + (size_t)i * sizeof(W), sizeof(W));
+            if (b != a) return false;
+        }
+    }
+    return true;
+}
+
+// Host-side packing of a static field (T, x fastest, host column 0 at
+// physical x = hx0, row 0 at y = hy0, size w x h) into its strided SField
+// form: constant fields and fields that vary along one axis only become
+// broadcast vectors.
+struct PackedStatic { std::vector<unsigned char> buf; int sx = 0, sy = 0; };
+PackedStatic pack_static(const sw_ctx* ctx, const void* host, int w, int h, int hx0, int hy0) {
     const size_t ts = ctx->tsz;
     const unsigned char* src = static_cast<const unsigned char*>(host);
     auto el = [&](int i, int j) { return src + ((size_t)j * w + i) * ts; };
-    bool const_x = true, const_y = true;
-    for (int j = 0; j < h && const_x; j++)
-        for (int i = 1; i < w; i++)
-            if (std::memcmp(el(i, j), el(0, j), ts)) { const_x = false; break; }
-    for (int j = 1; j < h && const_y; j++)
-        if (std::memcmp(el(0, j), el(0, 0), ts * (size_t)w)) const_y = false;
+    const size_t bytes = (size_t)w * h * ts;
+    const bool const_x = all_row_ranges(h, bytes, [&](int j0, int j1) {
+        return ts == 2 ? rows_const_x<uint16_t>(src, w, j0, j1)
+             : ts == 4 ? rows_const_x<uint32_t>(src, w, j0, j1) : rows_const_x<uint64_t>(src, w, j0, j1);
+    });
+    const bool const_y = all_row_ranges(h, bytes, [&](int j0, int j1) {
+        for (int j = std::max(j0, 1); j < j1; j++)
+            if (std::memcmp(el(0, j), el(0, 0), ts * (size_t)w)) return false;
+        return true;
+    });
     const Geom& g = ctx->g;
-    std::vector<unsigned char> buf;
+    PackedStatic out;
+    std::vector<unsigned char>& buf = out.buf;
     if (const_x && const_y) {
         buf.assign(ts, 0);
         std::memcpy(buf.data(), el(0, 0), ts);
@@ -1096,9 +1044,54 @@ int upload_static(sw_ctx* ctx, sw_ctx::SF& out, const void* host, int w, int h, 
             std::memcpy(&buf[((size_t)(hy0 + j + ROW0) * g.P + (hx0 + COL0)) * ts], el(0, j), ts * (size_t)w);
         out.sx = 1; out.sy = g.P;
     }
-    CK(cached_malloc(&out.p, buf.size()));
-    ctx->allocs.push_back({out.p, buf.size()});
-    CK(cudaMemcpy(out.p, buf.data(), buf.size(), cudaMemcpyHostToDevice));
+    return out;
+}
+
+// Upload a static field into out.  A field already on the device with the
+// same packed layout is overwritten in place (its address, and so every
+// captured step graph, stays valid); SW_ERR_UNSUPPORTED tells a caller that
+// refreshes a context that the layout changed.  The copy is asynchronous on
+// the context's stream: the packed buffer is kept in ctx->staging until the
+// caller synchronises.
+int upload_static(sw_ctx* ctx, sw_ctx::SF& out, const void* host, int w, int h, int hx0, int hy0) {
+    PackedStatic pk = pack_static(ctx, host, w, h, hx0, hy0);
+    if (out.p) {
+        if (out.bytes != pk.buf.size() || out.sx != pk.sx || out.sy != pk.sy) return SW_ERR_UNSUPPORTED;
+    } else {
+        CK(cached_malloc(&out.p, pk.buf.size()));
+        ctx->allocs.push_back({out.p, pk.buf.size()});
+        out.bytes = pk.buf.size();
+        out.sx = pk.sx; out.sy = pk.sy;
+    }
+    CK(cudaMemcpyAsync(out.p, pk.buf.data(), pk.buf.size(), cudaMemcpyHostToDevice, ctx->stream));
+    ctx->staging.push_back(std::move(pk.buf));
+    return SW_OK;
+}
+
+// The static fields of a context (src/grid.jl:93-95, src/forcing.jl:1-53):
+// uploaded at creation, and again when a cached context is reused.
+int upload_statics(sw_ctx* ctx, const sw_static* st) {
+    const sw_config* cfg = &ctx->cfg;
+    const Geom& g = ctx->g;
+    const int N = g.N, M = g.M, nux = g.ep ? N : N - 1;
+    int rc;
+    if ((rc = upload_static(ctx, ctx->fq, st->f_q, N + 1, M + 1, 0, 0))) return rc;
+    if ((rc = upload_static(ctx, ctx->Fx, st->Fx, nux, M, 1 - g.ep, 0))) return rc;
+    if ((rc = upload_static(ctx, ctx->Fy, st->Fy, N, M - 1, 0, 1))) return rc;
+    if ((rc = upload_static(ctx, ctx->H, st->H, N + 2, M + 2, -1, -1))) return rc;
+    if (cfg->dynamics == SW_LINEAR) {
+        if (!st->f_u || !st->f_v) return fail(ctx, SW_ERR_ARG, "linear dynamics needs f_u and f_v");
+        if ((rc = upload_static(ctx, ctx->fu, st->f_u, nux, M, 1 - g.ep, 0))) return rc;
+        if ((rc = upload_static(ctx, ctx->fv, st->f_v, N, M - 1, 0, 1))) return rc;
+    }
+    if (cfg->surface_relax) {
+        if (!st->eta_ref) return fail(ctx, SW_ERR_ARG, "surface_relax needs eta_ref");
+        if ((rc = upload_static(ctx, ctx->eref, st->eta_ref, N, M, 0, 0))) return rc;
+    }
+    if (cfg->surface_forcing) {
+        if (!st->Feta) return fail(ctx, SW_ERR_ARG, "surface_forcing needs Feta");
+        if ((rc = upload_static(ctx, ctx->Feta, st->Feta, N, M, 0, 0))) return rc;
+    }
     return SW_OK;
 }
 
@@ -1215,6 +1208,120 @@ int run_steps(sw_ctx* ctx, long long nsteps, sw_status* status) {
     if (code == SW_ERR_DEPARTURE) ctx->err = "tracer departure point outside the domain";
     if (code == SW_NAN_DETECTED) ctx->err = "NaNs detected at time step " + std::to_string(ctx->step);
     return code;
+}
+
+// The environment settings a context reads at creation (kernel choices and
+// test caps); a cached context is reused only under the same settings.
+std::string env_settings() {
+    std::string s;
+    for (const char* k : {"SWB200_TMA", "SWB200_GRAPHS", "SWB200_STAGE_BLOCKS", "SWB200_TAIL_TY", "SWB200_STAGE_TY",
+                          "SWB200_TEST_WAIT_LIMIT", "SWB200_TEST_SKIP_CHUNK"}) {
+        const char* v = getenv(k);
+        s += k;
+        s += '=';
+        s += v ? v : "";
+        s += ';';
+    }
+    return s;
+}
+
+// ----------------------------------------------------------------- drop-in cache
+// sw_time_integration keeps the contexts of its finished calls (at most
+// DROPIN_CACHE) and gives one to a later call whose configuration equals it in
+// everything but nt, in the same CUDA context and under the same environment
+// settings.  Such a call skips creation (allocation, tensor-map encoding, step
+// graph capture): it zeroes the context's buffers as creation would, uploads
+// the static fields again (in place; if their packed layout changed, the
+// context is rebuilt) and then runs exactly as on a new context.
+constexpr size_t DROPIN_CACHE = 4;
+struct DropinCache {
+    std::mutex mu;
+    std::vector<sw_ctx*> idle;     // oldest first
+};
+DropinCache& dropin_cache() {
+    static DropinCache* c = new DropinCache();   // never destroyed: may be used during process exit
+    return *c;
+}
+
+bool same_run_config(const sw_config& a, const sw_config& b) {
+    sw_config x = a, y = b;
+    x.nt = y.nt = 0;
+    return std::memcmp(&x, &y, sizeof(sw_config)) == 0;
+}
+
+sw_ctx* take_dropin(const sw_config* cfg) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    const unsigned long long cid = current_context_id();
+    if (!cid) return nullptr;
+    const std::string env = env_settings();
+    DropinCache& c = dropin_cache();
+    std::lock_guard<std::mutex> lock(c.mu);
+    for (size_t k = c.idle.size(); k-- > 0;) {
+        sw_ctx* x = c.idle[k];
+        if (x->device == dev && x->context_id == cid && x->env == env && same_run_config(x->cfg, *cfg)) {
+            c.idle.erase(c.idle.begin() + (long)k);
+            return x;
+        }
+    }
+    return nullptr;
+}
+
+// Zero the context's buffers (as sw_create leaves them) and upload the static
+// fields of this call; anything but SW_OK means: do not use this context.
+int refresh_dropin(sw_ctx* ctx, const sw_config* cfg, const sw_static* st) {
+    ctx->cfg.nt = cfg->nt;
+    ctx->err.clear();
+    for (auto& z : ctx->zeroed) CK(cudaMemsetAsync(z.first, 0, z.second, ctx->stream));
+    int rc = upload_statics(ctx, st);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->staging.clear();
+    return SW_OK;
+}
+
+}  // namespace
+
+extern "C" void sw_destroy(sw_ctx* ctx);
+
+namespace {
+
+void put_dropin(sw_ctx* ctx) {
+    sw_ctx* evict = nullptr;
+    {
+        DropinCache& c = dropin_cache();
+        std::lock_guard<std::mutex> lock(c.mu);
+        c.idle.push_back(ctx);
+        if (c.idle.size() > DROPIN_CACHE) {
+            evict = c.idle.front();
+            c.idle.erase(c.idle.begin());
+        }
+    }
+    if (evict) {
+        int cur = 0;
+        cudaGetDevice(&cur);
+        cudaSetDevice(evict->device);
+        sw_destroy(evict);
+        cudaSetDevice(cur);
+    }
+}
+
+// destroys every cached drop-in context (sw_trim_memory)
+void release_dropin_contexts() {
+    std::vector<sw_ctx*> all;
+    {
+        DropinCache& c = dropin_cache();
+        std::lock_guard<std::mutex> lock(c.mu);
+        all.swap(c.idle);
+    }
+    int cur = 0;
+    cudaGetDevice(&cur);
+    for (sw_ctx* x : all) {
+        cudaSetDevice(x->device);
+        if (current_context_id() == x->context_id) sw_destroy(x);
+        else delete x;      // its CUDA context is gone, and its blocks and stream with it
+    }
+    cudaSetDevice(cur);
 }
 
 }  // namespace
@@ -1510,6 +1617,11 @@ extern "C" {
 
 int sw_abi_version(void) { return SWB200_ABI_VERSION; }
 
+#ifndef SWB_FAST_BUILD
+#define SWB_FAST_BUILD 0
+#endif
+int sw_build_kind(void) { return SWB_FAST_BUILD ? SW_BUILD_FAST : SW_BUILD_PARITY; }
+
 const char* sw_strerror(int code) { return err_name(code); }
 
 const char* sw_last_error(const sw_ctx* ctx) { return ctx ? ctx->err.c_str() : ""; }
@@ -1701,13 +1813,15 @@ void sw_batch_destroy(sw_batch* b) {
 }
 
 int sw_trim_memory(void) {
+    release_dropin_contexts();
     BlockCache& c = block_cache();
     std::lock_guard<std::mutex> lock(c.mu);
     int cur = 0;
     cudaGetDevice(&cur);
     for (auto& kv : c.dev) {
-        cudaSetDevice(kv.first.first);
-        cudaFree(kv.second);
+        // blocks of a context that no longer exists are dropped, not freed
+        if (cudaSetDevice(kv.first.device) != cudaSuccess) continue;
+        if (current_context_id() == kv.first.context) cudaFree(kv.second);
     }
     cudaSetDevice(cur);
     for (auto& kv : c.pinned) cudaFreeHost(kv.second);
@@ -1754,10 +1868,13 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
     ctx->tsz = fmt_size(cfg->T);
     ctx->tpsz = fmt_size(cfg->Tprog);
     CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    ctx->context_id = current_context_id();
+    ctx->env = env_settings();
 
     auto alloc = [&](void** p, size_t bytes) -> int {
         CK(cached_malloc(p, bytes));
         ctx->allocs.push_back({*p, bytes});
+        ctx->zeroed.push_back({*p, bytes});
         CK(cudaMemsetAsync(*p, 0, bytes, ctx->stream));
         return SW_OK;
     };
@@ -1787,24 +1904,7 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
     CK(cached_malloc_host((void**)&ctx->hst, sizeof(DevStatus)));
     std::memset(ctx->hst, 0, sizeof(DevStatus));
 
-    const int N = g.N, M = g.M, nux = g.ep ? N : N - 1;
-    if ((rc = upload_static(ctx, ctx->fq, st->f_q, N + 1, M + 1, 0, 0))) return rc;
-    if ((rc = upload_static(ctx, ctx->Fx, st->Fx, nux, M, 1 - g.ep, 0))) return rc;
-    if ((rc = upload_static(ctx, ctx->Fy, st->Fy, N, M - 1, 0, 1))) return rc;
-    if ((rc = upload_static(ctx, ctx->H, st->H, N + 2, M + 2, -1, -1))) return rc;
-    if (cfg->dynamics == SW_LINEAR) {
-        if (!st->f_u || !st->f_v) return fail(ctx, SW_ERR_ARG, "linear dynamics needs f_u and f_v");
-        if ((rc = upload_static(ctx, ctx->fu, st->f_u, nux, M, 1 - g.ep, 0))) return rc;
-        if ((rc = upload_static(ctx, ctx->fv, st->f_v, N, M - 1, 0, 1))) return rc;
-    }
-    if (cfg->surface_relax) {
-        if (!st->eta_ref) return fail(ctx, SW_ERR_ARG, "surface_relax needs eta_ref");
-        if ((rc = upload_static(ctx, ctx->eref, st->eta_ref, N, M, 0, 0))) return rc;
-    }
-    if (cfg->surface_forcing) {
-        if (!st->Feta) return fail(ctx, SW_ERR_ARG, "surface_forcing needs Feta");
-        if ((rc = upload_static(ctx, ctx->Feta, st->Feta, N, M, 0, 0))) return rc;
-    }
+    if ((rc = upload_statics(ctx, st))) return rc;
 
     {
         int dev = 0;
@@ -1813,21 +1913,25 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
         const char* env = getenv("SWB200_TMA");
         bool want = !(env && env[0] == '0');
         bool ok = want && encode_fn() != nullptr;
-        const char* envp = getenv("SWB200_PACKED");
-        ctx->packed = (envp && envp[0] == '1');
+        // a cap on the TMA stage kernel's persistent blocks (SWB200_STAGE_BLOCKS),
+        // so that small grids also run blocks that take several tiles each
+        const char* envb = getenv("SWB200_STAGE_BLOCKS");
+        ctx->stage_blocks_cap = envb ? std::max(1, atoi(envb)) : 0;
+        // test only: a shorter bounded wait and a chunk that is never filled,
+        // to make rk_stage_tma's waits run out (SW_ERR_TIMEOUT)
+        const char* envw = getenv("SWB200_TEST_WAIT_LIMIT");
+        if (envw && atoi(envw) > 0) ctx->spin_limit = (uint32_t)atoi(envw);
+        const char* envk = getenv("SWB200_TEST_SKIP_CHUNK");
+        ctx->test_skip_chunk = envk ? atoi(envk) : -1;
         for (Fields3* f : {&ctx->S[0], &ctx->S[1], &ctx->A, &ctx->B, &ctx->Acc})
             for (void* p : {f->u, f->v, f->e}) {
                 if (!ok) break;
                 sw_ctx::Maps mp;
                 ok = make_map(&mp.in, p, ctx->tpsz, g.P, g.R, BOXW_IN, STAGE_TMA_K) &&
-                     make_map(&mp.x, p, ctx->tpsz, g.P, g.R, BOXW_X, STAGE_TMA_K) &&
-                     (!ctx->packed || (make_map(&mp.in2, p, ctx->tpsz, g.P, g.R, BOXW_IN2, STAGE2_K) &&
-                                       make_map(&mp.x2, p, ctx->tpsz, g.P, g.R, BOXW_X2, STAGE2_K)));
+                     make_map(&mp.x, p, ctx->tpsz, g.P, g.R, BOXW_X, STAGE_TMA_K);
                 ctx->tmaps[p] = mp;
             }
         ctx->use_tma = ok;
-        const char* envt = getenv("SWB200_TAIL_TMA");
-        ctx->tail_tma = (envt && envt[0] == '1');
         const char* envg = getenv("SWB200_GRAPHS");
         ctx->use_graphs = !(envg && envg[0] == '0');
         ctx->tail_ty = pick_strip_ty(*cfg, g, ctx->nsm, "SWB200_TAIL_TY");
@@ -1845,6 +1949,7 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
         auto* e = new Engine<jf16, jf16>(); ctx->eng.reset(e); if ((rc = e->init(ctx))) return rc;
     }
     CK(cudaStreamSynchronize(ctx->stream));
+    ctx->staging.clear();
     *out = holder.release();
     return SW_OK;
 }
@@ -1969,9 +2074,14 @@ int sw_diagnostics(sw_ctx* ctx, sw_diag* out) {
 
 int sw_time_integration(const sw_config* cfg, const sw_static* st, void* u, void* v, void* eta, void* sst,
                         sw_status* status) {
-    sw_ctx* ctx = nullptr;
-    int rc = sw_create(cfg, st, &ctx);
-    if (rc) return rc;
+    if (!cfg || !st) return SW_ERR_ARG;
+    sw_ctx* ctx = take_dropin(cfg);
+    if (ctx && refresh_dropin(ctx, cfg, st) != SW_OK) {
+        sw_destroy(ctx);
+        ctx = nullptr;
+    }
+    int rc = SW_OK;
+    if (!ctx && (rc = sw_create(cfg, st, &ctx))) return rc;
     rc = sw_set_state(ctx, u, v, eta, sst);
     if (!rc) {
         int rr = sw_run(ctx, cfg->nt, status);
@@ -1983,7 +2093,8 @@ int sw_time_integration(const sw_config* cfg, const sw_static* st, void* u, void
         }
     }
     if (rc && rc != SW_NAN_DETECTED) fprintf(stderr, "swb200: %s\n", ctx->err.c_str());
-    sw_destroy(ctx);
+    if (rc == SW_OK || rc == SW_NAN_DETECTED) put_dropin(ctx);
+    else sw_destroy(ctx);
     return rc;
 }
 

@@ -58,6 +58,11 @@ struct StageArgs {
     const T* qS; const T* KEuS; const T* KEvS;
     GhostRule<Tp> gr;
     DevStatus* st;
+    // bounded waits of the TMA kernel: polls per wait, and (test only, -1
+    // otherwise) a chunk of block 0's first tile that the producer leaves out,
+    // so that its consumers' wait runs out
+    uint32_t spin_limit;
+    int skip_chunk;
 };
 
 // deta at the T-cell (c, r) from the flux divergences: continuity_itself!,
@@ -422,7 +427,7 @@ __device__ __forceinline__ bool stage_tile(const StageArgs<T, Tp>& A, const Tp* 
     const int cb = c + COL0;
 
     auto slot_ptr = [&](int j) { return ring + ((gbase + j) % S) * SL::ELEMS; };
-    auto wait_chunk = [&](int j) { return mbar_wait(&full[(gbase + j) % S], ((gbase + j) / S) & 1, A.st); };
+    auto wait_chunk = [&](int j) { return mbar_wait(&full[(gbase + j) % S], ((gbase + j) / S) & 1, A.st, A.spin_limit); };
     auto release = [&](int j) {
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[(gbase + j) % S]);
@@ -626,8 +631,9 @@ rk_stage_tma(const __grid_constant__ StageArgs<T, Tp> A, const __grid_constant__
         uint32_t gc = 0;
         bool ok = true;
         auto acquire = [&](int slot) {
-            return gc < (uint32_t)S || mbar_wait(&empty[slot], ((gc / S) - 1) & 1, A.st);
+            return gc < (uint32_t)S || mbar_wait(&empty[slot], ((gc / S) - 1) & 1, A.st, A.spin_limit);
         };
+        bool first_tile = true;
         for (;;) {
             const int t = atomicAdd(&sched->next, 1);
             const int slot0 = gc % S;
@@ -646,6 +652,7 @@ rk_stage_tma(const __grid_constant__ StageArgs<T, Tp> A, const __grid_constant__
             for (int j = 0; j < NCH; j++, gc++) {
                 const int slot = gc % S;
                 if (!acquire(slot)) { ok = false; break; }
+                if (first_tile && j == A.skip_chunk && blockIdx.x == 0) continue;   // test only: never filled
                 slot_tile[slot] = t;
                 mbar_arrive_expect_tx(&full[slot], SL::TX_BYTES);
                 Tp* b = ring + slot * SL::ELEMS;
@@ -665,9 +672,11 @@ rk_stage_tma(const __grid_constant__ StageArgs<T, Tp> A, const __grid_constant__
                 }
             }
             if (!ok) break;
+            first_tile = false;
         }
         // all issued copies must land before the block may exit
-        for (uint32_t q = (gc >= (uint32_t)S ? gc - S : 0); q < gc; q++) mbar_wait(&full[q % S], (q / S) & 1, A.st);
+        for (uint32_t q = (gc >= (uint32_t)S ? gc - S : 0); q < gc; q++)
+            mbar_wait(&full[q % S], (q / S) & 1, A.st, A.spin_limit);
         // the last producer of the launch resets the scheduler for the next one
         if (atomicAdd(&sched->done, 1) == npersist - 1) {
             sched->next = 0;
@@ -679,7 +688,7 @@ rk_stage_tma(const __grid_constant__ StageArgs<T, Tp> A, const __grid_constant__
 
     // -------------------------------------------------------------- consumers
     for (uint32_t gbase = 0;; gbase += NCH) {
-        if (!mbar_wait(&full[gbase % S], (gbase / S) & 1, A.st)) return;
+        if (!mbar_wait(&full[gbase % S], (gbase / S) & 1, A.st, A.spin_limit)) return;
         const int t = slot_tile[gbase % S];
         if (t < 0) return;
         const int cx0 = (t % nbx) * BAND, y0 = (t / nbx) * TY;

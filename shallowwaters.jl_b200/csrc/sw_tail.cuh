@@ -21,7 +21,6 @@
 #include "sw_common.cuh"
 #include "sw_ghost.cuh"
 #include "sw_stage.cuh"
-#include "sw_tma.cuh"
 
 namespace swb {
 
@@ -238,265 +237,6 @@ template <class T, class Tp, bool PER, int DRAG, bool SMAG, int TY>
 __global__ void __launch_bounds__(128, SWB_TAIL_MINB)
 tail_kernel(TailArgs<T, Tp> A) {
     tail_body<T, Tp, PER, DRAG, SMAG, TY>(A, (int)blockIdx.x);
-}
-
-// ===========================================================================
-// TMA-fed tail.  Same arithmetic and order as tail_kernel; the rows of u0, v0
-// (and eta0 for quadratic drag) arrive through the producer/consumer pipeline
-// of rk_stage_tma (sw_stage.cuh): persistent blocks of 4 consumer warps (a
-// 112-column band) and 1 producer warp taking tiles of band x TY rows from the
-// shared tile counter and copying K-row chunks (120 columns: the band and a
-// 4-column halo each side) into a ring of S shared-memory slots.  A tile
-// needs rows y0-3 .. y0+TY+1; row q of the tile (q = y - (y0-3)) is row q%K of
-// chunk q/K.  With ROWH (H constant along x) lane k of each warp holds H at
-// row y0-3+k and the rows are broadcast by shuffles; otherwise H is loaded
-// per lane.  Float32 only (the tensor maps of the stage kernel).  Measured at
-// 2048x1024 it is slower than the streaming tail_kernel (41-48 us against
-// 37 us): the tail is bound by instruction latency, not by loads in flight,
-// so the runtime uses it only when asked (SWB200_TAIL_TMA=1).
-struct TailMaps {
-    CUtensorMap u, v, e;     // X0 u, v and eta0, box BOXW_IN x K
-};
-
-template <int K, int S, bool QUAD>
-struct TailSlot {
-    static constexpr int IN = (K * BOXW_IN + 31) / 32 * 32;          // region stride: 128-byte multiples
-    static constexpr int ELEMS = (QUAD ? 3 : 2) * IN;
-    static constexpr uint32_t BYTES = ELEMS * sizeof(float);
-    static constexpr uint32_t TX_BYTES = (QUAD ? 3 : 2) * K * BOXW_IN * sizeof(float);   // bytes copied
-    static constexpr int U = 0, V = IN, E = 2 * IN;
-    static_assert((IN * sizeof(float)) % 128 == 0, "TMA destinations need 128-B alignment");
-};
-
-template <int K, int S, bool QUAD>
-__host__ __device__ constexpr int tail_tma_smem() {
-    return S * TailSlot<K, S, QUAD>::BYTES + 2 * S * 8 + S * 4;
-}
-
-#ifndef SWB_TAIL_TMA_MINB
-#define SWB_TAIL_TMA_MINB 5
-#endif
-template <bool PER, int DRAG, bool SMAG, int TY, int K, int S, bool ROWH>
-__global__ void __launch_bounds__(160, SWB_TAIL_TMA_MINB)
-tail_tma(const __grid_constant__ TailArgs<float, float> A, const __grid_constant__ TailMaps MP, int npersist,
-         TileSched* sched) {
-    using T = float;
-    using Tp = float;
-    constexpr bool QUAD = (DRAG == SW_DRAG_QUADRATIC);
-    using SL = TailSlot<K, S, QUAD>;
-    constexpr int NCH = (TY + 5 + K - 1) / K;
-    static_assert(TY + 5 <= 32, "the tile's H rows must fit in one warp");
-    if ((int)blockIdx.x >= npersist) {
-        if (A.st->stop) return;
-        tail_ring(A, ((int)blockIdx.x - npersist) * 160 + threadIdx.x, ((int)gridDim.x - npersist) * 160);
-        return;
-    }
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    float* ring = reinterpret_cast<float*>(smem_raw);
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + S * SL::BYTES);
-    uint64_t* empty = full + S;
-    int* slot_tile = reinterpret_cast<int*>(empty + S);
-
-    const Geom& g = A.g;
-    const int N = g.N, M = g.M, P = g.P;
-    const int nbx = (N + BAND - 1) / BAND, nby = (M + TY - 1) / TY, ntiles = nbx * nby;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-
-    __shared__ int stop_flag;
-    if (threadIdx.x == 0) {
-        stop_flag = A.st->stop;
-        for (int s = 0; s < S; s++) {
-            mbar_init(&full[s], 1);
-            mbar_init(&empty[s], 4);
-        }
-        fence_mbar_init();
-    }
-    __syncthreads();
-    if (stop_flag) return;
-
-    if (warp == 4) {
-        // ------------------------------------------------------------ producer
-        if (lane != 0) return;
-        uint32_t gc = 0;
-        auto acquire = [&](int slot) { return gc < (uint32_t)S || mbar_wait(&empty[slot], ((gc / S) - 1) & 1, A.st); };
-        for (bool ok = true; ok;) {
-            const int t = atomicAdd(&sched->next, 1);
-            if (t >= ntiles) {
-                if (acquire(gc % S)) {
-                    slot_tile[gc % S] = -1;
-                    mbar_arrive(&full[gc % S]);
-                    gc++;
-                }
-                break;
-            }
-            const int cx0 = (t % nbx) * BAND, y0 = (t / nbx) * TY;
-            for (int j = 0; j < NCH; j++, gc++) {
-                const int slot = gc % S;
-                if (!acquire(slot)) { ok = false; break; }
-                slot_tile[slot] = t;
-                mbar_arrive_expect_tx(&full[slot], SL::TX_BYTES);
-                float* b = ring + slot * SL::ELEMS;
-                const int yd = y0 - 3 + j * K + ROW0;
-                tma_load_2d(b + SL::U, &MP.u, cx0, yd, &full[slot]);
-                tma_load_2d(b + SL::V, &MP.v, cx0, yd, &full[slot]);
-                if (QUAD) tma_load_2d(b + SL::E, &MP.e, cx0, yd, &full[slot]);
-            }
-        }
-        for (uint32_t q = (gc >= (uint32_t)S ? gc - S : 0); q < gc; q++) mbar_wait(&full[q % S], (q / S) & 1, A.st);
-        if (atomicAdd(&sched->done, 1) == npersist - 1) {
-            sched->next = 0;
-            sched->done = 0;
-        }
-        return;
-    }
-
-    // -------------------------------------------------------------- consumers
-    const T half = T(0.5), q4 = T(0.25);
-    const int sc_in = warp * STRIP + lane + 2;
-    const bool out_lane = lane >= 2 && lane < 2 + STRIP;
-    for (uint32_t gbase = 0;; gbase += NCH) {
-        if (!mbar_wait(&full[gbase % S], (gbase / S) & 1, A.st)) return;
-        const int t = slot_tile[gbase % S];
-        if (t < 0) return;
-        const int cx0 = (t % nbx) * BAND, y0 = (t / nbx) * TY;
-        const int c = cx0 + warp * STRIP + lane - 2;
-        const bool col_u = out_lane && c >= (PER ? 0 : 1) && c < N;
-        const bool col_a = out_lane && c >= 0 && c < N;
-        const bool gx_u = PER && (c <= 1 || c >= N - 2);
-        const bool gx_v = c <= 1 || c >= N - 2;
-        const int cb = c + COL0;
-        auto ofs = [&](int y) { return (y + ROW0) * P + cb; };
-        auto row_ptr = [&](int q) { return ring + ((gbase + q / K) % S) * SL::ELEMS + (q % K) * BOXW_IN + sc_in; };
-        auto release = [&](int j) {
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&empty[(gbase + j) % S]);
-        };
-        // H rows y0-3 .. y0+TY+1
-        T tH = T(0);
-        if (QUAD && ROWH) tH = A.H.p[(y0 - 3 + (lane < TY + 5 ? lane : TY + 4) + ROW0) * A.H.sy];
-        auto Hrow = [&](int q, int y) { return ROWH ? __shfl_sync(0xffffffffu, tH, q) : A.H.at(c, y); };
-        auto ldrow = [&](int q, T& uu, T& vv, T& hh) {
-            const float* pr = row_ptr(q);
-            uu = pr[SL::U];
-            vv = pr[SL::V];
-            hh = QUAD ? pr[SL::E] + Hrow(q, y0 - 3 + q) : T(0);
-        };
-        int r = y0 - 3;
-        T u_r, v_r, h_r, u_r1, v_r1, h_r1, u_r2, v_r2, h_r2;
-        ldrow(0, u_r, v_r, h_r);
-        ldrow(1, u_r1, v_r1, h_r1);
-        ldrow(2, u_r2, v_r2, h_r2);
-        T ul_r1 = shup(u_r1), ur_r1 = shdn(u_r1), vl_r1 = shup(v_r1), vr_r1 = shdn(v_r1), hl_r1 = shup(h_r1);
-        T hl_r = shup(h_r);
-        T h_rm1 = T(0);
-        T DSq_r1 = T(0), DSqR_r1 = T(0);
-        T nu_r = T(0), nul_r = T(0);
-        T Lu_r = T(0), Lv_r = T(0);
-        T S11_r = T(0), S11l_r = T(0), S12_r = T(0), S21_r = T(0), S21r_r = T(0), S22_rm1 = T(0);
-        T sKE_rm1 = T(0), sKE_r = T(0), sKEl_r = T(0);
-        int nrel = 0;
-
-#pragma unroll 1
-        for (int i = 0; i < TY + 3; i++, r++) {
-            if (i > 0) {
-                const int q = i + 2;                       // the tile's new row
-                if (q % K == 0 && !mbar_wait(&full[(gbase + q / K) % S], ((gbase + q / K) / S) & 1, A.st)) return;
-                ldrow(q, u_r2, v_r2, h_r2);
-            }
-            const T ul_r2 = shup(u_r2), ur_r2 = shdn(u_r2), vl_r2 = shup(v_r2), vr_r2 = shdn(v_r2);
-            const T hl_r2 = QUAD ? shup(h_r2) : T(0);
-            const bool out_row = r >= y0 && r < M;
-            const Tp U0 = u_r, V0 = v_r;
-
-            T Lu_r1, Lv_r1;
-            {
-                T cc = u_r1;
-                Lu_r1 = ((ul_r1 - cc) + (ur_r1 - cc)) + ((u_r - cc) + (u_r2 - cc));
-                cc = v_r1;
-                Lv_r1 = ((vl_r1 - cc) + (vr_r1 - cc)) + ((v_r - cc) + (v_r2 - cc));
-            }
-            const T Lur_r1 = shdn(Lu_r1), Lvl_r1 = shup(Lv_r1);
-            T nu_r1, nuq_r1;
-            if (SMAG) {
-                T sd = (u_r2 - u_r1) + (v_r2 - vl_r2);
-                const T DSq_r2 = sd * sd;
-                const T DSqR_r2 = shdn(DSq_r2);
-                const T DS = q4 * (DSq_r1 + DSqR_r1) + q4 * (DSq_r2 + DSqR_r2);
-                sd = (ur_r1 - u_r1) + (v_r2 - v_r1);
-                const T DT = sd * sd;
-                nu_r1 = A.cSmag * sqrt(DS + DT);
-                const T nul_r1 = shup(nu_r1);
-                nuq_r1 = q4 * (nul_r + nu_r) + q4 * (nul_r1 + nu_r1);
-                DSq_r1 = DSq_r2; DSqR_r1 = DSqR_r2;
-                nul_r = nul_r1;
-            } else {
-                nu_r1 = A.nuB;
-                nuq_r1 = A.nuB;
-            }
-            const T S11_r1 = nu_r1 * (Lur_r1 - Lu_r1);
-            const T S11l_r1 = shup(S11_r1);
-            const T S12_r1 = nuq_r1 * (Lu_r1 - Lu_r);
-            const T S21_r1 = nuq_r1 * (Lv_r1 - Lvl_r1);
-            const T S21r_r1 = shdn(S21_r1);
-            const T S22_r = nu_r * (Lv_r1 - Lv_r);
-            T sKE_r1 = T(0), sKEl_r1 = T(0);
-            if (QUAD) {
-                const T KEu = half * (ur_r1 * ur_r1 + u_r1 * u_r1);
-                const T KEv = half * (v_r2 * v_r2 + v_r1 * v_r1);
-                sKE_r1 = sqrt(KEu + KEv);
-                sKEl_r1 = shup(sKE_r1);
-            }
-            if (out_row) {
-                if (col_u) {
-                    T Bu;
-                    if (QUAD) {
-                        const T ke = half * (sKE_r + sKEl_r);
-                        const T hu = half * (h_r + hl_r);
-                        Bu = A.cD * ke * u_r / hu;
-                    } else if (DRAG == SW_DRAG_LINEAR) {
-                        Bu = A.rD * u_r;
-                    } else {
-                        Bu = T(0);
-                    }
-                    const T LLu1 = S11_r - S11l_r;
-                    const T LLu2 = S12_r1 - S12_r;
-                    const Tp val = U0 + A.Dt_diff * (cvt<Tp>(Bu) + cvt<Tp>(LLu1) + cvt<Tp>(LLu2));
-                    A.uo[ofs(r)] = val;
-                    if (gx_u || (!PER && (r <= 1 || r >= M - 2))) A.gr.u(A.uo, g, c, r, val);
-                }
-                if (col_a && r >= 1) {
-                    T Bv;
-                    if (QUAD) {
-                        const T ke = half * (sKE_r + sKE_rm1);
-                        const T hv = half * (h_r + h_rm1);
-                        Bv = A.cD * ke * v_r / hv;
-                    } else if (DRAG == SW_DRAG_LINEAR) {
-                        Bv = A.rD * v_r;
-                    } else {
-                        Bv = T(0);
-                    }
-                    const T LLv1 = S21r_r - S21_r;
-                    const T LLv2 = S22_r - S22_rm1;
-                    const Tp val = V0 + A.Dt_diff * (cvt<Tp>(Bv) + cvt<Tp>(LLv1) + cvt<Tp>(LLv2));
-                    A.vo[ofs(r)] = val;
-                    if (gx_v) A.gr.v(A.vo, g, c, r, val);
-                }
-            }
-            // chunk j is done once its last row has been read
-            if ((i + 2) % K == K - 1) { release((i + 2) / K); nrel++; }
-
-            h_rm1 = h_r;
-            u_r = u_r1; v_r = v_r1; h_r = h_r1; hl_r = hl_r1;
-            u_r1 = u_r2; v_r1 = v_r2; h_r1 = h_r2; hl_r1 = hl_r2;
-            ul_r1 = ul_r2; ur_r1 = ur_r2; vl_r1 = vl_r2; vr_r1 = vr_r2;
-            nu_r = nu_r1;
-            Lu_r = Lu_r1; Lv_r = Lv_r1;
-            S11_r = S11_r1; S11l_r = S11l_r1; S12_r = S12_r1; S21_r = S21_r1; S21r_r = S21r_r1;
-            S22_rm1 = S22_r;
-            sKE_rm1 = sKE_r; sKE_r = sKE_r1; sKEl_r = sKEl_r1;
-        }
-        for (int j = nrel; j < NCH; j++) release(j);
-    }
 }
 
 }  // namespace swb

@@ -14,7 +14,8 @@
 namespace swb {
 
 // polls of a bounded mbarrier wait (each poll suspends in hardware, then
-// sleeps briefly): well above any real wait, well below a hang
+// sleeps briefly): well above any real wait, well below a hang.  Kernels take
+// the limit as an argument (this is the default), so a test can shorten it.
 constexpr uint32_t MBAR_SPIN_LIMIT = 1u << 22;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -52,10 +53,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait for the phase with the given parity to complete.  Returns
-// false (and records a timeout) if it does not.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, DevStatus* st) {
-    for (uint32_t it = 0; it < MBAR_SPIN_LIMIT; ++it) {
+// Bounded wait for the phase with the given parity to complete, at most
+// `limit` polls.  Returns false (and records a timeout) if it does not.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, DevStatus* st, uint32_t limit) {
+    for (uint32_t it = 0; it < limit; ++it) {
         if (mbar_try_wait(bar, parity)) return true;
         if (it > 16) __nanosleep(64);
     }

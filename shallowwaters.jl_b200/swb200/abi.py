@@ -176,7 +176,12 @@ def state_ptrs(u, v, η, sst):
 
 _PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB_PATH = os.environ.get("SWB200_LIB", os.path.join(_PKG_DIR, "libswb200.so"))
-_lib = None
+# the two builds of the same sources: "parity" (no FMA contraction, bit-exact
+# with the reference's arithmetic) and "fast" (FMA contraction, equal to
+# rounding); see include/swb200.h sw_build_kind
+BUILDS = {"parity": LIB_PATH, "fast": os.path.join(_PKG_DIR, "libswb200_fast.so")}
+SW_BUILD_PARITY, SW_BUILD_FAST = 0, 1
+_libs = {}
 
 EXPORTS = {
     "sw_time_integration": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -207,17 +212,20 @@ EXPORTS = {
     "sw_strerror": (C.c_char_p, [C.c_int]),
     "sw_last_error": (C.c_char_p, [C.c_void_p]),
     "sw_abi_version": (C.c_int, []),
+    "sw_build_kind": (C.c_int, []),
 }
 
 
-def load_library(path: str | None = None):
-    """Load libswb200.so; raises if it is missing (there is no CPU fallback)."""
-    global _lib
-    if _lib is not None and path is None:
-        return _lib
-    p = path or LIB_PATH
+def load_library(path: str | None = None, build: str = "parity"):
+    """Load libswb200.so (build="parity") or libswb200_fast.so (build="fast");
+    raises if it is missing (there is no CPU fallback)."""
+    if path is None and build in _libs:
+        return _libs[build]
+    if build not in BUILDS:
+        raise ValueError(f"build must be one of {sorted(BUILDS)}")
+    p = path or BUILDS[build]
     if not os.path.exists(p):
-        raise RuntimeError(f"libswb200.so not found at {p}; build it with "
+        raise RuntimeError(f"{os.path.basename(p)} not found at {p}; build it with "
                            f"`python __graft_entry__.py` or `make -C shallowwaters.jl_b200/csrc`")
     lib = C.CDLL(p)
     for name, (res, args) in EXPORTS.items():
@@ -227,7 +235,10 @@ def load_library(path: str | None = None):
     if lib.sw_abi_version() != ABI_VERSION:
         raise RuntimeError(f"libswb200 ABI {lib.sw_abi_version()} != {ABI_VERSION}")
     if path is None:
-        _lib = lib
+        want = SW_BUILD_FAST if build == "fast" else SW_BUILD_PARITY
+        if lib.sw_build_kind() != want:
+            raise RuntimeError(f"{p} is not the {build} build")
+        _libs[build] = lib
     return lib
 
 

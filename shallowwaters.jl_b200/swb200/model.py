@@ -17,8 +17,10 @@ from .model_setup import ModelSetup
 
 
 class Model:
-    def __init__(self, S: ModelSetup, *, storage="native", storage_scale_uv=1024.0, lib=None):
-        self.lib = lib or abi.load_library()
+    def __init__(self, S: ModelSetup, *, storage="native", storage_scale_uv=1024.0, build="parity", lib=None):
+        """build: "parity" (libswb200.so, bit-exact with the reference's
+        arithmetic) or "fast" (libswb200_fast.so, FMA contraction)."""
+        self.lib = lib or abi.load_library(build=build)
         self.S = S
         self.cfg = abi.make_config(S, storage=storage, storage_scale_uv=storage_scale_uv)
         self.static = abi.StaticFields(S)

@@ -25,7 +25,7 @@ class NaNsDetected(RuntimeError):
 
 
 def time_integration(Prog: PrognosticVars, S: ModelSetup, *, nt=None, storage="native",
-                     storage_scale_uv=1024.0, lib=None):
+                     storage_scale_uv=1024.0, build="parity", lib=None):
     """Drop-in for time_integration(Prog, Diag, S) (src/time_integration.jl:2-250).
 
     Runs on the GPU through ``sw_time_integration``.  Returns
@@ -33,7 +33,7 @@ def time_integration(Prog: PrognosticVars, S: ModelSetup, *, nt=None, storage="n
     is the one the reference returns (u, v, η before the failing step) and
     ``status.code == SW_NAN_DETECTED``.
     """
-    lib = lib or abi.load_library()
+    lib = lib or abi.load_library(build=build)
     cfg = abi.make_config(S, nt=nt, storage=storage, storage_scale_uv=storage_scale_uv)
     st = abi.StaticFields(S)
     Tp = S.parameters.Tprog

@@ -34,6 +34,16 @@ def test_library_loads_and_exports_every_declared_symbol():
     assert lib.sw_strerror(3) == b"NaNs detected"
 
 
+@pytest.mark.parametrize("build,kind", [("parity", abi.SW_BUILD_PARITY), ("fast", abi.SW_BUILD_FAST)])
+def test_both_builds_load_and_export_every_declared_symbol(build, kind):
+    """libswb200.so (no FMA contraction) and libswb200_fast.so export the same
+    ABI and say which build they are."""
+    lib = abi.load_library(build=build)
+    for n in declared_functions():
+        assert hasattr(lib, n), f"{n} missing from the {build} build"
+    assert lib.sw_build_kind() == kind
+
+
 def test_python_mirror_covers_exports():
     assert set(declared_functions()) <= set(abi.EXPORTS)
 

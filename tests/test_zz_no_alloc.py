@@ -53,11 +53,18 @@ def _model(kw, seed, nsteps):
     return S, m
 
 
-def test_noalloc_diagnostics_match_sw_diagnostics_on_two_calls():
+TYPES = {"f32": dict(T=np.float32), "f64": dict(T=np.float64), "f32_f64": dict(T=np.float32, Tprog=np.float64)}
+
+
+@pytest.mark.parametrize("types", list(TYPES))
+def test_noalloc_diagnostics_match_sw_diagnostics_on_two_calls(types):
+    """Each (T, Tprog) pair the entry point takes: 4- and 8-byte state and
+    depth, and the mixed pair whose depth and state have different sizes."""
     lib = abi.load_library()
+    tk = TYPES[types]
 
     # call 1: 200x100 periodic channel, three partial blocks of scratch
-    S1, m1 = _model(dict(nx=200, Ndays=0.2, Uadv=1000), seed=11, nsteps=15)
+    S1, m1 = _model(dict(nx=200, Ndays=0.2, Uadv=1000, **tk), seed=11, nsteps=15)
     ref1 = m1.diagnostics()
     rc, d1 = _noalloc(lib, S1, m1.get_state())
     assert rc == abi.SW_OK
@@ -67,7 +74,7 @@ def test_noalloc_diagnostics_match_sw_diagnostics_on_two_calls():
 
     # call 2: 40x20 nonperiodic seamount (one block) with two NaNs planted in
     # the tracer, read back through the library so both paths see the same state
-    S2, m2 = _model(dict(nx=40, Ndays=0.2, Uadv=1000, bc="nonperiodic", topography="seamount"), seed=12,
+    S2, m2 = _model(dict(nx=40, Ndays=0.2, Uadv=1000, bc="nonperiodic", topography="seamount", **tk), seed=12,
                     nsteps=9)
     st = m2.get_state()
     sst = st.sst.copy()
