@@ -825,7 +825,12 @@ struct Engine : EngineBase {
             if ((i % c.nadvstep) == 0) {
                 TracerArgs<T, Tp> a = tracer_args(ctx, ctx->p, ctx->sp);
                 const bool um_is_u = (c.nadvstep == 1);
-                dim3 grid((g.N + 127) / 128, std::min(g.M, 4096));
+                // each thread takes rows b, b + gy, ...: up to 8 rows on grids
+                // large enough to fill the GPU without it, so the per-thread
+                // set-up is shared by several cells
+                const long long want = (long long)ctx->nsm * 2048;
+                const int rpt = (int)std::max(1LL, std::min(8LL, (long long)g.N * g.M / want));
+                dim3 grid((g.N + 127) / 128, std::min((g.M + rpt - 1) / rpt, 4096));
                 int rc = launch(ctx, 2, [&] {
                     if (g.ep) tracer_dispatch2<true>(a, um_is_u, c.tracer_consumption != 0, grid, ctx->stream);
                     else tracer_dispatch2<false>(a, um_is_u, c.tracer_consumption != 0, grid, ctx->stream);

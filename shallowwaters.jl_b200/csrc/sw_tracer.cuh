@@ -30,11 +30,15 @@ struct TracerArgs {
     DevStatus* st;
 };
 
-// Julia's Int(floor(x)); NaN, Inf and indices no array can take are flagged
+// Julia's Int(floor(x)); NaN, Inf and indices no array can take are flagged.
+// Within the range the conversion rounds toward -inf in one instruction.
+__device__ __forceinline__ int floor_to_int(float x) { return __float2int_rd(x); }
+__device__ __forceinline__ int floor_to_int(double x) { return __double2int_rd(x); }
+__device__ __forceinline__ int floor_to_int(jf16 x) { return (int)floorf(float(x)); }
 template <class T>
 __device__ __forceinline__ int ifloor(T x, int& bad) {
     if (!(fabs(x) < T(1.0e9))) { bad = 1; return 0; }
-    return (int)floor(x);
+    return floor_to_int(x);
 }
 
 // bilin (src/tracer_advection.jl:243-246)
@@ -79,11 +83,18 @@ __device__ __forceinline__ void tracer_body(const TracerArgs<T, Tp>& A, int bx, 
     const bool gx = a == 0 || a == N - 1;
     // element (x, y) of a field sits at (y + ROW0) * P + x + COL0
     auto at = [&](int x, int y) { return (y + ROW0) * P + x + COL0; };
+    // the output never aliases the inputs: loads of later rows may be issued early
+    const Tp* __restrict__ pu = A.u;
+    const Tp* __restrict__ pv = A.v;
+    const T* __restrict__ pum = A.um;
+    const T* __restrict__ pvm = A.vm;
+    const Tp* __restrict__ psst = A.sst;
+    Tp* __restrict__ psst_o = A.sst_o;
     for (int b = by; b < M; b += gy) {
         // departure!: u_T = Ix!(u), v_T = Iy!(v); backtraj! at half step (:75-76, :96-124)
         const int o = at(a, b);
-        const T uT = half * (cvt<T>(A.u[o + 1]) + cvt<T>(A.u[o]));
-        const T vT = half * (cvt<T>(A.v[o + P]) + cvt<T>(A.v[o]));
+        const T uT = half * (cvt<T>(pu[o + 1]) + cvt<T>(pu[o]));
+        const T vT = half * (cvt<T>(pv[o + P]) + cvt<T>(pv[o]));
         T xd = (-A.half_dtadvu) * uT;
         T yd = (-A.half_dtadvv) * vT;
         int xi = ifloor(xd, bad), yi = ifloor(yd, bad);
@@ -96,11 +107,11 @@ __device__ __forceinline__ void tracer_body(const TracerArgs<T, Tp>& A, int bx, 
             const int k = at(F0, b0);
             T m00, m10, m20, m01, m11, m21;
             if (UM_IS_U) {
-                m00 = cvt<T>(A.u[k]); m10 = cvt<T>(A.u[k + 1]); m20 = cvt<T>(A.u[k + 2]);
-                m01 = cvt<T>(A.u[k + P]); m11 = cvt<T>(A.u[k + P + 1]); m21 = cvt<T>(A.u[k + P + 2]);
+                m00 = cvt<T>(pu[k]); m10 = cvt<T>(pu[k + 1]); m20 = cvt<T>(pu[k + 2]);
+                m01 = cvt<T>(pu[k + P]); m11 = cvt<T>(pu[k + P + 1]); m21 = cvt<T>(pu[k + P + 2]);
             } else {
-                m00 = A.um[k]; m10 = A.um[k + 1]; m20 = A.um[k + 2];
-                m01 = A.um[k + P]; m11 = A.um[k + P + 1]; m21 = A.um[k + P + 2];
+                m00 = pum[k]; m10 = pum[k + 1]; m20 = pum[k + 2];
+                m01 = pum[k + P]; m11 = pum[k + P + 1]; m21 = pum[k + P + 2];
             }
             ui = bilin(half * (m10 + m00), half * (m20 + m10), half * (m11 + m01), half * (m21 + m11), x0, y0);
         }
@@ -112,11 +123,11 @@ __device__ __forceinline__ void tracer_body(const TracerArgs<T, Tp>& A, int bx, 
             const int k = at(a0, G0);
             T m00, m01, m02, m10, m11, m12;
             if (UM_IS_U) {
-                m00 = cvt<T>(A.v[k]); m01 = cvt<T>(A.v[k + P]); m02 = cvt<T>(A.v[k + 2 * P]);
-                m10 = cvt<T>(A.v[k + 1]); m11 = cvt<T>(A.v[k + P + 1]); m12 = cvt<T>(A.v[k + 2 * P + 1]);
+                m00 = cvt<T>(pv[k]); m01 = cvt<T>(pv[k + P]); m02 = cvt<T>(pv[k + 2 * P]);
+                m10 = cvt<T>(pv[k + 1]); m11 = cvt<T>(pv[k + P + 1]); m12 = cvt<T>(pv[k + 2 * P + 1]);
             } else {
-                m00 = A.vm[k]; m01 = A.vm[k + P]; m02 = A.vm[k + 2 * P];
-                m10 = A.vm[k + 1]; m11 = A.vm[k + P + 1]; m12 = A.vm[k + 2 * P + 1];
+                m00 = pvm[k]; m01 = pvm[k + P]; m02 = pvm[k + 2 * P];
+                m10 = pvm[k + 1]; m11 = pvm[k + P + 1]; m12 = pvm[k + 2 * P + 1];
             }
             vi = bilin(half * (m01 + m00), half * (m11 + m10), half * (m02 + m01), half * (m12 + m11), x0, y0);
         }
@@ -132,12 +143,12 @@ __device__ __forceinline__ void tracer_body(const TracerArgs<T, Tp>& A, int bx, 
             const int b0 = axis<T, false>(yi + b, yi, yd, 0, M - 2, 0, y0);
             if (a0 < -1 || a0 > N - 1) { bad = 1; a0 = 0; }
             const int k = at(a0, b0);
-            s = bilin(cvt<T>(A.sst[k]), cvt<T>(A.sst[k + 1]), cvt<T>(A.sst[k + P]), cvt<T>(A.sst[k + P + 1]), x0, y0);
+            s = bilin(cvt<T>(psst[k]), cvt<T>(psst[k + 1]), cvt<T>(psst[k + P]), cvt<T>(psst[k + P + 1]), x0, y0);
         }
         if (CONS) s += A.jSST * (A.SSTmin - s);              // tracer_consumption! (:262-275)
         const Tp out = cvt<Tp>(s);
-        A.sst_o[o] = out;
-        if (gx) A.gr.sst(A.sst_o, g, a, b, out);             // ghost_points_sst! (:40)
+        psst_o[o] = out;
+        if (gx) A.gr.sst(psst_o, g, a, b, out);             // ghost_points_sst! (:40)
     }
     if (bad) {   // the reference throws here; halt the device-side loop
         atomicCAS(&A.st->error, 0, (int)SW_ERR_DEPARTURE);
