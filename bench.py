@@ -41,6 +41,26 @@ L2_FLUSH = 256 << 20
 # writes X0 (44 B)
 STAGE_BYTES_PER_CELL = (44 + 68 + 68 + 44) / 4
 STEP_BYTES_PER_CELL = 264
+# the 16-bit storage form (scaled 16-bit state pairs, stage values and
+# increments; FP32 X0 after the last stage): stage 1 reads the state's hi and
+# writes X1 and D (26 B with H, Fx), stages 2-3 read X1, hi, D and write X1, D
+# (38 B), stage 4 reads X1, hi, lo, D and writes the FP32 X0 and eta's new pair
+# (48 B); the tail reads X0 (u, v, eta) and H and writes the u, v pairs (24 B);
+# the tracer reads u, v (hi) and sst and writes sst (8 B)
+STAGE_BYTES_PER_CELL_16 = (26 + 38 + 38 + 48) / 4
+STEP_BYTES_PER_CELL_16 = 182
+
+
+def packed_static_bytes(static):
+    """Bytes the library uploads for the static fields: a field constant along
+    x or y (or both) is stored as one row, one column or one value."""
+    total = 0
+    for a in static.arrays.values():
+        a = np.asarray(a)
+        cx = bool(np.all(a == a[:, :1]))
+        cy = bool(np.all(a == a[:1, :]))
+        total += a.itemsize * (1 if cx and cy else a.shape[0] if cx else a.shape[1] if cy else a.size)
+    return total
 
 
 def workload_params(nx=2048, seed=1234):
@@ -261,6 +281,7 @@ def main():
     ap.add_argument("--nx", type=int, default=2048)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="time only --form/--build, not the other forms")
     ap.add_argument("--workload", default="channel", choices=["channel", "ensemble", "adjoint"],
                     help="channel: the 2048x1024 headline run; ensemble: seeded members of uneven size; "
                          "adjoint: the gradient of the 512x256 twin experiment")
@@ -357,33 +378,55 @@ def main():
     clk = ClockSampler(dev_uuid)
     clk.start()
     clk.wait_first(10.0)
-    m = Model(S, storage=storage, build=args.build)
-    m.set_state(Prog)
-    m.run(args.warmup)
 
-    barrier()
-    n0 = m.kernel_launches
-    step_ms, st = m.run_timed(args.steps, L2_FLUSH)
-    launches = m.kernel_launches - n0
-    barrier()
-    if st.code != 0:
-        raise SystemExit(f"run failed with code {st.code}")
-    t_dev = allmax(step_ms) / 1e3
-    # per-kernel device times: a second, shorter run with an event pair around
-    # every launch (no graphs), used for the kernel shares and the roofline
-    prof, st = m.run_profiled(min(args.steps, 200), L2_FLUSH)
-    if st.code != 0:
-        raise SystemExit(f"profiled run failed with code {st.code}")
-    value = args.gpus * cells * args.steps / t_dev
-    stage_ms = prof.kernel_ms[0] / max(prof.launches[0], 1)
-    stage_ms = allmax(stage_ms)
-    achieved = STAGE_BYTES_PER_CELL * cells / (stage_ms / 1e3) / 1e9
+    def time_form(storage, build):
+        """Device time of args.steps steps (L2 flushed between steps), then a
+        profiled pass for the per-kernel times; returns a dict."""
+        m = Model(S, storage=storage, build=build)
+        m.set_state(Prog)
+        m.run(args.warmup)
+        barrier()
+        n0 = m.kernel_launches
+        step_ms, st = m.run_timed(args.steps, L2_FLUSH)
+        launches = m.kernel_launches - n0
+        barrier()
+        if st.code != 0:
+            raise SystemExit(f"run failed with code {st.code}")
+        t_dev = allmax(step_ms) / 1e3
+        # per-kernel device times: a second, shorter run with an event pair
+        # around every launch (no graphs), for the kernel shares and the roofline
+        prof, st = m.run_profiled(min(args.steps, 200), L2_FLUSH)
+        if st.code != 0:
+            raise SystemExit(f"profiled run failed with code {st.code}")
+        m.close()
+        stage_ms = allmax(prof.kernel_ms[0] / max(prof.launches[0], 1))
+        kernels = {abi.PROFILE_NAMES[k]: {"launches": int(prof.launches[k]),
+                                          "avg_us": 1e3 * prof.kernel_ms[k] / prof.launches[k],
+                                          "share": prof.kernel_ms[k] / max(sum(prof.kernel_ms), 1e-12)}
+                   for k in range(abi.PROFILE_KINDS) if prof.launches[k]}
+        return {"t_dev": t_dev, "value": args.gpus * cells * args.steps / t_dev, "stage_ms": stage_ms,
+                "kernels": kernels, "launches": launches}
+
+    main = time_form(storage, args.build)
+    t_dev, value, kernels, launches = main["t_dev"], main["value"], main["kernels"], main["launches"]
+    stage_bytes = STAGE_BYTES_PER_CELL if storage == "native" else STAGE_BYTES_PER_CELL_16
+    step_bytes = STEP_BYTES_PER_CELL if storage == "native" else STEP_BYTES_PER_CELL_16
+    achieved = stage_bytes * cells / (main["stage_ms"] / 1e3) / 1e9
     peak, peak_kind = peaks()
-    kernels = {abi.PROFILE_NAMES[k]: {"launches": int(prof.launches[k]),
-                                      "avg_us": 1e3 * prof.kernel_ms[k] / prof.launches[k],
-                                      "share": prof.kernel_ms[k] / max(sum(prof.kernel_ms), 1e-12)}
-               for k in range(abi.PROFILE_KINDS) if prof.launches[k]}
-    m.close()
+    # the other forms of the metric on the same workload: the FMA build, and
+    # the 16-bit storage forms (their error against Float64 is in the precision
+    # study); each with its device time per step and ratio to this line's value
+    others = {}
+    if storage == "native" and not args.no_forms:
+        for name, (stg, bld) in {"fp32_fast_build": ("native", "fast"), "bf16": ("bf16", args.build),
+                                 "f16": ("f16", args.build)}.items():
+            if bld == args.build and stg == storage:
+                continue
+            r = time_form(stg, bld)
+            others[name] = {"value": r["value"], "ratio_to_value": r["value"] / value,
+                            "ms_per_step": 1e3 * r["t_dev"] / args.steps,
+                            "bytes_per_cell_step": STEP_BYTES_PER_CELL if stg == "native" else STEP_BYTES_PER_CELL_16,
+                            "kernels_us": {k: round(v["avg_us"], 2) for k, v in r["kernels"].items()}}
 
     # e2e: drop-in call with pinned host buffers (create, upload, run, download)
     from swb200 import time_integration  # noqa: F401
@@ -415,11 +458,30 @@ def main():
     t_e2e = allmax(statistics.median(e2e_call(cfg) for _ in range(3)))
     clk.stop()
     state_bytes = sum(a.nbytes for a in pinned)
-    static_bytes = sum(a.nbytes for a in static.arrays.values())
+    static_bytes = packed_static_bytes(static)
+    # the same call's phases, timed through the context API on the same pinned
+    # buffers: upload (with the state's ghost points), steps, download
+    phases = {}
+    with Model(S, storage=storage, build=args.build) as mp:
+        for _ in range(2):
+            barrier()
+            t0 = time.perf_counter()
+            mp.set_state(type(Prog)(*pinned))
+            t1 = time.perf_counter()
+            mp.run(args.steps)
+            t2 = time.perf_counter()
+            rc = mp.lib.sw_get_state(mp.ctx, *abi.state_ptrs(*pinned))
+            t3 = time.perf_counter()
+            if rc != 0:
+                raise SystemExit(f"sw_get_state failed: {rc}")
+        phases = {"set_state_ms": 1e3 * (t1 - t0), "run_ms": 1e3 * (t2 - t1), "get_state_ms": 1e3 * (t3 - t2)}
     e2e = {"value": args.gpus * cells * args.steps / t_e2e, "unit": UNIT,
            "h2d_bytes_per_step": (state_bytes + static_bytes) / args.steps,
            "d2h_bytes_per_step": state_bytes / args.steps,
-           "call": "sw_time_integration (create + upload + run + download + destroy), median of 3 after 1 warm-up call"}
+           "call": "sw_time_integration with pinned host buffers: static fields packed and uploaded, state "
+                   "uploaded, K steps, state downloaded; the context of the warm-up call is reused "
+                   "(median of 3 after 1 warm-up call)",
+           "call_ms": 1e3 * t_e2e, "phases_context_api": phases}
 
     cpu = None
     if rank == 0 and args.gpus == 1 and not args.no_cpu:
@@ -435,12 +497,15 @@ def main():
             "value": value, "ms_per_step": 1e3 * t_dev / args.steps,
             "e2e": e2e,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": ncu_traffic(cells),
-                         "kernel": "rk_stage_tma", "bytes_per_cell": STAGE_BYTES_PER_CELL,
+                         "frac": achieved / peak, "traffic": ncu_traffic(cells) if storage == "native" else None,
+                         "kernel": "rk_stage_tma" if storage == "native" else "s16_stage_kernel",
+                         "bytes_per_cell": stage_bytes,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                          else "fallback 6.65 TB/s"},
-            "step_roofline": {"bytes_per_cell_step": STEP_BYTES_PER_CELL,
-                              "achieved_gbs": STEP_BYTES_PER_CELL * cells * args.steps / t_dev / 1e9 / args.gpus},
+            "step_roofline": {"bytes_per_cell_step": step_bytes,
+                              "achieved_gbs": step_bytes * cells * args.steps / t_dev / 1e9 / args.gpus,
+                              "frac": step_bytes * cells * args.steps / t_dev / 1e9 / args.gpus / peak},
+            "other_forms": others,
             "kernels": kernels,
             "cpu_baseline": cpu,
             "gpu_launches": int(launches),

@@ -30,36 +30,47 @@ struct GhostRule {
     // periodic  u[1]=u[end-3], u[2]=u[end-2], u[end-1]=u[3], u[end]=u[4]  (:64-69)
     // nonperiodic u[:,1]=(1-α)u[:,4], u[:,2]=(1-α)u[:,3], u[:,end-1]=(1-α)u[:,end-2],
     //             u[:,end]=(1-α)u[:,end-3]                                 (:51-56)
-    __device__ inline void u(Tp* __restrict__ dst, const Geom& g, int F, int b, Tp val) const {
+    // Each rule has a form for arrays of another element type D: put(x)
+    // converts the Tp value written there (the 16-bit storage form).
+    template <class D, class Put>
+    __device__ inline void u(D* __restrict__ dst, const Geom& g, int F, int b, Tp val, Put put) const {
         if (ep) {
             Tp c = comm(val);
-            if (F == 0 || F == 1) dst[g.idx(F + N, b)] = c;
-            if (F == N - 2 || F == N - 1) dst[g.idx(F - N, b)] = c;
+            if (F == 0 || F == 1) dst[g.idx(F + N, b)] = put(c);
+            if (F == N - 2 || F == N - 1) dst[g.idx(F - N, b)] = put(c);
         } else {
             Tp c = oma * val;
-            if (b == 0) dst[g.idx(F, -1)] = c;
-            if (b == 1) dst[g.idx(F, -2)] = c;
-            if (b == M - 1) dst[g.idx(F, M)] = c;
-            if (b == M - 2) dst[g.idx(F, M + 1)] = c;
+            if (b == 0) dst[g.idx(F, -1)] = put(c);
+            if (b == 1) dst[g.idx(F, -2)] = put(c);
+            if (b == M - 1) dst[g.idx(F, M)] = put(c);
+            if (b == M - 2) dst[g.idx(F, M + 1)] = put(c);
         }
     }
+    __device__ inline void u(Tp* __restrict__ dst, const Geom& g, int F, int b, Tp val) const {
+        u(dst, g, F, b, val, Same{});
+    }
     // v at (a, G): periodic x copies (:93-98); nonperiodic (1-α) mirror in x (:80-85)
-    __device__ inline void v(Tp* __restrict__ dst, const Geom& g, int a, int G, Tp val) const {
+    template <class D, class Put>
+    __device__ inline void v(D* __restrict__ dst, const Geom& g, int a, int G, Tp val, Put put) const {
         if (ep) {
             Tp c = comm(val);
-            if (a == 0 || a == 1) dst[g.idx(a + N, G)] = c;
-            if (a == N - 2 || a == N - 1) dst[g.idx(a - N, G)] = c;
+            if (a == 0 || a == 1) dst[g.idx(a + N, G)] = put(c);
+            if (a == N - 2 || a == N - 1) dst[g.idx(a - N, G)] = put(c);
         } else {
             Tp c = oma * val;
-            if (a == 0) dst[g.idx(-1, G)] = c;
-            if (a == 1) dst[g.idx(-2, G)] = c;
-            if (a == N - 1) dst[g.idx(N, G)] = c;
-            if (a == N - 2) dst[g.idx(N + 1, G)] = c;
+            if (a == 0) dst[g.idx(-1, G)] = put(c);
+            if (a == 1) dst[g.idx(-2, G)] = put(c);
+            if (a == N - 1) dst[g.idx(N, G)] = put(c);
+            if (a == N - 2) dst[g.idx(N + 1, G)] = put(c);
         }
+    }
+    __device__ inline void v(Tp* __restrict__ dst, const Geom& g, int a, int G, Tp val) const {
+        v(dst, g, a, G, val, Same{});
     }
     // eta at (a, b): columns first, then rows over all columns, so the corners
     // take the column-copied value (src/ghost_points.jl:102-133)
-    __device__ inline void eta(Tp* __restrict__ dst, const Geom& g, int a, int b, Tp val) const {
+    template <class D, class Put>
+    __device__ inline void eta(D* __restrict__ dst, const Geom& g, int a, int b, Tp val, Put put) const {
         int xs[2], nx = 0;
         Tp cx = ep ? comm(val) : val;
         if (ep) {
@@ -69,28 +80,38 @@ struct GhostRule {
             if (a == 0) xs[nx++] = -1;
             if (a == N - 1) xs[nx++] = N;
         }
-        for (int k = 0; k < nx; k++) dst[g.idx(xs[k], b)] = cx;
+        for (int k = 0; k < nx; k++) dst[g.idx(xs[k], b)] = put(cx);
         if (b == 0 || b == M - 1) {
             int yt = (b == 0) ? -1 : M;
-            dst[g.idx(a, yt)] = val;
-            for (int k = 0; k < nx; k++) dst[g.idx(xs[k], yt)] = cx;
+            dst[g.idx(a, yt)] = put(val);
+            for (int k = 0; k < nx; k++) dst[g.idx(xs[k], yt)] = put(cx);
             if (b == 0 && b == M - 1) {   // M == 1: both rows
-                dst[g.idx(a, M)] = val;
-                for (int k = 0; k < nx; k++) dst[g.idx(xs[k], M)] = cx;
+                dst[g.idx(a, M)] = put(val);
+                for (int k = 0; k < nx; k++) dst[g.idx(xs[k], M)] = put(cx);
             }
         }
     }
+    __device__ inline void eta(Tp* __restrict__ dst, const Geom& g, int a, int b, Tp val) const {
+        eta(dst, g, a, b, val, Same{});
+    }
     // sst at (a, b): periodic / zero-gradient copies in x (src/ghost_points.jl:136-179)
-    __device__ inline void sst(Tp* __restrict__ dst, const Geom& g, int a, int b, Tp val) const {
+    template <class D, class Put>
+    __device__ inline void sst(D* __restrict__ dst, const Geom& g, int a, int b, Tp val, Put put) const {
         if (ep) {
             Tp c = comm(val);
-            if (a == N - 1) dst[g.idx(-1, b)] = c;
-            if (a == 0) dst[g.idx(N, b)] = c;
+            if (a == N - 1) dst[g.idx(-1, b)] = put(c);
+            if (a == 0) dst[g.idx(N, b)] = put(c);
         } else {
-            if (a == 0) dst[g.idx(-1, b)] = val;
-            if (a == N - 1) dst[g.idx(N, b)] = val;
+            if (a == 0) dst[g.idx(-1, b)] = put(val);
+            if (a == N - 1) dst[g.idx(N, b)] = put(val);
         }
     }
+    __device__ inline void sst(Tp* __restrict__ dst, const Geom& g, int a, int b, Tp val) const {
+        sst(dst, g, a, b, val, Same{});
+    }
+    struct Same {
+        __device__ __forceinline__ Tp operator()(Tp x) const { return x; }
+    };
 };
 
 // The untouched halo cells of u and v, enumerated 0..count-1.

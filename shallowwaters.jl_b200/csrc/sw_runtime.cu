@@ -37,6 +37,7 @@
 #include "sw_linear.cuh"
 #include "sw_advcor.cuh"
 #include "sw_storage.cuh"
+#include "sw_s16.cuh"
 #include "sw_batch.cuh"
 #include "sw_diag.cuh"
 #include "sw_tail.cuh"
@@ -167,8 +168,12 @@ struct EngineBase {
     virtual int nan_check(sw_ctx* ctx, long long i) = 0;     // the check of step i (state before it)
     virtual int diagnostics(sw_ctx* ctx, sw_diag* out) = 0;
     virtual int prologue(sw_ctx* ctx) = 0;                   // work of time_integration before its loop
-    virtual int store_round_state(sw_ctx* ctx) = 0;          // 16-bit storage form of the current state
     virtual int ghost_state(sw_ctx* ctx) = 0;
+    // the storage form's own copy of the state: made from the FP32 buffers
+    // S[p], sst[sp] after an upload, and written back into them before a
+    // download or a diagnostics pass (no-ops for the native storage)
+    virtual int state_uploaded(sw_ctx*) { return SW_OK; }
+    virtual int state_to_fp32(sw_ctx*) { return SW_OK; }
 };
 
 struct sw_ctx {
@@ -199,6 +204,7 @@ struct sw_ctx {
     std::map<const void*, Maps> tmaps;
     bool use_tma = false;
     int stage_blocks_cap = 0;     // > 0: at most this many persistent blocks in rk_stage_tma
+    int tracer_rows = 1;          // rows per thread of the tracer kernel (SWB200_TRACER_ROWS)
     uint32_t spin_limit = MBAR_SPIN_LIMIT;   // polls per bounded wait of rk_stage_tma
     int test_skip_chunk = -1;     // test only: a chunk rk_stage_tma's producer leaves out
     // CUDA graphs of one time step, keyed by the buffer parities and the
@@ -385,6 +391,15 @@ __global__ void ghost_state_kernel(Geom g, Tp* u, Tp* v, Tp* e, GhostRule<Tp> gr
         Ring::v_at((int)r, N, M, a, G);
         gr.v(v, g, a, G, v[g.idx(a, G)]);
     }
+}
+
+// The tracer's launch grid: 128 columns by gy rows of blocks; each thread
+// takes rows b, b + gy, ... (ctx->tracer_rows of them; one thread per cell by
+// default, which measured faster at 2048 x 1024 than 6 rows per thread).
+dim3 tracer_grid(const sw_ctx* ctx) {
+    const Geom& g = ctx->g;
+    const int rpt = std::max(1, ctx->tracer_rows);
+    return dim3((g.N + 127) / 128, std::min((g.M + rpt - 1) / rpt, 4096));
 }
 
 template <class T, class Tp>
@@ -825,12 +840,7 @@ struct Engine : EngineBase {
             if ((i % c.nadvstep) == 0) {
                 TracerArgs<T, Tp> a = tracer_args(ctx, ctx->p, ctx->sp);
                 const bool um_is_u = (c.nadvstep == 1);
-                // each thread takes rows b, b + gy, ...: up to 8 rows on grids
-                // large enough to fill the GPU without it, so the per-thread
-                // set-up is shared by several cells
-                const long long want = (long long)ctx->nsm * 2048;
-                const int rpt = (int)std::max(1LL, std::min(8LL, (long long)g.N * g.M / want));
-                dim3 grid((g.N + 127) / 128, std::min((g.M + rpt - 1) / rpt, 4096));
+                const dim3 grid = tracer_grid(ctx);
                 int rc = launch(ctx, 2, [&] {
                     if (g.ep) tracer_dispatch2<true>(a, um_is_u, c.tracer_consumption != 0, grid, ctx->stream);
                     else tracer_dispatch2<false>(a, um_is_u, c.tracer_consumption != 0, grid, ctx->stream);
@@ -840,36 +850,7 @@ struct Engine : EngineBase {
             }
         }
 
-        // ------------------------------- 16-bit storage form (sw_storage.cuh)
-        if (c.storage != SW_STORE_NATIVE)
-            if (int rc = store_round(ctx, Y)) return rc;
         return SW_OK;
-    }
-
-    // rounds the state F (and the current tracer) to the 16-bit storage form
-    // in place, then re-applies the ghost rules to the rounded interior
-    int store_round(sw_ctx* ctx, const Fields3& F) {
-        if constexpr (std::is_same<T, float>::value && std::is_same<Tp, float>::value) {
-            const sw_config& c = ctx->cfg;
-            const float s = (float)c.storage_scale_uv, inv = 1.0f / s;
-            int rc = launch(ctx, 5, [&] {
-                auto args = [&](auto kern) {
-                    kern<<<4 * ctx->nsm, 256, 0, ctx->stream>>>((float*)F.u, (float*)F.v, (float*)F.e,
-                                                                  (float*)ctx->sst[ctx->sp], (long long)ctx->nelem, s, inv);
-                };
-                if (c.storage == SW_STORE_BF16) args(store_round_kernel<__nv_bfloat16>);
-                else args(store_round_kernel<__half>);
-            });
-            if (rc) return rc;
-            return launch(ctx, 5, [&] {
-                ghost_state_kernel<Tp><<<148, 256, 0, ctx->stream>>>(ctx->g, (Tp*)F.u, (Tp*)F.v, (Tp*)F.e, rule(ctx));
-            });
-        } else {
-            return fail(ctx, SW_ERR_UNSUPPORTED, "16-bit storage needs T = Tprog = Float32");
-        }
-    }
-    int store_round_state(sw_ctx* ctx) override {
-        return ctx->cfg.storage == SW_STORE_NATIVE ? SW_OK : store_round(ctx, ctx->S[ctx->p]);
     }
 
     // advection/Coriolis refresh (nstep_advcor > 0) from u, v, eta with valid
@@ -935,6 +916,213 @@ struct Engine : EngineBase {
     }
 };
 
+// The 16-bit storage form (sw_s16.cuh): T = Tprog = Float32 arithmetic on a
+// state held in 16-bit pairs.  The FP32 buffers of the context carry the
+// state only across uploads, downloads and diagnostics (S[p], sst[sp]); the
+// last RK stage's X0 goes to Acc (u0, v0, eta0) as in the native form.  The
+// rest of a step lives in 16-bit arrays: the state pairs of both parities, the
+// stage values X1 (two sets), the increments D and the tracer (two parities).
+template <class S16>
+struct Engine16 : Engine<float, float> {
+    using Base = Engine<float, float>;
+    struct F3 { S16* u = nullptr; S16* v = nullptr; S16* e = nullptr; };
+    F3 hi[2], lo[2], X1[2], D;
+    S16* sst16[2] = {nullptr, nullptr};
+    float s = 1024.f, inv_s = 1.f / 1024.f;
+
+    int init(sw_ctx* ctx) {
+        const sw_config& c = ctx->cfg;
+        s = (float)c.storage_scale_uv;
+        inv_s = (float)(1.0 / c.storage_scale_uv);
+        const size_t bytes = ctx->nelem * sizeof(S16);
+        auto alloc = [&](S16** p) -> int {
+            void* q = nullptr;
+            CK(cached_malloc(&q, bytes));
+            ctx->allocs.push_back({q, bytes});
+            ctx->zeroed.push_back({q, bytes});
+            CK(cudaMemsetAsync(q, 0, bytes, ctx->stream));
+            *p = static_cast<S16*>(q);
+            return SW_OK;
+        };
+        for (F3* f : {&hi[0], &hi[1], &lo[0], &lo[1], &X1[0], &X1[1], &D})
+            for (S16** p : {&f->u, &f->v, &f->e})
+                if (int rc = alloc(p)) return rc;
+        for (S16** p : {&sst16[0], &sst16[1]})
+            if (int rc = alloc(p)) return rc;
+        return SW_OK;
+    }
+
+    int state_uploaded(sw_ctx* ctx) override {
+        const Fields3& F = ctx->S[ctx->p];
+        const int p = ctx->p;
+        return launch(ctx, 5, [&] {
+            s16_pack_kernel<S16><<<4 * ctx->nsm, 256, 0, ctx->stream>>>(
+                (const float*)F.u, (const float*)F.v, (const float*)F.e, (const float*)ctx->sst[ctx->sp],
+                hi[p].u, lo[p].u, hi[p].v, lo[p].v, hi[p].e, lo[p].e, sst16[ctx->sp], (long long)ctx->nelem, s);
+        });
+    }
+    int state_to_fp32(sw_ctx* ctx) override {
+        const Fields3& F = ctx->S[ctx->p];
+        const int p = ctx->p;
+        return launch(ctx, 5, [&] {
+            s16_unpack_kernel<S16><<<4 * ctx->nsm, 256, 0, ctx->stream>>>(
+                hi[p].u, lo[p].u, hi[p].v, lo[p].v, hi[p].e, lo[p].e, sst16[ctx->sp], (float*)F.u, (float*)F.v,
+                (float*)F.e, (float*)ctx->sst[ctx->sp], (long long)ctx->nelem, inv_s);
+        });
+    }
+    int diagnostics(sw_ctx* ctx, sw_diag* out) override {
+        if (int rc = state_to_fp32(ctx)) return rc;
+        return Base::diagnostics(ctx, out);
+    }
+    int nan_check(sw_ctx* ctx, long long i) override {
+        const int p = ctx->p;
+        return launch(ctx, 4, [&] {
+            s16_nan_check_kernel<S16><<<148, 256, 0, ctx->stream>>>(ctx->g, hi[p].u, hi[p].v, hi[p].e,
+                                                                    sst16[ctx->sp], i, ctx->dst);
+        });
+    }
+
+    template <bool PER, bool FIRST, bool LAST, int TY>
+    static void stage16(const S16StageArgs<S16>& a, int nblk, cudaStream_t st) {
+        s16_stage_kernel<S16, PER, FIRST, LAST, TY><<<nblk, 128, 0, st>>>(a);
+    }
+    template <bool PER, bool FIRST, bool LAST>
+    static void stage16_ty(const S16StageArgs<S16>& a, int nblk, cudaStream_t st, int ty) {
+        if (ty == 8) stage16<PER, FIRST, LAST, 8>(a, nblk, st);
+        else if (ty == 16) stage16<PER, FIRST, LAST, 16>(a, nblk, st);
+        else stage16<PER, FIRST, LAST, 32>(a, nblk, st);
+    }
+    template <bool PER, int DRAG, bool SMAG>
+    static void tail16(const TailArgs<float, float>& a, const TailStorePair<S16>& o, int nblk, cudaStream_t st, int ty) {
+        if (ty == 8) s16_tail_kernel<S16, PER, DRAG, SMAG, 8><<<nblk, 128, 0, st>>>(a, o);
+        else if (ty == 16) s16_tail_kernel<S16, PER, DRAG, SMAG, 16><<<nblk, 128, 0, st>>>(a, o);
+        else s16_tail_kernel<S16, PER, DRAG, SMAG, 32><<<nblk, 128, 0, st>>>(a, o);
+    }
+    template <bool PER>
+    static void tail16_opts(const TailArgs<float, float>& a, const TailStorePair<S16>& o, int drag, bool smag,
+                            int nblk, cudaStream_t st, int ty) {
+        if (smag) {
+            if (drag == SW_DRAG_QUADRATIC) tail16<PER, SW_DRAG_QUADRATIC, true>(a, o, nblk, st, ty);
+            else if (drag == SW_DRAG_LINEAR) tail16<PER, SW_DRAG_LINEAR, true>(a, o, nblk, st, ty);
+            else tail16<PER, SW_DRAG_NONE, true>(a, o, nblk, st, ty);
+        } else {
+            if (drag == SW_DRAG_QUADRATIC) tail16<PER, SW_DRAG_QUADRATIC, false>(a, o, nblk, st, ty);
+            else if (drag == SW_DRAG_LINEAR) tail16<PER, SW_DRAG_LINEAR, false>(a, o, nblk, st, ty);
+            else tail16<PER, SW_DRAG_NONE, false>(a, o, nblk, st, ty);
+        }
+    }
+    template <bool PER>
+    static void tracer16(const TracerArgs<float, float>& a, const TracerIO16<S16>& io, bool um_is_u, bool cons,
+                         dim3 grid, cudaStream_t st) {
+        if (um_is_u) {
+            if (cons) s16_tracer_kernel<S16, PER, true, true><<<grid, 128, 0, st>>>(a, io);
+            else s16_tracer_kernel<S16, PER, true, false><<<grid, 128, 0, st>>>(a, io);
+        } else {
+            if (cons) s16_tracer_kernel<S16, PER, false, true><<<grid, 128, 0, st>>>(a, io);
+            else s16_tracer_kernel<S16, PER, false, false><<<grid, 128, 0, st>>>(a, io);
+        }
+    }
+
+    // One time step from the pairs of parity p to those of 1 - p: RK stages
+    // (src/time_integration.jl:55-78), the tail (:216-221) and the tracer
+    // (:226-228), as in Engine::step, on the 16-bit arrays.
+    int step(sw_ctx* ctx, long long i) override {
+        const sw_config& c = ctx->cfg;
+        const Geom& g = ctx->g;
+        const int p = ctx->p, q = 1 - p;
+        const bool tail_now = (i % c.nstep_diff) == 0;
+        const float Fxt = c.seasonal_wind_x ? (float)std::sin(c.omegaFx * (double)ctx->t) : 1.f;
+        const float Fyt = c.seasonal_wind_y ? (float)std::sin(c.omegaFy * (double)ctx->t) : 1.f;
+
+        S16StageArgs<S16> a;
+        a.g = g;
+        a.nsx = (g.N + STRIP - 1) / STRIP; a.nsy = (g.M + ctx->stage_ty - 1) / ctx->stage_ty;
+        a.nring_blocks = ring_blocks(g, 128);
+        a.uh = hi[p].u; a.vh = hi[p].v; a.eh = hi[p].e;
+        a.ul = lo[p].u; a.vl = lo[p].v; a.el = lo[p].e;
+        a.uD = D.u; a.vD = D.v; a.eD = D.e;
+        a.uDo = D.u; a.vDo = D.v; a.eDo = D.e;
+        a.u0o = (float*)ctx->Acc.u; a.v0o = (float*)ctx->Acc.v; a.e0o = (float*)ctx->Acc.e;
+        a.eho = hi[q].e; a.elo = lo[q].e;
+        a.H = sf<float>(ctx->H); a.fq = sf<float>(ctx->fq); a.Fx = sf<float>(ctx->Fx); a.Fy = sf<float>(ctx->Fy);
+        a.g_ = (float)c.g; a.Fxt = Fxt; a.Fyt = Fyt;
+        a.s = s; a.inv_s = inv_s;
+        a.gr = rule(ctx);
+        a.st = ctx->dst;
+        const int nblk = (a.nsx * a.nsy + 3) / 4 + a.nring_blocks;
+        for (int k = 1; k <= c.RKo; k++) {
+            const F3& in = (k == 1) ? hi[p] : X1[k % 2 == 0 ? 0 : 1];
+            const F3& out1 = X1[k % 2 == 1 ? 0 : 1];
+            a.u1 = in.u; a.v1 = in.v; a.e1 = in.e;
+            a.u1o = out1.u; a.v1o = out1.v; a.e1o = out1.e;
+            a.a = (float)c.RKaDt[k - 1];
+            a.b = (k < c.RKo) ? (float)c.RKbDt[k - 1] : 0.f;
+            const bool first = k == 1, last = k == c.RKo;
+            const int rc = launch(ctx, 0, [&] {
+                if (g.ep) {
+                    if (first) stage16_ty<true, true, false>(a, nblk, ctx->stream, ctx->stage_ty);
+                    else if (last) stage16_ty<true, false, true>(a, nblk, ctx->stream, ctx->stage_ty);
+                    else stage16_ty<true, false, false>(a, nblk, ctx->stream, ctx->stage_ty);
+                } else {
+                    if (first) stage16_ty<false, true, false>(a, nblk, ctx->stream, ctx->stage_ty);
+                    else if (last) stage16_ty<false, false, true>(a, nblk, ctx->stream, ctx->stage_ty);
+                    else stage16_ty<false, false, false>(a, nblk, ctx->stream, ctx->stage_ty);
+                }
+            });
+            if (rc) return rc;
+        }
+
+        if (tail_now) {
+            TailArgs<float, float> t = tail_args(ctx, p);
+            t.e0 = (const float*)ctx->Acc.e;     // the last stage's FP32 eta (depth of the drag)
+            const TailStorePair<S16> o{hi[q].u, lo[q].u, hi[q].v, lo[q].v, s};
+            const int nb = (t.nsx * t.nsy + 3) / 4 + t.nring_blocks;
+            const bool smag = c.diffusion == SW_DIFF_SMAGORINSKY;
+            const int rc = launch(ctx, 1, [&] {
+                if (g.ep) tail16_opts<true>(t, o, c.bottom_drag, smag, nb, ctx->stream, ctx->tail_ty);
+                else tail16_opts<false>(t, o, c.bottom_drag, smag, nb, ctx->stream, ctx->tail_ty);
+            });
+            if (rc) return rc;
+        } else {
+            const int rc = launch(ctx, 5, [&] {
+                s16_pack_uv_kernel<S16><<<4 * ctx->nsm, 256, 0, ctx->stream>>>(
+                    (const float*)ctx->Acc.u, (const float*)ctx->Acc.v, hi[q].u, lo[q].u, hi[q].v, lo[q].v,
+                    (long long)ctx->nelem, s, ctx->dst);
+            });
+            if (rc) return rc;
+        }
+        ctx->t += c.dtint;
+
+        if (c.tracer_advection) {
+            if (c.nadvstep > 1 && ((i + c.nadvstep_half) % c.nadvstep) == 0) {
+                const int rc = launch(ctx, 5, [&] {
+                    s16_copy_uv_kernel<S16><<<296, 256, 0, ctx->stream>>>(hi[q].u, hi[q].v, (float*)ctx->um,
+                                                                          (float*)ctx->vm, (long long)ctx->nelem,
+                                                                          inv_s, ctx->dst);
+                });
+                if (rc) return rc;
+            }
+            if ((i % c.nadvstep) == 0) {
+                TracerArgs<float, float> t = tracer_args(ctx, p, ctx->sp);
+                t.u = reinterpret_cast<const float*>(hi[q].u);
+                t.v = reinterpret_cast<const float*>(hi[q].v);
+                t.sst = reinterpret_cast<const float*>(sst16[ctx->sp]);
+                t.sst_o = reinterpret_cast<float*>(sst16[1 - ctx->sp]);
+                const TracerIO16<S16> io{inv_s};
+                const bool um_is_u = c.nadvstep == 1;
+                const dim3 grid = tracer_grid(ctx);
+                const int rc = launch(ctx, 2, [&] {
+                    if (g.ep) tracer16<true>(t, io, um_is_u, c.tracer_consumption != 0, grid, ctx->stream);
+                    else tracer16<false>(t, io, um_is_u, c.tracer_consumption != 0, grid, ctx->stream);
+                });
+                if (rc) return rc;
+                ctx->sp = 1 - ctx->sp;
+            }
+        }
+        return SW_OK;
+    }
+};
+
 // ------------------------------------------------------------------ helpers
 
 int check_config(const sw_config* c, std::string& why) {
@@ -967,6 +1155,12 @@ int check_config(const sw_config* c, std::string& why) {
         if (!(s > 0) || std::frexp(s, &ex) != 0.5 || c->T != SW_FLOAT32 || c->Tprog != SW_FLOAT32) {
             why = "16-bit storage needs T = Tprog = Float32 and a power-of-two storage_scale_uv";
             return SW_ERR_ARG;
+        }
+        if (c->time_scheme != SW_RK || c->dynamics != SW_NONLINEAR || c->adv_scheme != SW_ARAKAWA_HSU ||
+            c->nstep_advcor != 0 || c->surface_relax || c->surface_forcing) {
+            why = "the 16-bit storage form is built for RK, nonlinear dynamics with Arakawa-Hsu advection, "
+                  "nstep_advcor = 0 and the plain continuity equation";
+            return SW_ERR_UNSUPPORTED;
         }
     }
     bool ok = (c->T == SW_FLOAT32 && c->Tprog == SW_FLOAT32) || (c->T == SW_FLOAT64 && c->Tprog == SW_FLOAT64) ||
@@ -1220,7 +1414,7 @@ int run_steps(sw_ctx* ctx, long long nsteps, sw_status* status) {
 std::string env_settings() {
     std::string s;
     for (const char* k : {"SWB200_TMA", "SWB200_GRAPHS", "SWB200_STAGE_BLOCKS", "SWB200_TAIL_TY", "SWB200_STAGE_TY",
-                          "SWB200_TEST_WAIT_LIMIT", "SWB200_TEST_SKIP_CHUNK"}) {
+                          "SWB200_TEST_WAIT_LIMIT", "SWB200_TEST_SKIP_CHUNK", "SWB200_TRACER_ROWS"}) {
         const char* v = getenv(k);
         s += k;
         s += '=';
@@ -1920,6 +2114,8 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
         bool ok = want && encode_fn() != nullptr;
         // a cap on the TMA stage kernel's persistent blocks (SWB200_STAGE_BLOCKS),
         // so that small grids also run blocks that take several tiles each
+        const char* envr = getenv("SWB200_TRACER_ROWS");
+        if (envr && atoi(envr) >= 1 && atoi(envr) <= 64) ctx->tracer_rows = atoi(envr);
         const char* envb = getenv("SWB200_STAGE_BLOCKS");
         ctx->stage_blocks_cap = envb ? std::max(1, atoi(envb)) : 0;
         // test only: a shorter bounded wait and a chunk that is never filled,
@@ -1942,7 +2138,11 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
         ctx->tail_ty = pick_strip_ty(*cfg, g, ctx->nsm, "SWB200_TAIL_TY");
         ctx->stage_ty = pick_strip_ty(*cfg, g, ctx->nsm, "SWB200_STAGE_TY");
     }
-    if (cfg->T == SW_FLOAT32 && cfg->Tprog == SW_FLOAT32) {
+    if (cfg->storage == SW_STORE_BF16) {
+        auto* e = new Engine16<__nv_bfloat16>(); ctx->eng.reset(e); if ((rc = e->init(ctx))) return rc;
+    } else if (cfg->storage == SW_STORE_F16) {
+        auto* e = new Engine16<__half>(); ctx->eng.reset(e); if ((rc = e->init(ctx))) return rc;
+    } else if (cfg->T == SW_FLOAT32 && cfg->Tprog == SW_FLOAT32) {
         auto* e = new Engine<float, float>(); ctx->eng.reset(e); if ((rc = e->init(ctx))) return rc;
     } else if (cfg->T == SW_FLOAT64 && cfg->Tprog == SW_FLOAT64) {
         auto* e = new Engine<double, double>(); ctx->eng.reset(e); if ((rc = e->init(ctx))) return rc;
@@ -1975,7 +2175,7 @@ int sw_set_state(sw_ctx* ctx, const void* u, const void* v, const void* eta, con
     // ghost_points!(u,v,eta) opens every step (src/time_integration.jl:48); it is
     // idempotent after the first, so it is applied once here
     if ((rc = ctx->eng->ghost_state(ctx))) return rc;
-    if ((rc = ctx->eng->store_round_state(ctx))) return rc;
+    if ((rc = ctx->eng->state_uploaded(ctx))) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
     return SW_OK;
 }
@@ -1984,6 +2184,7 @@ int sw_get_state(sw_ctx* ctx, void* u, void* v, void* eta, void* sst) {
     if (!ctx || !u || !v || !eta || !sst) return SW_ERR_ARG;
     const Fields3& X = ctx->S[ctx->p];
     int rc;
+    if ((rc = ctx->eng->state_to_fp32(ctx))) return rc;
     if ((rc = copy_out(ctx, u, X.u, shape_u(ctx->g)))) return rc;
     if ((rc = copy_out(ctx, v, X.v, shape_v(ctx->g)))) return rc;
     if ((rc = copy_out(ctx, eta, X.e, shape_e(ctx->g)))) return rc;

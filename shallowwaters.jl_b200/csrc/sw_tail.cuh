@@ -37,9 +37,26 @@ struct TailArgs {
     DevStatus* st;
 };
 
+// Where the tail's new u, v go.  TailStoreNative: into A.uo, A.vo (Tprog),
+// with their ghost copies when gs.  The 16-bit storage form stores pairs
+// instead (sw_s16.cuh).
+template <class Tp>
+struct TailStoreNative {
+    template <class Args>
+    __device__ __forceinline__ void u(const Args& A, const Geom& g, int F, int b, int o, Tp val, bool gs) const {
+        A.uo[o] = val;
+        if (gs) A.gr.u(A.uo, g, F, b, val);
+    }
+    template <class Args>
+    __device__ __forceinline__ void v(const Args& A, const Geom& g, int a, int G, int o, Tp val, bool gs) const {
+        A.vo[o] = val;
+        if (gs) A.gr.v(A.vo, g, a, G, val);
+    }
+};
+
 // untouched halo cells keep u0 (and so do their ghost copies)
-template <class T, class Tp>
-__device__ void tail_ring(const TailArgs<T, Tp>& A, int k0, int kstride) {
+template <class T, class Tp, class ST = TailStoreNative<Tp>>
+__device__ void tail_ring(const TailArgs<T, Tp>& A, int k0, int kstride, const ST& out = ST()) {
     const Geom& g = A.g;
     const int nu = Ring::u_count(g.ep, g.N, g.M), nv = Ring::v_count(g.N);
     for (int k = k0; k < nu + nv; k += kstride) {
@@ -47,14 +64,12 @@ __device__ void tail_ring(const TailArgs<T, Tp>& A, int k0, int kstride) {
             int F, b;
             Ring::u_at(k, g.ep, g.N, g.M, F, b);
             Tp x = A.u0[g.idx(F, b)];
-            A.uo[g.idx(F, b)] = x;
-            A.gr.u(A.uo, g, F, b, x);
+            out.u(A, g, F, b, g.idx(F, b), x, true);
         } else {
             int a, G;
             Ring::v_at(k - nu, g.N, g.M, a, G);
             Tp x = A.v0[g.idx(a, G)];
-            A.vo[g.idx(a, G)] = x;
-            A.gr.v(A.vo, g, a, G, x);
+            out.v(A, g, a, G, g.idx(a, G), x, true);
         }
     }
 }
@@ -64,14 +79,14 @@ __device__ void tail_ring(const TailArgs<T, Tp>& A, int k0, int kstride) {
 #endif
 // DRAG: enum sw_bottom_drag; SMAG: Smagorinsky (else constant νB)
 // The streaming tail for block bx of its grid (strip blocks, then ring blocks).
-template <class T, class Tp, bool PER, int DRAG, bool SMAG, int TY>
-__device__ __forceinline__ void tail_body(const TailArgs<T, Tp>& A, int bx) {
+template <class T, class Tp, bool PER, int DRAG, bool SMAG, int TY, class ST = TailStoreNative<Tp>>
+__device__ __forceinline__ void tail_body(const TailArgs<T, Tp>& A, int bx, const ST& out = ST()) {
     if (A.st->stop) return;
     const Geom& g = A.g;
     const int nstrips = A.nsx * A.nsy;
     const int nstrip_blocks = (nstrips + 3) / 4;
     if (bx >= nstrip_blocks) {
-        tail_ring(A, (bx - nstrip_blocks) * 128 + threadIdx.x, A.nring_blocks * 128);
+        tail_ring(A, (bx - nstrip_blocks) * 128 + threadIdx.x, A.nring_blocks * 128, out);
         return;
     }
     const int w = bx * 4 + (int)(threadIdx.x >> 5);
@@ -197,8 +212,7 @@ SWB_ROW_UNROLL
                 const T LLu1 = S11_r - S11l_r;
                 const T LLu2 = S12_r1 - S12_r;
                 Tp val = U0 + A.Dt_diff * (cvt<Tp>(Bu) + cvt<Tp>(LLu1) + cvt<Tp>(LLu2));
-                A.uo[ofs(r)] = val;
-                if (gx_u || (!PER && (r <= 1 || r >= M - 2))) A.gr.u(A.uo, g, c, r, val);
+                out.u(A, g, c, r, ofs(r), val, gx_u || (!PER && (r <= 1 || r >= M - 2)));
             }
             if (col_a && r >= 1) {
                 T Bv;
@@ -214,8 +228,7 @@ SWB_ROW_UNROLL
                 const T LLv1 = S21r_r - S21_r;
                 const T LLv2 = S22_r - S22_rm1;
                 Tp val = V0 + A.Dt_diff * (cvt<Tp>(Bv) + cvt<Tp>(LLv1) + cvt<Tp>(LLv2));
-                A.vo[ofs(r)] = val;
-                if (gx_v) A.gr.v(A.vo, g, c, r, val);
+                out.v(A, g, c, r, ofs(r), val, gx_v);
             }
         }
 

@@ -68,10 +68,24 @@ __device__ __forceinline__ int axis(int k0, int xi, T xy, int lo, int hi, int n,
     }
 }
 
+// How the tracer reads u, v and sst and writes sst.  TracerIONative: arrays of
+// Tprog.  The 16-bit storage form reads and writes scaled 16-bit numbers
+// (sw_s16.cuh); its pointers travel in TracerArgs as Tprog pointers.
+template <class T, class Tp>
+struct TracerIONative {
+    using EU = Tp;                       // element type of u, v
+    using ES = Tp;                       // element type of sst
+    __device__ __forceinline__ T u(EU x) const { return cvt<T>(x); }
+    __device__ __forceinline__ T s(ES x) const { return cvt<T>(x); }
+    __device__ __forceinline__ ES operator()(Tp x) const { return x; }   // Tprog value -> sst element
+};
+
 // 2-D launch: x over columns, y over rows (grid-stride in y)
 // The tracer for column block bx and rows by, by + gy, ... (128 threads).
-template <class T, class Tp, bool PER, bool UM_IS_U, bool CONS>
-__device__ __forceinline__ void tracer_body(const TracerArgs<T, Tp>& A, int bx, int by, int gy) {
+template <class T, class Tp, bool PER, bool UM_IS_U, bool CONS, class IO = TracerIONative<T, Tp>>
+__device__ __forceinline__ void tracer_body(const TracerArgs<T, Tp>& A, int bx, int by, int gy, const IO& io = IO()) {
+    using EU = typename IO::EU;
+    using ES = typename IO::ES;
     if (A.st->stop) return;
     const Geom& g = A.g;
     const int N = g.N, M = g.M;
@@ -84,17 +98,17 @@ __device__ __forceinline__ void tracer_body(const TracerArgs<T, Tp>& A, int bx, 
     // element (x, y) of a field sits at (y + ROW0) * P + x + COL0
     auto at = [&](int x, int y) { return (y + ROW0) * P + x + COL0; };
     // the output never aliases the inputs: loads of later rows may be issued early
-    const Tp* __restrict__ pu = A.u;
-    const Tp* __restrict__ pv = A.v;
+    const EU* __restrict__ pu = reinterpret_cast<const EU*>(A.u);
+    const EU* __restrict__ pv = reinterpret_cast<const EU*>(A.v);
     const T* __restrict__ pum = A.um;
     const T* __restrict__ pvm = A.vm;
-    const Tp* __restrict__ psst = A.sst;
-    Tp* __restrict__ psst_o = A.sst_o;
+    const ES* __restrict__ psst = reinterpret_cast<const ES*>(A.sst);
+    ES* __restrict__ psst_o = reinterpret_cast<ES*>(A.sst_o);
     for (int b = by; b < M; b += gy) {
         // departure!: u_T = Ix!(u), v_T = Iy!(v); backtraj! at half step (:75-76, :96-124)
         const int o = at(a, b);
-        const T uT = half * (cvt<T>(pu[o + 1]) + cvt<T>(pu[o]));
-        const T vT = half * (cvt<T>(pv[o + P]) + cvt<T>(pv[o]));
+        const T uT = half * (io.u(pu[o + 1]) + io.u(pu[o]));
+        const T vT = half * (io.u(pv[o + P]) + io.u(pv[o]));
         T xd = (-A.half_dtadvu) * uT;
         T yd = (-A.half_dtadvv) * vT;
         int xi = ifloor(xd, bad), yi = ifloor(yd, bad);
@@ -107,8 +121,8 @@ __device__ __forceinline__ void tracer_body(const TracerArgs<T, Tp>& A, int bx, 
             const int k = at(F0, b0);
             T m00, m10, m20, m01, m11, m21;
             if (UM_IS_U) {
-                m00 = cvt<T>(pu[k]); m10 = cvt<T>(pu[k + 1]); m20 = cvt<T>(pu[k + 2]);
-                m01 = cvt<T>(pu[k + P]); m11 = cvt<T>(pu[k + P + 1]); m21 = cvt<T>(pu[k + P + 2]);
+                m00 = io.u(pu[k]); m10 = io.u(pu[k + 1]); m20 = io.u(pu[k + 2]);
+                m01 = io.u(pu[k + P]); m11 = io.u(pu[k + P + 1]); m21 = io.u(pu[k + P + 2]);
             } else {
                 m00 = pum[k]; m10 = pum[k + 1]; m20 = pum[k + 2];
                 m01 = pum[k + P]; m11 = pum[k + P + 1]; m21 = pum[k + P + 2];
@@ -123,8 +137,8 @@ __device__ __forceinline__ void tracer_body(const TracerArgs<T, Tp>& A, int bx, 
             const int k = at(a0, G0);
             T m00, m01, m02, m10, m11, m12;
             if (UM_IS_U) {
-                m00 = cvt<T>(pv[k]); m01 = cvt<T>(pv[k + P]); m02 = cvt<T>(pv[k + 2 * P]);
-                m10 = cvt<T>(pv[k + 1]); m11 = cvt<T>(pv[k + P + 1]); m12 = cvt<T>(pv[k + 2 * P + 1]);
+                m00 = io.u(pv[k]); m01 = io.u(pv[k + P]); m02 = io.u(pv[k + 2 * P]);
+                m10 = io.u(pv[k + 1]); m11 = io.u(pv[k + P + 1]); m12 = io.u(pv[k + 2 * P + 1]);
             } else {
                 m00 = pvm[k]; m01 = pvm[k + P]; m02 = pvm[k + 2 * P];
                 m10 = pvm[k + 1]; m11 = pvm[k + P + 1]; m12 = pvm[k + 2 * P + 1];
@@ -143,12 +157,12 @@ __device__ __forceinline__ void tracer_body(const TracerArgs<T, Tp>& A, int bx, 
             const int b0 = axis<T, false>(yi + b, yi, yd, 0, M - 2, 0, y0);
             if (a0 < -1 || a0 > N - 1) { bad = 1; a0 = 0; }
             const int k = at(a0, b0);
-            s = bilin(cvt<T>(psst[k]), cvt<T>(psst[k + 1]), cvt<T>(psst[k + P]), cvt<T>(psst[k + P + 1]), x0, y0);
+            s = bilin(io.s(psst[k]), io.s(psst[k + 1]), io.s(psst[k + P]), io.s(psst[k + P + 1]), x0, y0);
         }
         if (CONS) s += A.jSST * (A.SSTmin - s);              // tracer_consumption! (:262-275)
         const Tp out = cvt<Tp>(s);
-        psst_o[o] = out;
-        if (gx) A.gr.sst(psst_o, g, a, b, out);             // ghost_points_sst! (:40)
+        psst_o[o] = io(out);
+        if (gx) A.gr.sst(psst_o, g, a, b, out, io);             // ghost_points_sst! (:40)
     }
     if (bad) {   // the reference throws here; halt the device-side loop
         atomicCAS(&A.st->error, 0, (int)SW_ERR_DEPARTURE);

@@ -296,54 +296,6 @@ def test_output_frames_match_oracle(tmp_path):
         assert_bitwise(u[-1], out.u.astype(np.float32), "last frame")
 
 
-def _r16(x, form):
-    """float32 -> nearest 16-bit value (ties to even), back as float32."""
-    x = np.asarray(x, np.float32)
-    if form == "f16":
-        return x.astype(np.float16).astype(np.float32)
-    b = x.view(np.uint32).astype(np.uint64)
-    b = ((b + 0x7FFF + ((b >> 16) & 1)) >> 16) << 16
-    return b.astype(np.uint32).view(np.float32)
-
-
-def _round_pair(x, s, form):
-    y = np.asarray(x, np.float32) * np.float32(s)
-    hi = _r16(y, form)
-    lo = _r16(y - hi, form)
-    return ((hi + lo) * np.float32(1.0 / s)).astype(np.float32)
-
-
-@pytest.mark.parametrize("form,bc", [("bf16", "periodic"), ("f16", "periodic"), ("bf16", "nonperiodic")])
-def test_storage_form_is_a_rounded_fp32_step(form, bc):
-    """16-bit storage form: every step is the FP32 step of the stored state
-    followed by rounding u, v (scale 2^10) and eta to compensated 16-bit pairs,
-    the tracer to one 16-bit value, and the ghost rules."""
-    from swb200.initial_conditions import ghost_points
-    P = Parameter(nx=40, Ndays=0.2, Uadv=1000, bc=bc, α=0.5 if bc == "nonperiodic" else 1.0)
-    S = model_setup(P)
-    Prog = initial_conditions(P.Tprog, S, **seeded_inputs(S, 9))
-    s = 1024.0
-
-    def store(st):
-        u, v, e = (_round_pair(st[0], s, form), _round_pair(st[1], s, form), _round_pair(st[2], 1.0, form))
-        ghost_points(u, v, e, S)
-        return [u, v, e, _r16(st[3], form)]
-
-    m = Model(S, storage=form, storage_scale_uv=s)
-    m.set_state(Prog)
-    ref = store(list(Prog))
-    for x, y, name in zip(m.get_state(), ref, ("u", "v", "η", "sst")):
-        assert_bitwise(x, y, f"{name} stored at set_state")
-    o = O.Oracle(S)
-    for k in range(1, 6):
-        o.set_state(type(Prog)(*ref))
-        o.run(1)
-        ref = store(list(o.get_state()))
-        m.run(1)
-        for x, y, name in zip(m.get_state(), ref, ("u", "v", "η", "sst")):
-            assert_bitwise(x, y, f"{name} after {k} steps ({form})")
-
-
 def test_contexts_reuse_memory_and_trim():
     """Destroyed contexts leave their blocks to the next context of the same
     shape (zeroed again at creation); sw_trim_memory returns them to CUDA."""
