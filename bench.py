@@ -203,16 +203,25 @@ def bench_ensemble(args, rank, world, barrier, allmax):
     t = allmax(secs)
     value = sum(costs) / t
     threaded = seq = None
+    sample = members
     if world == 1:
         one = {}                                    # a single batch, for the time of its steps alone
         run_ensemble(members, costs=costs, batched=True, info=one, chunks=1)
         binfo["run_seconds"] = one["run_seconds"]
+        # the looped single-member runs (contexts on threads, and one after
+        # another) on every member, or on every k-th member when
+        # --compare-members bounds their time; their value is their own
+        # cell-updates over their own time
+        if 0 < args.compare_members < len(members):
+            step = len(members) / args.compare_members
+            sample = [members[int(k * step)] for k in range(args.compare_members)]
+        scost = sum(member_cost(m) for m in sample)
         t0 = time.perf_counter()
-        run_local(members, threads=args.threads)
-        threaded = sum(costs) / (time.perf_counter() - t0)
+        run_local(sample, threads=args.threads)
+        threaded = scost / (time.perf_counter() - t0)
         t0 = time.perf_counter()
-        run_local(members, threads=1)
-        seq = sum(costs) / (time.perf_counter() - t0)
+        run_local(sample, threads=1)
+        seq = scost / (time.perf_counter() - t0)
     if rank == 0:
         print(json.dumps({
             "metric": "ensemble cell-updates/s", "value": value, "unit": UNIT, "n_gpus": world,
@@ -225,6 +234,7 @@ def bench_ensemble(args, rank, world, barrier, allmax):
             "seconds": t, "batch_run_seconds": binfo.get("run_seconds"),
             "batch_run_value": (sum(costs) / binfo["run_seconds"]) if world == 1 and binfo.get("run_seconds") else None,
             "threaded_value": threaded, "threads": args.threads, "sequential_value": seq,
+            "compared_members": len(sample),
             "nan_members": int((table[:, COLUMNS.index("nan_count")] > 0).sum())}))
     return 0
 
@@ -294,6 +304,8 @@ def main():
     ap.add_argument("--days", type=float, default=1.0, help="model days per ensemble member")
     ap.add_argument("--threads", type=int, default=8, help="members run at once per GPU")
     ap.add_argument("--chunks", type=int, default=2, help="ensemble batches per GPU, pipelined with their set-up")
+    ap.add_argument("--compare-members", type=int, default=0,
+                    help="run the looped single-member comparison on this many members (0: all)")
     ap.add_argument("--build", default="parity", choices=["parity", "fast"],
                     help="parity: libswb200.so (no FMA contraction, bit-exact with the oracle); "
                          "fast: libswb200_fast.so (FMA contraction, equal to the oracle to rounding)")

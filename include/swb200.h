@@ -197,6 +197,13 @@ int sw_set_state(sw_ctx* ctx, const void* u, const void* v,
 int sw_run(sw_ctx* ctx, int64_t nsteps, sw_status* status);
 /* Download the current state with halo (Tprog). */
 int sw_get_state(sw_ctx* ctx, void* u, void* v, void* eta, void* sst);
+/* The u, v, eta (with halo, Tprog) that the last right-hand-side evaluation
+ * of the last step read: the input of its last RK stage or SSP sub-stage, or
+ * the current state before any step.  The reference's output writes q and the
+ * relative vorticity from its work arrays (src/output.jl:105-115), which hold
+ * the values of that evaluation (src/PV_advection.jl:2-18, src/rhs.jl:89-128);
+ * they follow from this state, H and f_q.  Native storage only. */
+int sw_get_rhs_input(sw_ctx* ctx, void* u, void* v, void* eta);
 /* FP64 reductions over the current state. */
 int sw_diagnostics(sw_ctx* ctx, sw_diag* out);
 /* sw_diagnostics for callers that cannot allocate device memory (for example
@@ -288,10 +295,16 @@ void sw_batch_destroy(sw_batch* b);
  * after nsteps, with halo) may be NULL.  ncheckpoints >= nsteps keeps every
  * step state on the device and, memory permitting (off with
  * SWB200_ADJ_STORE=0), every step's RK stage inputs and tail input as well, so
- * the reverse sweep recomputes only each pass's intermediates; fewer slots
- * recompute states with the binomial checkpoint schedule.  ncheckpoints is an
- * upper bound: when that many state slots do not fit in device memory, half
- * as many are tried (down to one); stats->checkpoints reports the number used.  The derivative of sqrt at 0 (drag and Smagorinsky at
+ * the reverse sweep recomputes only each pass's intermediates.  With fewer
+ * checkpoints than steps the schedule is two-level: a state slot at the start
+ * of each segment of ceil(nsteps / ncheckpoints) steps, and the reverse sweep
+ * recomputes one segment at a time while keeping its steps' stage inputs, so
+ * every step is recomputed once; when a segment's stage inputs do not fit in
+ * device memory (or with SWB200_ADJ_SCHEDULE=binomial) the binomial
+ * checkpoint schedule recomputes states from the slots alone.  ncheckpoints
+ * is an upper bound: when that many state slots do not fit in device memory,
+ * half as many are tried (down to one, binomial schedule);
+ * stats->checkpoints reports the number used.  The derivative of sqrt at 0 (drag and Smagorinsky at
  * rest) is taken as 0.  Gradients are summed with atomics, so repeated calls
  * agree to rounding, not bit for bit.  stats may be NULL. */
 typedef struct sw_adjoint_stats {
@@ -302,7 +315,8 @@ typedef struct sw_adjoint_stats {
     int32_t checkpoints;               /* state slots used                            */
     int32_t launches_per_forward_step;
     int32_t launches_per_adjoint_step;
-    int32_t stored_stage_states;       /* 1: every step's stage inputs were kept (no forward recomputation) */
+    int32_t stored_stage_states;       /* 1: every step's stage inputs were kept (no forward recomputation);
+                                          2: kept per segment (two-level schedule); 0: not kept */
 } sw_adjoint_stats;
 int sw_adjoint_run(const sw_config* cfg, const sw_static* st,
                    const void* u, const void* v, const void* eta, const void* eta_obs,

@@ -1370,7 +1370,8 @@ struct Adjoint {
         return carve(c, &st.base, &st.elems);
     }
 
-    int setup(const sw_config& c, const sw_static& stt, bool want_store, long long nsteps) {
+    // want_store: keep nrecords steps' stage inputs (all steps, or one segment)
+    int setup(const sw_config& c, const sw_static& stt, bool want_store, long long nrecords) {
         if (!host && cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return SW_ERR_CUDA;
         w.nx = c.nx; w.ny = c.ny; w.ep = c.periodic ? 1 : 0;
         w.nux = w.ep ? c.nx : c.nx - 1; w.nuy = c.ny; w.nvx = c.nx; w.nvy = c.ny - 1;
@@ -1468,7 +1469,7 @@ struct Adjoint {
             if (!carve(cv, &w.tail_adj, &w.tail_adj_elems)) return SW_ERR_NOMEM;
         }
         if (want_store) {   // one record per step; without the memory the steps are recomputed instead
-            const size_t n = (size_t)nsteps * w.stage_block_elems;
+            const size_t n = (size_t)nrecords * w.stage_block_elems;
             void* p = nullptr;
             if (host) p = std::calloc(n, sizeof(T));
             else if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) { p = nullptr; cudaGetLastError(); }
@@ -1548,9 +1549,10 @@ struct Adjoint {
         if (host) { Launcher L = launcher(); adj_step(L, w, false, t == 1); return cudaSuccess; }
         return cudaGraphLaunch(g_adj[t], s);
     }
-    cudaError_t adjoint_stored(long long k) {   // Xb <- adjoint of the step from state k, from its kept stage states
+    // Xb <- adjoint of the step from state k, from its stage states kept in record rec
+    cudaError_t adjoint_stored(long long k, long long rec) {
         Launcher L = launcher();
-        L.copy(w.stage_block, records + (size_t)k * w.stage_block_elems, w.stage_block_elems * sizeof(T));
+        L.copy(w.stage_block, records + (size_t)rec * w.stage_block_elems, w.stage_block_elems * sizeof(T));
         adj_steps++;
         const int t = tail_of(k) ? 1 : 0;
         set_force(k);
@@ -1607,10 +1609,20 @@ int adjoint_run(bool host, const sw_config& c, const sw_static& st, const void* 
     A.host = host;
     // Keeping every step's stage inputs (rko + 1 states a step) spares the
     // reverse sweep the recomputation of the forward step; it needs a slot per
-    // step and is off with SWB200_ADJ_STORE=0.
+    // step and is off with SWB200_ADJ_STORE=0.  With fewer checkpoints than
+    // steps the default schedule is two-level: a state slot at the start of
+    // each segment of seg = ceil(nsteps / ncheckpoints) steps, and the reverse
+    // sweep recomputes one segment at a time, keeping its steps' stage inputs
+    // (seg records), so every step is recomputed once.  When those records do
+    // not fit, or with SWB200_ADJ_SCHEDULE=binomial, the binomial schedule
+    // runs instead on the state slots alone.
     const char* env = getenv("SWB200_ADJ_STORE");
-    const bool want_store = ncheckpoints >= nsteps && !(env && env[0] == '0');
-    int rc = A.setup(c, st, want_store, nsteps);
+    const char* envs = getenv("SWB200_ADJ_SCHEDULE");
+    const bool store_ok = !(env && env[0] == '0');
+    const bool all_steps = ncheckpoints >= nsteps;
+    const bool want_segments = !all_steps && store_ok && !(envs && std::string(envs) == "binomial");
+    const long long seg = want_segments ? (nsteps + ncheckpoints - 1) / std::max<long long>(1, ncheckpoints) : 0;
+    int rc = A.setup(c, st, store_ok && (all_steps || want_segments), all_steps ? nsteps : seg);
     if (!rc) rc = A.make_forcing(c, nsteps);
     if (rc) {
         if (!A.err.empty()) fprintf(stderr, "swb200: %s\n", A.err.c_str());
@@ -1633,8 +1645,17 @@ int adjoint_run(bool host, const sw_config& c, const sw_static& st, const void* 
         else if (rowsum) cudaFree(rowsum);
         rowsum = nullptr;
     };
-    int nslots = A.stored ? 1 : (int)std::max<long long>(1, std::min<long long>(ncheckpoints, nsteps));
+    const bool segments = want_segments && A.stored;      // the segment's records fit
+    const bool stored_all = all_steps && A.stored;
+    int nslots = stored_all ? 1
+               : segments ? (int)((nsteps + seg - 1) / seg)
+                          : (int)std::max<long long>(1, std::min<long long>(ncheckpoints, nsteps));
     if (!A.make_slots(nslots)) {
+        free_rowsum();
+        return SW_ERR_NOMEM;
+    }
+    if (segments && (int)A.slots.size() < nslots) {
+        // fewer slots than segments: no room for the two-level schedule
         free_rowsum();
         return SW_ERR_NOMEM;
     }
@@ -1667,7 +1688,8 @@ int adjoint_run(bool host, const sw_config& c, const sw_static& st, const void* 
     for (long long k = 1; k <= nsteps && e == cudaSuccess; k++) {
         e = A.advance(k - 1, 1);
         if (keep_all && k < nsteps) A.copy(A.slots[k], w.X);
-        if (A.stored) {
+        if (segments && k % seg == 0 && k < nsteps) A.copy(A.slots[k / seg], w.X);
+        if (stored_all) {
             Launcher L = A.launcher();
             L.copy(A.records + (size_t)(k - 1) * w.stage_block_elems, w.stage_block, w.stage_block_elems * sizeof(T));
         }
@@ -1686,8 +1708,20 @@ int adjoint_run(bool host, const sw_config& c, const sw_static& st, const void* 
     if (e == cudaSuccess) e = A.zero(w.bFx.d, w.bFx.size() * sizeof(T));
     // reverse sweep
     if (e == cudaSuccess) {
-        if (A.stored) {
-            for (long long k = nsteps - 1; k >= 0 && e == cudaSuccess; k--) e = A.adjoint_stored(k);
+        if (stored_all) {
+            for (long long k = nsteps - 1; k >= 0 && e == cudaSuccess; k--) e = A.adjoint_stored(k, k);
+        } else if (segments) {
+            for (long long j = nslots - 1; j >= 0 && e == cudaSuccess; j--) {
+                const long long a = j * seg, b = std::min<long long>(nsteps, a + seg);
+                A.copy(w.X, A.slots[j]);
+                for (long long k = a; k < b && e == cudaSuccess; k++) {
+                    e = A.advance(k, 1);
+                    Launcher L = A.launcher();
+                    L.copy(A.records + (size_t)(k - a) * w.stage_block_elems, w.stage_block,
+                           w.stage_block_elems * sizeof(T));
+                }
+                for (long long k = b - 1; k >= a && e == cudaSuccess; k--) e = A.adjoint_stored(k, k - a);
+            }
         } else if (keep_all) {
             for (long long k = nsteps - 1; k >= 0 && e == cudaSuccess; k--) e = A.adjoint_of(A.slots[k], k);
         } else {
@@ -1722,7 +1756,7 @@ int adjoint_run(bool host, const sw_config& c, const sw_static& st, const void* 
         stats->checkpoints = nslots;
         stats->launches_per_forward_step = A.launches_fwd;
         stats->launches_per_adjoint_step = A.launches_adj;
-        stats->stored_stage_states = A.stored ? 1 : 0;
+        stats->stored_stage_states = stored_all ? 1 : segments ? 2 : 0;
     }
     return SW_OK;
 }

@@ -210,7 +210,10 @@ struct sw_ctx {
     // CUDA graphs of one time step, keyed by the buffer parities and the
     // sub-steps that are due (see step_key); off with SWB200_GRAPHS=0
     bool use_graphs = true;
-    struct StepGraph { cudaGraphExec_t exec = nullptr; long long launches = 0; bool flips_sp = false; };
+    struct StepGraph { cudaGraphExec_t exec = nullptr; long long launches = 0; bool flips_sp = false; Fields3 rhs_in; };
+    // the buffers the last right-hand-side evaluation of the last step read
+    // (the input of the last RK stage or SSP sub-stage); null before a step
+    Fields3 rhs_in;
     std::map<unsigned, StepGraph> graphs;
     int nsm = 148;
     int tail_ty = TAIL_TY;        // rows per warp strip of the streaming tail (see pick_strip_ty)
@@ -659,6 +662,7 @@ struct Engine : EngineBase {
             if (combo) cmb = is_last ? &fin : free_buf(out);
             if (!out || (combo && !cmb)) return fail(ctx, SW_ERR_ARG, "no free SSP stage buffer");
             a.u1 = (const Tp*)cur->u; a.v1 = (const Tp*)cur->v; a.e1 = (const Tp*)cur->e;
+            if (is_last) ctx->rhs_in = *cur;
             a.uZ = (const Tp*)snap->u; a.vZ = (const Tp*)snap->v; a.eZ = (const Tp*)snap->e;
             a.u1o = (Tp*)out->u; a.v1o = (Tp*)out->v; a.e1o = (Tp*)out->e;
             if (combo) {
@@ -786,6 +790,7 @@ struct Engine : EngineBase {
             StageArgs<T, Tp> a = stage_args(ctx, k, ctx->p, tail_now, Fxt, Fyt);
             const Fields3& in = (k == 1) ? X : ((k % 2 == 0) ? ctx->A : ctx->B);
             const bool first = (k == 1), last = (k == c.RKo);
+            if (last) ctx->rhs_in = in;
             int rc;
             if (c.dynamics == SW_LINEAR) {
                 rc = launch(ctx, 0, [&] { lin_rk_dispatch(ctx, a, g.ep != 0, first, last); });
@@ -1345,6 +1350,7 @@ int do_step(sw_ctx* ctx, long long i) {
         sw_ctx::StepGraph sg;
         sg.launches = ctx->launches - l0;
         sg.flips_sp = ctx->sp != sp0;
+        sg.rhs_in = ctx->rhs_in;
         ctx->t = t0; ctx->launches = l0; ctx->sp = sp0;
         if (!rc && e == cudaSuccess) e = cudaGraphInstantiate(&sg.exec, graph, 0);
         if (graph) cudaGraphDestroy(graph);
@@ -1361,6 +1367,7 @@ int do_step(sw_ctx* ctx, long long i) {
     ctx->launches += it->second.launches;
     ctx->t += c.dtint;
     if (it->second.flips_sp) ctx->sp = 1 - ctx->sp;
+    ctx->rhs_in = it->second.rhs_in;
     return SW_OK;
 }
 
@@ -2162,6 +2169,7 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
 int sw_set_state(sw_ctx* ctx, const void* u, const void* v, const void* eta, const void* sst) {
     if (!ctx || !u || !v || !eta || !sst) return SW_ERR_ARG;
     ctx->p = 0; ctx->sp = 0; ctx->step = 0; ctx->t = 0;
+    ctx->rhs_in = Fields3();
     int rc;
     if ((rc = copy_in(ctx, ctx->S[0].u, u, shape_u(ctx->g)))) return rc;
     if ((rc = copy_in(ctx, ctx->S[0].v, v, shape_v(ctx->g)))) return rc;
@@ -2189,6 +2197,19 @@ int sw_get_state(sw_ctx* ctx, void* u, void* v, void* eta, void* sst) {
     if ((rc = copy_out(ctx, v, X.v, shape_v(ctx->g)))) return rc;
     if ((rc = copy_out(ctx, eta, X.e, shape_e(ctx->g)))) return rc;
     if ((rc = copy_out(ctx, sst, ctx->sst[ctx->sp], shape_s(ctx->g)))) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SW_OK;
+}
+
+int sw_get_rhs_input(sw_ctx* ctx, void* u, void* v, void* eta) {
+    if (!ctx || !u || !v || !eta) return SW_ERR_ARG;
+    if (ctx->cfg.storage != SW_STORE_NATIVE)
+        return fail(ctx, SW_ERR_UNSUPPORTED, "the 16-bit storage form keeps its stage values in 16 bits");
+    const Fields3& X = ctx->rhs_in.u ? ctx->rhs_in : ctx->S[ctx->p];
+    int rc;
+    if ((rc = copy_out(ctx, u, X.u, shape_u(ctx->g)))) return rc;
+    if ((rc = copy_out(ctx, v, X.v, shape_v(ctx->g)))) return rc;
+    if ((rc = copy_out(ctx, eta, X.e, shape_e(ctx->g)))) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
     return SW_OK;
 }

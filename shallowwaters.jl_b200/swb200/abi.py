@@ -190,6 +190,7 @@ EXPORTS = {
     "sw_set_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "sw_run": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p]),
     "sw_get_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "sw_get_rhs_input": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "sw_diagnostics": (C.c_int, [C.c_void_p, C.c_void_p]),
     "sw_run_profiled": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p]),
     "sw_run_timed": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.POINTER(C.c_double), C.c_void_p]),

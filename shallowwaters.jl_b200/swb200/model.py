@@ -59,6 +59,18 @@ class Model:
         abi.check(self.lib, rc, self.ctx)
         return PrognosticVars(u, v, e, s)
 
+    def get_rhs_input(self):
+        """u, v, η (with halo) that the last right-hand-side evaluation of the
+        last step read (the input of its last RK stage or SSP sub-stage): the
+        state the reference's vorticity work arrays describe after a step."""
+        G, Tp = self.S.grid, self.Tp
+        u = np.zeros((G.nuy + 4, G.nux + 4), Tp)
+        v = np.zeros((G.nvy + 4, G.nvx + 4), Tp)
+        e = np.zeros((G.ny + 2, G.nx + 2), Tp)
+        rc = self.lib.sw_get_rhs_input(self.ctx, *abi.state_ptrs(u, v, e, e)[:3])
+        abi.check(self.lib, rc, self.ctx)
+        return u, v, e
+
     def run(self, nsteps: int) -> abi.SwStatus:
         st = abi.SwStatus()
         rc = self.lib.sw_run(self.ctx, int(nsteps), C.byref(st))

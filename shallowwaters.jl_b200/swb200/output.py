@@ -125,9 +125,12 @@ class NcFiles:
             var.units, var.long_name, var.missing_value = unit, long_name, np.float32(-999999.0)
             self.files[key] = (nc, name)
 
-    def write(self, i, new, old):
+    def write(self, i, new, old, rhs=None):
         """output_nc!(i) (src/output.jl:63-133): ``new`` is the state after step i
-        and ``old`` the one before it, both with halo."""
+        and ``old`` the one before it, both with halo.  ``rhs`` is the (u, v, η)
+        the reference's vorticity work arrays were last computed from (the
+        input of the step's last right-hand-side evaluation); q and relvort
+        come from it, or from ``new`` when it is not given."""
         from .initial_conditions import remove_halo
         S = self.S
         new, old = tuple(new), tuple(old)
@@ -138,7 +141,8 @@ class NcFiles:
                   "du": un.astype(f32) - uo.astype(f32), "dv": vn.astype(f32) - vo.astype(f32),
                   "dη": en.astype(f32) - eo.astype(f32)}
         if "q" in self.files or "ζ" in self.files:
-            frames["q"], frames["ζ"] = vorticities(new[0], new[1], new[2], S)
+            src = rhs if rhs is not None else new
+            frames["q"], frames["ζ"] = vorticities(src[0], src[1], src[2], S)
         k = self.iout
         for key, (nc, name) in self.files.items():
             nc.variables[name][k] = frames[key]

@@ -85,7 +85,19 @@ def _time_integration_with_output(Prog: PrognosticVars, S: ModelSetup, *, storag
     try:
         m.set_state(Prog)
         state = m.get_state()
-        nc.write(0, state, state)                       # output_nc!(0, ...) of the initial state
+        # q and relvort: the reference computes them from the initial state before
+        # its loop (src/time_integration.jl:27-29), then in every right-hand
+        # side of nonlinear dynamics; linear dynamics never recomputes them
+        # (the 16-bit storage form keeps its stage values in 16 bits: its frames
+        # take them from the new state)
+        initial = tuple(np.asarray(a) for a in Prog[:3])
+
+        def rhs_state():
+            if S.parameters.dynamics != "nonlinear":
+                return initial
+            return m.get_rhs_input() if storage == "native" else None
+
+        nc.write(0, state, state, initial)              # output_nc!(0, ...) of the initial state
         i = 0
         status = abi.SwStatus()
         while i < G.nt:
@@ -101,7 +113,7 @@ def _time_integration_with_output(Prog: PrognosticVars, S: ModelSetup, *, storag
                 if status.code != abi.SW_OK:
                     break
                 i += n
-                nc.write(i, m.get_state(), before)
+                nc.write(i, m.get_state(), before, rhs_state())
             else:
                 status = m.run(n)
                 if status.code != abi.SW_OK:

@@ -174,9 +174,17 @@ def test_host_check_of_the_adjoint_passes(host_check_lib, opts):
         Jd, dJ = oracle.jvp(S, Prog, obs, n, du=d[0], dv=d[1], deta=d[2], dFx=d[3])
         assert J == pytest.approx(Jd, rel=1e-13)
         assert directional(g, d) == pytest.approx(dJ, rel=1e-10)
-    J3, g3, _, bad3 = host_check_gradient(host_check_lib, S, Prog, obs, n, 3)
+    J3, g3, _, bad3 = host_check_gradient(host_check_lib, S, Prog, obs, n, 3)     # two-level schedule
     assert bad3 == 0 and J3 == J
     for a, b in zip(g3, g):
+        assert np.array_equal(a, b)
+    os.environ["SWB200_ADJ_SCHEDULE"] = "binomial"
+    try:
+        J3b, g3b, _, bad3b = host_check_gradient(host_check_lib, S, Prog, obs, n, 3)
+    finally:
+        del os.environ["SWB200_ADJ_SCHEDULE"]
+    assert bad3b == 0 and J3b == J
+    for a, b in zip(g3b, g):
         assert np.array_equal(a, b)
     os.environ["SWB200_ADJ_STORE"] = "0"       # every state kept, steps recomputed instead of stored
     try:
@@ -247,12 +255,22 @@ def test_checkpoint_schedule_does_not_change_the_gradient(monkeypatch):
     assert rec.stats.stored_stage_states == 0 and rec.J == full.J
     for a, b in ((rec.u, full.u), (rec.v, full.v), (rec.eta, full.eta), (rec.Fx, full.Fx)):
         np.testing.assert_allclose(a, b, rtol=1e-9, atol=1e-12 * np.abs(b).max())
-    for nc in (6, 2, 1):
-        r = gradient(S, Prog, obs, n, ncheckpoints=nc)
-        assert r.J == full.J
-        assert r.stats.checkpoints == nc and r.stats.forward_steps > n
-        for a, b in ((r.u, full.u), (r.v, full.v), (r.eta, full.eta), (r.Fx, full.Fx)):
-            np.testing.assert_allclose(a, b, rtol=1e-9, atol=1e-12 * np.abs(b).max())
+    # two-level schedule (state slots per segment, stage inputs kept per
+    # segment: each step recomputed once) and the binomial one
+    for schedule in ("segments", "binomial"):
+        if schedule == "binomial":
+            monkeypatch.setenv("SWB200_ADJ_SCHEDULE", "binomial")
+        for nc in (6, 2, 1):
+            r = gradient(S, Prog, obs, n, ncheckpoints=nc)
+            assert r.J == full.J
+            assert r.stats.checkpoints == nc and r.stats.forward_steps > n
+            if schedule == "segments":
+                assert r.stats.stored_stage_states == 2 and r.stats.forward_steps == 2 * n
+            else:
+                assert r.stats.stored_stage_states == 0
+            for a, b in ((r.u, full.u), (r.v, full.v), (r.eta, full.eta), (r.Fx, full.Fx)):
+                np.testing.assert_allclose(a, b, rtol=1e-9, atol=1e-12 * np.abs(b).max())
+    monkeypatch.delenv("SWB200_ADJ_SCHEDULE")
 
 
 @pytest.mark.gpu

@@ -296,6 +296,28 @@ def test_output_frames_match_oracle(tmp_path):
         assert_bitwise(u[-1], out.u.astype(np.float32), "last frame")
 
 
+@pytest.mark.parametrize("kw", [dict(), dict(bc="nonperiodic", diffusion="Smagorinsky"),
+                                dict(time_scheme="SSPRK2", RKs=3, cfl=1.2)])
+def test_vorticity_frames_equal_the_reference_work_arrays(kw):
+    """q from the last right-hand-side input (sw_get_rhs_input) equals the
+    oracle's q work array after the same steps, bit for bit: the values the
+    reference's q frame writes (src/output.jl:105-108)."""
+    from swb200.output import vorticities
+    P = Parameter(nx=40, Ndays=0.3, Uadv=1000, **kw)
+    S = model_setup(P)
+    Prog = initial_conditions(P.Tprog, S, **seeded_inputs(S, 17))
+    o = O.Oracle(S)
+    o.set_state(Prog)
+    m = Model(S)
+    m.set_state(Prog)
+    for n in (1, 5):
+        o.run(n)
+        m.run(n)
+        q, _ = vorticities(*m.get_rhs_input(), S)
+        qo = o.field("q")[:q.shape[0], :q.shape[1]].astype(np.float32)
+        assert_bitwise(q, qo, f"q after {n} more steps")
+
+
 def test_contexts_reuse_memory_and_trim():
     """Destroyed contexts leave their blocks to the next context of the same
     shape (zeroed again at creation); sw_trim_memory returns them to CUDA."""
