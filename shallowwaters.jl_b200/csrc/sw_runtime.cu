@@ -17,7 +17,6 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <atomic>
 #include <map>
 #include <cmath>
 #include <cstdio>
@@ -55,7 +54,7 @@ namespace {
 #endif
 constexpr int STAGE_TY = SWB_STAGE_TY;  // rows per warp strip of the stage kernel
 constexpr int TAIL_TY = SWB_TAIL_TY;
-constexpr int PADX = 72, PADY = 44;     // column/row padding: strips read up to TY+3 rows and 30 columns past the edge
+constexpr int PADX = 72, PADY = 44;     // column/row padding: strips read up to TY+6 rows and 30 columns past the edge
 constexpr int RING_BLOCKS_MAX = 32;
 
 const char* err_name(int c) {
@@ -931,7 +930,7 @@ template <class S16>
 struct Engine16 : Engine<float, float> {
     using Base = Engine<float, float>;
     struct F3 { S16* u = nullptr; S16* v = nullptr; S16* e = nullptr; };
-    F3 hi[2], lo[2], X1[2], D;
+    F3 hi[2], lo[2], X1[2], D[2];   // D: the increments, read from one and written to the other
     S16* sst16[2] = {nullptr, nullptr};
     float s = 1024.f, inv_s = 1.f / 1024.f;
 
@@ -949,7 +948,7 @@ struct Engine16 : Engine<float, float> {
             *p = static_cast<S16*>(q);
             return SW_OK;
         };
-        for (F3* f : {&hi[0], &hi[1], &lo[0], &lo[1], &X1[0], &X1[1], &D})
+        for (F3* f : {&hi[0], &hi[1], &lo[0], &lo[1], &X1[0], &X1[1], &D[0], &D[1]})
             for (S16** p : {&f->u, &f->v, &f->e})
                 if (int rc = alloc(p)) return rc;
         for (S16** p : {&sst16[0], &sst16[1]})
@@ -1045,8 +1044,6 @@ struct Engine16 : Engine<float, float> {
         a.nring_blocks = ring_blocks(g, 128);
         a.uh = hi[p].u; a.vh = hi[p].v; a.eh = hi[p].e;
         a.ul = lo[p].u; a.vl = lo[p].v; a.el = lo[p].e;
-        a.uD = D.u; a.vD = D.v; a.eD = D.e;
-        a.uDo = D.u; a.vDo = D.v; a.eDo = D.e;
         a.u0o = (float*)ctx->Acc.u; a.v0o = (float*)ctx->Acc.v; a.e0o = (float*)ctx->Acc.e;
         a.eho = hi[q].e; a.elo = lo[q].e;
         a.H = sf<float>(ctx->H); a.fq = sf<float>(ctx->fq); a.Fx = sf<float>(ctx->Fx); a.Fy = sf<float>(ctx->Fy);
@@ -1060,6 +1057,9 @@ struct Engine16 : Engine<float, float> {
             const F3& out1 = X1[k % 2 == 1 ? 0 : 1];
             a.u1 = in.u; a.v1 = in.v; a.e1 = in.e;
             a.u1o = out1.u; a.v1o = out1.v; a.e1o = out1.e;
+            const F3& din = D[k % 2], &dout = D[(k + 1) % 2];
+            a.uD = din.u; a.vD = din.v; a.eD = din.e;
+            a.uDo = dout.u; a.vDo = dout.v; a.eDo = dout.e;
             a.a = (float)c.RKaDt[k - 1];
             a.b = (k < c.RKo) ? (float)c.RKbDt[k - 1] : 0.f;
             const bool first = k == 1, last = k == c.RKo;
@@ -1175,37 +1175,40 @@ int check_config(const sw_config* c, std::string& why) {
     return SW_OK;
 }
 
-// Runs f(j0, j1) over row ranges covering [0, h), on up to 8 host threads
-// when the field is large (work = bytes to scan); true if every call was.
-template <class F>
-bool all_row_ranges(int h, size_t work, F&& f) {
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const int nt = (int)std::min<size_t>(std::min(8u, hw), std::max<size_t>(1, work >> 22));
-    if (nt <= 1 || h < 2 * nt) return f(0, h);
-    std::atomic<bool> ok{true};
-    std::vector<std::thread> th;
-    for (int k = 0; k < nt; k++) {
-        const int j0 = (int)((long long)h * k / nt), j1 = (int)((long long)h * (k + 1) / nt);
-        th.emplace_back([&, j0, j1] { if (!f(j0, j1)) ok = false; });
+// Rows [j0, j1) of a w-wide host field with W-sized elements (bitwise):
+// whether every row is constant along x, and whether every row equals row 0.
+template <class W>
+void scan_rows(const unsigned char* src, int w, int j0, int j1, bool& cx, bool& cy) {
+    const W* base = reinterpret_cast<const W*>(src);
+    for (int j = j0; j < j1 && (cx || cy); j++) {
+        const W* r = base + (size_t)j * w;
+        const W a = r[0];
+        bool rx = cx, ry = cy && j > 0;
+        for (int i = 0; i < w && (rx || ry); i++) {
+            if (rx && r[i] != a) rx = false;
+            if (ry && r[i] != base[i]) ry = false;
+        }
+        cx = rx;
+        if (j > 0) cy = ry;
     }
-    for (auto& t : th) t.join();
-    return ok;
 }
 
-// Rows [j0, j1) of a w-wide host field with W-sized elements: is every row
-// constant along x (bitwise)?
+// Both tests over the whole field, on the OpenMP threads when it is large
+// (host arrays are element-aligned, so they are read as W words).
 template <class W>
-bool rows_const_x(const unsigned char* src, int w, int j0, int j1) {
-    for (int j = j0; j < j1; j++) {
-        const unsigned char* r = src + (size_t)j * w * sizeof(W);
-        W a, b;
-        std::memcpy(&a, r, sizeof(W));
-        for (int i = 1; i < w; i++) {
-            std::memcpy(&b, r + (size_t)i * sizeof(W), sizeof(W));
-            if (b != a) return false;
-        }
+void scan_field(const unsigned char* src, int w, int h, bool& const_x, bool& const_y) {
+    bool cx = true, cy = true;
+    const long long bytes = (long long)w * h * sizeof(W);
+    const int nt = (int)std::min<long long>(8, std::max<long long>(1, bytes >> 21));
+#pragma omp parallel for num_threads(nt) reduction(&& : cx, cy) schedule(static) if (nt > 1)
+    for (int k = 0; k < nt; k++) {
+        bool x = true, y = true;
+        scan_rows<W>(src, w, (int)((long long)h * k / nt), (int)((long long)h * (k + 1) / nt), x, y);
+        cx = cx && x;
+        cy = cy && y;
     }
-    return true;
+    const_x = cx;
+    const_y = cy;
 }
 
 // Host-side packing of a static field (T, x fastest, host column 0 at
@@ -1217,16 +1220,10 @@ PackedStatic pack_static(const sw_ctx* ctx, const void* host, int w, int h, int 
     const size_t ts = ctx->tsz;
     const unsigned char* src = static_cast<const unsigned char*>(host);
     auto el = [&](int i, int j) { return src + ((size_t)j * w + i) * ts; };
-    const size_t bytes = (size_t)w * h * ts;
-    const bool const_x = all_row_ranges(h, bytes, [&](int j0, int j1) {
-        return ts == 2 ? rows_const_x<uint16_t>(src, w, j0, j1)
-             : ts == 4 ? rows_const_x<uint32_t>(src, w, j0, j1) : rows_const_x<uint64_t>(src, w, j0, j1);
-    });
-    const bool const_y = all_row_ranges(h, bytes, [&](int j0, int j1) {
-        for (int j = std::max(j0, 1); j < j1; j++)
-            if (std::memcmp(el(0, j), el(0, 0), ts * (size_t)w)) return false;
-        return true;
-    });
+    bool const_x = true, const_y = true;
+    if (ts == 2) scan_field<uint16_t>(src, w, h, const_x, const_y);
+    else if (ts == 4) scan_field<uint32_t>(src, w, h, const_x, const_y);
+    else scan_field<uint64_t>(src, w, h, const_x, const_y);
     const Geom& g = ctx->g;
     PackedStatic out;
     std::vector<unsigned char>& buf = out.buf;

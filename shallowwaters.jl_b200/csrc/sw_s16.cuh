@@ -65,7 +65,7 @@ struct S16StageArgs {
     const S16* ul; const S16* vl; const S16* el;   // state lo (read by the last stage)
     const S16* uD; const S16* vD; const S16* eD;   // increment so far (not read by the first stage)
     S16* u1o; S16* v1o; S16* e1o;                  // X1' (not the last stage)
-    S16* uDo; S16* vDo; S16* eDo;                  // increment out (not the last stage)
+    S16* uDo; S16* vDo; S16* eDo;                  // increment out (not the last stage; not the D read)
     float* u0o; float* v0o; float* e0o;            // last stage: X0 in FP32, with ghost copies
     S16* eho; S16* elo;                            // last stage: the new eta pair, with ghost copies
     SField<float> H, fq, Fx, Fy;
@@ -78,6 +78,11 @@ struct S16StageArgs {
 
 template <class S16>
 __device__ __forceinline__ float ld16(const S16* p, int k, float inv_s) { return from16(p[k]) * inv_s; }
+
+#ifndef SWB_S16_PF
+#define SWB_S16_PF 3       // input rows of the stage kernel in flight ahead of the one consumed
+#endif
+constexpr int S16_PF = SWB_S16_PF;
 
 // untouched halo cells of u and v: X1' = X, D' = D, X0 = X + D
 template <class S16, bool FIRST, bool LAST>
@@ -147,6 +152,9 @@ s16_stage_kernel(const __grid_constant__ S16StageArgs<S16> A) {
     const S16* __restrict__ pu = A.u1 + cb;
     const S16* __restrict__ pv = A.v1 + cb;
     const S16* __restrict__ pe = A.e1 + cb;
+    const S16* __restrict__ xh[3] = {A.uh + cb, A.vh + cb, A.eh + cb};
+    const S16* __restrict__ xl[3] = {A.ul + cb, A.vl + cb, A.el + cb};
+    const S16* __restrict__ xd[3] = {A.uD + cb, A.vD + cb, A.eD + cb};
     const int Hsy = A.H.sy;
     const float* __restrict__ pH = A.H.p + cb * A.H.sx;
     const float* __restrict__ pfq = A.fq.p + cb * A.fq.sx;
@@ -168,17 +176,45 @@ s16_stage_kernel(const __grid_constant__ S16StageArgs<S16> A) {
         hN_r = ld16(A.e1, g.idx(N, r), inv) + A.H.at(N, r);
         hNm1_r = ld16(A.e1, g.idx(N - 1, r), inv) + A.H.at(N - 1, r);
     }
-    S16 pu1 = pu[row(r + 1)], pv1 = pv[row(r + 1)], pe1 = pe[row(r + 1)];
-    float pH1 = pH[(r + 1 + ROW0) * Hsy];
+    // software pipeline: input rows r+1 .. r+S16_PF in flight; the point-wise
+    // operands (hi, lo, D) of the output row one iteration ahead
+    S16 qu[S16_PF], qv[S16_PF], qe[S16_PF];
+    float qH[S16_PF];
+#pragma unroll
+    for (int k = 0; k < S16_PF; k++) {
+        qu[k] = pu[row(r + 1 + k)]; qv[k] = pv[row(r + 1 + k)]; qe[k] = pe[row(r + 1 + k)];
+        qH[k] = pH[(r + 1 + k + ROW0) * Hsy];
+    }
+    S16 nh[3], nl[3], nd[3];
+#pragma unroll
+    for (int f = 0; f < 3; f++) nh[f] = nl[f] = nd[f] = to16<S16>(0.f);
+    auto load_pw = [&](int y) {
+        if (FIRST || y < y0 || !out_lane) return;
+        const int oy = row(y);
+#pragma unroll
+        for (int f = 0; f < 3; f++) {
+            nh[f] = xh[f][oy];
+            nd[f] = xd[f][oy];
+            if (LAST) nl[f] = xl[f][oy];
+        }
+    };
+    load_pw(r);
 
     for (; r < y0 + TY; r++) {
-        const float u_r1 = from16(pu1) * inv, v_r1 = from16(pv1) * inv, e_r1 = from16(pe1) * inv;
-        const float h_r1 = e_r1 + pH1;
+        const float u_r1 = from16(qu[0]) * inv, v_r1 = from16(qv[0]) * inv, e_r1 = from16(qe[0]) * inv;
+        const float h_r1 = e_r1 + qH[0];
+#pragma unroll
+        for (int k = 0; k + 1 < S16_PF; k++) { qu[k] = qu[k + 1]; qv[k] = qv[k + 1]; qe[k] = qe[k + 1]; qH[k] = qH[k + 1]; }
         {
-            const int o2 = row(r + 2);
-            pu1 = pu[o2]; pv1 = pv[o2]; pe1 = pe[o2];
-            pH1 = pH[(r + 2 + ROW0) * Hsy];
+            const int on = row(r + 1 + S16_PF);
+            qu[S16_PF - 1] = pu[on]; qv[S16_PF - 1] = pv[on]; qe[S16_PF - 1] = pe[on];
+            qH[S16_PF - 1] = pH[(r + 1 + S16_PF + ROW0) * Hsy];
         }
+        // the output row's point-wise operands (issued one iteration earlier); issue the next row's
+        S16 ch[3], cl[3], cd[3];
+#pragma unroll
+        for (int f = 0; f < 3; f++) { ch[f] = nh[f]; cl[f] = nl[f]; cd[f] = nd[f]; }
+        load_pw(r + 1);
         const float hl_r1 = shup(h_r1), vl_r1 = shup(v_r1), ur_r1 = shdn(u_r1);
         float q_r1;
         const float fq = pfq[(r + 1 + ROW0) * fqsy];
@@ -211,18 +247,18 @@ s16_stage_kernel(const __grid_constant__ S16StageArgs<S16> A) {
             const int o = row(r) + cb;
             // X: the state's hi (on the first stage that is the input row itself);
             // on the last stage X0 = (hi + lo) + D, else the increment D (0 first)
-            auto base = [&](const S16* ph, const S16* pl, const S16* pD) {
-                if (LAST) return ((from16(ph[o]) + from16(pl[o])) + from16(pD[o])) * inv;
-                return FIRST ? 0.f : from16(pD[o]) * inv;
+            auto base = [&](int f) {
+                if (LAST) return ((from16(ch[f]) + from16(cl[f])) + from16(cd[f])) * inv;
+                return FIRST ? 0.f : from16(cd[f]) * inv;
             };
             if (col_u) {
                 const float qhv = qa * V_r1 + qb * Vl_r1 + qc * Vl_r + qd * V_r;
                 const float dpdx = p_r - pl_r;
                 const float du = (qhv - dpdx) + A.Fxt * A.Fx.at(c, r);
                 const bool gs = gx_u || (!PER && (r <= 1 || r >= M - 2));
-                const float x0 = base(A.uh, A.ul, A.uD) + A.a * du;
+                const float x0 = base(0) + A.a * du;
                 if (!LAST) {
-                    const float X = FIRST ? u_r : from16(A.uh[o]) * inv;
+                    const float X = FIRST ? u_r : from16(ch[0]) * inv;
                     const float x1 = X + A.b * du;
                     A.u1o[o] = put(x1);
                     if (gs) A.gr.u(A.u1o, g, c, r, x1, put);
@@ -237,9 +273,9 @@ s16_stage_kernel(const __grid_constant__ S16StageArgs<S16> A) {
                     const float qhu = qhu_part + qcr * Ur_r + qd * U_r;
                     const float dpdy = p_r - p_rm1;
                     const float dv = -(qhu + dpdy) + A.Fyt * A.Fy.at(c, r);
-                    const float x0 = base(A.vh, A.vl, A.vD) + A.a * dv;
+                    const float x0 = base(1) + A.a * dv;
                     if (!LAST) {
-                        const float X = FIRST ? v_r : from16(A.vh[o]) * inv;
+                        const float X = FIRST ? v_r : from16(ch[1]) * inv;
                         const float x1 = X + A.b * dv;
                         A.v1o[o] = put(x1);
                         if (gx_v) A.gr.v(A.v1o, g, c, r, x1, put);
@@ -253,9 +289,9 @@ s16_stage_kernel(const __grid_constant__ S16StageArgs<S16> A) {
                 const float dVdy = V_r1 - V_r;
                 const float de = -(dUdx + dVdy);
                 const bool gs = gx_e || r == 0 || r == M - 1;
-                const float x0 = base(A.eh, A.el, A.eD) + A.a * de;
+                const float x0 = base(2) + A.a * de;
                 if (!LAST) {
-                    const float X = FIRST ? e_r : from16(A.eh[o]) * inv;
+                    const float X = FIRST ? e_r : from16(ch[2]) * inv;
                     const float x1 = X + A.b * de;
                     A.e1o[o] = put(x1);
                     if (gs) A.gr.eta(A.e1o, g, c, r, x1, put);

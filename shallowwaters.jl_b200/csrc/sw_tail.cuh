@@ -77,6 +77,10 @@ __device__ void tail_ring(const TailArgs<T, Tp>& A, int k0, int kstride, const S
 #ifndef SWB_TAIL_MINB
 #define SWB_TAIL_MINB 1    // resident blocks per SM the register budget is sized for
 #endif
+#ifndef SWB_TAIL_PF
+#define SWB_TAIL_PF 4      // input rows in flight ahead of the one consumed
+#endif
+constexpr int TAIL_PF = SWB_TAIL_PF;
 // DRAG: enum sw_bottom_drag; SMAG: Smagorinsky (else constant νB)
 // The streaming tail for block bx of its grid (strip blocks, then ring blocks).
 template <class T, class Tp, bool PER, int DRAG, bool SMAG, int TY, class ST = TailStoreNative<Tp>>
@@ -128,24 +132,33 @@ __device__ __forceinline__ void tail_body(const TailArgs<T, Tp>& A, int bx, cons
     T S11_r = T(0), S11l_r = T(0), S12_r = T(0), S21_r = T(0), S21r_r = T(0), S22_rm1 = T(0);
     T sKE_rm1 = T(0), sKE_r = T(0), sKEl_r = T(0);
 
-    // software pipeline: at iteration r, row r+2 is consumed while rows r+3
-    // and r+4 are in flight
+    // software pipeline: at iteration r, row r+2 is consumed while rows r+3 ..
+    // r+2+TAIL_PF are in flight (the loads' latency under a full device of
+    // streaming warps spans several iterations)
     T u_r2 = cvt<T>(A.u0[ofs(r + 2)]), v_r2 = cvt<T>(A.v0[ofs(r + 2)]);
     T h_r2 = QUAD ? cvt<T>(A.e0[ofs(r + 2)]) + A.H.at(c, r + 2) : T(0);
-    Tp pu1 = A.u0[ofs(r + 3)], pv1 = A.v0[ofs(r + 3)], pe1 = QUAD ? A.e0[ofs(r + 3)] : Tp(0);
-    T pH1 = QUAD ? A.H.at(c, r + 3) : T(0);
-    Tp pu2 = A.u0[ofs(r + 4)], pv2 = A.v0[ofs(r + 4)], pe2 = QUAD ? A.e0[ofs(r + 4)] : Tp(0);
-    T pH2 = QUAD ? A.H.at(c, r + 4) : T(0);
+    Tp pu[TAIL_PF], pv[TAIL_PF], pe[TAIL_PF];
+    T pH[TAIL_PF];
+#pragma unroll
+    for (int k = 0; k < TAIL_PF; k++) {
+        pu[k] = A.u0[ofs(r + 3 + k)];
+        pv[k] = A.v0[ofs(r + 3 + k)];
+        pe[k] = QUAD ? A.e0[ofs(r + 3 + k)] : Tp(0);
+        pH[k] = QUAD ? A.H.at(c, r + 3 + k) : T(0);
+    }
 
 SWB_ROW_UNROLL
     for (; r < y0 + TY; r++) {
         if (r > y0 - 3) {
-            u_r2 = cvt<T>(pu1); v_r2 = cvt<T>(pv1);
-            h_r2 = QUAD ? cvt<T>(pe1) + pH1 : T(0);
-            pu1 = pu2; pv1 = pv2; pe1 = pe2; pH1 = pH2;
-            const int o4 = ofs(r + 4);
-            pu2 = A.u0[o4]; pv2 = A.v0[o4];
-            if (QUAD) { pe2 = A.e0[o4]; pH2 = A.H.at(c, r + 4); }
+            u_r2 = cvt<T>(pu[0]); v_r2 = cvt<T>(pv[0]);
+            h_r2 = QUAD ? cvt<T>(pe[0]) + pH[0] : T(0);
+#pragma unroll
+            for (int k = 0; k + 1 < TAIL_PF; k++) {
+                pu[k] = pu[k + 1]; pv[k] = pv[k + 1]; pe[k] = pe[k + 1]; pH[k] = pH[k + 1];
+            }
+            const int on = ofs(r + 2 + TAIL_PF);
+            pu[TAIL_PF - 1] = A.u0[on]; pv[TAIL_PF - 1] = A.v0[on];
+            if (QUAD) { pe[TAIL_PF - 1] = A.e0[on]; pH[TAIL_PF - 1] = A.H.at(c, r + 2 + TAIL_PF); }
         }
         const T ul_r2 = shup(u_r2), ur_r2 = shdn(u_r2), vl_r2 = shup(v_r2), vr_r2 = shdn(v_r2);
         const T hl_r2 = QUAD ? shup(h_r2) : T(0);

@@ -90,7 +90,7 @@ def _time_integration_with_output(Prog: PrognosticVars, S: ModelSetup, *, storag
         # side of nonlinear dynamics; linear dynamics never recomputes them
         # (the 16-bit storage form keeps its stage values in 16 bits: its frames
         # take them from the new state)
-        initial = tuple(np.asarray(a) for a in Prog[:3])
+        initial = (np.asarray(Prog.u), np.asarray(Prog.v), np.asarray(Prog.η))
 
         def rhs_state():
             if S.parameters.dynamics != "nonlinear":
