@@ -25,7 +25,6 @@
 #include <memory>
 #include <mutex>
 #include <string>
-#include <thread>
 #include <vector>
 
 #include "swb200.h"
@@ -203,7 +202,6 @@ struct sw_ctx {
     std::map<const void*, Maps> tmaps;
     bool use_tma = false;
     int stage_blocks_cap = 0;     // > 0: at most this many persistent blocks in rk_stage_tma
-    int tracer_rows = 1;          // rows per thread of the tracer kernel (SWB200_TRACER_ROWS)
     uint32_t spin_limit = MBAR_SPIN_LIMIT;   // polls per bounded wait of rk_stage_tma
     int test_skip_chunk = -1;     // test only: a chunk rk_stage_tma's producer leaves out
     // CUDA graphs of one time step, keyed by the buffer parities and the
@@ -395,13 +393,10 @@ __global__ void ghost_state_kernel(Geom g, Tp* u, Tp* v, Tp* e, GhostRule<Tp> gr
     }
 }
 
-// The tracer's launch grid: 128 columns by gy rows of blocks; each thread
-// takes rows b, b + gy, ... (ctx->tracer_rows of them; one thread per cell by
-// default, which measured faster at 2048 x 1024 than 6 rows per thread).
+// The launch grid of tracer_tile_kernel: blocks of 128 columns x TRC_ROWS rows.
 dim3 tracer_grid(const sw_ctx* ctx) {
     const Geom& g = ctx->g;
-    const int rpt = std::max(1, ctx->tracer_rows);
-    return dim3((g.N + 127) / 128, std::min((g.M + rpt - 1) / rpt, 4096));
+    return dim3((g.N + 127) / 128, (g.M + TRC_ROWS - 1) / TRC_ROWS);
 }
 
 template <class T, class Tp>
@@ -529,12 +524,13 @@ struct Engine : EngineBase {
     }
     template <bool PER>
     static void tracer_dispatch2(const TracerArgs<T, Tp>& a, bool um_is_u, bool cons, dim3 grid, cudaStream_t s) {
+        using IO = TracerIONative<T, Tp>;
         if (um_is_u) {
-            if (cons) tracer_kernel<T, Tp, PER, true, true><<<grid, 128, 0, s>>>(a);
-            else tracer_kernel<T, Tp, PER, true, false><<<grid, 128, 0, s>>>(a);
+            if (cons) tracer_tile_kernel<T, Tp, PER, true, true, IO><<<grid, 128, 0, s>>>(a, IO());
+            else tracer_tile_kernel<T, Tp, PER, true, false, IO><<<grid, 128, 0, s>>>(a, IO());
         } else {
-            if (cons) tracer_kernel<T, Tp, PER, false, true><<<grid, 128, 0, s>>>(a);
-            else tracer_kernel<T, Tp, PER, false, false><<<grid, 128, 0, s>>>(a);
+            if (cons) tracer_tile_kernel<T, Tp, PER, false, true, IO><<<grid, 128, 0, s>>>(a, IO());
+            else tracer_tile_kernel<T, Tp, PER, false, false, IO><<<grid, 128, 0, s>>>(a, IO());
         }
     }
 
@@ -1018,12 +1014,13 @@ struct Engine16 : Engine<float, float> {
     template <bool PER>
     static void tracer16(const TracerArgs<float, float>& a, const TracerIO16<S16>& io, bool um_is_u, bool cons,
                          dim3 grid, cudaStream_t st) {
+        using IO = TracerIO16<S16>;
         if (um_is_u) {
-            if (cons) s16_tracer_kernel<S16, PER, true, true><<<grid, 128, 0, st>>>(a, io);
-            else s16_tracer_kernel<S16, PER, true, false><<<grid, 128, 0, st>>>(a, io);
+            if (cons) tracer_tile_kernel<float, float, PER, true, true, IO><<<grid, 128, 0, st>>>(a, io);
+            else tracer_tile_kernel<float, float, PER, true, false, IO><<<grid, 128, 0, st>>>(a, io);
         } else {
-            if (cons) s16_tracer_kernel<S16, PER, false, true><<<grid, 128, 0, st>>>(a, io);
-            else s16_tracer_kernel<S16, PER, false, false><<<grid, 128, 0, st>>>(a, io);
+            if (cons) tracer_tile_kernel<float, float, PER, false, true, IO><<<grid, 128, 0, st>>>(a, io);
+            else tracer_tile_kernel<float, float, PER, false, false, IO><<<grid, 128, 0, st>>>(a, io);
         }
     }
 
@@ -1418,7 +1415,7 @@ int run_steps(sw_ctx* ctx, long long nsteps, sw_status* status) {
 std::string env_settings() {
     std::string s;
     for (const char* k : {"SWB200_TMA", "SWB200_GRAPHS", "SWB200_STAGE_BLOCKS", "SWB200_TAIL_TY", "SWB200_STAGE_TY",
-                          "SWB200_TEST_WAIT_LIMIT", "SWB200_TEST_SKIP_CHUNK", "SWB200_TRACER_ROWS"}) {
+                          "SWB200_TEST_WAIT_LIMIT", "SWB200_TEST_SKIP_CHUNK"}) {
         const char* v = getenv(k);
         s += k;
         s += '=';
@@ -2118,8 +2115,6 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
         bool ok = want && encode_fn() != nullptr;
         // a cap on the TMA stage kernel's persistent blocks (SWB200_STAGE_BLOCKS),
         // so that small grids also run blocks that take several tiles each
-        const char* envr = getenv("SWB200_TRACER_ROWS");
-        if (envr && atoi(envr) >= 1 && atoi(envr) <= 64) ctx->tracer_rows = atoi(envr);
         const char* envb = getenv("SWB200_STAGE_BLOCKS");
         ctx->stage_blocks_cap = envb ? std::max(1, atoi(envb)) : 0;
         // test only: a shorter bounded wait and a chunk that is never filled,

@@ -364,12 +364,6 @@ struct TracerIO16 {
     __device__ __forceinline__ ES operator()(float x) const { return to16<S16>(x); }
 };
 
-template <class S16, bool PER, bool UM_IS_U, bool CONS>
-__global__ void __launch_bounds__(128)
-s16_tracer_kernel(TracerArgs<float, float> A, TracerIO16<S16> io) {
-    tracer_body<float, float, PER, UM_IS_U, CONS>(A, (int)blockIdx.x, (int)blockIdx.y, (int)gridDim.y, io);
-}
-
 // Whole buffers: FP32 state -> pairs (u, v, eta) and 16-bit sst.
 template <class S16>
 __global__ void __launch_bounds__(256)
