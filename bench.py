@@ -41,14 +41,15 @@ L2_FLUSH = 256 << 20
 # writes X0 (44 B)
 STAGE_BYTES_PER_CELL = (44 + 68 + 68 + 44) / 4
 STEP_BYTES_PER_CELL = 264
-# the 16-bit storage form (scaled 16-bit state pairs, stage values and
-# increments; FP32 X0 after the last stage): stage 1 reads the state's hi and
-# writes X1 and D (26 B with H, Fx), stages 2-3 read X1, hi, D and write X1, D
-# (38 B), stage 4 reads X1, hi, lo, D and writes the FP32 X0 and eta's new pair
-# (48 B); the tail reads X0 (u, v, eta) and H and writes the u, v pairs (24 B);
-# the tracer reads u, v (hi) and sst and writes sst (8 B)
-STAGE_BYTES_PER_CELL_16 = (26 + 38 + 38 + 48) / 4
-STEP_BYTES_PER_CELL_16 = 182
+# the 16-bit storage form (scaled 16-bit state pairs, stage increments and
+# accumulated increments; FP32 X0 after the last stage): stage 1 reads the
+# state's pair and writes the stage increment and D (32 B with H, Fx), stages
+# 2-3 read the pair, the increment and D and write both increments (44 B),
+# stage 4 reads the pair, the increment and D and writes the FP32 X0 and eta's
+# new pair (48 B); the tail reads X0 (u, v, eta) and H and writes the u, v
+# pairs (24 B); the tracer reads u, v (hi) and sst and writes sst (8 B)
+STAGE_BYTES_PER_CELL_16 = (32 + 44 + 44 + 48) / 4
+STEP_BYTES_PER_CELL_16 = 200
 
 
 def packed_static_bytes(static):

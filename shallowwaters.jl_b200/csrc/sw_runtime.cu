@@ -393,10 +393,12 @@ __global__ void ghost_state_kernel(Geom g, Tp* u, Tp* v, Tp* e, GhostRule<Tp> gr
     }
 }
 
-// The launch grid of tracer_tile_kernel: blocks of 128 columns x TRC_ROWS rows.
+// The tracer's launch grid: 128 columns by one row per block row, one thread
+// per cell (measured faster at 2048 x 1024 than several rows per thread, and
+// than staging the tile's velocities and tracer in shared memory).
 dim3 tracer_grid(const sw_ctx* ctx) {
     const Geom& g = ctx->g;
-    return dim3((g.N + 127) / 128, (g.M + TRC_ROWS - 1) / TRC_ROWS);
+    return dim3((g.N + 127) / 128, std::min(g.M, 4096));
 }
 
 template <class T, class Tp>
@@ -524,13 +526,12 @@ struct Engine : EngineBase {
     }
     template <bool PER>
     static void tracer_dispatch2(const TracerArgs<T, Tp>& a, bool um_is_u, bool cons, dim3 grid, cudaStream_t s) {
-        using IO = TracerIONative<T, Tp>;
         if (um_is_u) {
-            if (cons) tracer_tile_kernel<T, Tp, PER, true, true, IO><<<grid, 128, 0, s>>>(a, IO());
-            else tracer_tile_kernel<T, Tp, PER, true, false, IO><<<grid, 128, 0, s>>>(a, IO());
+            if (cons) tracer_kernel<T, Tp, PER, true, true><<<grid, 128, 0, s>>>(a);
+            else tracer_kernel<T, Tp, PER, true, false><<<grid, 128, 0, s>>>(a);
         } else {
-            if (cons) tracer_tile_kernel<T, Tp, PER, false, true, IO><<<grid, 128, 0, s>>>(a, IO());
-            else tracer_tile_kernel<T, Tp, PER, false, false, IO><<<grid, 128, 0, s>>>(a, IO());
+            if (cons) tracer_kernel<T, Tp, PER, false, true><<<grid, 128, 0, s>>>(a);
+            else tracer_kernel<T, Tp, PER, false, false><<<grid, 128, 0, s>>>(a);
         }
     }
 
@@ -926,7 +927,7 @@ template <class S16>
 struct Engine16 : Engine<float, float> {
     using Base = Engine<float, float>;
     struct F3 { S16* u = nullptr; S16* v = nullptr; S16* e = nullptr; };
-    F3 hi[2], lo[2], X1[2], D[2];   // D: the increments, read from one and written to the other
+    F3 hi[2], lo[2], X1[2], D[2];   // X1: stage increments δ, D: accumulated increments (each read from one and written to the other)
     S16* sst16[2] = {nullptr, nullptr};
     float s = 1024.f, inv_s = 1.f / 1024.f;
 
@@ -1014,13 +1015,12 @@ struct Engine16 : Engine<float, float> {
     template <bool PER>
     static void tracer16(const TracerArgs<float, float>& a, const TracerIO16<S16>& io, bool um_is_u, bool cons,
                          dim3 grid, cudaStream_t st) {
-        using IO = TracerIO16<S16>;
         if (um_is_u) {
-            if (cons) tracer_tile_kernel<float, float, PER, true, true, IO><<<grid, 128, 0, st>>>(a, io);
-            else tracer_tile_kernel<float, float, PER, true, false, IO><<<grid, 128, 0, st>>>(a, io);
+            if (cons) s16_tracer_kernel<S16, PER, true, true><<<grid, 128, 0, st>>>(a, io);
+            else s16_tracer_kernel<S16, PER, true, false><<<grid, 128, 0, st>>>(a, io);
         } else {
-            if (cons) tracer_tile_kernel<float, float, PER, false, true, IO><<<grid, 128, 0, st>>>(a, io);
-            else tracer_tile_kernel<float, float, PER, false, false, IO><<<grid, 128, 0, st>>>(a, io);
+            if (cons) s16_tracer_kernel<S16, PER, false, true><<<grid, 128, 0, st>>>(a, io);
+            else s16_tracer_kernel<S16, PER, false, false><<<grid, 128, 0, st>>>(a, io);
         }
     }
 
@@ -1050,10 +1050,11 @@ struct Engine16 : Engine<float, float> {
         a.st = ctx->dst;
         const int nblk = (a.nsx * a.nsy + 3) / 4 + a.nring_blocks;
         for (int k = 1; k <= c.RKo; k++) {
-            const F3& in = (k == 1) ? hi[p] : X1[k % 2 == 0 ? 0 : 1];
-            const F3& out1 = X1[k % 2 == 1 ? 0 : 1];
-            a.u1 = in.u; a.v1 = in.v; a.e1 = in.e;
-            a.u1o = out1.u; a.v1o = out1.v; a.e1o = out1.e;
+            // stage k reads the increment δ of stage k-1 (X1 = state + δ) and writes its own
+            const F3& din1 = X1[k % 2 == 0 ? 0 : 1];
+            const F3& dout1 = X1[k % 2 == 1 ? 0 : 1];
+            a.ud = din1.u; a.vd = din1.v; a.ed = din1.e;
+            a.udo = dout1.u; a.vdo = dout1.v; a.edo = dout1.e;
             const F3& din = D[k % 2], &dout = D[(k + 1) % 2];
             a.uD = din.u; a.vD = din.v; a.eD = din.e;
             a.uDo = dout.u; a.vDo = dout.v; a.eDo = dout.e;

@@ -10,18 +10,19 @@
 //           lo = round16(s*x - hi).  lo is the Kahan compensation term: it
 //           keeps the rounding error of hi, so increments far below one unit
 //           in the last place of hi still accumulate from step to step.
-//   X1      the RK stage values, one 16-bit number each
-//   D       the RK increment accumulated so far, sum of a_k*dt*d_k, one
-//           16-bit number each (it starts from zero, not from the state)
+//   δ       the stage increment b_k*dt*d_k: the input of stage k+1 is
+//           X1 = (hi + lo) + δ, formed in FP32 (the increment is small against
+//           the state, so its 16 bits cost the stage input almost nothing)
+//   D       the RK increment accumulated so far, sum of a_k*dt*d_k
 //   sst     one 16-bit number
 // Tendencies, the stage combination and the tail are computed in FP32 from
-// those values.  The last stage forms X0 = (hi + lo) + D + a_4*dt*d_4 in
+// those values.  The last stage forms X0 = (hi + lo) + (D + a_4*dt*d_4) in
 // FP32: u and v (and eta, for the depth of the quadratic drag) go to FP32
 // buffers that the tail reads once and turns into the new pairs; eta goes to
 // its new pair directly.  Bytes per cell and step (RK4, tail and tracer every
 // step, static fields counted as full FP32 fields like in the FP32 count):
-//   stage 1  26   stages 2, 3  38 each   stage 4  48   tail 24   tracer 8
-// 182 bytes against the 264 of plain Float32.
+//   stage 1  32   stages 2, 3  44 each   stage 4  48   tail 24   tracer 8
+// 200 bytes against the 264 of plain Float32.
 //
 // Execution follows the streaming stage kernel of sw_stage.cuh (one warp per
 // 28-column strip, rows streamed upward with a register window and warp
@@ -60,12 +61,12 @@ template <class S16>
 struct S16StageArgs {
     Geom g;
     int nsx, nsy, nring_blocks;
-    const S16* u1; const S16* v1; const S16* e1;   // stage input X1 (stage 1: the state's hi)
     const S16* uh; const S16* vh; const S16* eh;   // state hi
-    const S16* ul; const S16* vl; const S16* el;   // state lo (read by the last stage)
-    const S16* uD; const S16* vD; const S16* eD;   // increment so far (not read by the first stage)
-    S16* u1o; S16* v1o; S16* e1o;                  // X1' (not the last stage)
-    S16* uDo; S16* vDo; S16* eDo;                  // increment out (not the last stage; not the D read)
+    const S16* ul; const S16* vl; const S16* el;   // state lo
+    const S16* ud; const S16* vd; const S16* ed;   // stage increment δ in (not read by the first stage)
+    const S16* uD; const S16* vD; const S16* eD;   // accumulated increment D in (not read by the first stage)
+    S16* udo; S16* vdo; S16* edo;                  // δ out, with ghost copies (not the last stage)
+    S16* uDo; S16* vDo; S16* eDo;                  // D out (not the last stage)
     float* u0o; float* v0o; float* e0o;            // last stage: X0 in FP32, with ghost copies
     S16* eho; S16* elo;                            // last stage: the new eta pair, with ghost copies
     SField<float> H, fq, Fx, Fy;
@@ -79,12 +80,7 @@ struct S16StageArgs {
 template <class S16>
 __device__ __forceinline__ float ld16(const S16* p, int k, float inv_s) { return from16(p[k]) * inv_s; }
 
-#ifndef SWB_S16_PF
-#define SWB_S16_PF 3       // input rows of the stage kernel in flight ahead of the one consumed
-#endif
-constexpr int S16_PF = SWB_S16_PF;
-
-// untouched halo cells of u and v: X1' = X, D' = D, X0 = X + D
+// untouched halo cells of u and v: δ' = 0 (X1 = X), D' = D, X0 = X + D
 template <class S16, bool FIRST, bool LAST>
 __device__ void s16_stage_ring(const S16StageArgs<S16>& A, int k0, int kstride) {
     const Geom& g = A.g;
@@ -96,19 +92,18 @@ __device__ void s16_stage_ring(const S16StageArgs<S16>& A, int k0, int kstride) 
         if (isu) Ring::u_at(k, g.ep, g.N, g.M, x, y);
         else Ring::v_at(k - nu, g.N, g.M, x, y);
         const int gi = g.idx(x, y);
-        const S16* ph = isu ? A.uh : A.vh;
         if (!LAST) {
-            S16* o1 = isu ? A.u1o : A.v1o;
+            S16* od = isu ? A.udo : A.vdo;
             S16* oD = isu ? A.uDo : A.vDo;
-            o1[gi] = ph[gi];
+            od[gi] = to16<S16>(0.f);
             oD[gi] = FIRST ? to16<S16>(0.f) : (isu ? A.uD : A.vD)[gi];
-            const float xv = ld16(ph, gi, A.inv_s);
-            if (isu) A.gr.u(o1, g, x, y, xv, put);
-            else A.gr.v(o1, g, x, y, xv, put);
+            if (isu) A.gr.u(od, g, x, y, 0.f, put);
+            else A.gr.v(od, g, x, y, 0.f, put);
         } else {
+            const S16* ph = isu ? A.uh : A.vh;
             const S16* pl = isu ? A.ul : A.vl;
             const S16* pD = isu ? A.uD : A.vD;
-            const float x0 = ((from16(ph[gi]) + from16(pl[gi])) + from16(pD[gi])) * A.inv_s;
+            const float x0 = (from16(ph[gi]) + from16(pl[gi])) * A.inv_s + from16(pD[gi]) * A.inv_s;
             float* o0 = isu ? A.u0o : A.v0o;
             o0[gi] = x0;
             if (isu) A.gr.u(o0, g, x, y, x0);
@@ -149,21 +144,40 @@ s16_stage_kernel(const __grid_constant__ S16StageArgs<S16> A) {
     const PutLo16<S16> putlo{A.s};
 
     const int cb = c + COL0;
-    const S16* __restrict__ pu = A.u1 + cb;
-    const S16* __restrict__ pv = A.v1 + cb;
-    const S16* __restrict__ pe = A.e1 + cb;
-    const S16* __restrict__ xh[3] = {A.uh + cb, A.vh + cb, A.eh + cb};
-    const S16* __restrict__ xl[3] = {A.ul + cb, A.vl + cb, A.el + cb};
-    const S16* __restrict__ xd[3] = {A.uD + cb, A.vD + cb, A.eD + cb};
+    const S16* __restrict__ ph[3] = {A.uh + cb, A.vh + cb, A.eh + cb};
+    const S16* __restrict__ pl[3] = {A.ul + cb, A.vl + cb, A.el + cb};
+    const S16* __restrict__ pd[3] = {A.ud + cb, A.vd + cb, A.ed + cb};
+    const S16* __restrict__ pD[3] = {A.uD + cb, A.vD + cb, A.eD + cb};
     const int Hsy = A.H.sy;
     const float* __restrict__ pH = A.H.p + cb * A.H.sx;
     const float* __restrict__ pfq = A.fq.p + cb * A.fq.sx;
     const int fqsy = A.fq.sy;
     auto row = [&](int y) { return (y + ROW0) * P; };
-    auto in = [&](const S16* p, int k) { return from16(p[k]) * inv; };
+    // the state (hi + lo) and the stage input X1 = state + δ of field f at offset k
+    struct In { S16 h, l, d; };
+    auto fetch = [&](int f, int k) {
+        In v;
+        v.h = ph[f][k];
+        v.l = pl[f][k];
+        v.d = FIRST ? to16<S16>(0.f) : pd[f][k];
+        return v;
+    };
+    auto state = [&](const In& v) { return (from16(v.h) + from16(v.l)) * inv; };
+    auto stage_in = [&](const In& v) { return FIRST ? state(v) : state(v) + from16(v.d) * inv; };
+    // the same at a column of its own (the periodic q wrap)
+    auto at_col = [&](int f, int x, int y) {
+        const S16* hh = f == 0 ? A.uh : f == 1 ? A.vh : A.eh;
+        const S16* ll = f == 0 ? A.ul : f == 1 ? A.vl : A.el;
+        const S16* dd = f == 0 ? A.ud : f == 1 ? A.vd : A.ed;
+        const int k = g.idx(x, y);
+        const float xs = (from16(hh[k]) + from16(ll[k])) * inv;
+        return FIRST ? xs : xs + from16(dd[k]) * inv;
+    };
 
     int r = y0 - 2;
-    float u_r = in(pu, row(r)), v_r = in(pv, row(r)), e_r = in(pe, row(r));
+    In cu = fetch(0, row(r)), cv = fetch(1, row(r)), ce = fetch(2, row(r));
+    float u_r = stage_in(cu), v_r = stage_in(cv), e_r = stage_in(ce);
+    float us_r = state(cu), vs_r = state(cv), es_r = state(ce);     // the state itself (last stage's X0)
     float h_r = e_r + pH[(r + ROW0) * Hsy];
     float hl_r = shup(h_r), ur_r = shdn(u_r);
     float U_r = u_r * (half * (h_r + hl_r));
@@ -172,58 +186,49 @@ s16_stage_kernel(const __grid_constant__ S16StageArgs<S16> A) {
     float p_rm1 = 0.f, qhu_part = 0.f;
     float uN_r = 0.f, hN_r = 0.f, hNm1_r = 0.f;
     if (wrap) {
-        uN_r = ld16(A.u1, g.idx(N, r), inv);
-        hN_r = ld16(A.e1, g.idx(N, r), inv) + A.H.at(N, r);
-        hNm1_r = ld16(A.e1, g.idx(N - 1, r), inv) + A.H.at(N - 1, r);
+        uN_r = at_col(0, N, r);
+        hN_r = at_col(2, N, r) + A.H.at(N, r);
+        hNm1_r = at_col(2, N - 1, r) + A.H.at(N - 1, r);
     }
-    // software pipeline: input rows r+1 .. r+S16_PF in flight; the point-wise
-    // operands (hi, lo, D) of the output row one iteration ahead
-    S16 qu[S16_PF], qv[S16_PF], qe[S16_PF];
-    float qH[S16_PF];
+    // software pipeline: the next input row one iteration ahead, and the
+    // output row's accumulated increment D
+    In nu = fetch(0, row(r + 1)), nv = fetch(1, row(r + 1)), ne = fetch(2, row(r + 1));
+    float nH = pH[(r + 1 + ROW0) * Hsy];
+    S16 nD[3];
 #pragma unroll
-    for (int k = 0; k < S16_PF; k++) {
-        qu[k] = pu[row(r + 1 + k)]; qv[k] = pv[row(r + 1 + k)]; qe[k] = pe[row(r + 1 + k)];
-        qH[k] = pH[(r + 1 + k + ROW0) * Hsy];
-    }
-    S16 nh[3], nl[3], nd[3];
+    for (int f = 0; f < 3; f++) nD[f] = to16<S16>(0.f);
+    auto load_D = [&](int y) {
+        if constexpr (!FIRST) {
+            if (y >= y0 && out_lane) {
 #pragma unroll
-    for (int f = 0; f < 3; f++) nh[f] = nl[f] = nd[f] = to16<S16>(0.f);
-    auto load_pw = [&](int y) {
-        if (FIRST || y < y0 || !out_lane) return;
-        const int oy = row(y);
-#pragma unroll
-        for (int f = 0; f < 3; f++) {
-            nh[f] = xh[f][oy];
-            nd[f] = xd[f][oy];
-            if (LAST) nl[f] = xl[f][oy];
+                for (int f = 0; f < 3; f++) nD[f] = pD[f][row(y)];
+            }
         }
     };
-    load_pw(r);
+    load_D(r);
 
     for (; r < y0 + TY; r++) {
-        const float u_r1 = from16(qu[0]) * inv, v_r1 = from16(qv[0]) * inv, e_r1 = from16(qe[0]) * inv;
-        const float h_r1 = e_r1 + qH[0];
-#pragma unroll
-        for (int k = 0; k + 1 < S16_PF; k++) { qu[k] = qu[k + 1]; qv[k] = qv[k + 1]; qe[k] = qe[k + 1]; qH[k] = qH[k + 1]; }
+        const float u_r1 = stage_in(nu), v_r1 = stage_in(nv), e_r1 = stage_in(ne);
+        const float us_r1 = LAST ? state(nu) : 0.f, vs_r1 = LAST ? state(nv) : 0.f, es_r1 = LAST ? state(ne) : 0.f;
+        const float h_r1 = e_r1 + nH;
         {
-            const int on = row(r + 1 + S16_PF);
-            qu[S16_PF - 1] = pu[on]; qv[S16_PF - 1] = pv[on]; qe[S16_PF - 1] = pe[on];
-            qH[S16_PF - 1] = pH[(r + 1 + S16_PF + ROW0) * Hsy];
+            const int o2 = row(r + 2);
+            nu = fetch(0, o2); nv = fetch(1, o2); ne = fetch(2, o2);
+            nH = pH[(r + 2 + ROW0) * Hsy];
         }
-        // the output row's point-wise operands (issued one iteration earlier); issue the next row's
-        S16 ch[3], cl[3], cd[3];
+        S16 cD[3];
 #pragma unroll
-        for (int f = 0; f < 3; f++) { ch[f] = nh[f]; cl[f] = nl[f]; cd[f] = nd[f]; }
-        load_pw(r + 1);
+        for (int f = 0; f < 3; f++) cD[f] = nD[f];
+        load_D(r + 1);
         const float hl_r1 = shup(h_r1), vl_r1 = shup(v_r1), ur_r1 = shdn(u_r1);
         float q_r1;
         const float fq = pfq[(r + 1 + ROW0) * fqsy];
         float uN_r1 = 0.f, hN_r1 = 0.f, hNm1_r1 = 0.f;
         if (wrap) {
-            uN_r1 = ld16(A.u1, g.idx(N, r + 1), inv);
-            hN_r1 = ld16(A.e1, g.idx(N, r + 1), inv) + A.H.at(N, r + 1);
-            hNm1_r1 = ld16(A.e1, g.idx(N - 1, r + 1), inv) + A.H.at(N - 1, r + 1);
-            const float vN = ld16(A.v1, g.idx(N, r + 1), inv), vNm1 = ld16(A.v1, g.idx(N - 1, r + 1), inv);
+            uN_r1 = at_col(0, N, r + 1);
+            hN_r1 = at_col(2, N, r + 1) + A.H.at(N, r + 1);
+            hNm1_r1 = at_col(2, N - 1, r + 1) + A.H.at(N - 1, r + 1);
+            const float vN = at_col(1, N, r + 1), vNm1 = at_col(1, N - 1, r + 1);
             q_r1 = pv_q<float>(fq, vN, vNm1, uN_r1, uN_r, hNm1_r, hN_r, hNm1_r1, hN_r1);
         } else {
             q_r1 = pv_q<float>(fq, v_r1, vl_r1, u_r1, u_r, hl_r, h_r, hl_r1, h_r1);
@@ -245,25 +250,21 @@ s16_stage_kernel(const __grid_constant__ S16StageArgs<S16> A) {
 
         if (r >= y0 && r < M) {
             const int o = row(r) + cb;
-            // X: the state's hi (on the first stage that is the input row itself);
-            // on the last stage X0 = (hi + lo) + D, else the increment D (0 first)
-            auto base = [&](int f) {
-                if (LAST) return ((from16(ch[f]) + from16(cl[f])) + from16(cd[f])) * inv;
-                return FIRST ? 0.f : from16(cd[f]) * inv;
-            };
+            // D' = D + a d (the first stage starts from 0); the last stage's X0 = state + D'
+            auto incr = [&](int f, float d) { return (FIRST ? 0.f : from16(cD[f]) * inv) + A.a * d; };
             if (col_u) {
                 const float qhv = qa * V_r1 + qb * Vl_r1 + qc * Vl_r + qd * V_r;
                 const float dpdx = p_r - pl_r;
                 const float du = (qhv - dpdx) + A.Fxt * A.Fx.at(c, r);
                 const bool gs = gx_u || (!PER && (r <= 1 || r >= M - 2));
-                const float x0 = base(0) + A.a * du;
+                const float dD = incr(0, du);
                 if (!LAST) {
-                    const float X = FIRST ? u_r : from16(ch[0]) * inv;
-                    const float x1 = X + A.b * du;
-                    A.u1o[o] = put(x1);
-                    if (gs) A.gr.u(A.u1o, g, c, r, x1, put);
-                    A.uDo[o] = put(x0);
+                    const float dl = A.b * du;                   // δ' : X1' = X + b d
+                    A.udo[o] = put(dl);
+                    if (gs) A.gr.u(A.udo, g, c, r, dl, put);
+                    A.uDo[o] = put(dD);
                 } else {
+                    const float x0 = us_r + dD;
                     A.u0o[o] = x0;
                     if (gs) A.gr.u(A.u0o, g, c, r, x0);
                 }
@@ -273,14 +274,14 @@ s16_stage_kernel(const __grid_constant__ S16StageArgs<S16> A) {
                     const float qhu = qhu_part + qcr * Ur_r + qd * U_r;
                     const float dpdy = p_r - p_rm1;
                     const float dv = -(qhu + dpdy) + A.Fyt * A.Fy.at(c, r);
-                    const float x0 = base(1) + A.a * dv;
+                    const float dD = incr(1, dv);
                     if (!LAST) {
-                        const float X = FIRST ? v_r : from16(ch[1]) * inv;
-                        const float x1 = X + A.b * dv;
-                        A.v1o[o] = put(x1);
-                        if (gx_v) A.gr.v(A.v1o, g, c, r, x1, put);
-                        A.vDo[o] = put(x0);
+                        const float dl = A.b * dv;
+                        A.vdo[o] = put(dl);
+                        if (gx_v) A.gr.v(A.vdo, g, c, r, dl, put);
+                        A.vDo[o] = put(dD);
                     } else {
+                        const float x0 = vs_r + dD;
                         A.v0o[o] = x0;
                         if (gx_v) A.gr.v(A.v0o, g, c, r, x0);
                     }
@@ -289,14 +290,14 @@ s16_stage_kernel(const __grid_constant__ S16StageArgs<S16> A) {
                 const float dVdy = V_r1 - V_r;
                 const float de = -(dUdx + dVdy);
                 const bool gs = gx_e || r == 0 || r == M - 1;
-                const float x0 = base(2) + A.a * de;
+                const float dD = incr(2, de);
                 if (!LAST) {
-                    const float X = FIRST ? e_r : from16(ch[2]) * inv;
-                    const float x1 = X + A.b * de;
-                    A.e1o[o] = put(x1);
-                    if (gs) A.gr.eta(A.e1o, g, c, r, x1, put);
-                    A.eDo[o] = put(x0);
+                    const float dl = A.b * de;
+                    A.edo[o] = put(dl);
+                    if (gs) A.gr.eta(A.edo, g, c, r, dl, put);
+                    A.eDo[o] = put(dD);
                 } else {
+                    const float x0 = es_r + dD;
                     A.e0o[o] = x0;
                     A.eho[o] = put(x0);
                     A.elo[o] = putlo(x0);
@@ -310,6 +311,7 @@ s16_stage_kernel(const __grid_constant__ S16StageArgs<S16> A) {
         }
         qhu_part = qa * U_r + qbr * Ur_r;
         u_r = u_r1; v_r = v_r1; e_r = e_r1; h_r = h_r1; hl_r = hl_r1; ur_r = ur_r1;
+        us_r = us_r1; vs_r = vs_r1; es_r = es_r1;
         q_r = q_r1; ql_r = ql_r1; qr_r = qr_r1;
         U_r = U_r1; Ur_r = Ur_r1;
         V_r = V_r1; Vl_r = Vl_r1;
@@ -363,6 +365,12 @@ struct TracerIO16 {
     __device__ __forceinline__ float s(ES x) const { return from16(x); }
     __device__ __forceinline__ ES operator()(float x) const { return to16<S16>(x); }
 };
+
+template <class S16, bool PER, bool UM_IS_U, bool CONS>
+__global__ void __launch_bounds__(128)
+s16_tracer_kernel(TracerArgs<float, float> A, TracerIO16<S16> io) {
+    tracer_body<float, float, PER, UM_IS_U, CONS>(A, (int)blockIdx.x, (int)blockIdx.y, (int)gridDim.y, io);
+}
 
 // Whole buffers: FP32 state -> pairs (u, v, eta) and 16-bit sst.
 template <class S16>

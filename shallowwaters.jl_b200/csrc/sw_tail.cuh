@@ -78,7 +78,7 @@ __device__ void tail_ring(const TailArgs<T, Tp>& A, int k0, int kstride, const S
 #define SWB_TAIL_MINB 1    // resident blocks per SM the register budget is sized for
 #endif
 #ifndef SWB_TAIL_PF
-#define SWB_TAIL_PF 4      // input rows in flight ahead of the one consumed
+#define SWB_TAIL_PF 2      // input rows in flight ahead of the one consumed (4 and 6 measured slower)
 #endif
 constexpr int TAIL_PF = SWB_TAIL_PF;
 // DRAG: enum sw_bottom_drag; SMAG: Smagorinsky (else constant νB)
@@ -133,8 +133,7 @@ __device__ __forceinline__ void tail_body(const TailArgs<T, Tp>& A, int bx, cons
     T sKE_rm1 = T(0), sKE_r = T(0), sKEl_r = T(0);
 
     // software pipeline: at iteration r, row r+2 is consumed while rows r+3 ..
-    // r+2+TAIL_PF are in flight (the loads' latency under a full device of
-    // streaming warps spans several iterations)
+    // r+2+TAIL_PF are in flight
     T u_r2 = cvt<T>(A.u0[ofs(r + 2)]), v_r2 = cvt<T>(A.v0[ofs(r + 2)]);
     T h_r2 = QUAD ? cvt<T>(A.e0[ofs(r + 2)]) + A.H.at(c, r + 2) : T(0);
     Tp pu[TAIL_PF], pv[TAIL_PF], pe[TAIL_PF];

@@ -176,156 +176,6 @@ tracer_kernel(TracerArgs<T, Tp> A) {
     tracer_body<T, Tp, PER, UM_IS_U, CONS>(A, (int)blockIdx.x, (int)blockIdx.y, (int)gridDim.y);
 }
 
-// The tracer with shared-memory tiles.  A block of 128 threads takes 128
-// columns x TRC_ROWS rows.  It first stages, for its cells and a halo of two
-// cells, the mid-point velocities on the T-grid (um_T = Ix(um), vm_T =
-// Iy(vm), src/tracer_advection.jl:63-67) and the tracer in shared memory;
-// each cell's three bilinear gathers (interp_uv! of um_T and vm_T, adv_sst!)
-// then read their four corners from there whenever all four lie inside the
-// staged region, and from global memory, as tracer_body does, otherwise (long
-// or wrapped departures, and the staged region's clipped edges).  Every value
-// is formed by the same operations as in tracer_body, so the results are the
-// same bits; the tiles spare each cell the six-load gathers with their
-// averaging and 64-bit address arithmetic.
-constexpr int TRC_ROWS = 8;
-constexpr int TRC_W = 128 + 5, TRC_H = TRC_ROWS + 5;   // staged x in [a0-2, a0+131), y in [b0-2, b0+TRC_ROWS+3)
-
-template <class T, class Tp, bool PER, bool UM_IS_U, bool CONS, class IO>
-__global__ void __launch_bounds__(128)
-tracer_tile_kernel(TracerArgs<T, Tp> A, IO io) {
-    using EU = typename IO::EU;
-    using ES = typename IO::ES;
-    __shared__ T MU[TRC_H][TRC_W], MV[TRC_H][TRC_W], SS[TRC_H][TRC_W];
-    if (A.st->stop) return;                     // uniform over the launch
-    const Geom& g = A.g;
-    const int N = g.N, M = g.M, P = g.P;
-    const T half = T(0.5);
-    auto at = [&](int x, int y) { return (y + ROW0) * P + x + COL0; };
-    const EU* __restrict__ pu = reinterpret_cast<const EU*>(A.u);
-    const EU* __restrict__ pv = reinterpret_cast<const EU*>(A.v);
-    const T* __restrict__ pum = A.um;
-    const T* __restrict__ pvm = A.vm;
-    const ES* __restrict__ psst = reinterpret_cast<const ES*>(A.sst);
-    ES* __restrict__ psst_o = reinterpret_cast<ES*>(A.sst_o);
-
-    // the staged region: origin (tx0, ty0), computed up to (exclusive) txe, tye,
-    // which stay inside the buffers' padding (reads reach x + 1 and y + 1)
-    const int a0 = blockIdx.x * 128, by0 = blockIdx.y * TRC_ROWS;
-    const int tx0 = a0 - 2, ty0 = by0 - 2;
-    const int txe = min(tx0 + TRC_W, N + 70), tye = min(ty0 + TRC_H, M + 40);
-    for (int k = threadIdx.x; k < TRC_W * TRC_H; k += 128) {
-        const int tx = k % TRC_W, ty = k / TRC_W, x = tx0 + tx, y = ty0 + ty;
-        if (x >= txe || y >= tye) continue;
-        const int o = at(x, y);
-        if (UM_IS_U) {
-            MU[ty][tx] = half * (io.u(pu[o + 1]) + io.u(pu[o]));
-            MV[ty][tx] = half * (io.u(pv[o + P]) + io.u(pv[o]));
-        } else {
-            MU[ty][tx] = half * (pum[o + 1] + pum[o]);
-            MV[ty][tx] = half * (pvm[o + P] + pvm[o]);
-        }
-        SS[ty][tx] = io.s(psst[o]);
-    }
-    __syncthreads();
-
-    const int a = a0 + (int)threadIdx.x;
-    if (a >= N) return;
-    // all four corners (x..x+1, y..y+1) staged?
-    auto staged = [&](int x, int y) { return x >= tx0 && x + 1 < txe && y >= ty0 && y + 1 < tye; };
-    int bad = 0;
-    const bool gx = a == 0 || a == N - 1;
-    const int bend = min(by0 + TRC_ROWS, M);
-    for (int b = by0; b < bend; b++) {
-        // departure!: u_T = Ix!(u), v_T = Iy!(v); backtraj! at half step (:75-76, :96-124)
-        const int o = at(a, b);
-        T uT, vT;
-        if (UM_IS_U) {
-            uT = MU[b - ty0][a - tx0];
-            vT = MV[b - ty0][a - tx0];
-        } else {
-            uT = half * (io.u(pu[o + 1]) + io.u(pu[o]));
-            vT = half * (io.u(pv[o + P]) + io.u(pv[o]));
-        }
-        T xd = (-A.half_dtadvu) * uT;
-        T yd = (-A.half_dtadvv) * vT;
-        int xi = ifloor(xd, bad), yi = ifloor(yd, bad);
-        T ui, vi;
-        {   // interp_uv!(uinterp, um_T, ...) (:130-176)
-            T x0, y0;
-            int F0 = axis<T, PER>(xi + a, xi, xd, 0, N - 1, N, x0);
-            const int b0 = axis<T, false>(yi + b, yi, yd, 0, M, 0, y0);
-            if (F0 < -2 || F0 > N - 1) { bad = 1; F0 = 0; }
-            T c00, c10, c01, c11;
-            if (staged(F0, b0)) {
-                const int sx = F0 - tx0, sy = b0 - ty0;
-                c00 = MU[sy][sx]; c10 = MU[sy][sx + 1]; c01 = MU[sy + 1][sx]; c11 = MU[sy + 1][sx + 1];
-            } else {
-                const int k = at(F0, b0);
-                T m00, m10, m20, m01, m11, m21;
-                if (UM_IS_U) {
-                    m00 = io.u(pu[k]); m10 = io.u(pu[k + 1]); m20 = io.u(pu[k + 2]);
-                    m01 = io.u(pu[k + P]); m11 = io.u(pu[k + P + 1]); m21 = io.u(pu[k + P + 2]);
-                } else {
-                    m00 = pum[k]; m10 = pum[k + 1]; m20 = pum[k + 2];
-                    m01 = pum[k + P]; m11 = pum[k + P + 1]; m21 = pum[k + P + 2];
-                }
-                c00 = half * (m10 + m00); c10 = half * (m20 + m10); c01 = half * (m11 + m01); c11 = half * (m21 + m11);
-            }
-            ui = bilin(c00, c10, c01, c11, x0, y0);
-        }
-        {   // interp_uv!(vinterp, vm_T, ...)
-            T x0, y0;
-            int a0v = axis<T, PER>(xi + a, xi, xd, 0, N, N, x0);
-            const int G0 = axis<T, false>(yi + b, yi, yd, 0, M - 1, 0, y0);
-            if (a0v < -2 || a0v > N) { bad = 1; a0v = 0; }
-            T c00, c10, c01, c11;
-            if (staged(a0v, G0)) {
-                const int sx = a0v - tx0, sy = G0 - ty0;
-                c00 = MV[sy][sx]; c10 = MV[sy][sx + 1]; c01 = MV[sy + 1][sx]; c11 = MV[sy + 1][sx + 1];
-            } else {
-                const int k = at(a0v, G0);
-                T m00, m01, m02, m10, m11, m12;
-                if (UM_IS_U) {
-                    m00 = io.u(pv[k]); m01 = io.u(pv[k + P]); m02 = io.u(pv[k + 2 * P]);
-                    m10 = io.u(pv[k + 1]); m11 = io.u(pv[k + P + 1]); m12 = io.u(pv[k + 2 * P + 1]);
-                } else {
-                    m00 = pvm[k]; m01 = pvm[k + P]; m02 = pvm[k + 2 * P];
-                    m10 = pvm[k + 1]; m11 = pvm[k + P + 1]; m12 = pvm[k + 2 * P + 1];
-                }
-                c00 = half * (m01 + m00); c10 = half * (m11 + m10); c01 = half * (m02 + m01); c11 = half * (m12 + m11);
-            }
-            vi = bilin(c00, c10, c01, c11, x0, y0);
-        }
-        // backtraj! at full step (:83-84)
-        xd = (-A.dtadvu) * ui;
-        yd = (-A.dtadvv) * vi;
-        xi = ifloor(xd, bad);
-        yi = ifloor(yd, bad);
-        T sv;
-        {   // adv_sst! (:179-206)
-            T x0, y0;
-            int a0s = axis<T, PER>(xi + a, xi, xd, 0, N - 1, N, x0);
-            const int b0 = axis<T, false>(yi + b, yi, yd, 0, M - 2, 0, y0);
-            if (a0s < -1 || a0s > N - 1) { bad = 1; a0s = 0; }
-            if (staged(a0s, b0)) {
-                const int sx = a0s - tx0, sy = b0 - ty0;
-                sv = bilin(SS[sy][sx], SS[sy][sx + 1], SS[sy + 1][sx], SS[sy + 1][sx + 1], x0, y0);
-            } else {
-                const int k = at(a0s, b0);
-                sv = bilin(io.s(psst[k]), io.s(psst[k + 1]), io.s(psst[k + P]), io.s(psst[k + P + 1]), x0, y0);
-            }
-        }
-        if (CONS) sv += A.jSST * (A.SSTmin - sv);             // tracer_consumption! (:262-275)
-        const Tp out = cvt<Tp>(sv);
-        psst_o[o] = io(out);
-        if (gx) A.gr.sst(psst_o, g, a, b, out, io);           // ghost_points_sst! (:40)
-    }
-    if (bad) {   // the reference throws here; halt the device-side loop
-        atomicCAS(&A.st->error, 0, (int)SW_ERR_DEPARTURE);
-        atomicExch(&A.st->stop, 1);
-    }
-}
-
 // um, vm = u0, v0 converted to T (src/tracer_advection.jl:12-17), over whole buffers
 template <class T, class Tp>
 __global__ void copy_convert_kernel(const Tp* __restrict__ u, const Tp* __restrict__ v, T* __restrict__ um,
