@@ -172,6 +172,12 @@ struct Work {
     int nx, ny, nux, nuy, nvx, nvy, ep, rko;
     bool ssp = false;           // SSPRK2 (src/time_integration.jl:80-104) or 4SSPRK3 (:150-196) instead of RK
     bool four = false;          // 4SSPRK3: averaged updates, full ghost points, the third sub-stage's mix
+    // SSPRK3 (:112-156): s = n^2 sub-stages of Δt_Δn updates; sub-stage rki = kn mixes the snapshot u0
+    // (kna*u1 + knb*u0 + Δt_Δnc*du, dxaybzc!); the snapshot is the state after sub-stage rki = mn
+    // (or the step's start when mn = 1), eta ghosted in place there and at the last sub-stage
+    bool ssp3 = false;
+    int s3_kn = 0, s3_mn = 0;
+    T s3_cnc, s3_kna, s3_knb;
     int rks = 0, nst = 0;       // SSPRK2 sub-stages; stage states kept per step
     T cssp, ssp_a, ssp_b;       // Δt_Δs, 1/RKs, (RKs-1)/RKs (Tprog)
     T g, cD, rD, cSmag, nuB, Dt_diff, oma;   // oma = 1 - alpha (Tprog = T)
@@ -191,11 +197,11 @@ struct Work {
     // states
     State<T> X;                 // the state being advanced (in / out of a step)
     // stage states.  RK: Ys[k-1] = input of stage k after its ghost points
-    // (Ys[0] = ghosted start state).  SSPRK2: Ys[0] = ghosted start state,
+    // (Ys[0] = ghosted start state).  SSP schemes: Ys[0] = ghosted start state,
     // Ys[2k-1] = sub-stage k's input after ghost_points_eta!, Ys[2k] = its
     // state after the momentum update and ghost_points_uv!, Ys[2 RKs + 1] =
     // the state after the last sub-stage.
-    State<T> Ys[10];
+    State<T> Ys[20];
     State<T> Z;                 // RK result after ghost points = the tail's input
     T* stage_block = nullptr;   // Ys[0..nst-1] and Z, contiguous in this order
     size_t stage_block_elems = 0;
@@ -668,7 +674,7 @@ void stage_rev(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const St
 // arrays, du zero on the halo) after rhs! at the sub-stage input Yp (whose
 // stage_fwd intermediates are current); eta is carried over.
 template <class T>
-void ssp_mom(Launcher& L, const Work<T>& w, const State<T>& Yp, const State<T>& Ym) {
+void ssp_mom(Launcher& L, const Work<T>& w, const State<T>& Yp, const State<T>& Ym, const State<T>* Zs = nullptr) {
     const A2<T> p = w.p, Fx = w.Fx, Fy = w.Fy;
     const PVterms<T> pv = pvterms(w);
     const LinTerms<T> lt{w.f_u, w.f_v, w.g, w.ep};
@@ -678,6 +684,9 @@ void ssp_mom(Launcher& L, const Work<T>& w, const State<T>& Yp, const State<T>& 
     const bool timedep = w.timedep;
     const T* force = w.force;
     const State<T> yp = Yp, ym = Ym;
+    const bool kn = Zs != nullptr;   // SSPRK3's stage kn: kna*u1 + knb*u0 + Δt_Δnc*du (dxaybzc!)
+    const State<T> zs = kn ? *Zs : Yp;
+    const T kna = w.s3_kna, knb = w.s3_knb, cnc = w.s3_cnc;
     L.d2(nx + 4, ny + 4, [=] __host__ __device__(int I, int J) {
         const T zero = T(0);
         if (I <= yp.u.m && J <= yp.u.n) {
@@ -697,6 +706,8 @@ void ssp_mom(Launcher& L, const Work<T>& w, const State<T>& Yp, const State<T>& 
             if (four) {   // u0 = u1 + Δt_Δ*du; u1 = 0.5*(u1 + u0) (caxb!, cxab!)
                 const T t = yp.u(I, J) + c * d;
                 ym.u(I, J) = T(0.5) * (yp.u(I, J) + t);
+            } else if (kn) {
+                ym.u(I, J) = kna * yp.u(I, J) + knb * zs.u(I, J) + cnc * d;
             } else {
                 ym.u(I, J) = yp.u(I, J) + c * d;
             }
@@ -717,6 +728,8 @@ void ssp_mom(Launcher& L, const Work<T>& w, const State<T>& Yp, const State<T>& 
             if (four) {
                 const T t = yp.v(I, J) + c * d;
                 ym.v(I, J) = T(0.5) * (yp.v(I, J) + t);
+            } else if (kn) {
+                ym.v(I, J) = kna * yp.v(I, J) + knb * zs.v(I, J) + cnc * d;
             } else {
                 ym.v(I, J) = yp.v(I, J) + c * d;
             }
@@ -729,7 +742,7 @@ void ssp_mom(Launcher& L, const Work<T>& w, const State<T>& Yp, const State<T>& 
 // updated u1, v1 and the sub-stage's eta1, whose h_u, h_v stage_fwd formed)
 // and eta1 += Δt_Δs*deta; u1, v1 carried over into Yn
 template <class T>
-void ssp_cont(Launcher& L, const Work<T>& w, const State<T>& Ym, const State<T>& Yn) {
+void ssp_cont(Launcher& L, const Work<T>& w, const State<T>& Ym, const State<T>& Yn, const State<T>* Zs = nullptr) {
     const A2<T> hu = w.hu, hv = w.hv;
     const int nx = w.nx, ny = w.ny, ep = w.ep;
     const T c = w.cssp;
@@ -738,6 +751,9 @@ void ssp_cont(Launcher& L, const Work<T>& w, const State<T>& Ym, const State<T>&
     const bool relax = w.relax, forcing = w.forcing, four = w.four;
     const T gamma = w.gamma;
     const T* force = w.force;
+    const bool kn = Zs != nullptr;   // SSPRK3's stage kn: kna*eta1 + knb*eta0 + Δt_Δnc*deta
+    const State<T> zs = kn ? *Zs : Ym;
+    const T kna = w.s3_kna, knb = w.s3_knb, cnc = w.s3_cnc;
     L.d2(nx + 4, ny + 4, [=] __host__ __device__(int I, int J) {
         if (I <= ym.u.m && J <= ym.u.n) yn.u(I, J) = ym.u(I, J);
         if (I <= ym.v.m && J <= ym.v.n) yn.v(I, J) = ym.v(I, J);
@@ -756,6 +772,8 @@ void ssp_cont(Launcher& L, const Work<T>& w, const State<T>& Ym, const State<T>&
             if (four) {   // eta0 = eta1 + Δt_Δ*deta; eta1 = 0.5*(eta1 + eta0)
                 const T t = ym.e(I, J) + c * d;
                 yn.e(I, J) = T(0.5) * (ym.e(I, J) + t);
+            } else if (kn) {
+                yn.e(I, J) = kna * ym.e(I, J) + knb * zs.e(I, J) + cnc * d;
             } else {
                 yn.e(I, J) = ym.e(I, J) + c * d;
             }
@@ -798,6 +816,19 @@ void ssp_cont_rev(Launcher& L, const Work<T>& w, const State<T>& Ym, const State
             add(yb.e(I, J + 1), t); add(yb.e(I, J), t);
         }
     });
+}
+
+// d += a*x on one field, and x *= a
+template <class T>
+void field_axpy(Launcher& L, const A2<T>& d, T a, const A2<T>& x) {
+    T* dp = d.d;
+    const T* xp = x.d;
+    L.d1((long long)d.size(), [=] __host__ __device__(long long i) { dp[i] += a * xp[i]; });
+}
+template <class T>
+void field_scale(Launcher& L, const A2<T>& x, T a) {
+    T* xp = x.d;
+    L.d1((long long)x.size(), [=] __host__ __device__(long long i) { xp[i] = a * xp[i]; });
 }
 
 // d = x*a + y*b over whole states (cxayb!, src/time_integration.jl:293-305)
@@ -1110,7 +1141,14 @@ void fwd_step(Launcher& L, const Work<T>& w, bool tail = true) {
 // Z its stage inputs and tail input as the forward sweep kept them (stored =
 // true: only the passes' intermediates are recomputed).  On return Xb holds
 // the adjoint of the input, and bFx has this step's forcing adjoint added.
-// one SSPRK2 time step X -> X (src/time_integration.jl:80-104, 204-243)
+// SSPRK3's snapshot u0 at its stage kn: the state after sub-stage rki = mn
+// (sub-stage k = mn - 1), or the step's start when mn = 1
+template <class T>
+const State<T>& ssp3_snapshot(const Work<T>& w) {
+    return w.s3_mn <= 1 ? w.Ys[0] : w.Ys[2 * (w.s3_mn - 1) + 1];
+}
+
+// one SSPRK2, SSPRK3 or 4SSPRK3 time step X -> X (src/time_integration.jl:80-196, 204-243)
 template <class T>
 void fwd_step_ssp(Launcher& L, const Work<T>& w, bool tail) {
     copy_state(L, w.Ys[0], w.X);
@@ -1120,12 +1158,15 @@ void fwd_step_ssp(Launcher& L, const Work<T>& w, bool tail) {
         const State<T>&yp = w.Ys[2 * k - 1], &ym = w.Ys[2 * k], &yn = w.Ys[2 * k + 1];
         if (k > 1) ghost(L, w, yp, w.four ? GH_ALL : GH_ETA);
         stage_fwd(L, w, yp);
-        ssp_mom(L, w, yp, ym);
+        const State<T>* zs = (w.ssp3 && k + 1 == w.s3_kn) ? &ssp3_snapshot(w) : nullptr;
+        ssp_mom(L, w, yp, ym, zs);
         ghost(L, w, ym, GH_UV);
-        ssp_cont(L, w, ym, yn);
+        ssp_cont(L, w, ym, yn, zs);
         if (w.four && k == 3) combine(L, yn, w.ssp_a, w.Ys[0], w.ssp_b, yn);   // 2/3 X + 1/3 X1 (cxayb!)
+        // SSPRK3: ghost_points_eta! before the snapshot copy and the final copy (:148-152)
+        if (w.ssp3 && (k + 1 == w.s3_mn || k == w.rks)) ghost(L, w, yn, GH_ETA);
     }
-    if (w.four) copy_state(L, w.Z, w.Ys[2 * w.rks + 1]);
+    if (w.four || w.ssp3) copy_state(L, w.Z, w.Ys[2 * w.rks + 1]);
     else combine(L, w.Z, w.ssp_a, w.Ys[0], w.ssp_b, w.Ys[2 * w.rks + 1]);
     step_end(L, w, tail);
 }
@@ -1140,14 +1181,19 @@ void adj_step_ssp(Launcher& L, const Work<T>& w, bool stored, bool tail) {
     }
     ghostT(L, w, w.Xb, GH_ALL);    // Xb: adjoint of X0 = a*Ys[0] + b*Ys[2 RKs + 1]
     const State<T>& Yb = w.Yb[0];
-    if (w.four) {   // X0 is the last sub-stage's result
+    const State<T>& Zb = w.Yb[1];  // SSPRK3: adjoint of the snapshot u0
+    if (w.four || w.ssp3) {   // X0 is the last sub-stage's result
         copy_state(L, Yb, w.Xb);
         L.zero(w.acc.base, w.acc.elems * sizeof(T));
+        if (w.ssp3) {
+            L.zero(Zb.base, Zb.elems * sizeof(T));
+            ghostT(L, w, Yb, GH_ETA);   // the last sub-stage's ghost_points_eta!
+        }
     } else {        // X0 = a*Ys[0] + b*Ys[2 RKs + 1]
         combine(L, w.acc, w.ssp_a, w.Xb, T(0), w.Xb);
         combine(L, Yb, w.ssp_b, w.Xb, T(0), w.Xb);
     }
-    // d(new state)/d(tendency): Δt_Δs, or Δt_Δ/2 for the averaged 4SSPRK3 update
+    // d(new state)/d(tendency): Δt_Δs or Δt_Δn, or Δt_Δ/2 for the averaged 4SSPRK3 update
     const T coef = w.four ? T(0.5) * w.cssp : w.cssp;
     for (int k = w.rks; k >= 1; k--) {
         const State<T>&yp = w.Ys[2 * k - 1], &ym = w.Ys[2 * k];
@@ -1155,12 +1201,35 @@ void adj_step_ssp(Launcher& L, const Work<T>& w, bool stored, bool tail) {
             combine(L, w.acc, T(1), w.acc, w.ssp_a, Yb);
             combine(L, Yb, w.ssp_b, Yb, T(0), Yb);
         }
+        if (w.ssp3 && k + 1 == w.s3_mn && k < w.rks) {
+            // the state after this sub-stage was eta-ghosted in place and copied
+            // to the snapshot: its adjoint gathers the snapshot's
+            combine(L, Yb, T(1), Yb, T(1), Zb);
+            L.zero(Zb.base, Zb.elems * sizeof(T));
+            ghostT(L, w, Yb, GH_ETA);
+        }
+        // stage kn: new = kna*old + knb*snapshot + Δt_Δnc*d; the old value's
+        // adjoint is scaled by kna first, so the tendency's coefficient becomes
+        // Δt_Δnc/kna on the scaled adjoint
+        const bool kn = w.ssp3 && k + 1 == w.s3_kn;
+        const T ck = kn ? w.s3_cnc / w.s3_kna : coef;
         stage_fwd(L, w, yp);                              // h_u, h_v and the rhs intermediates of sub-stage k
-        ssp_cont_rev(L, w, ym, Yb, coef);                 // Yb: adjoint of Ym
+        if (kn) {
+            field_axpy(L, Zb.e, w.s3_knb, Yb.e);
+            field_scale(L, Yb.e, w.s3_kna);
+        }
+        ssp_cont_rev(L, w, ym, Yb, ck);                   // Yb: adjoint of Ym
         ghostT(L, w, Yb, GH_UV);
-        stage_rev(L, w, 1, yp, Yb, (const State<T>*)nullptr, Yb, true, coef);   // adjoint of Yp
+        if (kn) {
+            field_axpy(L, Zb.u, w.s3_knb, Yb.u);
+            field_axpy(L, Zb.v, w.s3_knb, Yb.v);
+            field_scale(L, Yb.u, w.s3_kna);
+            field_scale(L, Yb.v, w.s3_kna);
+        }
+        stage_rev(L, w, 1, yp, Yb, (const State<T>*)nullptr, Yb, true, ck);   // adjoint of Yp
         if (k > 1) ghostT(L, w, Yb, w.four ? GH_ALL : GH_ETA);
     }
+    if (w.ssp3 && w.s3_mn <= 1) combine(L, w.acc, T(1), w.acc, T(1), Zb);   // the snapshot was the start state
     const T* src = Yb.base;
     T* dst = w.acc.base;
     L.d1((long long)Yb.elems, [=] __host__ __device__(long long i) { dst[i] += src[i]; });
@@ -1233,8 +1302,8 @@ AdjCfgError adjoint_check(const sw_config& c) {
     if (c.T != c.Tprog || (c.T != SW_FLOAT32 && c.T != SW_FLOAT64) || c.Tcomm != c.T)
         return {SW_ERR_UNSUPPORTED, "the adjoint computes in T = Tprog = Tcomm, Float32 or Float64"};
     if (!((c.time_scheme == SW_RK && c.RKo >= 2 && c.RKo <= 4) || (c.time_scheme == SW_SSPRK2 && c.RKs >= 2 && c.RKs <= 4) ||
-          c.time_scheme == SW_4SSPRK3))
-        return {SW_ERR_UNSUPPORTED, "the adjoint follows RK2/3/4, SSPRK2 with 2-4 sub-stages and 4SSPRK3"};
+          (c.time_scheme == SW_SSPRK3 && c.ssp_n >= 2 && c.ssp_n <= 3) || c.time_scheme == SW_4SSPRK3))
+        return {SW_ERR_UNSUPPORTED, "the adjoint follows RK2/3/4, SSPRK2 with 2-4 sub-stages, SSPRK3 with n = 2 or 3 and 4SSPRK3"};
     if (c.dynamics == SW_NONLINEAR && c.nstep_advcor != 0)
         return {SW_ERR_UNSUPPORTED, "the adjoint follows nonlinear dynamics with nstep_advcor = 0"};
     if (c.nstep_diff < 1) return {SW_ERR_ARG, "nstep_diff"};
@@ -1377,9 +1446,12 @@ struct Adjoint {
         w.nux = w.ep ? c.nx : c.nx - 1; w.nuy = c.ny; w.nvx = c.nx; w.nvy = c.ny - 1;
         w.rko = c.RKo;
         w.four = c.time_scheme == SW_4SSPRK3;
-        w.ssp = c.time_scheme == SW_SSPRK2 || w.four;
-        w.rks = w.four ? 4 : c.RKs;
-        w.cssp = (T)(w.four ? c.Dt_D : c.Dt_Ds);
+        w.ssp3 = c.time_scheme == SW_SSPRK3;
+        w.ssp = c.time_scheme == SW_SSPRK2 || w.four || w.ssp3;
+        w.rks = w.four ? 4 : w.ssp3 ? c.ssp_s : c.RKs;
+        w.cssp = (T)(w.four ? c.Dt_D : w.ssp3 ? c.ssp_Dt_Dn : c.Dt_Ds);
+        w.s3_kn = c.ssp_kn; w.s3_mn = c.ssp_mn;
+        w.s3_cnc = (T)c.ssp_Dt_Dnc; w.s3_kna = (T)c.ssp_kna; w.s3_knb = (T)c.ssp_knb;
         w.ssp_a = (T)(w.four ? 2.0 / 3.0 : 1.0 / c.RKs);
         w.ssp_b = (T)(w.four ? 1.0 / 3.0 : (double)(c.RKs - 1) / c.RKs);
         w.nst = w.ssp ? 2 * w.rks + 2 : w.rko;

@@ -351,7 +351,7 @@ struct TailStorePair {
 
 template <class S16, bool PER, int DRAG, bool SMAG, int TY>
 __global__ void __launch_bounds__(128)
-s16_tail_kernel(TailArgs<float, float> A, TailStorePair<S16> out) {
+s16_tail_kernel(const __grid_constant__ TailArgs<float, float> A, const __grid_constant__ TailStorePair<S16> out) {
     tail_body<float, float, PER, DRAG, SMAG, TY>(A, (int)blockIdx.x, out);
 }
 
@@ -368,7 +368,7 @@ struct TracerIO16 {
 
 template <class S16, bool PER, bool UM_IS_U, bool CONS>
 __global__ void __launch_bounds__(128)
-s16_tracer_kernel(TracerArgs<float, float> A, TracerIO16<S16> io) {
+s16_tracer_kernel(const __grid_constant__ TracerArgs<float, float> A, const __grid_constant__ TracerIO16<S16> io) {
     tracer_body<float, float, PER, UM_IS_U, CONS>(A, (int)blockIdx.x, (int)blockIdx.y, (int)gridDim.y, io);
 }
 

@@ -104,7 +104,7 @@ __device__ void ssp_ring(const SspArgs<T, Tp>& A, int k0, int kstride) {
 // stage update of u1, v1.  Same row recurrence as rk_stage_kernel.
 template <class T, class Tp, bool PER, int MODE, bool COMBO, int TY>
 __global__ void __launch_bounds__(128)
-ssp_momentum_kernel(SspArgs<T, Tp> A) {
+ssp_momentum_kernel(const __grid_constant__ SspArgs<T, Tp> A) {
     if (A.st->stop) return;
     const Geom& g = A.g;
     const int nstrips = A.nsx * A.nsy;
@@ -237,7 +237,7 @@ ssp_momentum_kernel(SspArgs<T, Tp> A) {
 // deta = -(dUdx + dVdy) and the eta update.  One thread per T-cell.
 template <class T, class Tp, int MODE, bool COMBO>
 __global__ void __launch_bounds__(256)
-ssp_continuity_kernel(SspArgs<T, Tp> A) {
+ssp_continuity_kernel(const __grid_constant__ SspArgs<T, Tp> A) {
     if (A.st->stop) return;
     const Geom& g = A.g;
     const int a = (int)(blockIdx.x * blockDim.x + threadIdx.x);

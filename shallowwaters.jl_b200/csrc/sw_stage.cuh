@@ -336,7 +336,7 @@ SWB_ROW_UNROLL
 
 template <class T, class Tp, bool PER, bool FIRST, bool LAST, int TY>
 __global__ void __launch_bounds__(128)
-rk_stage_kernel(StageArgs<T, Tp> A) {
+rk_stage_kernel(const __grid_constant__ StageArgs<T, Tp> A) {
     rk_stage_body<T, Tp, PER, FIRST, LAST, TY>(A, (int)blockIdx.x);
 }
 

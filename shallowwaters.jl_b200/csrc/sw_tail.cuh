@@ -260,7 +260,7 @@ SWB_ROW_UNROLL
 
 template <class T, class Tp, bool PER, int DRAG, bool SMAG, int TY>
 __global__ void __launch_bounds__(128, SWB_TAIL_MINB)
-tail_kernel(TailArgs<T, Tp> A) {
+tail_kernel(const __grid_constant__ TailArgs<T, Tp> A) {
     tail_body<T, Tp, PER, DRAG, SMAG, TY>(A, (int)blockIdx.x);
 }
 

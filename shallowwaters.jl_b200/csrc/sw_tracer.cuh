@@ -172,7 +172,7 @@ __device__ __forceinline__ void tracer_body(const TracerArgs<T, Tp>& A, int bx, 
 
 template <class T, class Tp, bool PER, bool UM_IS_U, bool CONS>
 __global__ void __launch_bounds__(128)
-tracer_kernel(TracerArgs<T, Tp> A) {
+tracer_kernel(const __grid_constant__ TracerArgs<T, Tp> A) {
     tracer_body<T, Tp, PER, UM_IS_U, CONS>(A, (int)blockIdx.x, (int)blockIdx.y, (int)gridDim.y);
 }
 

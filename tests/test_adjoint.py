@@ -44,7 +44,9 @@ OPTIONS = [dict(), dict(bc="nonperiodic", α=0.5), dict(diffusion="constant"),
            dict(dynamics="linear", surface_relax=True), dict(dynamics="linear", time_scheme="SSPRK2", RKs=3, cfl=1.0,
                                                              bc="nonperiodic", α=0.5),
            dict(time_scheme="4SSPRK3", cfl=1.0), dict(time_scheme="4SSPRK3", cfl=1.0, bc="nonperiodic", α=0.5,
-                                                      adv_scheme="Sadourny")]
+                                                      adv_scheme="Sadourny"),
+           dict(time_scheme="SSPRK3", RKn=2, cfl=1.2),
+           dict(time_scheme="SSPRK3", RKn=3, cfl=2.0, bc="nonperiodic", α=0.5, surface_relax=True)]
 
 
 def setup(T=np.float64, seed=3, **kw):
@@ -98,7 +100,7 @@ def test_adjoint_entry_rejects_bad_arguments_and_unbuilt_options():
     with pytest.raises(abi.SwError) as e:
         grad(S, Prog, obs, 0)
     assert e.value.code == abi.SW_ERR_ARG
-    for kw in (dict(time_scheme="SSPRK3"), dict(nstep_advcor=2),
+    for kw in (dict(time_scheme="SSPRK3", RKn=4, cfl=2.0), dict(nstep_advcor=2),
                dict(T=np.float32, Tprog=np.float64)):
         S2, P2, o2, _ = setup(**kw)
         with pytest.raises(abi.SwError) as e:
