@@ -284,9 +284,9 @@ void sw_batch_destroy(sw_batch* b);
  * ForwardDiff/ChainRules route of the Julia ecosystem, which the reference
  * cannot take (its number types are restricted to AbstractFloat), so it has no
  * counterpart in the reference; the forward model it differentiates is
- * src/time_integration.jl:45-104,204-233.  Supported: T = Tprog = Tcomm in
- * Float32 or Float64; RK2/3/4, SSPRK2 (2-4 sub-stages) or 4SSPRK3 (the SSP
- * schemes with their semi-implicit continuity); linear dynamics, or nonlinear with Arakawa-Hsu
+ * src/time_integration.jl:45-233.  Supported: T = Tprog = Tcomm in
+ * Float32 or Float64; RK2/3/4, SSPRK2 (2-4 sub-stages), SSPRK3 (n = 2 or 3)
+ * or 4SSPRK3 (the SSP schemes with their semi-implicit continuity); linear dynamics, or nonlinear with Arakawa-Hsu
  * or Sadourny and nstep_advcor = 0; any nstep_diff, drag and diffusion;
  * either boundary; surface relaxation or forcing; seasonal wind.  Other
  * options give SW_ERR_UNSUPPORTED.  The tracer is passive and plays no part.

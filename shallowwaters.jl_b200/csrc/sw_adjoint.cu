@@ -3,12 +3,12 @@
 //   J = sum over the interior of (eta after nsteps - eta_obs)^2
 //
 // differentiated with respect to the initial state (u, v, eta with their
-// halos) and the wind forcing Fx.  The forward model is the RK or the SSPRK2
-// branch of time_integration (src/time_integration.jl:45-104, the SSPRK2 one
-// with its semi-implicit continuity, and the tail :204-233) with
-// nonlinear dynamics, Arakawa-Hsu PV advection, quadratic / linear / no bottom
-// drag and Smagorinsky / constant biharmonic diffusion, periodic or
-// nonperiodic boundaries.  The tracer is passive (it never feeds back into
+// halos) and the wind forcing Fx.  The forward model is the RK, SSPRK2, SSPRK3
+// or 4SSPRK3 branch of time_integration (src/time_integration.jl:45-196, the
+// SSP ones with their semi-implicit continuity, and the tail :204-233) with
+// nonlinear (Arakawa-Hsu or Sadourny PV advection) or linear dynamics,
+// quadratic / linear / no bottom drag and Smagorinsky / constant biharmonic
+// diffusion, periodic or nonperiodic boundaries.  The tracer is passive (it never feeds back into
 // u, v, eta), so it plays no part in J.
 //
 // Layout: every field is kept in the reference's own array shape (Julia
