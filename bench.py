@@ -190,25 +190,39 @@ def bench_ensemble(args, rank, world, barrier, allmax):
     N = 1 the same members are also run ``--threads`` contexts at a time and one
     after another, for comparison.  Each rank's span is taken between device
     synchronisations; the job time is the maximum over ranks."""
-    from swb200.ensemble import COLUMNS, c4_members, member_cost, run_batched, run_ensemble, run_local
+    from functools import partial
+    from swb200.ensemble import COLUMNS, c4_members, member_cost, run_batched, run_ensemble, run_local, run_member
+    storage = {"fp32": "native", "bf16": "bf16", "f16": "f16"}[args.form]
     members = c4_members(args.members, seed=2024, Ndays=args.days)
     costs = [member_cost(m) for m in members]
     warm = c4_members(4, seed=1, Ndays=0.05)                            # module load, graphs, caches
-    run_local(warm, threads=2)
-    run_batched(warm)
+    runner = partial(run_member, storage=storage)
+    run_local(warm, threads=2, runner=runner)
+    run_batched(warm, storage=storage)
     barrier()
     binfo = {}
     table, secs = run_ensemble(members, threads=args.threads, costs=costs, batched=True, info=binfo,
-                               chunks=args.chunks)
+                               chunks=args.chunks, storage=storage)
     barrier()
     t = allmax(secs)
     value = sum(costs) / t
     threaded = seq = None
     sample = members
+    vs_fp32 = None
     if world == 1:
         one = {}                                    # a single batch, for the time of its steps alone
-        run_ensemble(members, costs=costs, batched=True, info=one, chunks=1)
+        run_ensemble(members, costs=costs, batched=True, info=one, chunks=1, storage=storage)
         binfo["run_seconds"] = one["run_seconds"]
+        if storage != "native":
+            # the same members batched in Float32: each member's energy and
+            # mass against its Float32 run (mass: relative to the member's
+            # largest |mass| seen, as mass is near 0)
+            ref, _ = run_ensemble(members, costs=costs, batched=True, chunks=1)
+            ke, ms = COLUMNS.index("energy"), COLUMNS.index("mass")
+            de = np.abs(table[:, ke] - ref[:, ke]) / np.maximum(np.abs(ref[:, ke]), 1e-30)
+            dm = np.abs(table[:, ms] - ref[:, ms])
+            vs_fp32 = {"energy_rel_median": float(np.median(de)), "energy_rel_max": float(de.max()),
+                       "mass_abs_max": float(dm.max()), "mass_abs_fp32_max": float(np.abs(ref[:, ms]).max())}
         # the looped single-member runs (contexts on threads, and one after
         # another) on every member, or on every k-th member when
         # --compare-members bounds their time; their value is their own
@@ -218,15 +232,16 @@ def bench_ensemble(args, rank, world, barrier, allmax):
             sample = [members[int(k * step)] for k in range(args.compare_members)]
         scost = sum(member_cost(m) for m in sample)
         t0 = time.perf_counter()
-        run_local(sample, threads=args.threads)
+        run_local(sample, threads=args.threads, runner=runner)
         threaded = scost / (time.perf_counter() - t0)
         t0 = time.perf_counter()
-        run_local(sample, threads=1)
+        run_local(sample, threads=1, runner=runner)
         seq = scost / (time.perf_counter() - t0)
     if rank == 0:
         print(json.dumps({
             "metric": "ensemble cell-updates/s", "value": value, "unit": UNIT, "n_gpus": world,
-            "higher_is_better": True, "scaling": "strong", "dtype": "f32", "data": "synthetic (seeded members)",
+            "higher_is_better": True, "scaling": "strong", "dtype": "f32", "storage": args.form,
+            "data": "synthetic (seeded members)",
             "config": {"workload": f"{len(members)} members, nx in {{64..256}}, L_ratio 1-2, periodic/nonperiodic, "
                                    f"{args.days} days each", "mode": "batched: one launch per sub-step for all members",
                        "cell_updates": int(sum(costs)), "parallelism": f"members sharded over {world} GPU(s)",
@@ -235,7 +250,7 @@ def bench_ensemble(args, rank, world, barrier, allmax):
             "seconds": t, "batch_run_seconds": binfo.get("run_seconds"),
             "batch_run_value": (sum(costs) / binfo["run_seconds"]) if world == 1 and binfo.get("run_seconds") else None,
             "threaded_value": threaded, "threads": args.threads, "sequential_value": seq,
-            "compared_members": len(sample),
+            "compared_members": len(sample), "vs_fp32_members": vs_fp32,
             "nan_members": int((table[:, COLUMNS.index("nan_count")] > 0).sum())}))
     return 0
 

@@ -247,11 +247,13 @@ int sw_trim_memory(void);
 
 /* Ensembles advanced together: n members, each with its own config and static
  * fields (any grid size and parameters), advanced with one kernel launch per
- * sub-step for all members that share the boundary type and options.  Members
- * must be Float32, RK, nonlinear, nstep_diff = 1, without nstep_advcor,
- * seasonal wind or surface forcing (else SW_ERR_UNSUPPORTED).  Every member
- * computes exactly what a lone context computes.  No reference counterpart
- * (an ensemble there is a loop of run_model calls). */
+ * sub-step for all members that share the boundary type, options and state
+ * storage.  Members must be Float32, RK, nonlinear, nstep_diff = 1, without
+ * nstep_advcor, seasonal wind or surface forcing (else SW_ERR_UNSUPPORTED);
+ * their storage may be native or one of the 16-bit forms (with that form's
+ * own restrictions).  Every member computes exactly what a lone context with
+ * its config computes.  No reference counterpart (an ensemble there is a loop
+ * of run_model calls). */
 typedef struct sw_batch sw_batch;
 int sw_batch_create(int32_t n, const sw_config* cfgs, const sw_static* statics, sw_batch** out);
 /* Upload member m's state (as sw_set_state); resets the batch to step 0. */

@@ -37,6 +37,7 @@
 #include "sw_storage.cuh"
 #include "sw_s16.cuh"
 #include "sw_batch.cuh"
+#include "sw_batch16.cuh"
 #include "sw_diag.cuh"
 #include "sw_tail.cuh"
 #include "sw_tracer.cuh"
@@ -1024,6 +1025,57 @@ struct Engine16 : Engine<float, float> {
         }
     }
 
+    // The operands of RK stage k from the pairs of parity p: stage k reads the
+    // increment δ of stage k-1 (X1 = state + δ) and writes its own.
+    S16StageArgs<S16> stage16_args(sw_ctx* ctx, int k, int p, float Fxt, float Fyt) const {
+        const sw_config& c = ctx->cfg;
+        const Geom& g = ctx->g;
+        const int q = 1 - p;
+        S16StageArgs<S16> a;
+        a.g = g;
+        a.nsx = (g.N + STRIP - 1) / STRIP; a.nsy = (g.M + ctx->stage_ty - 1) / ctx->stage_ty;
+        a.nring_blocks = ring_blocks(g, 128);
+        a.uh = hi[p].u; a.vh = hi[p].v; a.eh = hi[p].e;
+        a.ul = lo[p].u; a.vl = lo[p].v; a.el = lo[p].e;
+        const F3& din1 = X1[k % 2 == 0 ? 0 : 1];
+        const F3& dout1 = X1[k % 2 == 1 ? 0 : 1];
+        a.ud = din1.u; a.vd = din1.v; a.ed = din1.e;
+        a.udo = dout1.u; a.vdo = dout1.v; a.edo = dout1.e;
+        const F3& din = D[k % 2], &dout = D[(k + 1) % 2];
+        a.uD = din.u; a.vD = din.v; a.eD = din.e;
+        a.uDo = dout.u; a.vDo = dout.v; a.eDo = dout.e;
+        a.u0o = (float*)ctx->Acc.u; a.v0o = (float*)ctx->Acc.v; a.e0o = (float*)ctx->Acc.e;
+        a.eho = hi[q].e; a.elo = lo[q].e;
+        a.H = sf<float>(ctx->H); a.fq = sf<float>(ctx->fq); a.Fx = sf<float>(ctx->Fx); a.Fy = sf<float>(ctx->Fy);
+        a.a = (float)c.RKaDt[k - 1];
+        a.b = (k < c.RKo) ? (float)c.RKbDt[k - 1] : 0.f;
+        a.g_ = (float)c.g; a.Fxt = Fxt; a.Fyt = Fyt;
+        a.s = s; a.inv_s = inv_s;
+        a.gr = rule(ctx);
+        a.st = ctx->dst;
+        return a;
+    }
+    // the tail from parity p: X0 of the last stage in, the new u, v pairs of 1 - p out
+    TailArgs<float, float> tail16_args(sw_ctx* ctx, int p) const {
+        TailArgs<float, float> t = tail_args(ctx, p);
+        t.e0 = (const float*)ctx->Acc.e;     // the last stage's FP32 eta (depth of the drag)
+        return t;
+    }
+    TailStorePair<S16> tail16_out(int p) const {
+        const int q = 1 - p;
+        return TailStorePair<S16>{hi[q].u, lo[q].u, hi[q].v, lo[q].v, s};
+    }
+    // the tracer after a step from parity p, from sst16[sp] to sst16[1 - sp]
+    TracerArgs<float, float> tracer16_args(sw_ctx* ctx, int p, int sp) const {
+        const int q = 1 - p;
+        TracerArgs<float, float> t = tracer_args(ctx, p, sp);
+        t.u = reinterpret_cast<const float*>(hi[q].u);
+        t.v = reinterpret_cast<const float*>(hi[q].v);
+        t.sst = reinterpret_cast<const float*>(sst16[sp]);
+        t.sst_o = reinterpret_cast<float*>(sst16[1 - sp]);
+        return t;
+    }
+
     // One time step from the pairs of parity p to those of 1 - p: RK stages
     // (src/time_integration.jl:55-78), the tail (:216-221) and the tracer
     // (:226-228), as in Engine::step, on the 16-bit arrays.
@@ -1035,31 +1087,9 @@ struct Engine16 : Engine<float, float> {
         const float Fxt = c.seasonal_wind_x ? (float)std::sin(c.omegaFx * (double)ctx->t) : 1.f;
         const float Fyt = c.seasonal_wind_y ? (float)std::sin(c.omegaFy * (double)ctx->t) : 1.f;
 
-        S16StageArgs<S16> a;
-        a.g = g;
-        a.nsx = (g.N + STRIP - 1) / STRIP; a.nsy = (g.M + ctx->stage_ty - 1) / ctx->stage_ty;
-        a.nring_blocks = ring_blocks(g, 128);
-        a.uh = hi[p].u; a.vh = hi[p].v; a.eh = hi[p].e;
-        a.ul = lo[p].u; a.vl = lo[p].v; a.el = lo[p].e;
-        a.u0o = (float*)ctx->Acc.u; a.v0o = (float*)ctx->Acc.v; a.e0o = (float*)ctx->Acc.e;
-        a.eho = hi[q].e; a.elo = lo[q].e;
-        a.H = sf<float>(ctx->H); a.fq = sf<float>(ctx->fq); a.Fx = sf<float>(ctx->Fx); a.Fy = sf<float>(ctx->Fy);
-        a.g_ = (float)c.g; a.Fxt = Fxt; a.Fyt = Fyt;
-        a.s = s; a.inv_s = inv_s;
-        a.gr = rule(ctx);
-        a.st = ctx->dst;
-        const int nblk = (a.nsx * a.nsy + 3) / 4 + a.nring_blocks;
         for (int k = 1; k <= c.RKo; k++) {
-            // stage k reads the increment δ of stage k-1 (X1 = state + δ) and writes its own
-            const F3& din1 = X1[k % 2 == 0 ? 0 : 1];
-            const F3& dout1 = X1[k % 2 == 1 ? 0 : 1];
-            a.ud = din1.u; a.vd = din1.v; a.ed = din1.e;
-            a.udo = dout1.u; a.vdo = dout1.v; a.edo = dout1.e;
-            const F3& din = D[k % 2], &dout = D[(k + 1) % 2];
-            a.uD = din.u; a.vD = din.v; a.eD = din.e;
-            a.uDo = dout.u; a.vDo = dout.v; a.eDo = dout.e;
-            a.a = (float)c.RKaDt[k - 1];
-            a.b = (k < c.RKo) ? (float)c.RKbDt[k - 1] : 0.f;
+            const S16StageArgs<S16> a = stage16_args(ctx, k, p, Fxt, Fyt);
+            const int nblk = (a.nsx * a.nsy + 3) / 4 + a.nring_blocks;
             const bool first = k == 1, last = k == c.RKo;
             const int rc = launch(ctx, 0, [&] {
                 if (g.ep) {
@@ -1076,9 +1106,8 @@ struct Engine16 : Engine<float, float> {
         }
 
         if (tail_now) {
-            TailArgs<float, float> t = tail_args(ctx, p);
-            t.e0 = (const float*)ctx->Acc.e;     // the last stage's FP32 eta (depth of the drag)
-            const TailStorePair<S16> o{hi[q].u, lo[q].u, hi[q].v, lo[q].v, s};
+            const TailArgs<float, float> t = tail16_args(ctx, p);
+            const TailStorePair<S16> o = tail16_out(p);
             const int nb = (t.nsx * t.nsy + 3) / 4 + t.nring_blocks;
             const bool smag = c.diffusion == SW_DIFF_SMAGORINSKY;
             const int rc = launch(ctx, 1, [&] {
@@ -1106,11 +1135,7 @@ struct Engine16 : Engine<float, float> {
                 if (rc) return rc;
             }
             if ((i % c.nadvstep) == 0) {
-                TracerArgs<float, float> t = tracer_args(ctx, p, ctx->sp);
-                t.u = reinterpret_cast<const float*>(hi[q].u);
-                t.v = reinterpret_cast<const float*>(hi[q].v);
-                t.sst = reinterpret_cast<const float*>(sst16[ctx->sp]);
-                t.sst_o = reinterpret_cast<float*>(sst16[1 - ctx->sp]);
+                const TracerArgs<float, float> t = tracer16_args(ctx, p, ctx->sp);
                 const TracerIO16<S16> io{inv_s};
                 const bool um_is_u = c.nadvstep == 1;
                 const dim3 grid = tracer_grid(ctx);
@@ -1542,14 +1567,17 @@ constexpr int BATCH_NTY = 3;
 constexpr int BATCH_TYS[BATCH_NTY] = {8, 16, 32};
 
 struct BatchGroup {
-    int per = 1, rko = 4, drag = 0;
+    int per = 1, rko = 4, drag = 0, storage = SW_STORE_NATIVE;
     bool smag = false, um_is_u = true, cons = false, tracer_any = false;
     std::vector<int> idx;                      // member indices
-    StageArgs<float, float>* stage[BATCH_NTY][2][4] = {};  // per tile height, parity of X, stage
-    TailArgs<float, float>* tail[BATCH_NTY][2] = {};
-    TracerArgs<float, float>* tracer[2] = {};   // 2n entries: k odd, then k even
-    BatchCopy* copy[2] = {};
-    BatchNan* nan[2] = {};                      // 2n entries: even, then odd tracer count
+    // argument tables: StageArgs, TailArgs, TracerArgs, BatchCopy, BatchNan for
+    // native members; S16StageArgs, S16TailBatchArgs, S16TracerBatchArgs,
+    // BatchCopy16, BatchNan16 of the storage type for 16-bit members
+    void* stage[BATCH_NTY][2][4] = {};          // per tile height, parity of X, stage
+    void* tail[BATCH_NTY][2] = {};
+    void* tracer[2] = {};                       // 2n entries: k odd, then k even
+    void* copy[2] = {};
+    void* nan[2] = {};                          // 2n entries: even, then odd tracer count
     BatchMember* memb = nullptr;
     int *b_stage[BATCH_NTY] = {}, *b_tail[BATCH_NTY] = {}, *b_tracer = nullptr, *nbx_tracer = nullptr,
         *b_copy = nullptr, *b_nan = nullptr;
@@ -1597,9 +1625,108 @@ int batch_check(const sw_config& c, std::string& why) {
     else if (c.dynamics != SW_NONLINEAR || c.nstep_advcor != 0) why = "batched members use nonlinear dynamics without nstep_advcor";
     else if (c.nstep_diff != 1) why = "batched members apply drag and diffusion every step (nstep_diff = 1)";
     else if (c.seasonal_wind_x || c.seasonal_wind_y || c.surface_forcing) why = "batched members have no time-dependent forcing";
-    else if (c.storage != SW_STORE_NATIVE) why = "batched members keep the native state storage";
     else return SW_OK;
     return SW_ERR_UNSUPPORTED;
+}
+
+template <class V>
+int upload_table(sw_batch* b, const std::vector<V>& host, void** dev) {
+    V* d = nullptr;
+    const int rc = upload_table(b, host, &d);
+    *dev = d;
+    return rc;
+}
+
+// the argument tables of a group of native members, per state parity p
+int batch_tables(sw_batch* b, BatchGroup& gr) {
+    using E = Engine<float, float>;
+    const int n = (int)gr.idx.size();
+    int rc;
+    for (int p = 0; p < 2; p++) {
+        for (int ti = 0; ti < BATCH_NTY; ti++) {
+            for (int k = 1; k <= gr.rko; k++) {
+                std::vector<StageArgs<float, float>> v;
+                for (int m : gr.idx) {
+                    v.push_back(dynamic_cast<E*>(b->mem[m]->eng.get())->stage_args(b->mem[m], k, p, true, 1.f, 1.f));
+                    v.back().nsy = (b->mem[m]->g.M + BATCH_TYS[ti] - 1) / BATCH_TYS[ti];
+                }
+                if ((rc = upload_table(b, v, &gr.stage[ti][p][k - 1]))) return rc;
+            }
+            std::vector<TailArgs<float, float>> vt;
+            for (int m : gr.idx) {
+                vt.push_back(dynamic_cast<E*>(b->mem[m]->eng.get())->tail_args(b->mem[m], p));
+                vt.back().nsy = (b->mem[m]->g.M + BATCH_TYS[ti] - 1) / BATCH_TYS[ti];
+            }
+            if ((rc = upload_table(b, vt, &gr.tail[ti][p]))) return rc;
+        }
+        std::vector<TracerArgs<float, float>> vr(2 * n);
+        std::vector<BatchCopy> vc;
+        std::vector<BatchNan> vn(2 * n);
+        for (int q = 0; q < n; q++) {
+            sw_ctx* ctx = b->mem[gr.idx[q]];
+            E* e = dynamic_cast<E*>(ctx->eng.get());
+            vr[q] = e->tracer_args(ctx, p, 0);          // k odd: sst[0] -> sst[1]
+            vr[n + q] = e->tracer_args(ctx, p, 1);      // k even: sst[1] -> sst[0]
+            const Fields3& X = ctx->S[p];
+            const Fields3& Y = ctx->S[1 - p];
+            vc.push_back(BatchCopy{(const float*)Y.u, (const float*)Y.v, (float*)ctx->um, (float*)ctx->vm,
+                                   (long long)ctx->nelem, ctx->dst});
+            for (int par = 0; par < 2; par++)
+                vn[par * n + q] = BatchNan{ctx->g, (const float*)X.u, (const float*)X.v, (const float*)X.e,
+                                           (const float*)ctx->sst[par], ctx->dst};
+        }
+        if ((rc = upload_table(b, vr, &gr.tracer[p]))) return rc;
+        if ((rc = upload_table(b, vc, &gr.copy[p]))) return rc;
+        if ((rc = upload_table(b, vn, &gr.nan[p]))) return rc;
+    }
+    return SW_OK;
+}
+
+// the same for 16-bit members, from the arguments their lone steps launch with
+// (Engine16::stage16_args, tail16_args, tail16_out, tracer16_args)
+template <class S16>
+int batch_tables16(sw_batch* b, BatchGroup& gr) {
+    using E = Engine16<S16>;
+    const int n = (int)gr.idx.size();
+    auto eng = [&](int m) { return dynamic_cast<E*>(b->mem[m]->eng.get()); };
+    int rc;
+    for (int p = 0; p < 2; p++) {
+        for (int ti = 0; ti < BATCH_NTY; ti++) {
+            for (int k = 1; k <= gr.rko; k++) {
+                std::vector<S16StageArgs<S16>> v;
+                for (int m : gr.idx) {
+                    v.push_back(eng(m)->stage16_args(b->mem[m], k, p, 1.f, 1.f));
+                    v.back().nsy = (b->mem[m]->g.M + BATCH_TYS[ti] - 1) / BATCH_TYS[ti];
+                }
+                if ((rc = upload_table(b, v, &gr.stage[ti][p][k - 1]))) return rc;
+            }
+            std::vector<S16TailBatchArgs<S16>> vt;
+            for (int m : gr.idx) {
+                vt.push_back(S16TailBatchArgs<S16>{eng(m)->tail16_args(b->mem[m], p), eng(m)->tail16_out(p)});
+                vt.back().t.nsy = (b->mem[m]->g.M + BATCH_TYS[ti] - 1) / BATCH_TYS[ti];
+            }
+            if ((rc = upload_table(b, vt, &gr.tail[ti][p]))) return rc;
+        }
+        std::vector<S16TracerBatchArgs<S16>> vr(2 * n);
+        std::vector<BatchCopy16<S16>> vc;
+        std::vector<BatchNan16<S16>> vn(2 * n);
+        for (int q = 0; q < n; q++) {
+            sw_ctx* ctx = b->mem[gr.idx[q]];
+            E* e = eng(gr.idx[q]);
+            const TracerIO16<S16> io{e->inv_s};
+            vr[q] = S16TracerBatchArgs<S16>{e->tracer16_args(ctx, p, 0), io};       // k odd: sst16[0] -> sst16[1]
+            vr[n + q] = S16TracerBatchArgs<S16>{e->tracer16_args(ctx, p, 1), io};   // k even: sst16[1] -> sst16[0]
+            const int r = 1 - p;
+            vc.push_back(BatchCopy16<S16>{e->hi[r].u, e->hi[r].v, (float*)ctx->um, (float*)ctx->vm,
+                                          (long long)ctx->nelem, e->inv_s, ctx->dst});
+            for (int par = 0; par < 2; par++)
+                vn[par * n + q] = BatchNan16<S16>{ctx->g, e->hi[p].u, e->hi[p].v, e->hi[p].e, e->sst16[par], ctx->dst};
+        }
+        if ((rc = upload_table(b, vr, &gr.tracer[p]))) return rc;
+        if ((rc = upload_table(b, vc, &gr.copy[p]))) return rc;
+        if ((rc = upload_table(b, vn, &gr.nan[p]))) return rc;
+    }
+    return SW_OK;
 }
 
 int batch_build(sw_batch* b) {
@@ -1608,7 +1735,7 @@ int batch_build(sw_batch* b) {
     for (int m = 0; m < (int)b->mem.size(); m++) {
         const sw_config& c = b->mem[m]->cfg;
         const std::vector<int> key = {c.periodic != 0, c.nadvstep == 1 || !c.tracer_advection, c.RKo,
-                                      c.bottom_drag, c.diffusion, c.tracer_consumption};
+                                      c.bottom_drag, c.diffusion, c.tracer_consumption, c.storage};
         auto it = key_group.find(key);
         if (it == key_group.end()) {
             it = key_group.emplace(key, (int)b->groups.size()).first;
@@ -1619,6 +1746,7 @@ int batch_build(sw_batch* b) {
             gr.drag = c.bottom_drag;
             gr.smag = c.diffusion == SW_DIFF_SMAGORINSKY;
             gr.cons = c.tracer_consumption != 0;
+            gr.storage = c.storage;
             b->groups.push_back(gr);
         }
         b->groups[it->second].idx.push_back(m);
@@ -1654,44 +1782,12 @@ int batch_build(sw_batch* b) {
         }
         int rc;
         b->shape_key += "|" + std::to_string(gr.per) + std::to_string(gr.um_is_u) + std::to_string(gr.rko) +
-                        std::to_string(gr.drag) + std::to_string(gr.smag) + std::to_string(gr.cons) + ";";
-        for (int p = 0; p < 2; p++) {
-            for (int ti = 0; ti < BATCH_NTY; ti++) {
-                for (int k = 1; k <= gr.rko; k++) {
-                    std::vector<StageArgs<float, float>> v;
-                    for (int m : gr.idx) {
-                        v.push_back(dynamic_cast<E*>(b->mem[m]->eng.get())->stage_args(b->mem[m], k, p, true, 1.f, 1.f));
-                        v.back().nsy = (b->mem[m]->g.M + BATCH_TYS[ti] - 1) / BATCH_TYS[ti];
-                    }
-                    if ((rc = upload_table(b, v, &gr.stage[ti][p][k - 1]))) return rc;
-                }
-                std::vector<TailArgs<float, float>> vt;
-                for (int m : gr.idx) {
-                    vt.push_back(dynamic_cast<E*>(b->mem[m]->eng.get())->tail_args(b->mem[m], p));
-                    vt.back().nsy = (b->mem[m]->g.M + BATCH_TYS[ti] - 1) / BATCH_TYS[ti];
-                }
-                if ((rc = upload_table(b, vt, &gr.tail[ti][p]))) return rc;
-            }
-            std::vector<TracerArgs<float, float>> vr(2 * n);
-            std::vector<BatchCopy> vc;
-            std::vector<BatchNan> vn(2 * n);
-            for (int q = 0; q < n; q++) {
-                sw_ctx* ctx = b->mem[gr.idx[q]];
-                E* e = dynamic_cast<E*>(ctx->eng.get());
-                vr[q] = e->tracer_args(ctx, p, 0);          // k odd: sst[0] -> sst[1]
-                vr[n + q] = e->tracer_args(ctx, p, 1);      // k even: sst[1] -> sst[0]
-                const Fields3& X = ctx->S[p];
-                const Fields3& Y = ctx->S[1 - p];
-                vc.push_back(BatchCopy{(const float*)Y.u, (const float*)Y.v, (float*)ctx->um, (float*)ctx->vm,
-                                       (long long)ctx->nelem, ctx->dst});
-                for (int par = 0; par < 2; par++)
-                    vn[par * n + q] = BatchNan{ctx->g, (const float*)X.u, (const float*)X.v, (const float*)X.e,
-                                               (const float*)ctx->sst[par], ctx->dst};
-            }
-            if ((rc = upload_table(b, vr, &gr.tracer[p]))) return rc;
-            if ((rc = upload_table(b, vc, &gr.copy[p]))) return rc;
-            if ((rc = upload_table(b, vn, &gr.nan[p]))) return rc;
-        }
+                        std::to_string(gr.drag) + std::to_string(gr.smag) + std::to_string(gr.cons) +
+                        std::to_string(gr.storage) + ";";
+        if (gr.storage == SW_STORE_BF16) rc = batch_tables16<__nv_bfloat16>(b, gr);
+        else if (gr.storage == SW_STORE_F16) rc = batch_tables16<__half>(b, gr);
+        else rc = batch_tables(b, gr);
+        if (rc) return rc;
         for (int ti = 0; ti < BATCH_NTY; ti++) {
             const std::vector<int> ps = prefix(cs[ti]), pt = prefix(ct[ti]);
             gr.n_stage[ti] = ps.back();
@@ -1728,12 +1824,13 @@ int batch_group_step(sw_batch* b, const BatchGroup& gr, int p, cudaStream_t s, i
     const int nst = gr.n_stage[ti], ntl = gr.n_tail[ti];
     const int* bst = gr.b_stage[ti];
     for (int k = 1; k <= gr.rko; k++) {
-        const StageArgs<float, float>* a = gr.stage[ti][p][k - 1];
+        const auto* a = static_cast<const StageArgs<float, float>*>(gr.stage[ti][p][k - 1]);
         if (k == 1) rk_stage_batch<float, float, PER, true, false, TY><<<nst, 128, 0, s>>>(a, bst, n, gr.memb, i);
         else if (k == gr.rko) rk_stage_batch<float, float, PER, false, true, TY><<<nst, 128, 0, s>>>(a, bst, n, gr.memb, i);
         else rk_stage_batch<float, float, PER, false, false, TY><<<nst, 128, 0, s>>>(a, bst, n, gr.memb, i);
     }
-    auto tail = [&](auto kern) { kern<<<ntl, 128, 0, s>>>(gr.tail[ti][p], gr.b_tail[ti], n, gr.memb, i); };
+    const auto* ta = static_cast<const TailArgs<float, float>*>(gr.tail[ti][p]);
+    auto tail = [&](auto kern) { kern<<<ntl, 128, 0, s>>>(ta, gr.b_tail[ti], n, gr.memb, i); };
     if (gr.smag) {
         if (gr.drag == SW_DRAG_QUADRATIC) tail(tail_batch<float, float, PER, SW_DRAG_QUADRATIC, true, TY>);
         else if (gr.drag == SW_DRAG_LINEAR) tail(tail_batch<float, float, PER, SW_DRAG_LINEAR, true, TY>);
@@ -1746,24 +1843,75 @@ int batch_group_step(sw_batch* b, const BatchGroup& gr, int p, cudaStream_t s, i
     launches += gr.rko + 1;
     if (gr.tracer_any) {
         if (!gr.um_is_u) {
-            copy_batch<<<gr.n_copy, 256, 0, s>>>(gr.copy[p], gr.b_copy, n, gr.memb, i);
+            copy_batch<<<gr.n_copy, 256, 0, s>>>(static_cast<const BatchCopy*>(gr.copy[p]), gr.b_copy, n, gr.memb, i);
             launches++;
         }
-        auto tr = [&](auto kern) { kern<<<gr.n_tracer, 128, 0, s>>>(gr.tracer[p], gr.b_tracer, gr.nbx_tracer, n, gr.memb, i); };
+        const auto* ra = static_cast<const TracerArgs<float, float>*>(gr.tracer[p]);
+        auto tr = [&](auto kern) { kern<<<gr.n_tracer, 128, 0, s>>>(ra, gr.b_tracer, gr.nbx_tracer, n, gr.memb, i); };
         if (gr.um_is_u) { if (gr.cons) tr(tracer_batch<float, float, PER, true, true>); else tr(tracer_batch<float, float, PER, true, false>); }
         else { if (gr.cons) tr(tracer_batch<float, float, PER, false, true>); else tr(tracer_batch<float, float, PER, false, false>); }
         launches++;
     }
-    nan_batch<<<gr.n_nan, 256, 0, s>>>(gr.nan[p], gr.b_nan, n, gr.memb, i);
+    nan_batch<<<gr.n_nan, 256, 0, s>>>(static_cast<const BatchNan*>(gr.nan[p]), gr.b_nan, n, gr.memb, i);
     return launches + 1;
+}
+
+// the same for a group of 16-bit members (the launches of Engine16::step)
+template <class S16, bool PER, int TY>
+int batch16_group_step(sw_batch* b, const BatchGroup& gr, int p, cudaStream_t s, int ti) {
+    const int n = (int)gr.idx.size();
+    const long long* i = b->d_step;
+    int launches = 0;
+    const int nst = gr.n_stage[ti], ntl = gr.n_tail[ti];
+    const int* bst = gr.b_stage[ti];
+    for (int k = 1; k <= gr.rko; k++) {
+        const auto* a = static_cast<const S16StageArgs<S16>*>(gr.stage[ti][p][k - 1]);
+        if (k == 1) s16_stage_batch<S16, PER, true, false, TY><<<nst, 128, 0, s>>>(a, bst, n, gr.memb, i);
+        else if (k == gr.rko) s16_stage_batch<S16, PER, false, true, TY><<<nst, 128, 0, s>>>(a, bst, n, gr.memb, i);
+        else s16_stage_batch<S16, PER, false, false, TY><<<nst, 128, 0, s>>>(a, bst, n, gr.memb, i);
+    }
+    const auto* ta = static_cast<const S16TailBatchArgs<S16>*>(gr.tail[ti][p]);
+    auto tail = [&](auto kern) { kern<<<ntl, 128, 0, s>>>(ta, gr.b_tail[ti], n, gr.memb, i); };
+    if (gr.smag) {
+        if (gr.drag == SW_DRAG_QUADRATIC) tail(s16_tail_batch<S16, PER, SW_DRAG_QUADRATIC, true, TY>);
+        else if (gr.drag == SW_DRAG_LINEAR) tail(s16_tail_batch<S16, PER, SW_DRAG_LINEAR, true, TY>);
+        else tail(s16_tail_batch<S16, PER, SW_DRAG_NONE, true, TY>);
+    } else {
+        if (gr.drag == SW_DRAG_QUADRATIC) tail(s16_tail_batch<S16, PER, SW_DRAG_QUADRATIC, false, TY>);
+        else if (gr.drag == SW_DRAG_LINEAR) tail(s16_tail_batch<S16, PER, SW_DRAG_LINEAR, false, TY>);
+        else tail(s16_tail_batch<S16, PER, SW_DRAG_NONE, false, TY>);
+    }
+    launches += gr.rko + 1;
+    if (gr.tracer_any) {
+        if (!gr.um_is_u) {
+            s16_copy_batch<S16><<<gr.n_copy, 256, 0, s>>>(static_cast<const BatchCopy16<S16>*>(gr.copy[p]), gr.b_copy,
+                                                          n, gr.memb, i);
+            launches++;
+        }
+        const auto* ra = static_cast<const S16TracerBatchArgs<S16>*>(gr.tracer[p]);
+        auto tr = [&](auto kern) { kern<<<gr.n_tracer, 128, 0, s>>>(ra, gr.b_tracer, gr.nbx_tracer, n, gr.memb, i); };
+        if (gr.um_is_u) { if (gr.cons) tr(s16_tracer_batch<S16, PER, true, true>); else tr(s16_tracer_batch<S16, PER, true, false>); }
+        else { if (gr.cons) tr(s16_tracer_batch<S16, PER, false, true>); else tr(s16_tracer_batch<S16, PER, false, false>); }
+        launches++;
+    }
+    s16_nan_batch<S16><<<gr.n_nan, 256, 0, s>>>(static_cast<const BatchNan16<S16>*>(gr.nan[p]), gr.b_nan, n,
+                                                gr.memb, i);
+    return launches + 1;
+}
+
+template <bool PER, int TY>
+int batch_group_step_storage(sw_batch* b, const BatchGroup& gr, int p, cudaStream_t s, int ti) {
+    if (gr.storage == SW_STORE_BF16) return batch16_group_step<__nv_bfloat16, PER, TY>(b, gr, p, s, ti);
+    if (gr.storage == SW_STORE_F16) return batch16_group_step<__half, PER, TY>(b, gr, p, s, ti);
+    return batch_group_step<PER, TY>(b, gr, p, s, ti);
 }
 
 template <bool PER>
 int batch_group_step_ty(sw_batch* b, const BatchGroup& gr, int p, cudaStream_t s, int ti) {
     switch (BATCH_TYS[ti]) {
-        case 8: return batch_group_step<PER, 8>(b, gr, p, s, ti);
-        case 16: return batch_group_step<PER, 16>(b, gr, p, s, ti);
-        default: return batch_group_step<PER, 32>(b, gr, p, s, ti);
+        case 8: return batch_group_step_storage<PER, 8>(b, gr, p, s, ti);
+        case 16: return batch_group_step_storage<PER, 16>(b, gr, p, s, ti);
+        default: return batch_group_step_storage<PER, 32>(b, gr, p, s, ti);
     }
 }
 

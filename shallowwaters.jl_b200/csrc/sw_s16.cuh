@@ -112,13 +112,12 @@ __device__ void s16_stage_ring(const S16StageArgs<S16>& A, int k0, int kstride) 
     }
 }
 
-// One RK stage of the 16-bit form (nonlinear, Arakawa-Hsu, plain continuity).
+// One RK stage of the 16-bit form (nonlinear, Arakawa-Hsu, plain continuity),
+// block bx of (nsx * nsy + 3) / 4 strip blocks and nring_blocks ring blocks.
 template <class S16, bool PER, bool FIRST, bool LAST, int TY>
-__global__ void __launch_bounds__(128)
-s16_stage_kernel(const __grid_constant__ S16StageArgs<S16> A) {
+__device__ __forceinline__ void s16_stage_body(const S16StageArgs<S16>& A, int bx) {
     if (A.st->stop) return;
     const Geom& g = A.g;
-    const int bx = (int)blockIdx.x;
     const int nstrips = A.nsx * A.nsy;
     const int nstrip_blocks = (nstrips + 3) / 4;
     if (bx >= nstrip_blocks) {
@@ -318,6 +317,12 @@ s16_stage_kernel(const __grid_constant__ S16StageArgs<S16> A) {
         p_rm1 = p_r;
         uN_r = uN_r1; hN_r = hN_r1; hNm1_r = hNm1_r1;
     }
+}
+
+template <class S16, bool PER, bool FIRST, bool LAST, int TY>
+__global__ void __launch_bounds__(128)
+s16_stage_kernel(const __grid_constant__ S16StageArgs<S16> A) {
+    s16_stage_body<S16, PER, FIRST, LAST, TY>(A, (int)blockIdx.x);
 }
 
 // The tail's new u, v as pairs (hi, lo), with the ghost copies of both.

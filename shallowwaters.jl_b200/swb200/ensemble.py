@@ -83,11 +83,11 @@ def partition(costs: List[int], nranks: int) -> List[List[int]]:
     return [sorted(p) for p in parts]
 
 
-def run_member(m: Member) -> np.ndarray:
+def run_member(m: Member, storage: str = "native") -> np.ndarray:
     """Run one member to its end on the current GPU; returns its row of COLUMNS."""
     from .model import Model
     P, S, Prog = member_setup(m)
-    with Model(S) as model:
+    with Model(S, storage=storage) as model:
         model.set_state(Prog)
         st = model.run(S.grid.nt)
         d = model.diagnostics()
@@ -95,12 +95,12 @@ def run_member(m: Member) -> np.ndarray:
                     dtype=np.float64)
 
 
-def _batch_create(members: List[Member], lib):
+def _batch_create(members: List[Member], lib, storage: str = "native"):
     """Host set-up of the members and the batch (sw_batch_create + states)."""
     import ctypes as C
     from . import abi
     setups = [member_setup(m) for m in members]
-    cfgs = (abi.SwConfig * len(members))(*[abi.make_config(S) for _, S, _ in setups])
+    cfgs = (abi.SwConfig * len(members))(*[abi.make_config(S, storage=storage) for _, S, _ in setups])
     statics = [abi.StaticFields(S) for _, S, _ in setups]
     sts = (abi.SwStatic * len(members))(*[st.struct for st in statics])
     b = C.c_void_p()
@@ -148,11 +148,13 @@ def _batch_run(lib, b, members, setups, states, return_states):
 
 
 def run_batched(members: List[Member], lib=None, return_states: bool = False, info: Optional[dict] = None,
-                chunks: int = 1):
+                chunks: int = 1, storage: str = "native"):
     """Run members as batches (sw_batch_*): one launch per sub-step for all
     members of a batch sharing the boundary type and options.  Returns
     {index: row of COLUMNS} (and the final states without halo when
-    ``return_states``).
+    ``return_states``).  ``storage`` ("native", "bf16", "f16") is the state
+    storage of every member (the 16-bit form keeps every array of the time
+    loop in 16 bits; Float32 members only).
 
     ``chunks`` > 1 splits the members (round robin by decreasing cost) into
     that many batches and pipelines them: while a batch runs on a worker
@@ -164,7 +166,7 @@ def run_batched(members: List[Member], lib=None, return_states: bool = False, in
     from . import abi
     lib = lib or abi.load_library()
     if chunks <= 1 or len(members) < 2 * chunks:
-        b, setups, states = _batch_create(members, lib)
+        b, setups, states = _batch_create(members, lib, storage)
         out, fin, inf = _batch_run(lib, b, members, setups, states, return_states)
         if info is not None:
             info.update(inf)
@@ -176,7 +178,7 @@ def run_batched(members: List[Member], lib=None, return_states: bool = False, in
     with cf.ThreadPoolExecutor(max_workers=chunks) as ex:
         try:
             for grp in groups:
-                b, setups, states = _batch_create(grp, lib)
+                b, setups, states = _batch_create(grp, lib, storage)
                 futs.append(ex.submit(_batch_run, lib, b, grp, setups, states, return_states))
         finally:
             results = [f.result() for f in futs]
@@ -205,11 +207,12 @@ def run_local(members: List[Member], threads: int = 8,
 
 def run_ensemble(members: List[Member], *, threads: int = 8, costs: Optional[List[int]] = None,
                  runner: Callable[[Member], np.ndarray] = run_member, batched: bool = False,
-                 info: Optional[dict] = None, chunks: int = 1):
+                 info: Optional[dict] = None, chunks: int = 1, storage: str = "native"):
     """Run an ensemble over all ranks of the default process group (or alone).
 
     Returns ``(table, seconds)``: the (len(members), len(COLUMNS)) FP64 table of
     every member's diagnostics, identical on all ranks, and this rank's time.
+    ``storage`` is the state storage of batched members (run_batched).
     """
     import torch
     import torch.distributed as dist
@@ -219,7 +222,10 @@ def run_ensemble(members: List[Member], *, threads: int = 8, costs: Optional[Lis
         costs = [member_cost(m) for m in members]
     mine = [members[i] for i in partition(costs, world)[rank]]
     t0 = time.perf_counter()
-    local = run_batched(mine, info=info, chunks=chunks) if batched and mine else run_local(mine, threads, runner)
+    if batched and mine:
+        local = run_batched(mine, info=info, chunks=chunks, storage=storage)
+    else:
+        local = run_local(mine, threads, runner)
     seconds = time.perf_counter() - t0
     table = np.zeros((len(members), len(COLUMNS)), dtype=np.float64)
     pos = {m.index: k for k, m in enumerate(members)}

@@ -86,14 +86,14 @@ def _batch_members():
     ]
 
 
-def _lone_states(members):
+def _lone_states(members, storage="native"):
     from swb200.ensemble import member_setup
     from swb200 import Model
     from swb200.initial_conditions import remove_halo
     out = {}
     for m in members:
         P, S, Prog = member_setup(m)
-        with Model(S) as model:
+        with Model(S, storage=storage) as model:
             model.set_state(Prog)
             st = model.run(S.grid.nt)
             out[m.index] = (remove_halo(*model.get_state(), S), st.steps_done, S.grid.nt)
@@ -165,3 +165,27 @@ def test_batched_members_equal_lone_runs():
         assert table[m.index][COLUMNS.index("steps")] == st.steps_done == S.grid.nt
         for x, y, name in zip(states[m.index], ref, ("u", "v", "η", "sst")):
             assert np.array_equal(x.view(np.uint32), y.view(np.uint32)), f"member {m.index}: {name}"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("storage,rows", [("bf16", "8"), ("bf16", "tuned"), ("f16", "16"), ("f16", "tuned")])
+def test_batched_16bit_members_equal_lone_runs(storage, rows, monkeypatch):
+    """Members in the 16-bit storage form, batched (one launch per sub-step
+    for all of them), end bit for bit where each ends alone in that form:
+    periodic and nonperiodic members, Smagorinsky, topography, tracers every
+    step and every few steps, tracer consumption, members finishing early."""
+    from swb200.ensemble import run_batched
+    if rows != "tuned":
+        monkeypatch.setenv("SWB200_BATCH_TY", rows)
+    else:
+        monkeypatch.delenv("SWB200_BATCH_TY", raising=False)
+    members = [m for m in _batch_members() if "adv_scheme" not in m.kwargs]
+    info = {}
+    table, states = run_batched(members, return_states=True, info=info, storage=storage)
+    if rows != "tuned":
+        assert info["tile_rows"] == int(rows)
+    for k, (ref, done, nt) in _lone_states(members, storage).items():
+        assert table[k][COLUMNS.index("steps")] == done == nt
+        assert table[k][COLUMNS.index("nan_count")] == 0
+        for x, y, name in zip(states[k], ref, ("u", "v", "η", "sst")):
+            assert np.array_equal(x.view(np.uint32), y.view(np.uint32)), f"member {k}: {name}"
