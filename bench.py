@@ -214,15 +214,16 @@ def bench_ensemble(args, rank, world, barrier, allmax):
         run_ensemble(members, costs=costs, batched=True, info=one, chunks=1, storage=storage)
         binfo["run_seconds"] = one["run_seconds"]
         if storage != "native":
-            # the same members batched in Float32: each member's energy and
-            # mass against its Float32 run (mass: relative to the member's
-            # largest |mass| seen, as mass is near 0)
+            # the same members batched in Float32: each member's energy
+            # against its Float32 run (relative), and its mass (the sum of
+            # eta) as the difference of mean eta in metres
             ref, _ = run_ensemble(members, costs=costs, batched=True, chunks=1)
-            ke, ms = COLUMNS.index("energy"), COLUMNS.index("mass")
+            ke, ms, nc = COLUMNS.index("energy"), COLUMNS.index("mass"), COLUMNS.index("cells")
             de = np.abs(table[:, ke] - ref[:, ke]) / np.maximum(np.abs(ref[:, ke]), 1e-30)
-            dm = np.abs(table[:, ms] - ref[:, ms])
+            dm = np.abs(table[:, ms] - ref[:, ms]) / ref[:, nc]
             vs_fp32 = {"energy_rel_median": float(np.median(de)), "energy_rel_max": float(de.max()),
-                       "mass_abs_max": float(dm.max()), "mass_abs_fp32_max": float(np.abs(ref[:, ms]).max())}
+                       "mean_eta_diff_max_m": float(dm.max()),
+                       "mean_eta_fp32_max_m": float((np.abs(ref[:, ms]) / ref[:, nc]).max())}
         # the looped single-member runs (contexts on threads, and one after
         # another) on every member, or on every k-th member when
         # --compare-members bounds their time; their value is their own
@@ -289,7 +290,12 @@ def bench_adjoint(args):
                                f"{ {'rk4': 'RK4', 'ssprk2': 'SSPRK2 (3 sub-stages)', '4ssprk3': '4SSPRK3'}[args.adj_scheme] }, "
                                f"Arakawa-Hsu, Smagorinsky, "
                                f"quadratic drag, {n} steps, J = sum (eta_T - eta_obs)^2, gradient w.r.t. u0, v0, "
-                               f"eta0 and Fx", "checkpoints": st_.checkpoints},
+                               f"eta0 and Fx", "checkpoints": st_.checkpoints,
+                   "schedule": {0: "checkpoint slots only (binomial, or every state kept)",
+                                1: "every step's stage inputs kept",
+                                2: "two-level: one slot per segment, segments recomputed in turn",
+                                3: "two-level: one slot per segment, each segment recomputed on a second "
+                                   "stream while the next is reversed"}[st_.stored_stage_states]},
         "forward_ms": fwd_ms, "adjoint_forward_sweep_ms": st_.forward_ms, "adjoint_reverse_sweep_ms": st_.reverse_ms,
         "adjoint_wall_s": wall, "forward_steps": st_.forward_steps, "adjoint_steps": st_.adjoint_steps,
         "launches_per_adjoint_step": st_.launches_per_adjoint_step,

@@ -318,7 +318,9 @@ typedef struct sw_adjoint_stats {
     int32_t launches_per_forward_step;
     int32_t launches_per_adjoint_step;
     int32_t stored_stage_states;       /* 1: every step's stage inputs were kept (no forward recomputation);
-                                          2: kept per segment (two-level schedule); 0: not kept */
+                                          2: kept per segment (two-level schedule); 3: the same, with
+                                          each segment recomputed on a second stream while the next
+                                          one is reversed; 0: not kept */
 } sw_adjoint_stats;
 int sw_adjoint_run(const sw_config* cfg, const sw_static* st,
                    const void* u, const void* v, const void* eta, const void* eta_obs,

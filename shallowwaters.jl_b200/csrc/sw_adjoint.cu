@@ -1319,11 +1319,17 @@ AdjCfgError adjoint_check(const sw_config& c) {
 template <class T>
 struct Adjoint {
     Work<T> w;
+    // Two-level schedule, overlapped: a second forward worker (its own state,
+    // stage states, intermediates and forcing multipliers; the static fields
+    // are shared) recomputes segment j - 1 on stream s2 while s reverses
+    // segment j, each segment's records in one of two halves of `records`
+    Work<T> wf;
+    bool overlap = false;
     bool host = false;
     std::vector<void*> blocks;
-    cudaStream_t s = nullptr;
+    cudaStream_t s = nullptr, s2 = nullptr;
     // step graphs, by whether the step ends with drag and diffusion ([1]) or not ([0])
-    cudaGraphExec_t g_fwd[2] = {}, g_adj[2] = {}, g_adj_st[2] = {};
+    cudaGraphExec_t g_fwd[2] = {}, g_adj[2] = {}, g_adj_st[2] = {}, g_fwd2[2] = {};
     int nstep_diff = 1;
     T* step_force = nullptr;    // per step k: Fxt, Fyt, Fetat at t = k*dtint (pinned host memory)
     T* records = nullptr;       // per step: Ys[0..nst-1] and Z as the forward sweep left them
@@ -1335,14 +1341,16 @@ struct Adjoint {
 
     ~Adjoint() {
         if (s) cudaStreamSynchronize(s);
+        if (s2) cudaStreamSynchronize(s2);
         if (step_force) { if (host) std::free(step_force); else cudaFreeHost(step_force); }
         for (int t = 0; t < 2; t++)
-            for (cudaGraphExec_t g : {g_fwd[t], g_adj[t], g_adj_st[t]})
+            for (cudaGraphExec_t g : {g_fwd[t], g_adj[t], g_adj_st[t], g_fwd2[t]})
                 if (g) cudaGraphExecDestroy(g);
         for (void* p : blocks) {
             if (host) std::free(p); else cudaFree(p);
         }
         if (s) cudaStreamDestroy(s);
+        if (s2) cudaStreamDestroy(s2);
     }
 
     Launcher launcher() { Launcher L{s}; L.host = host; return L; }
@@ -1351,7 +1359,7 @@ struct Adjoint {
         const size_t bytes = std::max<size_t>(elems, 1) * sizeof(T);
         void* p = nullptr;
         if (host) p = std::calloc(1, bytes);
-        else if (cudaMalloc(&p, bytes) != cudaSuccess) p = nullptr;
+        else if (cudaMalloc(&p, bytes) != cudaSuccess) { p = nullptr; (void)cudaGetLastError(); }
         if (!p) return nullptr;
         blocks.push_back(p);
         return static_cast<T*>(p);
@@ -1439,8 +1447,54 @@ struct Adjoint {
         return carve(c, &st.base, &st.elems);
     }
 
-    // want_store: keep nrecords steps' stage inputs (all steps, or one segment)
-    int setup(const sw_config& c, const sw_static& stt, bool want_store, long long nrecords) {
+    // what a forward step writes: the state X, the stage states Ys and the
+    // tail input Z (one block), the stage and tail intermediates
+    bool make_forward(Work<T>& x) {
+        if (!make_state(x.X)) return false;
+        const int nx = x.nx, ny = x.ny, nux = x.nux, nuy = x.nuy, nvx = x.nvx, nvy = x.nvy;
+        {
+            Carver cv;   // the stage states Ys[0..nst-1] and the tail input Z, contiguous (one copy saves them)
+            std::vector<State<T>*> st;
+            for (int k = 0; k < x.nst; k++) st.push_back(&x.Ys[k]);
+            st.push_back(&x.Z);
+            for (State<T>* y : st) {
+                cv.add(y->u, nux + 4, nuy + 4);
+                cv.add(y->v, nvx + 4, nvy + 4);
+                cv.add(y->e, nx + 2, ny + 2);
+            }
+            if (!carve(cv, &x.stage_block, &x.stage_block_elems)) return false;
+            for (State<T>* y : st) {
+                y->base = y->u.d;
+                y->elems = Carver::padded(y->u.m, y->u.n) + Carver::padded(y->v.m, y->v.n) + Carver::padded(y->e.m, y->e.n);
+            }
+        }
+        {
+            Carver cv;   // stage intermediates
+            cv.add(x.hu, nx + 1, ny + 2); cv.add(x.hv, nx + 2, ny + 1); cv.add(x.hq, nx + 1, ny + 1);
+            cv.add(x.U, nx + 1, ny + 2); cv.add(x.V, nx + 2, ny + 1); cv.add(x.q, nx + 1, ny + 1);
+            cv.add(x.qa, nx, ny); cv.add(x.qb, nx + 1, ny); cv.add(x.qc, nx + 1, ny); cv.add(x.qd, nx, ny);
+            cv.add(x.p, nx + 2, ny + 2);
+            cv.add(x.qu, nx + 1, ny); cv.add(x.qv, nx, ny + 1); cv.add(x.Vu, nx + 1, ny); cv.add(x.Uv, nx, ny + 1);
+            // tail intermediates
+            cv.add(x.thu, nx + 1, ny + 2); cv.add(x.thv, nx + 2, ny + 1); cv.add(x.sKE, nx + 2, ny + 2);
+            cv.add(x.sKEu, nx + 1, ny + 2); cv.add(x.sKEv, nx + 2, ny + 1);
+            cv.add(x.Bu, nx + 1, ny + 2); cv.add(x.Bv, nx + 2, ny + 1);
+            cv.add(x.Lu, nux + 2, nuy + 2); cv.add(x.Lv, nvx + 2, nvy + 2);
+            cv.add(x.dLudx, nux + 1, nuy + 2); cv.add(x.dLudy, nux + 2, nuy + 1);
+            cv.add(x.dLvdx, nvx + 1, nvy + 2); cv.add(x.dLvdy, nvx + 2, nvy + 1);
+            cv.add(x.sDT, nx + 2, ny + 2); cv.add(x.sDS, nvx + 3, nvy + 4); cv.add(x.DSq, nvx + 3, nvy + 4);
+            cv.add(x.rS, nx + 2, ny + 2); cv.add(x.nuS, nx + 2, ny + 2); cv.add(x.nuSq, nx + 1, ny + 1);
+            cv.add(x.S11, nux + 1, nuy + 2); cv.add(x.S12, nx + 1, ny + 1); cv.add(x.S21, nx + 1, ny + 1);
+            cv.add(x.S22, nvx + 2, nvy + 1);
+            if (!carve(cv)) return false;
+        }
+        return true;
+    }
+
+    // want_store: keep nrecords steps' stage inputs (all steps, or one
+    // segment); want_overlap: two segments' records and the second forward
+    // worker (falls back to one segment's records without it)
+    int setup(const sw_config& c, const sw_static& stt, bool want_store, long long nrecords, bool want_overlap) {
         if (!host && cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return SW_ERR_CUDA;
         w.nx = c.nx; w.ny = c.ny; w.ep = c.periodic ? 1 : 0;
         w.nux = w.ep ? c.nx : c.nx - 1; w.nuy = c.ny; w.nvx = c.nx; w.nvy = c.ny - 1;
@@ -1485,44 +1539,8 @@ struct Adjoint {
                 if (upload(dst[k]->d, src[k], dst[k]->size() * sizeof(T)) != cudaSuccess) return SW_ERR_CUDA;
             }
         }
-        if (!make_state(w.X) || !make_state(w.Xb) || !make_state(w.acc) || !make_state(w.Yb[0]) || !make_state(w.Yb[1]))
+        if (!make_forward(w) || !make_state(w.Xb) || !make_state(w.acc) || !make_state(w.Yb[0]) || !make_state(w.Yb[1]))
             return SW_ERR_NOMEM;
-        {
-            Carver cv;   // the stage states Ys[0..nst-1] and the tail input Z, contiguous (one copy saves them)
-            std::vector<State<T>*> st;
-            for (int k = 0; k < w.nst; k++) st.push_back(&w.Ys[k]);
-            st.push_back(&w.Z);
-            for (State<T>* x : st) {
-                cv.add(x->u, w.nux + 4, w.nuy + 4);
-                cv.add(x->v, w.nvx + 4, w.nvy + 4);
-                cv.add(x->e, w.nx + 2, w.ny + 2);
-            }
-            if (!carve(cv, &w.stage_block, &w.stage_block_elems)) return SW_ERR_NOMEM;
-            for (State<T>* x : st) {
-                x->base = x->u.d;
-                x->elems = Carver::padded(x->u.m, x->u.n) + Carver::padded(x->v.m, x->v.n) + Carver::padded(x->e.m, x->e.n);
-            }
-        }
-        {
-            Carver cv;   // stage intermediates
-            cv.add(w.hu, nx + 1, ny + 2); cv.add(w.hv, nx + 2, ny + 1); cv.add(w.hq, nx + 1, ny + 1);
-            cv.add(w.U, nx + 1, ny + 2); cv.add(w.V, nx + 2, ny + 1); cv.add(w.q, nx + 1, ny + 1);
-            cv.add(w.qa, nx, ny); cv.add(w.qb, nx + 1, ny); cv.add(w.qc, nx + 1, ny); cv.add(w.qd, nx, ny);
-            cv.add(w.p, nx + 2, ny + 2);
-            cv.add(w.qu, nx + 1, ny); cv.add(w.qv, nx, ny + 1); cv.add(w.Vu, nx + 1, ny); cv.add(w.Uv, nx, ny + 1);
-            // tail intermediates
-            cv.add(w.thu, nx + 1, ny + 2); cv.add(w.thv, nx + 2, ny + 1); cv.add(w.sKE, nx + 2, ny + 2);
-            cv.add(w.sKEu, nx + 1, ny + 2); cv.add(w.sKEv, nx + 2, ny + 1);
-            cv.add(w.Bu, nx + 1, ny + 2); cv.add(w.Bv, nx + 2, ny + 1);
-            cv.add(w.Lu, nux + 2, nuy + 2); cv.add(w.Lv, nvx + 2, nvy + 2);
-            cv.add(w.dLudx, nux + 1, nuy + 2); cv.add(w.dLudy, nux + 2, nuy + 1);
-            cv.add(w.dLvdx, nvx + 1, nvy + 2); cv.add(w.dLvdy, nvx + 2, nvy + 1);
-            cv.add(w.sDT, nx + 2, ny + 2); cv.add(w.sDS, nvx + 3, nvy + 4); cv.add(w.DSq, nvx + 3, nvy + 4);
-            cv.add(w.rS, nx + 2, ny + 2); cv.add(w.nuS, nx + 2, ny + 2); cv.add(w.nuSq, nx + 1, ny + 1);
-            cv.add(w.S11, nux + 1, nuy + 2); cv.add(w.S12, nx + 1, ny + 1); cv.add(w.S21, nx + 1, ny + 1);
-            cv.add(w.S22, nvx + 2, nvy + 1);
-            if (!carve(cv)) return SW_ERR_NOMEM;
-        }
         {
             Carver cv;   // stage adjoints (zeroed per stage)
             cv.add(w.bU, nx + 1, ny + 2); cv.add(w.bV, nx + 2, ny + 1); cv.add(w.bp, nx + 2, ny + 2);
@@ -1541,14 +1559,27 @@ struct Adjoint {
             if (!carve(cv, &w.tail_adj, &w.tail_adj_elems)) return SW_ERR_NOMEM;
         }
         if (want_store) {   // one record per step; without the memory the steps are recomputed instead
-            const size_t n = (size_t)nrecords * w.stage_block_elems;
-            void* p = nullptr;
-            if (host) p = std::calloc(n, sizeof(T));
-            else if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) { p = nullptr; cudaGetLastError(); }
-            if (p) {
-                blocks.push_back(p);
-                records = static_cast<T*>(p);
-                stored = true;
+            bool two = want_overlap && !host;
+            if (two) {
+                wf = w;    // shares the static fields; gets its own forward buffers and multipliers
+                Carver cv;
+                A2<T> fv;
+                cv.add(fv, 4, 1);
+                two = make_forward(wf) && carve(cv);
+                wf.force = fv.d;
+                two = two && cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking) == cudaSuccess;
+            }
+            for (int nb = two ? 2 : 1; nb >= 1 && !stored; nb--) {
+                const size_t n = (size_t)nb * (size_t)nrecords * w.stage_block_elems;
+                void* p = nullptr;
+                if (host) p = std::calloc(n, sizeof(T));
+                else if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) { p = nullptr; (void)cudaGetLastError(); }
+                if (p) {
+                    blocks.push_back(p);
+                    records = static_cast<T*>(p);
+                    stored = true;
+                    overlap = nb == 2;
+                }
             }
         }
         return host ? SW_OK : capture();
@@ -1574,6 +1605,22 @@ struct Adjoint {
                 if (t == 1 && k == 0) launches_fwd = L.launches;
                 else if (t == 1 && k == (stored ? 2 : 1)) launches_adj = L.launches;
             }
+        if (!overlap) return SW_OK;
+        for (int t = (nstep_diff > 1 ? 0 : 1); t < 2; t++) {   // the second worker's forward steps, on s2
+            if (cudaStreamBeginCapture(s2, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return SW_ERR_CUDA;
+            Launcher L{s2};
+            fwd_step(L, wf, t == 1);
+            cudaError_t e = cudaGetLastError();
+            cudaGraph_t graph = nullptr;
+            const cudaError_t ec = cudaStreamEndCapture(s2, &graph);
+            if (e == cudaSuccess) e = ec;
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&g_fwd2[t], graph, 0);
+            if (graph) cudaGraphDestroy(graph);
+            if (e != cudaSuccess) {
+                err = std::string("adjoint graph: ") + cudaGetErrorString(e);
+                return SW_ERR_CUDA;
+            }
+        }
         return SW_OK;
     }
 
@@ -1593,10 +1640,13 @@ struct Adjoint {
         }
         return SW_OK;
     }
-    void set_force(long long k) {   // before the replay of the step that starts at state k
+    // before the replay of the step that starts at state k (on worker w, or
+    // the second forward worker on s2)
+    void set_force(long long k, bool second = false) {
         if (!w.timedep) return;
-        if (host) std::memcpy(w.force, step_force + 3 * k, 3 * sizeof(T));
-        else cudaMemcpyAsync(w.force, step_force + 3 * k, 3 * sizeof(T), cudaMemcpyHostToDevice, s);
+        T* dst = second ? wf.force : w.force;
+        if (host) std::memcpy(dst, step_force + 3 * k, 3 * sizeof(T));
+        else cudaMemcpyAsync(dst, step_force + 3 * k, 3 * sizeof(T), cudaMemcpyHostToDevice, second ? s2 : s);
     }
 
     // the step i = k + 1 that starts at state k ends with drag and diffusion?
@@ -1610,6 +1660,16 @@ struct Adjoint {
             set_force(k);
             if (host) { Launcher L = launcher(); fwd_step(L, w, t == 1); }
             else e = cudaGraphLaunch(g_fwd[t], s);
+        }
+        fwd_steps += n;
+        return e;
+    }
+    // the second worker: its X from state `from` to state `from + n`, on s2
+    cudaError_t advance2(long long from, long long n) {
+        cudaError_t e = cudaSuccess;
+        for (long long k = from; k < from + n && e == cudaSuccess; k++) {
+            set_force(k, true);
+            e = cudaGraphLaunch(g_fwd2[tail_of(k) ? 1 : 0], s2);
         }
         fwd_steps += n;
         return e;
@@ -1673,6 +1733,59 @@ struct Adjoint {
     }
 };
 
+// The reverse sweep of the two-level schedule with the recomputation one
+// segment ahead: segment j's records (its steps' stage inputs) go to half
+// j % 2 of the records; the second worker recomputes segment j - 1 on s2
+// while s reverses segment j.  Events order the halves: the reverse of j
+// waits for the recomputation of j, the recomputation of j - 1 for the
+// reverse of j + 1 (the previous user of its half).  Every step is computed
+// as in the sequential order, on the same graphs' passes.
+template <class T>
+cudaError_t reverse_overlapped(Adjoint<T>& A, int nslots, long long seg, long long nsteps) {
+    Work<T>& w = A.w;
+    cudaEvent_t ev_start = nullptr, ev_rec[2] = {}, ev_rev[2] = {};
+    cudaError_t e = cudaSuccess;
+    for (cudaEvent_t* x : {&ev_start, &ev_rec[0], &ev_rec[1], &ev_rev[0], &ev_rev[1]})
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(x, cudaEventDisableTiming);
+    auto range = [&](long long j, long long& a, long long& b) {
+        a = j * seg;
+        b = std::min<long long>(nsteps, a + seg);
+    };
+    auto rec_of = [&](long long j, long long k) { return (j % 2) * seg + (k - j * seg); };
+    auto recompute = [&](long long j) {
+        long long a, b;
+        range(j, a, b);
+        Launcher L{A.s2};
+        copy_state(L, A.wf.X, A.slots[j]);
+        for (long long k = a; k < b && e == cudaSuccess; k++) {
+            e = A.advance2(k, 1);
+            L.copy(A.records + (size_t)rec_of(j, k) * w.stage_block_elems, A.wf.stage_block,
+                   w.stage_block_elems * sizeof(T));
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(ev_rec[j % 2], A.s2);
+    };
+    // the slots were written by the forward sweep on s
+    if (e == cudaSuccess) e = cudaEventRecord(ev_start, A.s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(A.s2, ev_start, 0);
+    const long long last = nslots - 1;
+    if (e == cudaSuccess) recompute(last);
+    for (long long j = last; j >= 0 && e == cudaSuccess; j--) {
+        if (j >= 1) {
+            if (j + 1 <= last) e = cudaStreamWaitEvent(A.s2, ev_rev[(j + 1) % 2], 0);
+            if (e == cudaSuccess) recompute(j - 1);
+        }
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(A.s, ev_rec[j % 2], 0);
+        long long a, b;
+        range(j, a, b);
+        for (long long k = b - 1; k >= a && e == cudaSuccess; k--) e = A.adjoint_stored(k, rec_of(j, k));
+        if (e == cudaSuccess) e = cudaEventRecord(ev_rev[j % 2], A.s);
+    }
+    // nothing on s2 is left unwaited: the last reverse waited for the last recomputation
+    for (cudaEvent_t x : {ev_start, ev_rec[0], ev_rec[1], ev_rev[0], ev_rev[1]})
+        if (x) cudaEventDestroy(x);
+    return e;
+}
+
 template <class T>
 int adjoint_run(bool host, const sw_config& c, const sw_static& st, const void* u, const void* v, const void* eta,
                 const void* eta_obs, int64_t nsteps, int32_t ncheckpoints, double* J, void* g_u, void* g_v,
@@ -1688,13 +1801,17 @@ int adjoint_run(bool host, const sw_config& c, const sw_static& st, const void* 
     // (seg records), so every step is recomputed once.  When those records do
     // not fit, or with SWB200_ADJ_SCHEDULE=binomial, the binomial schedule
     // runs instead on the state slots alone.
+    // The segments' recomputation runs on a second stream, one segment ahead
+    // of the reverse steps (SWB200_ADJ_OVERLAP=0: one after the other).
     const char* env = getenv("SWB200_ADJ_STORE");
     const char* envs = getenv("SWB200_ADJ_SCHEDULE");
+    const char* envo = getenv("SWB200_ADJ_OVERLAP");
     const bool store_ok = !(env && env[0] == '0');
     const bool all_steps = ncheckpoints >= nsteps;
     const bool want_segments = !all_steps && store_ok && !(envs && std::string(envs) == "binomial");
     const long long seg = want_segments ? (nsteps + ncheckpoints - 1) / std::max<long long>(1, ncheckpoints) : 0;
-    int rc = A.setup(c, st, store_ok && (all_steps || want_segments), all_steps ? nsteps : seg);
+    int rc = A.setup(c, st, store_ok && (all_steps || want_segments), all_steps ? nsteps : seg,
+                     want_segments && !(envo && envo[0] == '0'));
     if (!rc) rc = A.make_forcing(c, nsteps);
     if (rc) {
         if (!A.err.empty()) fprintf(stderr, "swb200: %s\n", A.err.c_str());
@@ -1782,6 +1899,8 @@ int adjoint_run(bool host, const sw_config& c, const sw_static& st, const void* 
     if (e == cudaSuccess) {
         if (stored_all) {
             for (long long k = nsteps - 1; k >= 0 && e == cudaSuccess; k--) e = A.adjoint_stored(k, k);
+        } else if (segments && A.overlap) {
+            e = reverse_overlapped(A, nslots, seg, nsteps);
         } else if (segments) {
             for (long long j = nslots - 1; j >= 0 && e == cudaSuccess; j--) {
                 const long long a = j * seg, b = std::min<long long>(nsteps, a + seg);
@@ -1828,7 +1947,7 @@ int adjoint_run(bool host, const sw_config& c, const sw_static& st, const void* 
         stats->checkpoints = nslots;
         stats->launches_per_forward_step = A.launches_fwd;
         stats->launches_per_adjoint_step = A.launches_adj;
-        stats->stored_stage_states = stored_all ? 1 : segments ? 2 : 0;
+        stats->stored_stage_states = stored_all ? 1 : segments ? (A.overlap ? 3 : 2) : 0;
     }
     return SW_OK;
 }

@@ -258,15 +258,21 @@ def test_checkpoint_schedule_does_not_change_the_gradient(monkeypatch):
     for a, b in ((rec.u, full.u), (rec.v, full.v), (rec.eta, full.eta), (rec.Fx, full.Fx)):
         np.testing.assert_allclose(a, b, rtol=1e-9, atol=1e-12 * np.abs(b).max())
     # two-level schedule (state slots per segment, stage inputs kept per
-    # segment: each step recomputed once) and the binomial one
-    for schedule in ("segments", "binomial"):
+    # segment: each step recomputed once), with the recomputation overlapped
+    # with the reverse steps (default) or after them, and the binomial one
+    for schedule in ("segments", "segments_in_turn", "binomial"):
+        if schedule == "segments_in_turn":
+            monkeypatch.setenv("SWB200_ADJ_OVERLAP", "0")
         if schedule == "binomial":
+            monkeypatch.delenv("SWB200_ADJ_OVERLAP")
             monkeypatch.setenv("SWB200_ADJ_SCHEDULE", "binomial")
         for nc in (6, 2, 1):
             r = gradient(S, Prog, obs, n, ncheckpoints=nc)
             assert r.J == full.J
             assert r.stats.checkpoints == nc and r.stats.forward_steps > n
             if schedule == "segments":
+                assert r.stats.stored_stage_states == 3 and r.stats.forward_steps == 2 * n
+            elif schedule == "segments_in_turn":
                 assert r.stats.stored_stage_states == 2 and r.stats.forward_steps == 2 * n
             else:
                 assert r.stats.stored_stage_states == 0
