@@ -90,9 +90,22 @@ __host__ __device__ __forceinline__ T sqrt_(T x) {
 #endif
 }
 
+// Programmatic dependent launch: a pass launched with programmatic stream
+// serialization may start while its predecessor runs; griddepcontrol.wait
+// holds its threads until the predecessor has completed and its writes are
+// visible, and launch_dependents then lets the next pass be scheduled.  The
+// passes of a step are short at the sizes the adjoint runs on, so hiding each
+// launch behind the previous pass shortens the chain.  Without the launch
+// attribute both instructions do nothing.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // one thread per point (i, j) of an m x n range, 1-based
 template <class F>
 __global__ void __launch_bounds__(256) for2d(int m, int n, F f) {
+    pdl_enter();
     const int i = (int)(blockIdx.x * 32 + threadIdx.x) + 1;
     const int j = (int)(blockIdx.y * 8 + threadIdx.y) + 1;
     if (i <= m && j <= n) f(i, j);
@@ -100,6 +113,7 @@ __global__ void __launch_bounds__(256) for2d(int m, int n, F f) {
 
 template <class F>
 __global__ void __launch_bounds__(256) for1d(long long n, F f) {
+    pdl_enter();
     for (long long k = blockIdx.x * 256LL + threadIdx.x; k < n; k += (long long)gridDim.x * 256LL) f(k);
 }
 
@@ -109,6 +123,25 @@ struct Launcher {
     cudaStream_t s;
     bool host = false;
     int launches = 0;
+    bool pdl = false;          // launch with programmatic stream serialization (see pdl_enter)
+    template <class K, class... Args>
+    void launch(K kern, dim3 g, dim3 b, Args... args) {
+        if (!pdl) {
+            kern<<<g, b, 0, s>>>(args...);
+            return;
+        }
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = g;
+        cfg.blockDim = b;
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, kern, args...);
+    }
     template <class F>
     void d2(int m, int n, F f) {
         if (host) {
@@ -116,7 +149,7 @@ struct Launcher {
                 for (int i = 1; i <= m; i++) f(i, j);
         } else {
             dim3 g((unsigned)((m + 31) / 32), (unsigned)((n + 7) / 8)), b(32, 8);
-            for2d<<<g, b, 0, s>>>(m, n, f);
+            launch(for2d<F>, g, b, m, n, f);
         }
         launches++;
     }
@@ -126,7 +159,7 @@ struct Launcher {
             for (long long k = 0; k < n; k++) f(k);
         } else {
             const long long nb = std::min<long long>((n + 255) / 256, 148LL * 16);
-            for1d<<<(unsigned)std::max<long long>(nb, 1), 256, 0, s>>>(n, f);
+            launch(for1d<F>, dim3((unsigned)std::max<long long>(nb, 1)), dim3(256), n, f);
         }
         launches++;
     }
@@ -205,6 +238,8 @@ struct Work {
     State<T> Z;                 // RK result after ghost points = the tail's input
     T* stage_block = nullptr;   // Ys[0..nst-1] and Z, contiguous in this order
     size_t stage_block_elems = 0;
+    size_t tail_inter_elems = 0;   // the tail intermediates, right after Z in the same block
+    bool tail_kept = false;     // records keep the tail intermediates: a stored reverse step does not recompute them
     State<T> Xb, acc, Yb[2];    // adjoints: of the step output / input, of the stage inputs
     // stage intermediates (src/preallocate.jl:70-152, 227-254)
     A2<T> hu, hv, hq, U, V, q, qa, qb, qc, qd, p;
@@ -217,6 +252,7 @@ struct Work {
     A2<T> bBu, bBv, bS11, bS12, bS21, bS22, bnuS, bLu, bLv, bsKE, bDSq;
     A2<T> bFx;                  // gradient with respect to Fx
     T* stage_adj = nullptr; size_t stage_adj_elems = 0;   // bU..bq, one block (zeroed per stage)
+    bool clear_stage_adj = true;  // stage_rev clears bU..bq first (not when they were cleared beforehand)
     T* tail_adj = nullptr; size_t tail_adj_elems = 0;     // bBu..bDSq, one block (zeroed per step)
 };
 
@@ -562,7 +598,9 @@ void stage_rev(Launcher& L, const Work<T>& w, int k, const State<T>& Y, const St
     const T a = mom_only ? coef : w.RKa[k - 1], b = (Wb && !mom_only) ? w.RKb[k - 1] : T(0);
     const State<T> x0 = Xb0, wb = Wb ? *Wb : Xb0, yb = Yb;
     const bool has_w = Wb != nullptr && !mom_only;
-    L.zero(w.stage_adj, w.stage_adj_elems * sizeof(T));
+    // (clearing the scratch where the passes read it instead of this memset
+    // measured 50 % slower: 491 against 335 ms for 2000 reverse steps)
+    if (w.clear_stage_adj) L.zero(w.stage_adj, w.stage_adj_elems * sizeof(T));
     // momentum_u^T, momentum_v^T (with PV_ArakawaHsu^T), continuity^T
     L.d2(nx, ny, [=] __host__ __device__(int i, int j) {
         if (i <= nux && j <= nuy) {
@@ -1174,7 +1212,7 @@ void fwd_step_ssp(Launcher& L, const Work<T>& w, bool tail) {
 template <class T>
 void adj_step_ssp(Launcher& L, const Work<T>& w, bool stored, bool tail) {
     if (!stored) fwd_step_ssp(L, w, tail);
-    else if (tail) tail_fwd(L, w, w.Z, (const State<T>*)nullptr);
+    else if (tail && !w.tail_kept) tail_fwd(L, w, w.Z, (const State<T>*)nullptr);
     if (tail) {
         ghostT(L, w, w.Xb, GH_UV);
         tail_rev(L, w, w.Z, w.Xb);
@@ -1241,7 +1279,7 @@ template <class T>
 void adj_step(Launcher& L, const Work<T>& w, bool stored, bool tail = true) {
     if (w.ssp) { adj_step_ssp(L, w, stored, tail); return; }
     if (!stored) fwd_step(L, w, tail);
-    else if (tail) tail_fwd(L, w, w.Z, (const State<T>*)nullptr);
+    else if (tail && !w.tail_kept) tail_fwd(L, w, w.Z, (const State<T>*)nullptr);
     if (tail) {
         ghostT(L, w, w.Xb, GH_UV);
         tail_rev(L, w, w.Z, w.Xb);
@@ -1262,6 +1300,65 @@ void adj_step(Launcher& L, const Work<T>& w, bool stored, bool tail = true) {
     }
     ghostT(L, w, w.acc, false);    // the step starts with ghost_points!
     copy_state(L, w.Xb, w.acc);
+}
+
+// The adjoint of an RK step from its kept stage inputs, with every stage's
+// intermediates in a buffer set of its own (ws[k-1] for stage k: copies of w
+// with their own hu .. Uv): stage_fwd of all stages runs on a side branch
+// (`side`, forked and joined with the events evf, evj) while the main branch
+// transposes the tail; the stage transposes then read them.  acc and the two
+// stage adjoints are set by one pass, the next stage adjoint is cleared by
+// the accumulation that frees it, and the last accumulation writes Xb.  Each
+// stage has its own scratch adjoints too (one block, ws_adj, cleared at the
+// fork).  The sums are those of adj_step, in the same order.
+template <class T>
+void adj_step_split(Launcher& L, Launcher* side, cudaEvent_t evf, cudaEvent_t evj, const Work<T>& w,
+                    const Work<T>* ws, T* ws_adj, size_t ws_adj_elems, bool tail) {
+    const bool fork = !L.host && side != nullptr;
+    if (fork) {
+        cudaEventRecord(evf, L.s);
+        cudaStreamWaitEvent(side->s, evf, 0);
+    }
+    Launcher& S = fork ? *side : L;
+    S.zero(ws_adj, ws_adj_elems * sizeof(T));   // every stage's scratch adjoints bU .. bUv
+    for (int k = 1; k <= w.rko; k++) stage_fwd(S, ws[k - 1], w.Ys[k - 1]);
+    if (fork) cudaEventRecord(evj, side->s);
+    if (tail) {
+        if (!w.tail_kept) tail_fwd(L, w, w.Z, (const State<T>*)nullptr);
+        ghostT(L, w, w.Xb, GH_UV);
+        tail_rev(L, w, w.Z, w.Xb);
+    }
+    ghostT(L, w, w.Xb, GH_ALL);    // Xb is now the adjoint of the RK sum X0
+    {
+        T* acc = w.acc.base; T* y0 = w.Yb[0].base; T* y1 = w.Yb[1].base;
+        const T* xb = w.Xb.base;
+        L.d1((long long)w.Xb.elems, [=] __host__ __device__(long long i) {
+            acc[i] = xb[i];
+            y0[i] = T(0);
+            y1[i] = T(0);
+        });
+    }
+    if (fork) cudaStreamWaitEvent(L.s, evj, 0);
+    const State<T>* Wb = nullptr;
+    for (int k = w.rko; k >= 1; k--) {
+        const State<T>& Yb = w.Yb[k % 2];
+        stage_rev(L, ws[k - 1], k, w.Ys[k - 1], w.Xb, Wb, Yb);
+        T* acc = w.acc.base;
+        const T* yb = Yb.base;
+        if (k > 1) {
+            ghostT(L, w, Yb, GH_ALL);            // Ys[k-1] = ghost(Y1)
+            T* nxt = w.Yb[(k + 1) % 2].base;     // Wb of this stage, the next stage's adjoint
+            L.d1((long long)Yb.elems, [=] __host__ __device__(long long i) {
+                acc[i] += yb[i];
+                nxt[i] = T(0);
+            });
+        } else {
+            T* xb = w.Xb.base;
+            L.d1((long long)Yb.elems, [=] __host__ __device__(long long i) { xb[i] = acc[i] + yb[i]; });
+        }
+        Wb = &Yb;
+    }
+    ghostT(L, w, w.Xb, GH_ALL);    // the step starts with ghost_points!
 }
 
 // J = sum (eta - obs)^2 over the interior, the differences and squares in
@@ -1325,6 +1422,15 @@ struct Adjoint {
     // segment j, each segment's records in one of two halves of `records`
     Work<T> wf;
     bool overlap = false;
+    // RK adjoint steps from kept stage inputs (adj_step_split): one set of
+    // stage intermediates per stage (ws[k-1]), computed on the side stream s3
+    // of the step graph's capture
+    Work<T> ws[4];
+    T* ws_adj = nullptr;        // the stages' scratch adjoints, one block
+    size_t ws_adj_elems = 0;
+    bool split = false;
+    cudaStream_t s3 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     bool host = false;
     std::vector<void*> blocks;
     cudaStream_t s = nullptr, s2 = nullptr;
@@ -1332,7 +1438,8 @@ struct Adjoint {
     cudaGraphExec_t g_fwd[2] = {}, g_adj[2] = {}, g_adj_st[2] = {}, g_fwd2[2] = {};
     int nstep_diff = 1;
     T* step_force = nullptr;    // per step k: Fxt, Fyt, Fetat at t = k*dtint (pinned host memory)
-    T* records = nullptr;       // per step: Ys[0..nst-1] and Z as the forward sweep left them
+    T* records = nullptr;       // per step: Ys[0..nst-1] and Z as the forward sweep left them (and the tail intermediates)
+    size_t rec_elems = 0;       // elements of a record
     bool stored = false;
     std::vector<State<T>> slots;
     long long fwd_steps = 0, adj_steps = 0;
@@ -1351,9 +1458,13 @@ struct Adjoint {
         }
         if (s) cudaStreamDestroy(s);
         if (s2) cudaStreamDestroy(s2);
+        if (s3) cudaStreamDestroy(s3);
+        for (cudaEvent_t x : {ev_fork, ev_join})
+            if (x) cudaEventDestroy(x);
     }
 
-    Launcher launcher() { Launcher L{s}; L.host = host; return L; }
+    bool pdl = false;           // programmatic dependent launch of the passes (SWB200_ADJ_PDL=0: off)
+    Launcher launcher() { Launcher L{s}; L.host = host; L.pdl = pdl; return L; }
 
     T* alloc(size_t elems) {
         const size_t bytes = std::max<size_t>(elems, 1) * sizeof(T);
@@ -1447,13 +1558,30 @@ struct Adjoint {
         return carve(c, &st.base, &st.elems);
     }
 
+    static void add_stage_adj(Carver& cv, Work<T>& x) {
+        const int nx = x.nx, ny = x.ny;
+        cv.add(x.bU, nx + 1, ny + 2); cv.add(x.bV, nx + 2, ny + 1); cv.add(x.bp, nx + 2, ny + 2);
+        cv.add(x.bqa, nx, ny); cv.add(x.bqb, nx + 1, ny); cv.add(x.bqc, nx + 1, ny); cv.add(x.bqd, nx, ny);
+        cv.add(x.bq, nx + 1, ny + 1);
+        cv.add(x.bqu, nx + 1, ny); cv.add(x.bqv, nx, ny + 1); cv.add(x.bVu, nx + 1, ny); cv.add(x.bUv, nx, ny + 1);
+    }
+    static void add_stage_inter(Carver& cv, Work<T>& x) {
+        const int nx = x.nx, ny = x.ny;
+        cv.add(x.hu, nx + 1, ny + 2); cv.add(x.hv, nx + 2, ny + 1); cv.add(x.hq, nx + 1, ny + 1);
+        cv.add(x.U, nx + 1, ny + 2); cv.add(x.V, nx + 2, ny + 1); cv.add(x.q, nx + 1, ny + 1);
+        cv.add(x.qa, nx, ny); cv.add(x.qb, nx + 1, ny); cv.add(x.qc, nx + 1, ny); cv.add(x.qd, nx, ny);
+        cv.add(x.p, nx + 2, ny + 2);
+        cv.add(x.qu, nx + 1, ny); cv.add(x.qv, nx, ny + 1); cv.add(x.Vu, nx + 1, ny); cv.add(x.Uv, nx, ny + 1);
+    }
+
     // what a forward step writes: the state X, the stage states Ys and the
-    // tail input Z (one block), the stage and tail intermediates
+    // tail input Z and, right after them, the tail intermediates (one block:
+    // one copy keeps a step's record), and the stage intermediates
     bool make_forward(Work<T>& x) {
         if (!make_state(x.X)) return false;
         const int nx = x.nx, ny = x.ny, nux = x.nux, nuy = x.nuy, nvx = x.nvx, nvy = x.nvy;
         {
-            Carver cv;   // the stage states Ys[0..nst-1] and the tail input Z, contiguous (one copy saves them)
+            Carver cv;   // the stage states Ys[0..nst-1] and the tail input Z
             std::vector<State<T>*> st;
             for (int k = 0; k < x.nst; k++) st.push_back(&x.Ys[k]);
             st.push_back(&x.Z);
@@ -1462,19 +1590,7 @@ struct Adjoint {
                 cv.add(y->v, nvx + 4, nvy + 4);
                 cv.add(y->e, nx + 2, ny + 2);
             }
-            if (!carve(cv, &x.stage_block, &x.stage_block_elems)) return false;
-            for (State<T>* y : st) {
-                y->base = y->u.d;
-                y->elems = Carver::padded(y->u.m, y->u.n) + Carver::padded(y->v.m, y->v.n) + Carver::padded(y->e.m, y->e.n);
-            }
-        }
-        {
-            Carver cv;   // stage intermediates
-            cv.add(x.hu, nx + 1, ny + 2); cv.add(x.hv, nx + 2, ny + 1); cv.add(x.hq, nx + 1, ny + 1);
-            cv.add(x.U, nx + 1, ny + 2); cv.add(x.V, nx + 2, ny + 1); cv.add(x.q, nx + 1, ny + 1);
-            cv.add(x.qa, nx, ny); cv.add(x.qb, nx + 1, ny); cv.add(x.qc, nx + 1, ny); cv.add(x.qd, nx, ny);
-            cv.add(x.p, nx + 2, ny + 2);
-            cv.add(x.qu, nx + 1, ny); cv.add(x.qv, nx, ny + 1); cv.add(x.Vu, nx + 1, ny); cv.add(x.Uv, nx, ny + 1);
+            const size_t states = cv.total();
             // tail intermediates
             cv.add(x.thu, nx + 1, ny + 2); cv.add(x.thv, nx + 2, ny + 1); cv.add(x.sKE, nx + 2, ny + 2);
             cv.add(x.sKEu, nx + 1, ny + 2); cv.add(x.sKEv, nx + 2, ny + 1);
@@ -1486,6 +1602,18 @@ struct Adjoint {
             cv.add(x.rS, nx + 2, ny + 2); cv.add(x.nuS, nx + 2, ny + 2); cv.add(x.nuSq, nx + 1, ny + 1);
             cv.add(x.S11, nux + 1, nuy + 2); cv.add(x.S12, nx + 1, ny + 1); cv.add(x.S21, nx + 1, ny + 1);
             cv.add(x.S22, nvx + 2, nvy + 1);
+            size_t all = 0;
+            if (!carve(cv, &x.stage_block, &all)) return false;
+            x.stage_block_elems = states;
+            x.tail_inter_elems = all - states;
+            for (State<T>* y : st) {
+                y->base = y->u.d;
+                y->elems = Carver::padded(y->u.m, y->u.n) + Carver::padded(y->v.m, y->v.n) + Carver::padded(y->e.m, y->e.n);
+            }
+        }
+        {
+            Carver cv;   // stage intermediates
+            add_stage_inter(cv, x);
             if (!carve(cv)) return false;
         }
         return true;
@@ -1496,6 +1624,8 @@ struct Adjoint {
     // worker (falls back to one segment's records without it)
     int setup(const sw_config& c, const sw_static& stt, bool want_store, long long nrecords, bool want_overlap) {
         if (!host && cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return SW_ERR_CUDA;
+        const char* env_pdl = getenv("SWB200_ADJ_PDL");
+        pdl = !host && !(env_pdl && env_pdl[0] == '0');
         w.nx = c.nx; w.ny = c.ny; w.ep = c.periodic ? 1 : 0;
         w.nux = w.ep ? c.nx : c.nx - 1; w.nuy = c.ny; w.nvx = c.nx; w.nvy = c.ny - 1;
         w.rko = c.RKo;
@@ -1543,10 +1673,7 @@ struct Adjoint {
             return SW_ERR_NOMEM;
         {
             Carver cv;   // stage adjoints (zeroed per stage)
-            cv.add(w.bU, nx + 1, ny + 2); cv.add(w.bV, nx + 2, ny + 1); cv.add(w.bp, nx + 2, ny + 2);
-            cv.add(w.bqa, nx, ny); cv.add(w.bqb, nx + 1, ny); cv.add(w.bqc, nx + 1, ny); cv.add(w.bqd, nx, ny);
-            cv.add(w.bq, nx + 1, ny + 1);
-            cv.add(w.bqu, nx + 1, ny); cv.add(w.bqv, nx, ny + 1); cv.add(w.bVu, nx + 1, ny); cv.add(w.bUv, nx, ny + 1);
+            add_stage_adj(cv, w);
             if (!carve(cv, &w.stage_adj, &w.stage_adj_elems)) return SW_ERR_NOMEM;
         }
         {
@@ -1569,18 +1696,47 @@ struct Adjoint {
                 wf.force = fv.d;
                 two = two && cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking) == cudaSuccess;
             }
-            for (int nb = two ? 2 : 1; nb >= 1 && !stored; nb--) {
-                const size_t n = (size_t)nb * (size_t)nrecords * w.stage_block_elems;
-                void* p = nullptr;
-                if (host) p = std::calloc(n, sizeof(T));
-                else if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) { p = nullptr; (void)cudaGetLastError(); }
-                if (p) {
-                    blocks.push_back(p);
-                    records = static_cast<T*>(p);
-                    stored = true;
-                    overlap = nb == 2;
+            // a record is the stage states and Z, and also the tail
+            // intermediates when they fit, except for the overlapped segments
+            // (measured: the f32 reverse sweep of 2000 steps at 512x256 with
+            // every step kept in 253 against 275 ms; overlapped, where the
+            // recomputation copies them too, no faster)
+            const int tr_max = want_overlap ? 0 : 1;
+            for (int nb = two ? 2 : 1; nb >= 1 && !stored; nb--)
+                for (int tr = tr_max; tr >= 0 && !stored; tr--) {
+                    const size_t re = w.stage_block_elems + (tr ? w.tail_inter_elems : 0);
+                    const size_t n = (size_t)nb * (size_t)nrecords * re;
+                    void* p = nullptr;
+                    if (host) p = std::calloc(n, sizeof(T));
+                    else if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) { p = nullptr; (void)cudaGetLastError(); }
+                    if (p) {
+                        blocks.push_back(p);
+                        records = static_cast<T*>(p);
+                        stored = true;
+                        overlap = nb == 2;
+                        rec_elems = re;
+                        w.tail_kept = tr == 1;
+                    }
                 }
+        }
+        const char* env_split = getenv("SWB200_ADJ_SPLIT");
+        const char* env_fork = getenv("SWB200_ADJ_FORK");
+        if (stored && !w.ssp && !w.linear && !(env_split && env_split[0] == '0')) {   // per-stage intermediates
+            split = true;
+            Carver ca;   // the stages' scratch adjoints, one block
+            for (int k = 0; k < w.rko && split; k++) {
+                ws[k] = w;
+                ws[k].clear_stage_adj = false;
+                Carver cv;
+                add_stage_inter(cv, ws[k]);
+                split = carve(cv);
+                add_stage_adj(ca, ws[k]);
             }
+            split = split && carve(ca, &ws_adj, &ws_adj_elems);
+            if (split && !host && !(env_fork && env_fork[0] == '0'))
+                split = cudaStreamCreateWithFlags(&s3, cudaStreamNonBlocking) == cudaSuccess &&
+                        cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming) == cudaSuccess &&
+                        cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming) == cudaSuccess;
         }
         return host ? SW_OK : capture();
     }
@@ -1590,8 +1746,12 @@ struct Adjoint {
             for (int k = 0; k < 3; k++) {
                 if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return SW_ERR_CUDA;
                 Launcher L = launcher();
+                Launcher side{s3};
+                side.pdl = pdl;
                 if (k == 0) fwd_step(L, w, t == 1);
+                else if (k == 2 && split) adj_step_split(L, s3 ? &side : nullptr, ev_fork, ev_join, w, ws, ws_adj, ws_adj_elems, t == 1);
                 else adj_step(L, w, k == 2, t == 1);
+                if (k == 2 && split) L.launches += side.launches;
                 cudaError_t e = cudaGetLastError();
                 cudaGraph_t graph = nullptr;
                 const cudaError_t ec = cudaStreamEndCapture(s, &graph);
@@ -1609,6 +1769,7 @@ struct Adjoint {
         for (int t = (nstep_diff > 1 ? 0 : 1); t < 2; t++) {   // the second worker's forward steps, on s2
             if (cudaStreamBeginCapture(s2, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return SW_ERR_CUDA;
             Launcher L{s2};
+            L.pdl = pdl;
             fwd_step(L, wf, t == 1);
             cudaError_t e = cudaGetLastError();
             cudaGraph_t graph = nullptr;
@@ -1684,11 +1845,15 @@ struct Adjoint {
     // Xb <- adjoint of the step from state k, from its stage states kept in record rec
     cudaError_t adjoint_stored(long long k, long long rec) {
         Launcher L = launcher();
-        L.copy(w.stage_block, records + (size_t)rec * w.stage_block_elems, w.stage_block_elems * sizeof(T));
+        L.copy(w.stage_block, records + (size_t)rec * rec_elems, rec_elems * sizeof(T));
         adj_steps++;
         const int t = tail_of(k) ? 1 : 0;
         set_force(k);
-        if (host) { adj_step(L, w, true, t == 1); return cudaSuccess; }
+        if (host) {
+            if (split) adj_step_split(L, (Launcher*)nullptr, nullptr, nullptr, w, ws, ws_adj, ws_adj_elems, t == 1);
+            else adj_step(L, w, true, t == 1);
+            return cudaSuccess;
+        }
         return cudaGraphLaunch(g_adj_st[t], s);
     }
     cudaError_t adjoint_of(const State<T>& state, long long k) {
@@ -1759,8 +1924,7 @@ cudaError_t reverse_overlapped(Adjoint<T>& A, int nslots, long long seg, long lo
         copy_state(L, A.wf.X, A.slots[j]);
         for (long long k = a; k < b && e == cudaSuccess; k++) {
             e = A.advance2(k, 1);
-            L.copy(A.records + (size_t)rec_of(j, k) * w.stage_block_elems, A.wf.stage_block,
-                   w.stage_block_elems * sizeof(T));
+            L.copy(A.records + (size_t)rec_of(j, k) * A.rec_elems, A.wf.stage_block, A.rec_elems * sizeof(T));
         }
         if (e == cudaSuccess) e = cudaEventRecord(ev_rec[j % 2], A.s2);
     };
@@ -1880,7 +2044,7 @@ int adjoint_run(bool host, const sw_config& c, const sw_static& st, const void* 
         if (segments && k % seg == 0 && k < nsteps) A.copy(A.slots[k / seg], w.X);
         if (stored_all) {
             Launcher L = A.launcher();
-            L.copy(A.records + (size_t)(k - 1) * w.stage_block_elems, w.stage_block, w.stage_block_elems * sizeof(T));
+            L.copy(A.records + (size_t)(k - 1) * A.rec_elems, w.stage_block, A.rec_elems * sizeof(T));
         }
     }
     record(1);
@@ -1908,8 +2072,7 @@ int adjoint_run(bool host, const sw_config& c, const sw_static& st, const void* 
                 for (long long k = a; k < b && e == cudaSuccess; k++) {
                     e = A.advance(k, 1);
                     Launcher L = A.launcher();
-                    L.copy(A.records + (size_t)(k - a) * w.stage_block_elems, w.stage_block,
-                           w.stage_block_elems * sizeof(T));
+                    L.copy(A.records + (size_t)(k - a) * A.rec_elems, w.stage_block, A.rec_elems * sizeof(T));
                 }
                 for (long long k = b - 1; k >= a && e == cudaSuccess; k--) e = A.adjoint_stored(k, k - a);
             }

@@ -248,17 +248,26 @@ namespace {
 
 // Strip height of the streaming tail and stage kernels for Float32 / Float64
 // contexts: the tallest of 32, 16, 8 rows whose strips still give four
-// blocks per SM, else 8 (the values do not depend on it).  The environment
-// variable `env` (SWB200_TAIL_TY, SWB200_STAGE_TY) = 8|16|32 forces one.
-// Other number types keep 32.
-int pick_strip_ty(const sw_config& c, const Geom& g, int nsm, const char* envname) {
+// blocks (16 warps) per SM, else 8; where the kernel has them (short_ok), the
+// tallest of 32 .. 2 rows with 16 strips per SM, else 1 (the values do not
+// depend on it).  The environment variable `env` (SWB200_TAIL_TY,
+// SWB200_STAGE_TY) forces one.  Other number types keep 32.
+int pick_strip_ty(const sw_config& c, const Geom& g, int nsm, const char* envname, bool short_ok) {
     if (c.T != c.Tprog || (c.T != SW_FLOAT32 && c.T != SW_FLOAT64)) return 32;
     const char* env = getenv(envname);
     if (env) {
         const int want = atoi(env);
         if (want == 8 || want == 16 || want == 32) return want;
+        if (short_ok && (want == 1 || want == 2 || want == 4)) return want;
     }
     const int nsx = (g.N + STRIP - 1) / STRIP;
+    if (short_ok) {
+        // down to one row: a strip's rows are a serial chain of dependent
+        // loads and shuffles, which only enough warps per SM hide
+        for (int ty : {32, 16, 8, 4, 2})
+            if ((long long)nsx * ((g.M + ty - 1) / ty) >= 16LL * nsm) return ty;
+        return 1;
+    }
     for (int ty : {32, 16, 8}) {
         const long long blocks = ((long long)nsx * ((g.M + ty - 1) / ty) + 3) / 4;
         if (blocks >= 4LL * nsm) return ty;
@@ -436,6 +445,9 @@ struct Engine : EngineBase {
     template <bool PER, bool FIRST, bool LAST>
     static void stage_launch(const StageArgs<T, Tp>& a, int nblk, cudaStream_t s, int ty) {
         if constexpr (SAME_TY) {
+            if (ty == 1) { rk_stage_kernel<T, Tp, PER, FIRST, LAST, 1><<<nblk, 128, 0, s>>>(a); return; }
+            if (ty == 2) { rk_stage_kernel<T, Tp, PER, FIRST, LAST, 2><<<nblk, 128, 0, s>>>(a); return; }
+            if (ty == 4) { rk_stage_kernel<T, Tp, PER, FIRST, LAST, 4><<<nblk, 128, 0, s>>>(a); return; }
             if (ty == 8) { rk_stage_kernel<T, Tp, PER, FIRST, LAST, 8><<<nblk, 128, 0, s>>>(a); return; }
             if (ty == 16) { rk_stage_kernel<T, Tp, PER, FIRST, LAST, 16><<<nblk, 128, 0, s>>>(a); return; }
         }
@@ -508,6 +520,9 @@ struct Engine : EngineBase {
     static void tail_launch(const TailArgs<T, Tp>& a, int nblk, cudaStream_t s, int ty) {
         constexpr bool SAME = std::is_same<T, Tp>::value && (std::is_same<T, float>::value || std::is_same<T, double>::value);
         if constexpr (SAME) {
+            if (ty == 1) { tail_kernel<T, Tp, PER, DRAG, SMAG, 1><<<nblk, 128, 0, s>>>(a); return; }
+            if (ty == 2) { tail_kernel<T, Tp, PER, DRAG, SMAG, 2><<<nblk, 128, 0, s>>>(a); return; }
+            if (ty == 4) { tail_kernel<T, Tp, PER, DRAG, SMAG, 4><<<nblk, 128, 0, s>>>(a); return; }
             if (ty == 8) { tail_kernel<T, Tp, PER, DRAG, SMAG, 8><<<nblk, 128, 0, s>>>(a); return; }
             if (ty == 16) { tail_kernel<T, Tp, PER, DRAG, SMAG, 16><<<nblk, 128, 0, s>>>(a); return; }
         }
@@ -2259,8 +2274,12 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, dev);
+        // The TMA stage kernel from two of its tiles per SM up; on smaller
+        // grids the streaming kernel with short strips (measured faster:
+        // 74 against 97 us per step at 512x256).  SWB200_TMA=0|1 forces it.
         const char* env = getenv("SWB200_TMA");
-        bool want = !(env && env[0] == '0');
+        const long long tma_tiles = (long long)((g.N + BAND - 1) / BAND) * ((g.M + STAGE_TMA_TY - 1) / STAGE_TMA_TY);
+        bool want = env ? env[0] != '0' : tma_tiles >= 2LL * ctx->nsm;
         bool ok = want && encode_fn() != nullptr;
         // a cap on the TMA stage kernel's persistent blocks (SWB200_STAGE_BLOCKS),
         // so that small grids also run blocks that take several tiles each
@@ -2283,8 +2302,10 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
         ctx->use_tma = ok;
         const char* envg = getenv("SWB200_GRAPHS");
         ctx->use_graphs = !(envg && envg[0] == '0');
-        ctx->tail_ty = pick_strip_ty(*cfg, g, ctx->nsm, "SWB200_TAIL_TY");
-        ctx->stage_ty = pick_strip_ty(*cfg, g, ctx->nsm, "SWB200_STAGE_TY");
+        // strips of 1, 2 or 4 rows: the plain RK stage kernel and the native-storage tail only
+        const bool native = cfg->storage == SW_STORE_NATIVE;
+        ctx->tail_ty = pick_strip_ty(*cfg, g, ctx->nsm, "SWB200_TAIL_TY", native);
+        ctx->stage_ty = pick_strip_ty(*cfg, g, ctx->nsm, "SWB200_STAGE_TY", native && cfg->time_scheme == SW_RK);
     }
     if (cfg->storage == SW_STORE_BF16) {
         auto* e = new Engine16<__nv_bfloat16>(); ctx->eng.reset(e); if ((rc = e->init(ctx))) return rc;

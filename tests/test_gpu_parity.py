@@ -111,8 +111,14 @@ CASES = {
 }
 
 
+@pytest.mark.parametrize("stage", ["auto", "tma"])
 @pytest.mark.parametrize("name", list(CASES))
-def test_bitwise_parity(name):
+def test_bitwise_parity(name, stage, monkeypatch):
+    """Every option case, bit for bit, with the stage kernel the grid size picks
+    (short streaming strips at these sizes) and with the TMA stage kernel
+    forced (SWB200_TMA=1; options it does not serve stay streaming)."""
+    if stage == "tma":
+        monkeypatch.setenv("SWB200_TMA", "1")
     kw = dict(BASE)
     kw.update(CASES[name])
     both(kw, 0, checkpoints=[1, 2, 7, 20])
@@ -192,7 +198,7 @@ def test_kernel_launch_count():
     assert m.kernel_launches - n0 >= 60
 
 
-@pytest.mark.parametrize("rows", ["8", "16", "32"])
+@pytest.mark.parametrize("rows", ["1", "2", "4", "8", "16", "32"])
 @pytest.mark.parametrize("kw", [dict(diffusion="Smagorinsky"), dict(bc="nonperiodic", α=0.5, T=np.float64)])
 def test_every_tail_strip_height_is_bit_exact(rows, kw, monkeypatch):
     """The streaming tail's strip height (chosen by grid size, forced here with
@@ -203,12 +209,15 @@ def test_every_tail_strip_height_is_bit_exact(rows, kw, monkeypatch):
     both(k, 0, checkpoints=[1, 5])
 
 
-@pytest.mark.parametrize("rows", ["8", "16", "32"])
+@pytest.mark.parametrize("rows", ["1", "2", "4", "8", "16", "32"])
 @pytest.mark.parametrize("kw", [dict(adv_scheme="Sadourny", diffusion="Smagorinsky"),
+                                dict(bc="nonperiodic", α=0.5, topography="seamount"),
                                 dict(time_scheme="SSPRK2", RKs=3, cfl=1.0, bc="nonperiodic", α=0.5, T=np.float64)])
 def test_every_stage_strip_height_is_bit_exact(rows, kw, monkeypatch):
     """The streaming stage and SSP momentum kernels' strip height (chosen by
-    grid size, forced here with SWB200_STAGE_TY) does not change a bit."""
+    grid size, forced here with SWB200_STAGE_TY; 1, 2 and 4 rows serve the RK
+    stage only, the SSP kernels keep their own) does not change a bit."""
+    monkeypatch.setenv("SWB200_TMA", "0")
     monkeypatch.setenv("SWB200_STAGE_TY", rows)
     k = dict(BASE)
     k.update(kw)

@@ -80,6 +80,7 @@ def test_channel_100x50_ten_days_bitwise():
 def test_option_table_with_capped_stage_blocks(name, blocks, monkeypatch):
     """The option table's cases with at most `blocks` persistent blocks in the
     TMA stage kernel: still bit for bit the oracle's results."""
+    monkeypatch.setenv("SWB200_TMA", "1")      # the TMA stage kernel at these sizes too
     monkeypatch.setenv("SWB200_STAGE_BLOCKS", blocks)
     kw = dict(BASE)
     kw.update(CASES[name])

@@ -28,6 +28,7 @@ def _setup():
 @pytest.mark.parametrize("chunk", ["0", "1"])
 def test_stage_wait_runs_out_and_reports_timeout(chunk, monkeypatch):
     S, Prog = _setup()
+    monkeypatch.setenv("SWB200_TMA", "1")      # the TMA stage kernel at this size too
     monkeypatch.setenv("SWB200_TEST_WAIT_LIMIT", "4096")
     monkeypatch.setenv("SWB200_TEST_SKIP_CHUNK", chunk)
     m = Model(S)
