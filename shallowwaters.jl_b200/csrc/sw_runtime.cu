@@ -572,6 +572,9 @@ struct Engine : EngineBase {
         }
         const int nb = (a.nsx * a.nsy + 3) / 4 + a.nring_blocks;
         if constexpr (SAME_TY) {
+            if (ctx->stage_ty == 1) { ssp_momentum_kernel<T, Tp, PER, MODE, FINAL, 1><<<nb, 128, 0, ctx->stream>>>(a); return; }
+            if (ctx->stage_ty == 2) { ssp_momentum_kernel<T, Tp, PER, MODE, FINAL, 2><<<nb, 128, 0, ctx->stream>>>(a); return; }
+            if (ctx->stage_ty == 4) { ssp_momentum_kernel<T, Tp, PER, MODE, FINAL, 4><<<nb, 128, 0, ctx->stream>>>(a); return; }
             if (ctx->stage_ty == 8) { ssp_momentum_kernel<T, Tp, PER, MODE, FINAL, 8><<<nb, 128, 0, ctx->stream>>>(a); return; }
             if (ctx->stage_ty == 16) { ssp_momentum_kernel<T, Tp, PER, MODE, FINAL, 16><<<nb, 128, 0, ctx->stream>>>(a); return; }
         }
@@ -2302,10 +2305,10 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
         ctx->use_tma = ok;
         const char* envg = getenv("SWB200_GRAPHS");
         ctx->use_graphs = !(envg && envg[0] == '0');
-        // strips of 1, 2 or 4 rows: the plain RK stage kernel and the native-storage tail only
+        // strips of 1, 2 or 4 rows: the RK stage, SSP momentum and tail kernels of the native storage
         const bool native = cfg->storage == SW_STORE_NATIVE;
         ctx->tail_ty = pick_strip_ty(*cfg, g, ctx->nsm, "SWB200_TAIL_TY", native);
-        ctx->stage_ty = pick_strip_ty(*cfg, g, ctx->nsm, "SWB200_STAGE_TY", native && cfg->time_scheme == SW_RK);
+        ctx->stage_ty = pick_strip_ty(*cfg, g, ctx->nsm, "SWB200_STAGE_TY", native);
     }
     if (cfg->storage == SW_STORE_BF16) {
         auto* e = new Engine16<__nv_bfloat16>(); ctx->eng.reset(e); if ((rc = e->init(ctx))) return rc;

@@ -212,11 +212,12 @@ def test_every_tail_strip_height_is_bit_exact(rows, kw, monkeypatch):
 @pytest.mark.parametrize("rows", ["1", "2", "4", "8", "16", "32"])
 @pytest.mark.parametrize("kw", [dict(adv_scheme="Sadourny", diffusion="Smagorinsky"),
                                 dict(bc="nonperiodic", α=0.5, topography="seamount"),
-                                dict(time_scheme="SSPRK2", RKs=3, cfl=1.0, bc="nonperiodic", α=0.5, T=np.float64)])
+                                dict(time_scheme="SSPRK2", RKs=3, cfl=1.0, bc="nonperiodic", α=0.5, T=np.float64),
+                                dict(time_scheme="SSPRK3", RKn=2, cfl=1.2, diffusion="Smagorinsky"),
+                                dict(time_scheme="4SSPRK3", cfl=1.0, bc="nonperiodic", α=1.0)])
 def test_every_stage_strip_height_is_bit_exact(rows, kw, monkeypatch):
     """The streaming stage and SSP momentum kernels' strip height (chosen by
-    grid size, forced here with SWB200_STAGE_TY; 1, 2 and 4 rows serve the RK
-    stage only, the SSP kernels keep their own) does not change a bit."""
+    grid size, forced here with SWB200_STAGE_TY) does not change a bit."""
     monkeypatch.setenv("SWB200_TMA", "0")
     monkeypatch.setenv("SWB200_STAGE_TY", rows)
     k = dict(BASE)
