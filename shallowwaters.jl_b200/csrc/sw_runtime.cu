@@ -15,6 +15,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
+#include <omp.h>
 
 #include <algorithm>
 #include <map>
@@ -1217,20 +1218,16 @@ int check_config(const sw_config* c, std::string& why) {
 }
 
 // Rows [j0, j1) of a w-wide host field with W-sized elements (bitwise):
-// whether every row is constant along x, and whether every row equals row 0.
+// whether every row is constant along x (the row equals itself shifted by one
+// element), and whether every row equals row 0.  memcmp compares in wide
+// words; a row stays in cache between its two comparisons.
 template <class W>
 void scan_rows(const unsigned char* src, int w, int j0, int j1, bool& cx, bool& cy) {
-    const W* base = reinterpret_cast<const W*>(src);
+    const size_t rb = (size_t)w * sizeof(W);
     for (int j = j0; j < j1 && (cx || cy); j++) {
-        const W* r = base + (size_t)j * w;
-        const W a = r[0];
-        bool rx = cx, ry = cy && j > 0;
-        for (int i = 0; i < w && (rx || ry); i++) {
-            if (rx && r[i] != a) rx = false;
-            if (ry && r[i] != base[i]) ry = false;
-        }
-        cx = rx;
-        if (j > 0) cy = ry;
+        const unsigned char* r = src + (size_t)j * rb;
+        if (cx && w > 1) cx = std::memcmp(r, r + sizeof(W), rb - sizeof(W)) == 0;
+        if (cy && j > 0) cy = std::memcmp(r, src, rb) == 0;
     }
 }
 
@@ -1240,7 +1237,8 @@ template <class W>
 void scan_field(const unsigned char* src, int w, int h, bool& const_x, bool& const_y) {
     bool cx = true, cy = true;
     const long long bytes = (long long)w * h * sizeof(W);
-    const int nt = (int)std::min<long long>(8, std::max<long long>(1, bytes >> 21));
+    static const int ncpu = std::max(1, omp_get_num_procs());
+    const int nt = (int)std::min<long long>(std::min(16, ncpu), std::max<long long>(1, bytes >> 20));
 #pragma omp parallel for num_threads(nt) reduction(&& : cx, cy) schedule(static) if (nt > 1)
     for (int k = 0; k < nt; k++) {
         bool x = true, y = true;
@@ -1295,8 +1293,7 @@ PackedStatic pack_static(const sw_ctx* ctx, const void* host, int w, int h, int 
 // refreshes a context that the layout changed.  The copy is asynchronous on
 // the context's stream: the packed buffer is kept in ctx->staging until the
 // caller synchronises.
-int upload_static(sw_ctx* ctx, sw_ctx::SF& out, const void* host, int w, int h, int hx0, int hy0) {
-    PackedStatic pk = pack_static(ctx, host, w, h, hx0, hy0);
+int upload_static(sw_ctx* ctx, sw_ctx::SF& out, PackedStatic&& pk) {
     if (out.p) {
         if (out.bytes != pk.buf.size() || out.sx != pk.sx || out.sy != pk.sy) return SW_ERR_UNSUPPORTED;
     } else {
@@ -1312,28 +1309,33 @@ int upload_static(sw_ctx* ctx, sw_ctx::SF& out, const void* host, int w, int h, 
 
 // The static fields of a context (src/grid.jl:93-95, src/forcing.jl:1-53):
 // uploaded at creation, and again when a cached context is reused.
+// All fields are scanned and packed on the host first, then copied: a copy
+// from pageable memory waits for the work before it on the stream, and the
+// scans should overlap that work (the state's copies of a refreshed context).
 int upload_statics(sw_ctx* ctx, const sw_static* st) {
     const sw_config* cfg = &ctx->cfg;
     const Geom& g = ctx->g;
     const int N = g.N, M = g.M, nux = g.ep ? N : N - 1;
-    int rc;
-    if ((rc = upload_static(ctx, ctx->fq, st->f_q, N + 1, M + 1, 0, 0))) return rc;
-    if ((rc = upload_static(ctx, ctx->Fx, st->Fx, nux, M, 1 - g.ep, 0))) return rc;
-    if ((rc = upload_static(ctx, ctx->Fy, st->Fy, N, M - 1, 0, 1))) return rc;
-    if ((rc = upload_static(ctx, ctx->H, st->H, N + 2, M + 2, -1, -1))) return rc;
+    struct Job { sw_ctx::SF* out; const void* host; int w, h, hx0, hy0; };
+    std::vector<Job> jobs = {{&ctx->fq, st->f_q, N + 1, M + 1, 0, 0}, {&ctx->Fx, st->Fx, nux, M, 1 - g.ep, 0},
+                             {&ctx->Fy, st->Fy, N, M - 1, 0, 1}, {&ctx->H, st->H, N + 2, M + 2, -1, -1}};
     if (cfg->dynamics == SW_LINEAR) {
         if (!st->f_u || !st->f_v) return fail(ctx, SW_ERR_ARG, "linear dynamics needs f_u and f_v");
-        if ((rc = upload_static(ctx, ctx->fu, st->f_u, nux, M, 1 - g.ep, 0))) return rc;
-        if ((rc = upload_static(ctx, ctx->fv, st->f_v, N, M - 1, 0, 1))) return rc;
+        jobs.push_back({&ctx->fu, st->f_u, nux, M, 1 - g.ep, 0});
+        jobs.push_back({&ctx->fv, st->f_v, N, M - 1, 0, 1});
     }
     if (cfg->surface_relax) {
         if (!st->eta_ref) return fail(ctx, SW_ERR_ARG, "surface_relax needs eta_ref");
-        if ((rc = upload_static(ctx, ctx->eref, st->eta_ref, N, M, 0, 0))) return rc;
+        jobs.push_back({&ctx->eref, st->eta_ref, N, M, 0, 0});
     }
     if (cfg->surface_forcing) {
         if (!st->Feta) return fail(ctx, SW_ERR_ARG, "surface_forcing needs Feta");
-        if ((rc = upload_static(ctx, ctx->Feta, st->Feta, N, M, 0, 0))) return rc;
+        jobs.push_back({&ctx->Feta, st->Feta, N, M, 0, 0});
     }
+    std::vector<PackedStatic> packed;
+    for (const Job& j : jobs) packed.push_back(pack_static(ctx, j.host, j.w, j.h, j.hx0, j.hy0));
+    for (size_t k = 0; k < jobs.size(); k++)
+        if (int rc = upload_static(ctx, *jobs[k].out, std::move(packed[k]))) return rc;
     return SW_OK;
 }
 
@@ -1513,12 +1515,44 @@ sw_ctx* take_dropin(const sw_config* cfg) {
 
 // Zero the context's buffers (as sw_create leaves them) and upload the static
 // fields of this call; anything but SW_OK means: do not use this context.
-int refresh_dropin(sw_ctx* ctx, const sw_config* cfg, const sw_static* st) {
+// sw_set_state in two parts: the state's copies into the device layout
+// (asynchronous), then the kernels that read it (the prologue, which may read
+// the static fields too, the ghost points and the storage form's copy).
+int state_copy_in(sw_ctx* ctx, const void* u, const void* v, const void* eta, const void* sst) {
+    ctx->p = 0; ctx->sp = 0; ctx->step = 0; ctx->t = 0;
+    ctx->rhs_in = Fields3();
+    int rc;
+    if ((rc = copy_in(ctx, ctx->S[0].u, u, shape_u(ctx->g)))) return rc;
+    if ((rc = copy_in(ctx, ctx->S[0].v, v, shape_v(ctx->g)))) return rc;
+    if ((rc = copy_in(ctx, ctx->S[0].e, eta, shape_e(ctx->g)))) return rc;
+    if ((rc = copy_in(ctx, ctx->sst[0], sst, shape_s(ctx->g)))) return rc;
+    CK(cudaMemsetAsync(ctx->dst, 0, sizeof(DevStatus), ctx->stream));
+    CK(cudaMemsetAsync(ctx->sched, 0, sizeof(TileSched), ctx->stream));
+    return SW_OK;
+}
+int state_prepare(sw_ctx* ctx) {
+    int rc;
+    // the prologue reads the state as given, before any ghost point copy
+    // (src/time_integration.jl:20-31)
+    if ((rc = ctx->eng->prologue(ctx))) return rc;
+    // ghost_points!(u,v,eta) opens every step (src/time_integration.jl:48); it is
+    // idempotent after the first, so it is applied once here
+    if ((rc = ctx->eng->ghost_state(ctx))) return rc;
+    return ctx->eng->state_uploaded(ctx);
+}
+
+// A cached context made ready for a call: its buffers zeroed, the state's
+// copies issued first so that the host's scan of the static fields overlaps
+// them, the static fields uploaded in place, then the state's kernels.
+int refresh_dropin(sw_ctx* ctx, const sw_config* cfg, const sw_static* st, const void* u, const void* v,
+                   const void* eta, const void* sst) {
     ctx->cfg.nt = cfg->nt;
     ctx->err.clear();
     for (auto& z : ctx->zeroed) CK(cudaMemsetAsync(z.first, 0, z.second, ctx->stream));
-    int rc = upload_statics(ctx, st);
-    if (rc) return rc;
+    int rc;
+    if ((rc = state_copy_in(ctx, u, v, eta, sst))) return rc;
+    if ((rc = upload_statics(ctx, st))) return rc;
+    if ((rc = state_prepare(ctx))) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->staging.clear();
     return SW_OK;
@@ -2333,22 +2367,8 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
 
 int sw_set_state(sw_ctx* ctx, const void* u, const void* v, const void* eta, const void* sst) {
     if (!ctx || !u || !v || !eta || !sst) return SW_ERR_ARG;
-    ctx->p = 0; ctx->sp = 0; ctx->step = 0; ctx->t = 0;
-    ctx->rhs_in = Fields3();
     int rc;
-    if ((rc = copy_in(ctx, ctx->S[0].u, u, shape_u(ctx->g)))) return rc;
-    if ((rc = copy_in(ctx, ctx->S[0].v, v, shape_v(ctx->g)))) return rc;
-    if ((rc = copy_in(ctx, ctx->S[0].e, eta, shape_e(ctx->g)))) return rc;
-    if ((rc = copy_in(ctx, ctx->sst[0], sst, shape_s(ctx->g)))) return rc;
-    CK(cudaMemsetAsync(ctx->dst, 0, sizeof(DevStatus), ctx->stream));
-    CK(cudaMemsetAsync(ctx->sched, 0, sizeof(TileSched), ctx->stream));
-    // the prologue reads the state as given, before any ghost point copy
-    // (src/time_integration.jl:20-31)
-    if ((rc = ctx->eng->prologue(ctx))) return rc;
-    // ghost_points!(u,v,eta) opens every step (src/time_integration.jl:48); it is
-    // idempotent after the first, so it is applied once here
-    if ((rc = ctx->eng->ghost_state(ctx))) return rc;
-    if ((rc = ctx->eng->state_uploaded(ctx))) return rc;
+    if ((rc = state_copy_in(ctx, u, v, eta, sst)) || (rc = state_prepare(ctx))) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
     return SW_OK;
 }
@@ -2467,14 +2487,17 @@ int sw_diagnostics(sw_ctx* ctx, sw_diag* out) {
 int sw_time_integration(const sw_config* cfg, const sw_static* st, void* u, void* v, void* eta, void* sst,
                         sw_status* status) {
     if (!cfg || !st) return SW_ERR_ARG;
+    if (!u || !v || !eta || !sst) return SW_ERR_ARG;
     sw_ctx* ctx = take_dropin(cfg);
-    if (ctx && refresh_dropin(ctx, cfg, st) != SW_OK) {
+    int rc = SW_OK;
+    if (ctx && refresh_dropin(ctx, cfg, st, u, v, eta, sst) != SW_OK) {
         sw_destroy(ctx);
         ctx = nullptr;
     }
-    int rc = SW_OK;
-    if (!ctx && (rc = sw_create(cfg, st, &ctx))) return rc;
-    rc = sw_set_state(ctx, u, v, eta, sst);
+    if (!ctx) {
+        if ((rc = sw_create(cfg, st, &ctx))) return rc;
+        rc = sw_set_state(ctx, u, v, eta, sst);
+    }
     if (!rc) {
         int rr = sw_run(ctx, cfg->nt, status);
         if (rr == SW_OK || rr == SW_NAN_DETECTED) {
