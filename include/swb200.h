@@ -264,13 +264,13 @@ int sw_batch_set_state(sw_batch* b, int32_t member, const void* u, const void* v
 int sw_batch_run(sw_batch* b, int64_t nsteps, sw_status* statuses);
 int sw_batch_get_state(sw_batch* b, int32_t member, void* u, void* v, void* eta, void* sst);
 int64_t sw_batch_launches(const sw_batch* b);
-/* Rows per warp strip of the batched stage and tail kernels: 8, 16 or 32,
+/* Rows per warp strip of the batched stage and tail kernels: 4, 8, 16 or 32,
  * or 0 before the first run that could choose.  sw_batch_run chooses it on
- * its first call of more than 33 global steps: each candidate advances 2
+ * its first call of more than 44 global steps: each candidate advances 2
  * untimed steps, then 3 interleaved rounds time 3 steps of each (real steps
  * of the run: every candidate computes identical values) and the best round
  * of each decides.  The choice is remembered for later batches of the same
- * member shapes in the process.  SWB200_BATCH_TY=8|16|32 in the environment
+ * member shapes in the process.  SWB200_BATCH_TY=4|8|16|32 in the environment
  * forces one; SWB200_TUNE_LOG=1 prints the timings. */
 int32_t sw_batch_tile_rows(const sw_batch* b);
 /* Member m's context (owned by the batch: do not destroy it), e.g. for

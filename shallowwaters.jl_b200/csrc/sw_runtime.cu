@@ -1615,8 +1615,8 @@ void release_dropin_contexts() {
 // Rows per warp strip of the batched stage and tail kernels: the candidates
 // the batch's autotuner times on the first steps of a run.  Every candidate
 // computes the same values (only the assignment of rows to warps differs).
-constexpr int BATCH_NTY = 3;
-constexpr int BATCH_TYS[BATCH_NTY] = {8, 16, 32};
+constexpr int BATCH_NTY = 4;
+constexpr int BATCH_TYS[BATCH_NTY] = {4, 8, 16, 32};
 
 struct BatchGroup {
     int per = 1, rko = 4, drag = 0, storage = SW_STORE_NATIVE;
@@ -1961,6 +1961,7 @@ int batch_group_step_storage(sw_batch* b, const BatchGroup& gr, int p, cudaStrea
 template <bool PER>
 int batch_group_step_ty(sw_batch* b, const BatchGroup& gr, int p, cudaStream_t s, int ti) {
     switch (BATCH_TYS[ti]) {
+        case 4: return batch_group_step_storage<PER, 4>(b, gr, p, s, ti);
         case 8: return batch_group_step_storage<PER, 8>(b, gr, p, s, ti);
         case 16: return batch_group_step_storage<PER, 16>(b, gr, p, s, ti);
         default: return batch_group_step_storage<PER, 32>(b, gr, p, s, ti);
