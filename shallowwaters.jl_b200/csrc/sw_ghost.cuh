@@ -33,7 +33,7 @@ struct GhostRule {
     // Each rule has a form for arrays of another element type D: put(x)
     // converts the Tp value written there (the 16-bit storage form).
     template <class D, class Put>
-    __device__ inline void u(D* __restrict__ dst, const Geom& g, int F, int b, Tp val, Put put) const {
+    __device__ __forceinline__ void u(D* __restrict__ dst, const Geom& g, int F, int b, Tp val, Put put) const {
         if (ep) {
             Tp c = comm(val);
             if (F == 0 || F == 1) dst[g.idx(F + N, b)] = put(c);
@@ -46,12 +46,12 @@ struct GhostRule {
             if (b == M - 2) dst[g.idx(F, M + 1)] = put(c);
         }
     }
-    __device__ inline void u(Tp* __restrict__ dst, const Geom& g, int F, int b, Tp val) const {
+    __device__ __forceinline__ void u(Tp* __restrict__ dst, const Geom& g, int F, int b, Tp val) const {
         u(dst, g, F, b, val, Same{});
     }
     // v at (a, G): periodic x copies (:93-98); nonperiodic (1-α) mirror in x (:80-85)
     template <class D, class Put>
-    __device__ inline void v(D* __restrict__ dst, const Geom& g, int a, int G, Tp val, Put put) const {
+    __device__ __forceinline__ void v(D* __restrict__ dst, const Geom& g, int a, int G, Tp val, Put put) const {
         if (ep) {
             Tp c = comm(val);
             if (a == 0 || a == 1) dst[g.idx(a + N, G)] = put(c);
@@ -64,39 +64,44 @@ struct GhostRule {
             if (a == N - 2) dst[g.idx(N + 1, G)] = put(c);
         }
     }
-    __device__ inline void v(Tp* __restrict__ dst, const Geom& g, int a, int G, Tp val) const {
+    __device__ __forceinline__ void v(Tp* __restrict__ dst, const Geom& g, int a, int G, Tp val) const {
         v(dst, g, a, G, val, Same{});
     }
     // eta at (a, b): columns first, then rows over all columns, so the corners
     // take the column-copied value (src/ghost_points.jl:102-133)
     template <class D, class Put>
-    __device__ inline void eta(D* __restrict__ dst, const Geom& g, int a, int b, Tp val, Put put) const {
-        int xs[2], nx = 0;
+    __device__ __forceinline__ void eta(D* __restrict__ dst, const Geom& g, int a, int b, Tp val, Put put) const {
+        // the (at most two) ghost columns copied from column a; NONE if there is none
+        constexpr int NONE = -1000000;
+        int xa = NONE, xb = NONE;
         Tp cx = ep ? comm(val) : val;
         if (ep) {
-            if (a == N - 1) xs[nx++] = -1;
-            if (a == 0) xs[nx++] = N;
+            if (a == N - 1) xa = -1;
+            if (a == 0) xb = N;
         } else {
-            if (a == 0) xs[nx++] = -1;
-            if (a == N - 1) xs[nx++] = N;
+            if (a == 0) xa = -1;
+            if (a == N - 1) xb = N;
         }
-        for (int k = 0; k < nx; k++) dst[g.idx(xs[k], b)] = put(cx);
+        if (xa != NONE) dst[g.idx(xa, b)] = put(cx);
+        if (xb != NONE) dst[g.idx(xb, b)] = put(cx);
         if (b == 0 || b == M - 1) {
             int yt = (b == 0) ? -1 : M;
             dst[g.idx(a, yt)] = put(val);
-            for (int k = 0; k < nx; k++) dst[g.idx(xs[k], yt)] = put(cx);
+            if (xa != NONE) dst[g.idx(xa, yt)] = put(cx);
+            if (xb != NONE) dst[g.idx(xb, yt)] = put(cx);
             if (b == 0 && b == M - 1) {   // M == 1: both rows
                 dst[g.idx(a, M)] = put(val);
-                for (int k = 0; k < nx; k++) dst[g.idx(xs[k], M)] = put(cx);
+                if (xa != NONE) dst[g.idx(xa, M)] = put(cx);
+                if (xb != NONE) dst[g.idx(xb, M)] = put(cx);
             }
         }
     }
-    __device__ inline void eta(Tp* __restrict__ dst, const Geom& g, int a, int b, Tp val) const {
+    __device__ __forceinline__ void eta(Tp* __restrict__ dst, const Geom& g, int a, int b, Tp val) const {
         eta(dst, g, a, b, val, Same{});
     }
     // sst at (a, b): periodic / zero-gradient copies in x (src/ghost_points.jl:136-179)
     template <class D, class Put>
-    __device__ inline void sst(D* __restrict__ dst, const Geom& g, int a, int b, Tp val, Put put) const {
+    __device__ __forceinline__ void sst(D* __restrict__ dst, const Geom& g, int a, int b, Tp val, Put put) const {
         if (ep) {
             Tp c = comm(val);
             if (a == N - 1) dst[g.idx(-1, b)] = put(c);
@@ -106,7 +111,7 @@ struct GhostRule {
             if (a == N - 1) dst[g.idx(N, b)] = put(val);
         }
     }
-    __device__ inline void sst(Tp* __restrict__ dst, const Geom& g, int a, int b, Tp val) const {
+    __device__ __forceinline__ void sst(Tp* __restrict__ dst, const Geom& g, int a, int b, Tp val) const {
         sst(dst, g, a, b, val, Same{});
     }
     struct Same {
