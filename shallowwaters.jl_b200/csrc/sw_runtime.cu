@@ -2317,12 +2317,14 @@ int sw_create(const sw_config* cfg, const sw_static* st, sw_ctx** out) {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, dev);
-        // The TMA stage kernel from two of its tiles per SM up; on smaller
-        // grids the streaming kernel with short strips (measured faster:
-        // 74 against 97 us per step at 512x256).  SWB200_TMA=0|1 forces it.
+        // The TMA stage kernel from four of its tiles per SM up (1536x768 and
+        // larger); on smaller grids the streaming kernel with short strips
+        // (measured faster: 110.8 against 115.4 us per step at 1024x512, 74
+        // against 97 at 512x256; at 1536x768 the TMA kernel takes 156 against
+        // 251 us).  SWB200_TMA=0|1 forces it.
         const char* env = getenv("SWB200_TMA");
         const long long tma_tiles = (long long)((g.N + BAND - 1) / BAND) * ((g.M + STAGE_TMA_TY - 1) / STAGE_TMA_TY);
-        bool want = env ? env[0] != '0' : tma_tiles >= 2LL * ctx->nsm;
+        bool want = env ? env[0] != '0' : tma_tiles >= 4LL * ctx->nsm;
         bool ok = want && encode_fn() != nullptr;
         // a cap on the TMA stage kernel's persistent blocks (SWB200_STAGE_BLOCKS),
         // so that small grids also run blocks that take several tiles each
